@@ -1,0 +1,168 @@
+"""ctypes bindings of libgs_cuda.so (include/gs_api.h).
+
+The library is loaded from the package directory only; there is no fallback:
+if it is missing or fails to load, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libgs_cuda.so"
+
+GS_OK = 0
+GS_ERR_BAD_ARG = -1
+GS_ERR_OOM = -2
+GS_ERR_CUDA = -3
+GS_ERR_DEVICE_TIMEOUT = -4
+GS_ERR_NO_SCENE = -5
+GS_ERR_BUDGET_REFUSED = -6
+GS_ERR_NO_DEVICE = -7
+GS_ERR_TOO_LARGE = -8
+
+GS_MODE_ALPHA = 0
+GS_MODE_STOCHASTIC = 1
+GS_MODE_GPS = 2
+
+GS_DEBUG_IDS = 0
+GS_DEBUG_KEYS = 1
+GS_DEBUG_PROJECTED = 2
+GS_DEBUG_SORTED_IDS = 3
+GS_DEBUG_SORTED_KEYS = 4
+GS_DEBUG_ACCUM = 5
+GS_DEBUG_SAMPLE = 6
+GS_DEBUG_DEPTH = 7
+
+# Every function include/gs_api.h declares (checked by the CPU test suite).
+EXPORTS = (
+    "gs_create", "gs_destroy", "gs_get_knobs", "gs_set_knobs", "gs_set_mode", "gs_upload_rows",
+    "gs_upload_rows_device", "gs_set_gps_budget", "gs_reset_accumulation", "gs_render", "gs_render_host",
+    "gs_read_stats", "gs_debug_read", "gs_profile_enable", "gs_stage_times", "gs_stage_names", "gs_status_str",
+    "gs_last_error", "gs_camera_uniforms", "gs_load_ply", "gs_pack_raw", "gs_sort_pairs_scratch_bytes",
+    "gs_sort_pairs",
+)
+
+
+class GsCamera(C.Structure):
+    """CameraUniforms (src/camera.h:23-38)."""
+
+    _fields_ = [
+        ("view", C.c_float * 16),
+        ("proj", C.c_float * 16),
+        ("viewport", C.c_float * 2),
+        ("orthographic", C.c_float),
+        ("persp_focal", C.c_float),
+        ("ortho_focal", C.c_float),
+        ("clip_y_sign", C.c_float),
+        ("clip_z_01", C.c_float),
+        ("pad", C.c_float * 1),
+    ]
+
+
+class GsKnobs(C.Structure):
+    _fields_ = [
+        ("render_mode", C.c_int32),
+        ("sh_degree", C.c_int32),
+        ("sh_lod_distance", C.c_float),
+        ("gps_supersample_factor", C.c_uint32),
+        ("stochastic_samples_per_frame", C.c_uint32),
+        ("stochastic_taa_current_samples", C.c_uint32),
+        ("stochastic_accumulation_enabled", C.c_int32),
+        ("stochastic_taa_enabled", C.c_int32),
+        ("black_background", C.c_int32),
+        ("splat_diagnostics_enabled", C.c_int32),
+        ("linear_color", C.c_int32),
+        ("write_invisible_records", C.c_int32),
+        ("reserved", C.c_int32 * 4),
+    ]
+
+
+class GsStats(C.Structure):
+    _fields_ = [
+        ("gaussian_count", C.c_uint32),
+        ("visible_count", C.c_uint32),
+        ("tile_entries", C.c_uint32),
+        ("tile_overflow", C.c_uint32),
+        ("diagnostics", C.c_uint32 * 8),
+        ("gps_requested_work_items", C.c_uint32),
+        ("gps_budget_exhausted", C.c_uint32),
+        ("gps_max_work_items", C.c_uint32),
+        ("sample_count", C.c_uint32),
+        ("frame_seed", C.c_uint32),
+        ("error_flags", C.c_uint32),
+        ("kernel_launches", C.c_uint32),
+        ("reserved", C.c_uint32 * 5),
+    ]
+
+
+assert C.sizeof(GsCamera) == 160
+assert C.sizeof(GsKnobs) == 64
+
+_lib = None
+
+
+class GsError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        msg = f"{where} failed: {status_str(status)} ({status})"
+        if detail:
+            msg += f": {detail}"
+        super().__init__(msg)
+
+
+def lib() -> C.CDLL:
+    """Load libgs_cuda.so; raises if it is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m gamesplat_b200.build`")
+    L = C.CDLL(str(LIB_PATH))
+    vp, u32, u64, i32, f32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_float
+    sig = {
+        "gs_create": (i32, [C.POINTER(vp), i32, vp]),
+        "gs_destroy": (None, [vp]),
+        "gs_get_knobs": (i32, [vp, C.POINTER(GsKnobs)]),
+        "gs_set_knobs": (i32, [vp, C.POINTER(GsKnobs)]),
+        "gs_set_mode": (i32, [vp, i32]),
+        "gs_upload_rows": (i32, [vp, vp, u64]),
+        "gs_upload_rows_device": (i32, [vp, vp, u64]),
+        "gs_set_gps_budget": (i32, [vp, u32]),
+        "gs_reset_accumulation": (i32, [vp]),
+        "gs_render": (i32, [vp, C.POINTER(GsCamera), vp]),
+        "gs_render_host": (i32, [vp, C.POINTER(GsCamera), vp]),
+        "gs_read_stats": (i32, [vp, C.POINTER(GsStats)]),
+        "gs_debug_read": (i32, [vp, i32, vp, u64]),
+        "gs_profile_enable": (i32, [vp, i32]),
+        "gs_stage_times": (i32, [vp, C.POINTER(C.c_float), C.POINTER(u32), i32, i32]),
+        "gs_stage_names": (C.c_char_p, []),
+        "gs_status_str": (C.c_char_p, [i32]),
+        "gs_last_error": (C.c_char_p, [vp]),
+        "gs_camera_uniforms": (i32, [C.POINTER(f32), f32, f32, f32, f32, f32, i32, f32, f32, i32, i32, i32,
+                                     C.POINTER(GsCamera)]),
+        "gs_load_ply": (C.c_int64, [C.c_char_p, vp, u64]),
+        "gs_pack_raw": (i32, [vp, u64, vp]),
+        "gs_sort_pairs_scratch_bytes": (C.c_size_t, [u32]),
+        "gs_sort_pairs": (i32, [vp, vp, vp, vp, u32, i32, i32, vp, C.c_size_t, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def status_str(status: int) -> str:
+    try:
+        return lib().gs_status_str(status).decode()
+    except Exception:  # pragma: no cover - only when the library cannot load
+        return "unknown"
+
+
+def check(status: int, where: str, ctx=None) -> None:
+    if status != GS_OK:
+        detail = ""
+        if ctx:
+            detail = lib().gs_last_error(ctx).decode()
+        raise GsError(status, where, detail)

@@ -1,0 +1,941 @@
+// Host orchestration of the B200 splatting path behind the C ABI
+// (include/gs_api.h).  Mirrors the reference renderer's per-frame sequence
+// (renderer_draw_frame, src/renderer.cpp:2139-2600) for the splatting
+// modes, with the GL passes replaced by CUDA kernels:
+//
+//   alpha       cull -> depth sort -> bin -> tile sort -> tile ranges -> raster
+//   stochastic  cull -> depth sort -> per sample (bin -> tile sort -> ranges ->
+//               stochastic raster -> accumulation / frame average) -> TAA
+//   gps         cull -> clear -> expand -> splat -> resolve -> accumulation
+//
+// All device buffers are owned by the context; the scene is copied in and the
+// caller keeps its host memory (src/renderer.cpp:736-1074).  Work is issued
+// on one stream without host synchronisation; element counts that depend on
+// the camera (visible splats, tile entries, GPS work) stay on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "gs_internal.h"
+#include "gs_extra.h"
+
+using gs::FrameCounters;
+using gs::RasterRecord;
+using gs::SortPlan;
+
+namespace {
+
+enum Stage { ST_CULL = 0, ST_SORT, ST_BIN, ST_TILE_SORT, ST_RASTER, ST_ACCUM, ST_GPS, ST_COUNT };
+const char* kStageNames = "cull,sort,bin,tile_sort,raster,accum,gps";
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct gs_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t num_sms = 148;
+    gs_knobs knobs{};
+    std::string last_error;
+
+    // scene
+    uint32_t n = 0;
+    float4* rows = nullptr;
+    float4* projected = nullptr;
+    uint32_t* keys[2] = {nullptr, nullptr};
+    uint32_t* ids[2] = {nullptr, nullptr};
+    RasterRecord* records = nullptr;
+    unsigned long long* cull_status = nullptr;
+    unsigned long long* sort_status = nullptr;
+    unsigned long long* bin_status = nullptr;
+    size_t sort_status_stride = 0;
+
+    // tile entries
+    uint32_t entry_cap = 0;
+    uint32_t* ekeys[2] = {nullptr, nullptr};
+    uint32_t* evals[2] = {nullptr, nullptr};
+    unsigned long long* tsort_status = nullptr;
+    size_t tsort_status_stride = 0;
+
+    // per-frame control block (zeroed each frame)
+    void* ctrl = nullptr;
+    size_t ctrl_bytes = 0;
+    FrameCounters* fc = nullptr;
+    SortPlan* depth_plan = nullptr;
+    SortPlan* tile_plan = nullptr;
+    uint32_t* depth_hist = nullptr;
+    uint32_t* tile_hist = nullptr;
+    uint2* tile_ranges = nullptr;
+    uint32_t tiles_cap = 0;
+
+    // camera
+    gs_camera* d_cam = nullptr;
+    gs_camera* h_cam = nullptr;   // pinned staging
+    FrameCounters* h_fc = nullptr;  // pinned readback
+    cudaEvent_t fc_event = nullptr;
+    bool fc_pending = false;
+    uint32_t epoch = 0;
+
+    // image targets
+    int width = 0, height = 0, tiles_x = 0, tiles_y = 0;
+    uint16_t* out16 = nullptr;     // internal RGBA16F (gs_render_host)
+    uint16_t* h_out16 = nullptr;   // pinned
+    size_t h_out16_bytes = 0;
+    gs::StochasticTargets st{};
+    gs::GpsTargets gps{};
+    uint32_t gps_max_work_items = 16u * 1024u * 1024u;
+
+    // stochastic / accumulation state (src/renderer.h:230-246)
+    uint32_t frame_seed = 0;
+    uint32_t sample_count = 0;
+    uint32_t accum_write_index = 0;
+    gs_camera prev_cam{};
+    bool prev_cam_valid = false;
+    bool taa_prev_valid = false;
+
+    // profiling
+    bool profiling = false;
+    struct Pending { cudaEvent_t a, b; int stage; uint32_t launches; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double stage_ms[ST_COUNT] = {};
+    uint32_t stage_launches[ST_COUNT] = {};
+    uint32_t last_launches = 0;
+    uint32_t frame_launches = 0;
+};
+
+namespace {
+
+int fail(gs_ctx* c, int status, const std::string& msg) {
+    if (c) c->last_error = msg;
+    return status;
+}
+
+int cuda_fail(gs_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, e == cudaErrorMemoryAllocation ? GS_ERR_OOM : GS_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define GS_CUDA(ctx, call)                                  \
+    do {                                                    \
+        cudaError_t _e = (call);                            \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(reinterpret_cast<void*>(p));
+    p = nullptr;
+}
+
+void release_scene(gs_ctx* c) {
+    dfree(c->rows);
+    dfree(c->projected);
+    for (int k = 0; k < 2; ++k) {
+        dfree(c->keys[k]);
+        dfree(c->ids[k]);
+        dfree(c->ekeys[k]);
+        dfree(c->evals[k]);
+    }
+    dfree(c->records);
+    dfree(c->cull_status);
+    dfree(c->sort_status);
+    dfree(c->bin_status);
+    dfree(c->tsort_status);
+    gs::release_gps_scene(c->gps);
+    c->n = 0;
+    c->entry_cap = 0;
+}
+
+void release_targets(gs_ctx* c) {
+    dfree(c->out16);
+    dfree(c->ctrl);
+    c->fc = nullptr;
+    gs::release_stochastic_targets(c->st);
+    gs::release_gps_targets(c->gps);
+    c->width = c->height = 0;
+    c->tiles_cap = 0;
+}
+
+cudaEvent_t take_event(gs_ctx* c) {
+    if (!c->event_pool.empty()) {
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct StageScope {
+    gs_ctx* c;
+    int stage;
+    cudaEvent_t a = nullptr;
+    uint32_t launches = 0;
+    StageScope(gs_ctx* ctx, int s) : c(ctx), stage(s) {
+        if (c->profiling) {
+            a = take_event(c);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    void add(int k) { launches += (uint32_t)k; }
+    ~StageScope() {
+        c->frame_launches += launches;
+        if (c->profiling) {
+            cudaEvent_t b = take_event(c);
+            cudaEventRecord(b, c->stream);
+            c->pending.push_back({a, b, stage, launches});
+        }
+    }
+};
+
+int entry_bits(uint32_t tiles) {
+    int bits = 1;
+    while (bits < 32 && (1u << bits) < tiles) ++bits;
+    return bits;
+}
+
+// Tile-entry buffers: (tile, splat) pairs.  Grown on overflow.
+int ensure_entries(gs_ctx* c, uint32_t cap) {
+    if (cap <= c->entry_cap) return GS_OK;
+    for (int k = 0; k < 2; ++k) {
+        dfree(c->ekeys[k]);
+        dfree(c->evals[k]);
+    }
+    dfree(c->tsort_status);
+    c->entry_cap = 0;
+    for (int k = 0; k < 2; ++k) {
+        GS_CUDA(c, dalloc(&c->ekeys[k], (size_t)cap * 4));
+        GS_CUDA(c, dalloc(&c->evals[k], (size_t)cap * 4));
+    }
+    c->tsort_status_stride = gs::sort_status_words(cap);
+    GS_CUDA(c, dalloc(&c->tsort_status, c->tsort_status_stride * 4 * sizeof(unsigned long long)));
+    GS_CUDA(c, cudaMemsetAsync(c->tsort_status, 0, c->tsort_status_stride * 4 * sizeof(unsigned long long), c->stream));
+    c->entry_cap = cap;
+    return GS_OK;
+}
+
+int ensure_targets(gs_ctx* c, int w, int h) {
+    if (w <= 0 || h <= 0) return fail(c, GS_ERR_BAD_ARG, "viewport must be positive");
+    if (w > 32767 || h > 32767) return fail(c, GS_ERR_TOO_LARGE, "viewport beyond 32767 pixels");
+    const int tx = (w + gs::kTileW - 1) / gs::kTileW, ty = (h + gs::kTileH - 1) / gs::kTileH;
+    if (c->width == w && c->height == h && c->ctrl) return GS_OK;
+    release_targets(c);
+    c->tiles_cap = (uint32_t)(tx * ty);
+    // control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges
+    size_t off = 0;
+    auto place = [&](size_t bytes) {
+        size_t o = off;
+        off = (off + bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    size_t o_fc = place(sizeof(FrameCounters));
+    size_t o_dp = place(sizeof(SortPlan));
+    size_t o_tp = place(sizeof(SortPlan));
+    size_t o_dh = place(4 * 256 * 4);
+    size_t o_th = place(4 * 256 * 4);
+    size_t o_tr = place((size_t)c->tiles_cap * sizeof(uint2));
+    c->ctrl_bytes = off;
+    GS_CUDA(c, dalloc(reinterpret_cast<char**>(&c->ctrl), c->ctrl_bytes));
+    char* base = static_cast<char*>(c->ctrl);
+    c->fc = reinterpret_cast<FrameCounters*>(base + o_fc);
+    c->depth_plan = reinterpret_cast<SortPlan*>(base + o_dp);
+    c->tile_plan = reinterpret_cast<SortPlan*>(base + o_tp);
+    c->depth_hist = reinterpret_cast<uint32_t*>(base + o_dh);
+    c->tile_hist = reinterpret_cast<uint32_t*>(base + o_th);
+    c->tile_ranges = reinterpret_cast<uint2*>(base + o_tr);
+    GS_CUDA(c, cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream));
+    GS_CUDA(c, dalloc(&c->out16, (size_t)w * h * 8));
+    c->width = w;
+    c->height = h;
+    c->tiles_x = tx;
+    c->tiles_y = ty;
+    c->sample_count = 0;
+    c->accum_write_index = 0;
+    c->taa_prev_valid = false;
+    return GS_OK;
+}
+
+// Grow the entry buffers if the last completed frame overflowed them.
+int check_previous_frame(gs_ctx* c) {
+    if (!c->fc_pending) return GS_OK;
+    if (cudaEventQuery(c->fc_event) != cudaSuccess) return GS_OK;
+    c->fc_pending = false;
+    if (c->h_fc->tile_overflow) {
+        uint64_t need = (uint64_t)c->h_fc->tile_entries + c->h_fc->tile_overflow;
+        uint64_t cap = std::min<uint64_t>(need + need / 4 + 1024, 0x3FFFFFFFull);
+        return ensure_entries(c, (uint32_t)cap);
+    }
+    return GS_OK;
+}
+
+void begin_frame(gs_ctx* c, const gs_camera* cam) {
+    std::memcpy(c->h_cam, cam, sizeof(gs_camera));
+    cudaMemcpyAsync(c->d_cam, c->h_cam, sizeof(gs_camera), cudaMemcpyHostToDevice, c->stream);
+    cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream);
+    ++c->epoch;
+    if (c->epoch == 0) ++c->epoch;
+    c->frame_launches = 0;
+}
+
+void end_frame(gs_ctx* c) {
+    cudaMemcpyAsync(c->h_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
+    cudaEventRecord(c->fc_event, c->stream);
+    c->fc_pending = true;
+    c->last_launches = c->frame_launches;
+}
+
+void run_cull(gs_ctx* c) {
+    StageScope sc(c, ST_CULL);
+    gs::CullParams p{};
+    p.rows = c->rows;
+    p.n = c->n;
+    p.cam = c->d_cam;
+    p.sh_degree = std::max(0, std::min(3, c->knobs.sh_degree));
+    p.sh_lod_distance = c->knobs.sh_lod_distance;
+    p.collect_stats = c->knobs.splat_diagnostics_enabled ? 1 : 0;
+    p.write_invisible = c->knobs.write_invisible_records ? 1 : 0;
+    p.projected = c->projected;
+    p.keys_out = c->keys[1];
+    p.ids_out = c->ids[1];
+    p.status = c->cull_status;
+    p.epoch = c->epoch;
+    p.fc = c->fc;
+    sc.add(gs::launch_cull(p, c->num_sms, c->stream));
+}
+
+void run_depth_sort(gs_ctx* c) {
+    StageScope sc(c, ST_SORT);
+    gs::SortParams p{};
+    p.keys_in = c->keys[1];
+    p.vals_in = c->ids[1];
+    p.keys_buf[0] = c->keys[0];
+    p.keys_buf[1] = c->keys[1];
+    p.vals_buf[0] = c->ids[0];
+    p.vals_buf[1] = c->ids[1];
+    p.land_in_buf0 = 0;
+    p.count_ptr = &c->fc->visible_count;
+    p.count_cap = c->n;
+    p.begin_bit = 0;
+    p.end_bit = 32;
+    p.hist = c->depth_hist;
+    p.plan = c->depth_plan;
+    p.status = c->sort_status;
+    p.status_stride = c->sort_status_stride;
+    p.epoch = c->epoch;
+    p.error_flags = &c->fc->error_flags;
+    sc.add(gs::launch_sort(p, c->num_sms, c->stream));
+}
+
+// Binning, tile sort and tile ranges for one raster pass.
+void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
+    {
+        StageScope sc(c, ST_BIN);
+        if (reset_ranges) {
+            // A second pass in the same frame: clear ranges, counters and the tile-sort plan.
+            cudaMemsetAsync(c->tile_ranges, 0, (size_t)c->tiles_cap * sizeof(uint2), c->stream);
+            cudaMemsetAsync(c->tile_plan, 0, sizeof(SortPlan), c->stream);
+            cudaMemsetAsync(c->tile_hist, 0, 4 * 256 * 4, c->stream);
+            // bin_ticket, tile_entries, tile_overflow are adjacent in FrameCounters.
+            cudaMemsetAsync(&c->fc->bin_ticket, 0, 3 * sizeof(uint32_t), c->stream);
+            ++c->epoch;
+            if (c->epoch == 0) ++c->epoch;
+        }
+        gs::BinParams p{};
+        p.depth_plan = c->depth_plan;
+        p.projected = c->projected;
+        p.cam = c->d_cam;
+        p.jitter_x = jx;
+        p.jitter_y = jy;
+        p.frame_seed = seed;
+        p.width = c->width;
+        p.height = c->height;
+        p.tiles_x = c->tiles_x;
+        p.tiles_y = c->tiles_y;
+        p.records = c->records;
+        p.entry_keys = c->ekeys[1];
+        p.entry_vals = c->evals[1];
+        p.entry_cap = c->entry_cap;
+        p.status = c->bin_status;
+        p.epoch = c->epoch;
+        p.fc = c->fc;
+        sc.add(gs::launch_bin(p, c->n, c->num_sms, c->stream));
+    }
+    {
+        StageScope sc(c, ST_TILE_SORT);
+        gs::SortParams p{};
+        p.keys_in = c->ekeys[1];
+        p.vals_in = c->evals[1];
+        p.keys_buf[0] = c->ekeys[0];
+        p.keys_buf[1] = c->ekeys[1];
+        p.vals_buf[0] = c->evals[0];
+        p.vals_buf[1] = c->evals[1];
+        p.land_in_buf0 = 0;
+        p.count_ptr = &c->fc->tile_entries;
+        p.count_cap = c->entry_cap;
+        p.begin_bit = 0;
+        p.end_bit = entry_bits(c->tiles_cap);
+        p.hist = c->tile_hist;
+        p.plan = c->tile_plan;
+        p.status = c->tsort_status;
+        p.status_stride = c->tsort_status_stride;
+        p.epoch = c->epoch;
+        p.error_flags = &c->fc->error_flags;
+        sc.add(gs::launch_sort(p, c->num_sms, c->stream));
+        sc.add(gs::launch_tile_ranges(c->tile_plan, c->fc, c->entry_cap, c->tile_ranges, c->tiles_cap, c->num_sms,
+                                       c->stream));
+    }
+}
+
+gs::RasterParams raster_params(gs_ctx* c, float bg) {
+    gs::RasterParams r{};
+    r.records = c->records;
+    r.record_cap = c->n;
+    r.tile_plan = c->tile_plan;
+    r.tile_ranges = c->tile_ranges;
+    r.width = c->width;
+    r.height = c->height;
+    r.tiles_x = c->tiles_x;
+    r.tiles_y = c->tiles_y;
+    r.bg = bg;
+    r.fc = c->fc;
+    return r;
+}
+
+float background(const gs_ctx* c) { return c->knobs.black_background ? 0.0f : 0.1f; }  // src/renderer.cpp:2146
+
+int render_alpha(gs_ctx* c, uint16_t* out) {
+    run_cull(c);
+    run_depth_sort(c);
+    run_binning(c, 0.0f, 0.0f, 0.0f, false);
+    StageScope sc(c, ST_RASTER);
+    gs::RasterParams r = raster_params(c, background(c));
+    r.out_rgba16f = out;
+    sc.add(gs::launch_raster_alpha(r, c->stream));
+    return GS_OK;
+}
+
+// src/renderer.cpp:246-255
+float halton(uint32_t index, uint32_t base) {
+    float f = 1.0f, r = 0.0f;
+    while (index > 0) {
+        f /= (float)base;
+        r += f * (float)(index % base);
+        index /= base;
+    }
+    return r;
+}
+
+int render_stochastic(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
+    int rc = gs::ensure_stochastic_targets(c->st, c->width, c->height, c->stream);
+    if (rc) return fail(c, rc, "stochastic target allocation failed");
+    const size_t npix = (size_t)c->width * c->height;
+    const float bg = background(c);
+    // src/renderer.cpp:2300-2330
+    bool prev_cam_valid = c->prev_cam_valid;
+    const bool cam_changed = c->prev_cam_valid && std::memcmp(&c->prev_cam, cam, sizeof(gs_camera)) != 0;
+    const gs_camera prev_cam = c->prev_cam;
+    if (!c->knobs.stochastic_taa_enabled && cam_changed) {
+        c->sample_count = 0;
+        c->taa_prev_valid = false;
+        prev_cam_valid = false;
+    }
+    c->prev_cam = *cam;
+    c->prev_cam_valid = true;
+    const uint32_t spf = std::max(1u, std::min(16u, c->knobs.stochastic_samples_per_frame));
+    const bool use_taa = c->knobs.stochastic_taa_enabled != 0;
+    uint32_t render_samples = use_taa ? std::max(1u, std::min(16u, c->knobs.stochastic_taa_current_samples)) : spf;
+    float inv_view[16];
+    if (use_taa && !gs::mat4_inverse(cam->view, inv_view)) {
+        c->sample_count = 0;
+        c->taa_prev_valid = false;
+        std::memcpy(inv_view, cam->view, sizeof(inv_view));
+        prev_cam_valid = false;
+    }
+
+    run_cull(c);
+    run_depth_sort(c);
+    uint32_t write_index = c->accum_write_index & 1u;
+    bool display_accum = false;
+    for (uint32_t i = 0; i < render_samples; ++i) {
+        c->frame_seed++;
+        float jx = 0.0f, jy = 0.0f;
+        if (use_taa) {
+            uint32_t jitter_index = (c->frame_seed % 1024u) + 1u;
+            jx = halton(jitter_index, 2u) - 0.5f;
+            jy = halton(jitter_index, 3u) - 0.5f;
+        }
+        run_binning(c, jx, jy, (float)c->frame_seed, i > 0);
+        {
+            StageScope sc(c, ST_RASTER);
+            gs::RasterParams r = raster_params(c, bg);
+            r.out_rgba32f = c->st.sample;
+            r.out_depth = c->st.depth;
+            r.rgba8 = c->knobs.linear_color ? 0 : 1;
+            sc.add(gs::launch_raster_stochastic(r, c->stream));
+        }
+        StageScope sa(c, ST_ACCUM);
+        if (use_taa && render_samples > 1) {
+            uint32_t w = i & 1u, rd = w ^ 1u;
+            sa.add(gs::launch_accum(c->st.sample, i == 0 ? c->st.sample : c->st.frame_avg[rd], (float)(i + 1),
+                                    c->st.frame_avg[w], npix, c->stream));
+        } else if (!use_taa && (c->knobs.stochastic_accumulation_enabled || render_samples > 1)) {
+            const bool acc = c->knobs.stochastic_accumulation_enabled != 0;
+            uint32_t next = acc ? c->sample_count + 1 : i + 1;
+            write_index = acc ? (c->accum_write_index & 1u) : (i & 1u);
+            uint32_t rd = write_index ^ 1u;
+            sa.add(gs::launch_accum(c->st.sample, next == 1 ? c->st.sample : c->st.accum[rd], (float)next,
+                                    c->st.accum[write_index], npix, c->stream));
+            display_accum = true;
+            if (acc) {
+                c->sample_count = next;
+                c->accum_write_index = write_index ^ 1u;
+            }
+        }
+    }
+    if (use_taa) {
+        StageScope sa(c, ST_ACCUM);
+        write_index = c->accum_write_index & 1u;
+        uint32_t rd = write_index ^ 1u;
+        const float4* current = render_samples > 1 ? c->st.frame_avg[(render_samples - 1) & 1u] : c->st.sample;
+        const bool has_history = c->taa_prev_valid && prev_cam_valid;
+        gs::TaaUniforms u{};
+        std::memcpy(u.inv_view, inv_view, sizeof(u.inv_view));
+        std::memcpy(u.prev_view, has_history ? prev_cam.view : cam->view, sizeof(u.prev_view));
+        u.viewport_orthographic[0] = cam->viewport[0];
+        u.viewport_orthographic[1] = cam->viewport[1];
+        u.viewport_orthographic[2] = cam->orthographic;
+        u.viewport_orthographic[3] = has_history ? prev_cam.orthographic : cam->orthographic;
+        u.focal_clip[0] = cam->persp_focal;
+        u.focal_clip[1] = cam->ortho_focal;
+        u.focal_clip[2] = cam->clip_y_sign;
+        u.focal_clip[3] = cam->clip_z_01;
+        u.prev_focal_clip[0] = has_history ? prev_cam.persp_focal : cam->persp_focal;
+        u.prev_focal_clip[1] = has_history ? prev_cam.ortho_focal : cam->ortho_focal;
+        u.prev_focal_clip[2] = has_history ? prev_cam.clip_y_sign : cam->clip_y_sign;
+        u.proj_z[0] = cam->proj[10];
+        u.proj_z[1] = cam->proj[14];
+        u.history_valid = has_history ? 1.0f : 0.0f;
+        u.view_changed = cam_changed ? 1.0f : 0.0f;
+        sa.add(gs::launch_taa(current, c->st.depth, c->st.accum[rd], c->st.xyz[rd], c->width, c->height, u,
+                              c->st.accum[write_index], c->st.xyz[write_index], c->stream));
+        c->taa_prev_valid = true;
+        c->sample_count++;
+        c->accum_write_index = write_index ^ 1u;
+        display_accum = true;
+    }
+    StageScope sd(c, ST_ACCUM);
+    c->st.display = display_accum ? c->st.accum[write_index] : c->st.sample;
+    sd.add(gs::launch_to_half(c->st.display, out, npix, c->stream));
+    return GS_OK;
+}
+
+int render_gps(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
+    int rc = gs::ensure_stochastic_targets(c->st, c->width, c->height, c->stream);
+    if (rc) return fail(c, rc, "stochastic target allocation failed");
+    uint32_t ss = std::max(1u, std::min(4u, c->knobs.gps_supersample_factor));
+    rc = gs::ensure_gps_targets(c->gps, c->width, c->height, ss, c->n, c->gps_max_work_items, c->stream);
+    if (rc) return fail(c, rc, "GPS target allocation failed");
+    const size_t npix = (size_t)c->width * c->height;
+    // src/renderer.cpp:2206-2211
+    if (c->prev_cam_valid && std::memcmp(&c->prev_cam, cam, sizeof(gs_camera)) != 0) {
+        c->sample_count = 0;
+        c->taa_prev_valid = false;
+    }
+    c->prev_cam = *cam;
+    c->prev_cam_valid = true;
+    c->frame_seed++;
+    run_cull(c);
+    {
+        StageScope sc(c, ST_GPS);
+        gs::GpsParams g{};
+        g.projected = c->projected;
+        g.vis_ids = c->ids[1];
+        g.fc = c->fc;
+        g.width = c->width;
+        g.height = c->height;
+        g.supersample = ss;
+        g.max_work_items = c->gps_max_work_items;
+        g.clip_z_01 = cam->clip_z_01;
+        g.linear_color = c->knobs.linear_color;
+        g.frame_seed = (float)c->frame_seed;
+        g.bg = background(c);
+        g.out_color = c->st.sample;
+        g.out_depth = c->st.depth;
+        sc.add(gs::launch_gps(c->gps, g, c->n, c->num_sms, c->stream));
+    }
+    StageScope sa(c, ST_ACCUM);
+    if (!c->knobs.stochastic_accumulation_enabled) {
+        c->sample_count = 0;
+        c->st.display = c->st.sample;
+    } else {
+        uint32_t w = c->accum_write_index & 1u, rd = w ^ 1u;
+        uint32_t next = c->sample_count + 1;
+        sa.add(gs::launch_accum(c->st.sample, next == 1 ? c->st.sample : c->st.accum[rd], (float)next, c->st.accum[w],
+                                npix, c->stream));
+        c->sample_count = next;
+        c->accum_write_index = w ^ 1u;
+        c->st.display = c->st.accum[w];
+    }
+    sa.add(gs::launch_to_half(c->st.display, out, npix, c->stream));
+    return GS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* gs_status_str(int s) {
+    switch (s) {
+        case GS_OK: return "ok";
+        case GS_ERR_BAD_ARG: return "bad argument";
+        case GS_ERR_OOM: return "out of memory";
+        case GS_ERR_CUDA: return "CUDA error";
+        case GS_ERR_DEVICE_TIMEOUT: return "device wait limit reached";
+        case GS_ERR_NO_SCENE: return "no scene uploaded";
+        case GS_ERR_BUDGET_REFUSED: return "GPS budget resize refused";
+        case GS_ERR_NO_DEVICE: return "no CUDA device";
+        case GS_ERR_TOO_LARGE: return "size beyond limit";
+        default: return "unknown status";
+    }
+}
+
+const char* gs_last_error(const gs_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
+
+const char* gs_stage_names(void) { return kStageNames; }
+
+int gs_create(gs_ctx** out, int device, void* stream) {
+    if (!out) return GS_ERR_BAD_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return GS_ERR_NO_DEVICE;
+    if (device < 0 || device >= ndev) return GS_ERR_BAD_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return GS_ERR_NO_DEVICE;
+    gs_ctx* c = new (std::nothrow) gs_ctx();
+    if (!c) return GS_ERR_OOM;
+    c->device = device;
+    c->stream = static_cast<cudaStream_t>(stream);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    c->num_sms = sms > 0 ? (uint32_t)sms : 148u;
+    // renderer_init defaults (src/renderer.cpp:588-599)
+    c->knobs.render_mode = GS_MODE_GPS;
+    c->knobs.sh_degree = 3;
+    c->knobs.sh_lod_distance = 0.0f;
+    c->knobs.gps_supersample_factor = 2;
+    c->knobs.stochastic_samples_per_frame = 1;
+    c->knobs.stochastic_taa_current_samples = 4;
+    c->knobs.stochastic_accumulation_enabled = 1;
+    c->knobs.stochastic_taa_enabled = 1;
+    c->knobs.black_background = 0;
+    c->knobs.splat_diagnostics_enabled = 0;
+    c->knobs.linear_color = 0;
+    c->knobs.write_invisible_records = 0;
+    if (cudaMalloc(reinterpret_cast<void**>(&c->d_cam), sizeof(gs_camera)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&c->h_cam), sizeof(gs_camera)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&c->h_fc), sizeof(FrameCounters)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->fc_event, cudaEventDisableTiming) != cudaSuccess) {
+        gs_destroy(c);
+        return GS_ERR_OOM;
+    }
+    std::memset(c->h_fc, 0, sizeof(FrameCounters));
+    *out = c;
+    return GS_OK;
+}
+
+void gs_destroy(gs_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    release_scene(c);
+    release_targets(c);
+    dfree(c->d_cam);
+    if (c->h_cam) cudaFreeHost(c->h_cam);
+    if (c->h_fc) cudaFreeHost(c->h_fc);
+    if (c->h_out16) cudaFreeHost(c->h_out16);
+    if (c->fc_event) cudaEventDestroy(c->fc_event);
+    for (auto& p : c->pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto e : c->event_pool) cudaEventDestroy(e);
+    delete c;
+}
+
+int gs_get_knobs(const gs_ctx* c, gs_knobs* out) {
+    if (!c || !out) return GS_ERR_BAD_ARG;
+    *out = c->knobs;
+    return GS_OK;
+}
+
+int gs_set_knobs(gs_ctx* c, const gs_knobs* k) {
+    if (!c || !k) return GS_ERR_BAD_ARG;
+    if (k->render_mode < 0 || k->render_mode > 2 || k->sh_degree < 0 || k->sh_degree > 3)
+        return fail(c, GS_ERR_BAD_ARG, "knob out of range");
+    const bool reset = k->render_mode != c->knobs.render_mode ||
+                       k->gps_supersample_factor != c->knobs.gps_supersample_factor ||
+                       k->black_background != c->knobs.black_background || k->sh_degree != c->knobs.sh_degree ||
+                       k->stochastic_taa_enabled != c->knobs.stochastic_taa_enabled ||
+                       k->linear_color != c->knobs.linear_color;
+    c->knobs = *k;
+    if (reset) gs_reset_accumulation(c);
+    return GS_OK;
+}
+
+int gs_set_mode(gs_ctx* c, int mode) {
+    if (!c || mode < 0 || mode > 2) return GS_ERR_BAD_ARG;
+    gs_knobs k = c->knobs;
+    k.render_mode = mode;
+    return gs_set_knobs(c, &k);
+}
+
+int gs_reset_accumulation(gs_ctx* c) {
+    if (!c) return GS_ERR_BAD_ARG;
+    // src/renderer.cpp renderer_reset_stochastic_accumulation
+    c->sample_count = 0;
+    c->accum_write_index = 0;
+    c->prev_cam_valid = false;
+    c->taa_prev_valid = false;
+    return GS_OK;
+}
+
+static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcpyKind kind) {
+    if (!c || (!rows && count)) return GS_ERR_BAD_ARG;
+    if (count == 0) return fail(c, GS_ERR_BAD_ARG, "empty scene");  // src/renderer.cpp:757
+    if (count > (1ull << 30) - 1) return fail(c, GS_ERR_TOO_LARGE, "more than 2^30-1 Gaussians");
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    release_scene(c);
+    const uint32_t n = (uint32_t)count;
+    GS_CUDA(c, dalloc(&c->rows, (size_t)n * 256));
+    GS_CUDA(c, dalloc(&c->projected, (size_t)n * 64));
+    for (int k = 0; k < 2; ++k) {
+        GS_CUDA(c, dalloc(&c->keys[k], (size_t)n * 4));
+        GS_CUDA(c, dalloc(&c->ids[k], (size_t)n * 4));
+    }
+    GS_CUDA(c, dalloc(&c->records, (size_t)n * sizeof(RasterRecord)));
+    const size_t cull_tiles = ((size_t)n + gs::kCullTile - 1) / gs::kCullTile;
+    GS_CUDA(c, dalloc(&c->cull_status, cull_tiles * sizeof(unsigned long long)));
+    c->sort_status_stride = gs::sort_status_words(n);
+    GS_CUDA(c, dalloc(&c->sort_status, c->sort_status_stride * 4 * sizeof(unsigned long long)));
+    const size_t bin_tiles = ((size_t)n + gs::kBinThreads - 1) / gs::kBinThreads;
+    GS_CUDA(c, dalloc(&c->bin_status, bin_tiles * sizeof(unsigned long long)));
+    GS_CUDA(c, cudaMemsetAsync(c->cull_status, 0, cull_tiles * 8, c->stream));
+    GS_CUDA(c, cudaMemsetAsync(c->sort_status, 0, c->sort_status_stride * 4 * 8, c->stream));
+    GS_CUDA(c, cudaMemsetAsync(c->bin_status, 0, bin_tiles * 8, c->stream));
+    GS_CUDA(c, cudaMemsetAsync(c->projected, 0, (size_t)n * 64, c->stream));
+    GS_CUDA(c, cudaMemcpyAsync(c->rows, rows, (size_t)n * 256, kind, c->stream));
+    c->n = n;
+    int rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(std::max<uint64_t>(8ull * n, 1u << 20), 0x3FFFFFFFull));
+    if (rc) return rc;
+    GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    gs_reset_accumulation(c);
+    return GS_OK;
+}
+
+int gs_upload_rows(gs_ctx* c, const float* rows, uint64_t count) {
+    return upload_common(c, rows, count, cudaMemcpyHostToDevice);
+}
+
+int gs_upload_rows_device(gs_ctx* c, const float* rows, uint64_t count) {
+    return upload_common(c, rows, count, cudaMemcpyDeviceToDevice);
+}
+
+int gs_set_gps_budget(gs_ctx* c, uint32_t max_work_items) {
+    if (!c) return GS_ERR_BAD_ARG;
+    if (max_work_items == 0) return fail(c, GS_ERR_BUDGET_REFUSED, "GPS budget must be >= 1");
+    int rc = gs::resize_gps_work(c->gps, max_work_items, c->stream);
+    if (rc) return fail(c, GS_ERR_BUDGET_REFUSED, "GPS work buffer resize refused; old budget kept");
+    c->gps_max_work_items = max_work_items;
+    gs_reset_accumulation(c);
+    return GS_OK;
+}
+
+int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
+    if (!c || !cam || !out) return GS_ERR_BAD_ARG;
+    if (!c->n) return fail(c, GS_ERR_NO_SCENE, "no scene uploaded");
+    cudaSetDevice(c->device);
+    int w = (int)(cam->viewport[0] + 0.5f), h = (int)(cam->viewport[1] + 0.5f);  // src/renderer.cpp:2193-2196
+    int rc = ensure_targets(c, w, h);
+    if (rc) return rc;
+    rc = check_previous_frame(c);
+    if (rc) return rc;
+    begin_frame(c, cam);
+    uint16_t* o = static_cast<uint16_t*>(out);
+    switch (c->knobs.render_mode) {
+        case GS_MODE_ALPHA: rc = render_alpha(c, o); break;
+        case GS_MODE_STOCHASTIC: rc = render_stochastic(c, cam, o); break;
+        default: rc = render_gps(c, cam, o); break;
+    }
+    end_frame(c);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    return rc;
+}
+
+int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
+    if (!c || !cam || !host_out) return GS_ERR_BAD_ARG;
+    int w = (int)(cam->viewport[0] + 0.5f), h = (int)(cam->viewport[1] + 0.5f);
+    int rc = ensure_targets(c, w, h);
+    if (rc) return rc;
+    const size_t bytes = (size_t)w * h * 8;
+    if (c->h_out16_bytes < bytes) {
+        if (c->h_out16) cudaFreeHost(c->h_out16);
+        c->h_out16 = nullptr;
+        c->h_out16_bytes = 0;
+        GS_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&c->h_out16), bytes));
+        c->h_out16_bytes = bytes;
+    }
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        // A re-render replays the same frame: restore the state a frame advances.
+        const uint32_t seed = c->frame_seed, samples = c->sample_count, widx = c->accum_write_index;
+        const gs_camera pcam = c->prev_cam;
+        const bool pvalid = c->prev_cam_valid, tvalid = c->taa_prev_valid;
+        rc = gs_render(c, cam, c->out16);
+        if (rc) return rc;
+        GS_CUDA(c, cudaMemcpyAsync(c->h_out16, c->out16, bytes, cudaMemcpyDeviceToHost, c->stream));
+        GS_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->fc_pending = false;
+        if (!c->h_fc->tile_overflow) break;
+        uint64_t need = (uint64_t)c->h_fc->tile_entries + c->h_fc->tile_overflow;
+        rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(need + need / 4 + 1024, 0x3FFFFFFFull));
+        if (rc) return rc;
+        c->frame_seed = seed;
+        c->sample_count = samples;
+        c->accum_write_index = widx;
+        c->prev_cam = pcam;
+        c->prev_cam_valid = pvalid;
+        c->taa_prev_valid = tvalid;
+    }
+    std::memcpy(host_out, c->h_out16, bytes);
+    if (c->h_fc->error_flags & ~(uint32_t)gs::kErrTileOverflow)
+        return fail(c, GS_ERR_DEVICE_TIMEOUT, "a device-side wait ran out");
+    return GS_OK;
+}
+
+int gs_read_stats(gs_ctx* c, gs_stats* s) {
+    if (!c || !s) return GS_ERR_BAD_ARG;
+    GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->fc_pending = false;
+    std::memset(s, 0, sizeof(*s));
+    const FrameCounters& f = *c->h_fc;
+    s->gaussian_count = c->n;
+    s->visible_count = f.visible_count;
+    s->tile_entries = f.tile_entries;
+    s->tile_overflow = f.tile_overflow;
+    for (int k = 0; k < 8; ++k) s->diagnostics[k] = f.diag[k];
+    s->gps_requested_work_items = f.gps_work[0];
+    s->gps_budget_exhausted = f.gps_work[1];
+    s->gps_max_work_items = c->gps_max_work_items;
+    s->sample_count = c->sample_count;
+    s->frame_seed = c->frame_seed;
+    s->error_flags = f.error_flags;
+    s->kernel_launches = c->last_launches;
+    return (f.error_flags & ~(uint32_t)gs::kErrTileOverflow) ? GS_ERR_DEVICE_TIMEOUT : GS_OK;
+}
+
+int gs_debug_read(gs_ctx* c, int which, void* dst, uint64_t bytes) {
+    if (!c || !dst) return GS_ERR_BAD_ARG;
+    GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    const uint64_t n = c->n;
+    const uint32_t vis = c->h_fc->visible_count;
+    const size_t npix = (size_t)c->width * c->height;
+    switch (which) {
+        case GS_DEBUG_IDS:
+        case GS_DEBUG_KEYS: {
+            // The reference keeps all-N arrays (culled = 0xFFFFFFFF); ours are
+            // compacted in index order, so expand them here.
+            if (bytes < n * 4) return GS_ERR_BAD_ARG;
+            std::vector<uint32_t> k(vis), id(vis);
+            GS_CUDA(c, cudaMemcpy(k.data(), c->keys[1], (size_t)vis * 4, cudaMemcpyDeviceToHost));
+            GS_CUDA(c, cudaMemcpy(id.data(), c->ids[1], (size_t)vis * 4, cudaMemcpyDeviceToHost));
+            uint32_t* o = static_cast<uint32_t*>(dst);
+            std::fill(o, o + n, 0xFFFFFFFFu);
+            for (uint32_t i = 0; i < vis; ++i) o[id[i]] = which == GS_DEBUG_IDS ? id[i] : k[i];
+            return GS_OK;
+        }
+        case GS_DEBUG_PROJECTED:
+            if (bytes < n * 64) return GS_ERR_BAD_ARG;
+            GS_CUDA(c, cudaMemcpy(dst, c->projected, n * 64, cudaMemcpyDeviceToHost));
+            return GS_OK;
+        case GS_DEBUG_SORTED_IDS:
+        case GS_DEBUG_SORTED_KEYS: {
+            if (bytes < n * 4) return GS_ERR_BAD_ARG;
+            SortPlan pl;
+            GS_CUDA(c, cudaMemcpy(&pl, c->depth_plan, sizeof(pl), cudaMemcpyDeviceToHost));
+            const uint32_t* src = which == GS_DEBUG_SORTED_IDS ? pl.vfinal : pl.kfinal;
+            uint32_t* o = static_cast<uint32_t*>(dst);
+            if (!src) return fail(c, GS_ERR_BAD_ARG, "no sort in the last frame");
+            GS_CUDA(c, cudaMemcpy(o, src, (size_t)vis * 4, cudaMemcpyDeviceToHost));
+            std::fill(o + vis, o + n, 0xFFFFFFFFu);
+            return GS_OK;
+        }
+        case GS_DEBUG_ACCUM:
+        case GS_DEBUG_SAMPLE: {
+            if (bytes < npix * 16) return GS_ERR_BAD_ARG;
+            const float4* src = which == GS_DEBUG_SAMPLE ? c->st.sample : c->st.display;
+            if (!src) return fail(c, GS_ERR_BAD_ARG, "no stochastic/GPS frame rendered");
+            GS_CUDA(c, cudaMemcpy(dst, src, npix * 16, cudaMemcpyDeviceToHost));
+            return GS_OK;
+        }
+        case GS_DEBUG_DEPTH:
+            if (bytes < npix * 4) return GS_ERR_BAD_ARG;
+            if (!c->st.depth) return fail(c, GS_ERR_BAD_ARG, "no stochastic/GPS frame rendered");
+            GS_CUDA(c, cudaMemcpy(dst, c->st.depth, npix * 4, cudaMemcpyDeviceToHost));
+            return GS_OK;
+        default:
+            return GS_ERR_BAD_ARG;
+    }
+}
+
+int gs_profile_enable(gs_ctx* c, int enable) {
+    if (!c) return GS_ERR_BAD_ARG;
+    c->profiling = enable != 0;
+    return GS_OK;
+}
+
+int gs_stage_times(gs_ctx* c, float* ms, uint32_t* launches, int max_stages, int reset) {
+    if (!c) return GS_ERR_BAD_ARG;
+    GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (auto& p : c->pending) {
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, p.a, p.b);
+        c->stage_ms[p.stage] += t;
+        c->stage_launches[p.stage] += p.launches;
+        c->event_pool.push_back(p.a);
+        c->event_pool.push_back(p.b);
+    }
+    c->pending.clear();
+    for (int k = 0; k < ST_COUNT && k < max_stages; ++k) {
+        if (ms) ms[k] = (float)c->stage_ms[k];
+        if (launches) launches[k] = c->stage_launches[k];
+    }
+    if (reset) {
+        std::fill(c->stage_ms, c->stage_ms + ST_COUNT, 0.0);
+        std::fill(c->stage_launches, c->stage_launches + ST_COUNT, 0u);
+    }
+    return ST_COUNT;
+}
+
+}  // extern "C"

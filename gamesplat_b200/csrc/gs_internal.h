@@ -1,0 +1,161 @@
+// Internal interfaces between the C++ host orchestration (gs_host.cpp) and the
+// CUDA kernels.  Not part of the public C ABI (include/gs_api.h).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/gs_api.h"
+
+namespace gs {
+
+// Device error flags (gs_stats.error_flags).
+enum : uint32_t {
+    kErrCullLookback = 1u << 0,
+    kErrSortLookback = 1u << 1,
+    kErrBinLookback = 1u << 2,
+    kErrRasterWait = 1u << 3,
+    kErrTileOverflow = 1u << 4,
+    kErrGpsWait = 1u << 5,
+};
+
+// Small per-frame device control block.  Zeroed at the start of each frame
+// (one memset), except where noted.
+struct FrameCounters {
+    uint32_t visible_count;      // cull output (shaders/cull.glsl:230)
+    uint32_t diag[8];            // SplatDiagnostics (shaders/cull.glsl:296-318)
+    uint32_t error_flags;        // gs::kErr* bits
+    uint32_t cull_ticket;        // tile tickets for persistent kernels
+    uint32_t bin_ticket;
+    uint32_t tile_entries;       // (tile, splat) pairs produced by binning
+    uint32_t tile_overflow;      // entries that did not fit
+    uint32_t gps_work[2];        // [0] requested work items, [1] overflow (gps.glsl work_count)
+    uint32_t raster_ticket;
+    uint32_t pad[2];
+};
+
+// Device-resident plan of one radix sort, written by its plan kernel from the
+// digit histograms: which passes do work (a pass whose digit is the same for
+// every key is the identity permutation of a stable sort and is skipped),
+// and the ping-pong buffers of each active pass.  Zeroed before each sort.
+struct SortPlan {
+    const uint32_t* kin[4];
+    const uint32_t* vin[4];
+    uint32_t* kout[4];
+    uint32_t* vout[4];
+    uint32_t active[4];
+    uint32_t ticket[4];
+    const uint32_t* kfinal;      // where the sorted keys are
+    const uint32_t* vfinal;      // where the sorted values are
+    uint32_t copy_needed;        // land_in_buf0 with no active pass
+    uint32_t count;
+    uint32_t pad[2];
+};
+
+// Onesweep radix sort configuration.
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // keys per CTA tile
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+
+// Cull configuration: 256 threads, 4 rounds of 256 Gaussians per CTA tile.
+constexpr int kCullThreads = 256;
+constexpr int kCullRounds = 4;
+constexpr int kCullTile = kCullThreads * kCullRounds;
+
+// Binning configuration.
+constexpr int kBinThreads = 256;
+constexpr int kTileW = 16;
+constexpr int kTileH = 16;
+
+// Raster record: one per visible splat in depth-sorted order, 64 bytes,
+// staged into shared memory by TMA bulk copies.
+struct __align__(16) RasterRecord {
+    float cx, cy, conic_x, conic_2y;     // centre (+jitter), conic.x, 2*conic.y
+    float conic_z, opacity, cutoff, r;   // cutoff = log((1/255)/max(opacity,1e-8))
+    float g, b;
+    uint32_t rect_x;                     // i0 | i1 << 16  (covered pixel columns)
+    uint32_t rect_y;                     // j0 | j1 << 16  (covered pixel rows, GL order)
+    uint32_t depth24;                    // window depth as D24 (stochastic depth test)
+    uint32_t splat_id;                   // original Gaussian index
+    float hash_z;                        // float(splat_id) + frame_seed
+    uint32_t pad;
+};
+static_assert(sizeof(RasterRecord) == 64, "RasterRecord must be 64 bytes");
+
+struct CullParams {
+    const float4* rows;          // N x 16 float4 (GpuGaussian)
+    uint32_t n;
+    const gs_camera* cam;        // device copy of the frame's CameraUniforms
+    int sh_degree;
+    float sh_lod_distance;
+    int collect_stats;
+    int write_invisible;         // also write the reference's invisible record
+    float4* projected;           // N x 4 float4 (CullProjectedSplatData)
+    uint32_t* keys_out;          // compacted visible keys, index order
+    uint32_t* ids_out;           // compacted visible ids
+    unsigned long long* status;  // per-tile look-back words (epoch-tagged)
+    uint32_t epoch;
+    FrameCounters* fc;
+};
+
+struct SortParams {
+    const uint32_t* keys_in;     // input pairs (never written)
+    const uint32_t* vals_in;
+    uint32_t* keys_buf[2];       // writable ping-pong buffers (keys_buf[1] may alias keys_in
+    uint32_t* vals_buf[2];       //  when land_in_buf0 == 0)
+    int land_in_buf0;            // 1: the result must end in keys_buf[0]/vals_buf[0]
+    const uint32_t* count_ptr;   // device-side element count
+    uint32_t count_cap;          // capacity (grid sizing)
+    int begin_bit, end_bit;
+    uint32_t* hist;              // 4 x 256 digit histograms (zeroed before the sort)
+    SortPlan* plan;              // zeroed before the sort
+    unsigned long long* status;  // per pass: tiles x 256 look-back words (epoch-tagged)
+    size_t status_stride;        // words per pass
+    uint32_t epoch;
+    uint32_t* error_flags;
+};
+
+struct BinParams {
+    const SortPlan* depth_plan;      // sorted ids at depth_plan->vfinal
+    const float4* projected;
+    const gs_camera* cam;
+    float jitter_x, jitter_y;
+    float frame_seed;
+    int width, height, tiles_x, tiles_y;
+    RasterRecord* records;           // N_vis records (sorted order)
+    uint32_t* entry_keys;            // tile id per entry
+    uint32_t* entry_vals;            // sorted position per entry
+    uint32_t entry_cap;
+    unsigned long long* status;      // per-CTA-tile look-back words (epoch-tagged)
+    uint32_t epoch;
+    FrameCounters* fc;
+};
+
+struct RasterParams {
+    const RasterRecord* records;
+    uint32_t record_cap;             // records allocated (bounds every record index)
+    const SortPlan* tile_plan;       // tile-sorted entry values at tile_plan->vfinal
+    const uint2* tile_ranges;        // [start, end) per tile
+    int width, height, tiles_x, tiles_y;
+    float bg;
+    uint16_t* out_rgba16f;           // width*height*4 halves, top row first
+    float4* out_rgba32f;             // optional float copy (stochastic sample), top row first
+    float* out_depth;                // optional window depth (stochastic), top row first
+    int rgba8;                       // quantise stochastic sample like RGBA8 UNORM
+    FrameCounters* fc;
+};
+
+// Launchers (each returns the number of kernels it launched).
+int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s);
+int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s);
+int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s);
+int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
+                       uint32_t num_tiles, uint32_t num_sms, cudaStream_t s);
+int launch_raster_alpha(const RasterParams& p, cudaStream_t s);
+int launch_raster_stochastic(const RasterParams& p, cudaStream_t s);
+
+size_t sort_status_words(uint32_t count_cap);   // look-back words per pass
+int sort_passes(int begin_bit, int end_bit);
+}  // namespace gs

@@ -1,0 +1,202 @@
+// Tile rasterizer: replaces the reference's GL instanced-quad draw, fragment
+// shader and fixed-function blender (shaders/splat.glsl:39-145,
+// src/renderer.cpp:266-320, 1687-1720).
+//
+// One CTA per 16x16 pixel tile, one pixel per thread (GL window coordinates,
+// row 0 at the bottom; the image is written top row first).  The tile's
+// depth-ordered splat list is walked front to back (reverse of the
+// reference's back-to-front draw order, so equal depth keys are visited in
+// descending splat index, which reproduces "later instance on top").
+// Batches of 128 64-byte RasterRecords are staged into shared memory by TMA
+// 1-D bulk copies (cp.async.bulk, completion on an mbarrier), double
+// buffered so the next batch lands while the current one is composited.
+//
+// Alpha mode: premultiplied "over" in FP32, front to back:
+//   C += T * alpha * rgb,  T *= 1 - alpha,  output (C + T*bg, 1 - T),
+// which equals the reference's back-to-front ONE / ONE_MINUS_SRC_ALPHA
+// blend into a (bg,bg,bg,0) target up to FP32 rounding.  A pixel stops once
+// T < 2^-13: the skipped remainder is below T * max(rgb, bg).  Coverage
+// (quad rectangle) and the two discards (power > 0, power < cutoff) are
+// evaluated bit-exactly like the CPU oracle; alpha uses the hardware exp.
+//
+// Stochastic mode: a fragment is kept iff hash13(fragcoord, id + seed) <
+// alpha; the depth test (LESS, writes on) keeps the kept fragment with the
+// smallest (D24 depth, instance index).  Walking front to back, a pixel stops
+// once a splat's D24 exceeds the kept one's by more than 8 (the float
+// depth-to-D24 mapping is monotone to within 5 units).  Deterministic exp and
+// hash, so the kept set matches the oracle bit for bit.
+#include <cuda_fp16.h>
+
+#include "gs_common.cuh"
+#include "gs_internal.h"
+#include "gs_tma.cuh"
+
+namespace gs {
+
+constexpr int kRasterThreads = kTileW * kTileH;
+constexpr int kBatch = 128;
+constexpr float kTransmittanceMin = 1.0f / 8192.0f;
+constexpr uint32_t kDepthMargin = 8;
+
+__device__ __forceinline__ float hash13(float p0, float p1, float p2) {
+    p0 = g_fract(mul(p0, 0.1031f));
+    p1 = g_fract(mul(p1, 0.1031f));
+    p2 = g_fract(mul(p2, 0.1031f));
+    float d = add(add(mul(p0, add(p1, 33.33f)), mul(p1, add(p2, 33.33f))), mul(p2, add(p0, 33.33f)));
+    p0 = add(p0, d);
+    p1 = add(p1, d);
+    p2 = add(p2, d);
+    return g_fract(mul(add(p0, p1), p2));
+}
+
+struct AlphaState {
+    float T, c0, c1, c2;
+};
+
+struct StochState {
+    uint32_t best_d24, best_id;
+    float r, g, b;
+};
+
+template <int kMode>  // 0 = alpha, 1 = stochastic
+__global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) {
+    __shared__ __align__(128) RasterRecord s_rec[2][kBatch];
+    __shared__ __align__(8) uint64_t s_bar[2];
+
+    const uint32_t tile = blockIdx.x;
+    const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
+    const int px = tx * kTileW + (int)(threadIdx.x % kTileW);
+    const int py = ty * kTileH + (int)(threadIdx.x / kTileW);
+    const bool inside = px < p.width && py < p.height;
+    const uint2 range = p.tile_ranges[tile];
+    const uint32_t n = range.y > range.x ? range.y - range.x : 0u;
+    const uint32_t* __restrict__ vals = p.tile_plan->vfinal;
+
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    const float fcx = (float)px + 0.5f, fcy = (float)py + 0.5f;
+    AlphaState A = {1.0f, 0.0f, 0.0f, 0.0f};
+    StochState S = {16777215u, 0xFFFFFFFFu, 0.0f, 0.0f, 0.0f};
+    bool done = !inside;
+    bool failed = false;
+    const uint32_t nb = (n + kBatch - 1) / kBatch;
+    uint32_t phase0 = 0, phase1 = 0;
+
+    auto issue = [&](uint32_t b) {
+        const uint32_t first = b * kBatch;
+        const uint32_t cnt = min((uint32_t)kBatch, n - first);
+        uint64_t* bar = &s_bar[b & 1];
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, cnt * (uint32_t)sizeof(RasterRecord));
+        if (threadIdx.x < cnt) {
+            const uint32_t s = min(vals[range.y - 1 - (first + threadIdx.x)], p.record_cap - 1u);
+            bulk_g2s(&s_rec[b & 1][threadIdx.x], p.records + s, (uint32_t)sizeof(RasterRecord), bar);
+        }
+    };
+
+    if (nb > 0) issue(0);
+    for (uint32_t b = 0; b < nb; ++b) {
+        if (b + 1 < nb) issue(b + 1);
+        const uint32_t ph = (b & 1) ? phase1 : phase0;
+        if (!mbar_wait_bounded(&s_bar[b & 1], ph)) failed = true;
+        if (b & 1) phase1 ^= 1u; else phase0 ^= 1u;
+        const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
+        const RasterRecord* recs = s_rec[b & 1];
+        if (!done && !failed) {
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
+                const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
+                const uint4 q2 = reinterpret_cast<const uint4*>(recs + j)[2];
+                if (kMode == 1 && S.best_id != 0xFFFFFFFFu) {
+                    const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
+                    if (q3.x > S.best_d24 + kDepthMargin) { done = true; break; }
+                }
+                const uint32_t i0 = q2.z & 0xFFFFu, i1 = q2.z >> 16, j0 = q2.w & 0xFFFFu, j1 = q2.w >> 16;
+                if ((uint32_t)(px - (int)i0) >= i1 - i0 || (uint32_t)(py - (int)j0) >= j1 - j0) continue;
+                const float dx = sub(fcx, q0.x), dy = sub(fcy, q0.y);
+                const float power = splat_power(dx, dy, q0.z, q0.w, q1.x);
+                if (!(power <= 0.0f) || power < q1.z) continue;
+                if (kMode == 0) {
+                    const float alpha = fminf(q1.y * __expf(power), 0.99f);
+                    const float w = alpha * A.T;
+                    A.c0 = fmaf(w, q1.w, A.c0);
+                    A.c1 = fmaf(w, __uint_as_float(q2.x), A.c1);
+                    A.c2 = fmaf(w, __uint_as_float(q2.y), A.c2);
+                    A.T = A.T * (1.0f - alpha);
+                    if (A.T < kTransmittanceMin) { done = true; break; }
+                } else {
+                    const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
+                    const uint32_t z24 = q3.x, id = q3.y;
+                    if (!(z24 < S.best_d24 || (z24 == S.best_d24 && id < S.best_id))) continue;
+                    const float alpha = g_min(mul(q1.y, det_expf(power)), 0.99f);
+                    const float rnd = hash13(fcx, fcy, __uint_as_float(q3.z));
+                    if (rnd >= alpha) continue;
+                    S.best_d24 = z24;
+                    S.best_id = id;
+                    S.r = q1.w;
+                    S.g = __uint_as_float(q2.x);
+                    S.b = __uint_as_float(q2.y);
+                }
+            }
+        }
+        const int all_done = __syncthreads_and(done || failed);
+        if (all_done) {
+            if (b + 1 < nb) {
+                const uint32_t ph2 = ((b + 1) & 1) ? phase1 : phase0;
+                if (!mbar_wait_bounded(&s_bar[(b + 1) & 1], ph2)) failed = true;
+            }
+            break;
+        }
+    }
+    if (failed) atomicOr(&p.fc->error_flags, kErrRasterWait);
+    if (!inside) return;
+    const size_t o = (size_t)(p.height - 1 - py) * p.width + px;
+    if (kMode == 0) {
+        const float r = fmaf(A.T, p.bg, A.c0), g = fmaf(A.T, p.bg, A.c1), b = fmaf(A.T, p.bg, A.c2);
+        const float a = 1.0f - A.T;
+        __half2 h01 = __floats2half2_rn(r, g), h23 = __floats2half2_rn(b, a);
+        uint2 packed;
+        packed.x = *reinterpret_cast<uint32_t*>(&h01);
+        packed.y = *reinterpret_cast<uint32_t*>(&h23);
+        reinterpret_cast<uint2*>(p.out_rgba16f)[o] = packed;
+    } else {
+        float4 c;
+        if (S.best_id == 0xFFFFFFFFu) c = make_float4(p.bg, p.bg, p.bg, 0.0f);
+        else c = make_float4(S.r, S.g, S.b, 1.0f);
+        if (p.rgba8) {
+            c.x = rintf(g_clamp(c.x, 0.0f, 1.0f) * 255.0f) / 255.0f;
+            c.y = rintf(g_clamp(c.y, 0.0f, 1.0f) * 255.0f) / 255.0f;
+            c.z = rintf(g_clamp(c.z, 0.0f, 1.0f) * 255.0f) / 255.0f;
+            c.w = rintf(g_clamp(c.w, 0.0f, 1.0f) * 255.0f) / 255.0f;
+        }
+        if (p.out_rgba32f) p.out_rgba32f[o] = c;
+        if (p.out_depth) p.out_depth[o] = (float)S.best_d24 / 16777215.0f;
+        if (p.out_rgba16f) {
+            __half2 h01 = __floats2half2_rn(c.x, c.y), h23 = __floats2half2_rn(c.z, c.w);
+            uint2 packed;
+            packed.x = *reinterpret_cast<uint32_t*>(&h01);
+            packed.y = *reinterpret_cast<uint32_t*>(&h23);
+            reinterpret_cast<uint2*>(p.out_rgba16f)[o] = packed;
+        }
+    }
+}
+
+int launch_raster_alpha(const RasterParams& p, cudaStream_t s) {
+    const uint32_t tiles = (uint32_t)p.tiles_x * (uint32_t)p.tiles_y;
+    if (tiles == 0) return 0;
+    raster_kernel<0><<<tiles, kRasterThreads, 0, s>>>(p);
+    return 1;
+}
+
+int launch_raster_stochastic(const RasterParams& p, cudaStream_t s) {
+    const uint32_t tiles = (uint32_t)p.tiles_x * (uint32_t)p.tiles_y;
+    if (tiles == 0) return 0;
+    raster_kernel<1><<<tiles, kRasterThreads, 0, s>>>(p);
+    return 1;
+}
+
+}  // namespace gs

@@ -1,0 +1,340 @@
+// Onesweep LSD radix sort of (uint32 key, uint32 value) pairs for the B200.
+//
+// Same result as the reference's 4 x (histogram, single-workgroup prefix,
+// bitmask-rank scatter) passes (shaders/sort.glsl:26-163,
+// src/renderer.cpp:1873-1962): a stable ascending sort, equal keys in input
+// order.  Structure:
+//   1. sort_hist_kernel   - one read of the keys builds the digit histograms
+//                           of every pass (warp-private shared histograms);
+//   2. sort_plan_kernel   - exclusive digit offsets; passes whose digit is the
+//                           same for all keys are skipped (identity for a
+//                           stable sort); ping-pong assignment of active passes;
+//   3. sort_pass_kernel   - per pass, persistent CTAs take 4096-key tiles in
+//                           ticket order, rank keys with warp match/ballot
+//                           (__match_any_sync), publish per-digit counts and
+//                           resolve their global offsets by decoupled
+//                           look-back (bounded spin), reorder the tile by digit
+//                           in shared memory and write runs coalesced;
+//   4. sort_copy_kernel   - only when the caller needs the result in a given
+//                           buffer and every pass was skipped.
+// Element counts are read on the device, so nothing here synchronises with
+// the host.
+#include "gs_common.cuh"
+#include "gs_internal.h"
+
+namespace gs {
+
+constexpr int kSortWarps = kSortThreads / 32;
+static_assert(kSortThreads == kRadix, "one thread per digit in the pass kernel");
+
+int sort_passes(int begin_bit, int end_bit) { return (end_bit - begin_bit + kRadixBits - 1) / kRadixBits; }
+
+size_t sort_status_words(uint32_t count_cap) {
+    size_t tiles = ((size_t)count_cap + kSortTile - 1) / kSortTile;
+    if (tiles == 0) tiles = 1;
+    return tiles * kRadix;
+}
+
+__device__ __forceinline__ uint32_t digit_of(uint32_t key, int shift, uint32_t dmask) { return (key >> shift) & dmask; }
+
+__global__ void __launch_bounds__(kSortThreads) sort_hist_kernel(SortParams p, int npasses) {
+    __shared__ uint32_t wh[kSortWarps][4][kRadix];  // warp-private histograms, 32 KB
+    const int warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kSortWarps * 4 * kRadix; i += kSortThreads) (&wh[0][0][0])[i] = 0u;
+    __syncthreads();
+    const uint32_t n = p.count_ptr ? *p.count_ptr : p.count_cap;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // Vector loads only when the caller's key pointer is 16-byte aligned.
+    const uint32_t n4 = (((uintptr_t)p.keys_in & 15u) == 0u) ? (n >> 2) : 0u;
+    const uint4* k4 = reinterpret_cast<const uint4*>(p.keys_in);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        uint4 k = __ldg(k4 + i);
+        for (int ps = 0; ps < npasses; ++ps) {
+            int shift = p.begin_bit + ps * kRadixBits;
+            uint32_t dmask = (1u << min(kRadixBits, p.end_bit - shift)) - 1u;
+            atomicAdd(&wh[warp][ps][digit_of(k.x, shift, dmask)], 1u);
+            atomicAdd(&wh[warp][ps][digit_of(k.y, shift, dmask)], 1u);
+            atomicAdd(&wh[warp][ps][digit_of(k.z, shift, dmask)], 1u);
+            atomicAdd(&wh[warp][ps][digit_of(k.w, shift, dmask)], 1u);
+        }
+    }
+    for (uint32_t i = (n4 << 2) + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint32_t k = __ldg(p.keys_in + i);
+        for (int ps = 0; ps < npasses; ++ps) {
+            int shift = p.begin_bit + ps * kRadixBits;
+            uint32_t dmask = (1u << min(kRadixBits, p.end_bit - shift)) - 1u;
+            atomicAdd(&wh[warp][ps][digit_of(k, shift, dmask)], 1u);
+        }
+    }
+    __syncthreads();
+    for (int ps = 0; ps < npasses; ++ps) {
+        uint32_t sum = 0;
+        for (int w = 0; w < kSortWarps; ++w) sum += wh[w][ps][threadIdx.x];
+        if (sum) atomicAdd(&p.hist[ps * kRadix + threadIdx.x], sum);
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads) sort_plan_kernel(SortParams p, int npasses) {
+    __shared__ uint32_t scan_tmp[33];
+    __shared__ uint32_t s_active[4];
+    const uint32_t n = p.count_ptr ? *p.count_ptr : p.count_cap;
+    const int t = threadIdx.x;
+    for (int ps = 0; ps < npasses; ++ps) {
+        uint32_t c = p.hist[ps * kRadix + t];
+        int all_in_one = __syncthreads_or(c == n);
+        uint32_t total;
+        uint32_t excl = block_excl_scan(c, scan_tmp, &total);
+        p.hist[ps * kRadix + t] = excl;
+        if (t == 0) s_active[ps] = all_in_one ? 0u : 1u;
+    }
+    __syncthreads();
+    if (t == 0) {
+        SortPlan* pl = p.plan;
+        int m = 0;
+        for (int ps = 0; ps < npasses; ++ps) m += (int)s_active[ps];
+        const uint32_t* kcur = p.keys_in;
+        const uint32_t* vcur = p.vals_in;
+        // Destination of the j-th active pass (j = 0..m-1): with land_in_buf0
+        // the last one writes buffer 0, alternating backwards; otherwise the
+        // first writes buffer 0, alternating forwards.
+        int j = 0;
+        for (int ps = 0; ps < 4; ++ps) {
+            pl->active[ps] = (ps < npasses) ? s_active[ps] : 0u;
+            if (!pl->active[ps]) continue;
+            int dst = p.land_in_buf0 ? ((m - 1 - j) & 1) : (j & 1);
+            pl->kin[ps] = kcur;
+            pl->vin[ps] = vcur;
+            pl->kout[ps] = p.keys_buf[dst];
+            pl->vout[ps] = p.vals_buf[dst];
+            kcur = p.keys_buf[dst];
+            vcur = p.vals_buf[dst];
+            ++j;
+        }
+        pl->copy_needed = (p.land_in_buf0 && m == 0) ? 1u : 0u;
+        pl->kfinal = pl->copy_needed ? p.keys_buf[0] : kcur;
+        pl->vfinal = pl->copy_needed ? p.vals_buf[0] : vcur;
+        pl->count = n;
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p, int pass) {
+    __shared__ uint32_t s_keys[kSortTile];
+    __shared__ uint32_t s_vals[kSortTile];
+    __shared__ uint32_t warp_hist[kSortWarps][kRadix];
+    __shared__ uint32_t s_local_start[kRadix];
+    __shared__ uint32_t s_global_base[kRadix];
+    __shared__ uint32_t scan_tmp[33];
+    __shared__ uint32_t s_tile;
+
+    SortPlan* pl = p.plan;
+    if (!pl->active[pass]) return;
+    const uint32_t n = pl->count;
+    const uint32_t* __restrict__ kin = pl->kin[pass];
+    const uint32_t* __restrict__ vin = pl->vin[pass];
+    uint32_t* __restrict__ kout = pl->kout[pass];
+    uint32_t* __restrict__ vout = pl->vout[pass];
+    const int shift = p.begin_bit + pass * kRadixBits;
+    const uint32_t dmask = (1u << min(kRadixBits, p.end_bit - shift)) - 1u;
+    const uint32_t* gdigit = p.hist + pass * kRadix;
+    u64* status = p.status + (size_t)pass * p.status_stride;
+    const uint32_t num_tiles = (n + kSortTile - 1) / kSortTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(&pl->ticket[pass], 1u);
+        for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&warp_hist[0][0])[i] = 0u;
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= num_tiles) break;
+        const uint32_t base = tile * kSortTile;
+        const uint32_t wbase = base + warp * (kSortItems * 32);
+
+        uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+        for (int k = 0; k < kSortItems; ++k) {
+            uint32_t idx = wbase + k * 32 + lane;
+            bool ok = idx < n;
+            key[k] = ok ? kin[idx] : 0u;
+            val[k] = ok ? vin[idx] : 0u;
+        }
+        // Warp ranking in index order (item k, then lane).
+#pragma unroll
+        for (int k = 0; k < kSortItems; ++k) {
+            uint32_t idx = wbase + k * 32 + lane;
+            uint32_t d = (idx < n) ? digit_of(key[k], shift, dmask) : (uint32_t)kRadix;
+            uint32_t peers = __match_any_sync(0xffffffffu, d);
+            int leader = __ffs(peers) - 1;
+            uint32_t before = 0;
+            if (lane == leader && d < (uint32_t)kRadix) {
+                before = warp_hist[warp][d];
+                warp_hist[warp][d] = before + __popc(peers);
+            }
+            before = __shfl_sync(0xffffffffu, before, leader);
+            rank[k] = before + __popc(peers & lt_mask);
+            __syncwarp();
+        }
+        __syncthreads();
+        // One thread per digit: tile count and per-warp exclusive offsets.
+        const uint32_t d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            uint32_t c = warp_hist[w][d];
+            warp_hist[w][d] = run;
+            run += c;
+        }
+        const uint32_t tile_count = run;
+        u64* st = status + (size_t)tile * kRadix + d;
+        uint32_t gexcl;
+        if (tile == 0) {
+            gexcl = gdigit[d];
+            st_release64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
+        } else {
+            st_release64(st, status_word(p.epoch, kFlagAgg, tile_count));
+            bool to = false;
+            gexcl = lookback(status + d, kRadix, tile, p.epoch, &to);
+            if (to) atomicOr(p.error_flags, kErrSortLookback);
+            st_release64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
+        }
+        uint32_t total;
+        uint32_t lstart = block_excl_scan(tile_count, scan_tmp, &total);
+        s_local_start[d] = lstart;
+        s_global_base[d] = gexcl - lstart;
+        __syncthreads();
+        // Reorder the tile by digit in shared memory.
+#pragma unroll
+        for (int k = 0; k < kSortItems; ++k) {
+            uint32_t idx = wbase + k * 32 + lane;
+            if (idx < n) {
+                uint32_t dk = digit_of(key[k], shift, dmask);
+                uint32_t lp = s_local_start[dk] + warp_hist[warp][dk] + rank[k];
+                s_keys[lp] = key[k];
+                s_vals[lp] = val[k];
+            }
+        }
+        __syncthreads();
+        const uint32_t nvalid = min((uint32_t)kSortTile, n - base);
+        for (uint32_t i = threadIdx.x; i < nvalid; i += kSortThreads) {
+            uint32_t k = s_keys[i];
+            uint32_t o = s_global_base[digit_of(k, shift, dmask)] + i;
+            if (o < n) {  // always true unless a look-back wait ran out
+                kout[o] = k;
+                vout[o] = s_vals[i];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void sort_copy_kernel(SortParams p) {
+    const SortPlan* pl = p.plan;
+    if (!pl->copy_needed) return;
+    const uint32_t n = pl->count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        p.keys_buf[0][i] = p.keys_in[i];
+        p.vals_buf[0][i] = p.vals_in[i];
+    }
+}
+
+static int g_pass_blocks_per_sm = 0;
+
+int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s) {
+    if (g_pass_blocks_per_sm == 0) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sort_pass_kernel, kSortThreads, 0);
+        g_pass_blocks_per_sm = b > 0 ? b : 1;
+    }
+    const int npasses = sort_passes(p.begin_bit, p.end_bit);
+    int launches = 0;
+    uint32_t tiles_cap = (p.count_cap + kSortTile - 1) / kSortTile;
+    uint32_t hist_grid = num_sms * 2;
+    uint32_t hist_need = (p.count_cap / 4 + kSortThreads - 1) / kSortThreads;
+    if (hist_grid > hist_need) hist_grid = hist_need > 0 ? hist_need : 1;
+    sort_hist_kernel<<<hist_grid, kSortThreads, 0, s>>>(p, npasses);
+    ++launches;
+    sort_plan_kernel<<<1, kSortThreads, 0, s>>>(p, npasses);
+    ++launches;
+    uint32_t pass_grid = num_sms * (uint32_t)g_pass_blocks_per_sm;
+    if (pass_grid > tiles_cap) pass_grid = tiles_cap > 0 ? tiles_cap : 1;
+    for (int ps = 0; ps < npasses; ++ps) {
+        sort_pass_kernel<<<pass_grid, kSortThreads, 0, s>>>(p, ps);
+        ++launches;
+    }
+    if (p.land_in_buf0) {
+        uint32_t g = (p.count_cap + 1023) / 1024;
+        if (g > num_sms * 4) g = num_sms * 4;
+        if (g == 0) g = 1;
+        sort_copy_kernel<<<g, 256, 0, s>>>(p);
+        ++launches;
+    }
+    return launches;
+}
+
+}  // namespace gs
+
+// ---------------------------------------------------------------------------
+// Stage-level C entry point: sort caller-owned device buffers.
+// Scratch layout: SortPlan | 4x256 histograms | error word | 4 passes of
+// look-back words | temporary keys | temporary values (256-byte aligned).
+// ---------------------------------------------------------------------------
+namespace {
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+struct SortScratch {
+    size_t plan, hist, err, status, tkeys, tvals, total, control_bytes;
+};
+SortScratch sort_scratch_layout(uint32_t n) {
+    SortScratch l{};
+    size_t off = 0;
+    l.plan = off; off += align256(sizeof(gs::SortPlan));
+    l.hist = off; off += align256(4 * 256 * 4);
+    l.err = off; off += align256(4);
+    l.status = off; off += align256(gs::sort_status_words(n) * 4 * sizeof(unsigned long long));
+    l.control_bytes = off;
+    l.tkeys = off; off += align256((size_t)n * 4);
+    l.tvals = off; off += align256((size_t)n * 4);
+    l.total = off;
+    return l;
+}
+}  // namespace
+
+extern "C" size_t gs_sort_pairs_scratch_bytes(uint32_t n) { return sort_scratch_layout(n).total; }
+
+extern "C" int gs_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                             uint32_t n, int begin_bit, int end_bit, void* scratch, size_t scratch_bytes,
+                             void* stream) {
+    if (begin_bit < 0 || end_bit > 32 || end_bit <= begin_bit) return GS_ERR_BAD_ARG;
+    if (n == 0) return GS_OK;
+    if (n > (1u << 30) - 1) return GS_ERR_TOO_LARGE;
+    if (!keys_in || !vals_in || !keys_out || !vals_out || !scratch) return GS_ERR_BAD_ARG;
+    if ((const void*)keys_in == (const void*)keys_out || (const void*)vals_in == (const void*)vals_out)
+        return GS_ERR_BAD_ARG;
+    const SortScratch l = sort_scratch_layout(n);
+    if (scratch_bytes < l.total) return GS_ERR_BAD_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char* base = static_cast<char*>(scratch);
+    if (cudaMemsetAsync(base, 0, l.control_bytes, s) != cudaSuccess) return GS_ERR_CUDA;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    gs::SortParams p{};
+    p.keys_in = keys_in;
+    p.vals_in = vals_in;
+    p.keys_buf[0] = keys_out;
+    p.vals_buf[0] = vals_out;
+    p.keys_buf[1] = reinterpret_cast<uint32_t*>(base + l.tkeys);
+    p.vals_buf[1] = reinterpret_cast<uint32_t*>(base + l.tvals);
+    p.land_in_buf0 = 1;
+    p.count_ptr = nullptr;
+    p.count_cap = n;
+    p.begin_bit = begin_bit;
+    p.end_bit = end_bit;
+    p.hist = reinterpret_cast<uint32_t*>(base + l.hist);
+    p.plan = reinterpret_cast<gs::SortPlan*>(base + l.plan);
+    p.status = reinterpret_cast<unsigned long long*>(base + l.status);
+    p.status_stride = gs::sort_status_words(n);
+    p.epoch = 1;
+    p.error_flags = reinterpret_cast<uint32_t*>(base + l.err);
+    gs::launch_sort(p, sms > 0 ? (uint32_t)sms : 148u, s);
+    return cudaGetLastError() == cudaSuccess ? GS_OK : GS_ERR_CUDA;
+}

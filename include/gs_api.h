@@ -1,0 +1,217 @@
+/* gs_api.h - C ABI of libgs_cuda.so, the B200 (sm_100a) splatting path of
+ * gamesplat.
+ *
+ * The entry points replace the renderer interface of the reference
+ * (src/renderer.h:249-266) for the per-frame splatting path: cull/SH/project
+ * (shaders/cull.glsl), radix depth sort (shaders/sort.glsl), sorted alpha
+ * compositing (shaders/splat.glsl + GL blend), stochastic splatting and the
+ * Gaussian Point Splatting passes (shaders/gps.glsl, shaders/accum.glsl).
+ *
+ * Conventions
+ *  - Plain C types only; no CUDA or C++ types cross the boundary.  A CUDA
+ *    stream is passed as an opaque pointer (cudaStream_t value, NULL = legacy
+ *    default stream).
+ *  - Every function returns a gs_status (0 = GS_OK, < 0 = error) and never
+ *    aborts or traps; the reference reports failures as bool + log line
+ *    (src/renderer.cpp:860-1073).
+ *  - All calls on one gs_ctx must be serialised by the caller, as the
+ *    reference renderer is used from one thread (src/main.cpp:1963).
+ *  - Work is stream-ordered; only gs_render_host, gs_read_stats and
+ *    gs_debug_read synchronise.
+ *  - Images are RGBA16F (IEEE half, 4 channels), row-major, top row first
+ *    (the orientation of the reference harness's linear_capture,
+ *    tests/gsanim_render.cpp:161-163).
+ */
+#ifndef GS_API_H
+#define GS_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_API_VERSION 1
+
+typedef enum gs_status {
+    GS_OK = 0,
+    GS_ERR_BAD_ARG = -1,          /* invalid argument or state */
+    GS_ERR_OOM = -2,              /* device or pinned-host allocation failed */
+    GS_ERR_CUDA = -3,             /* a CUDA runtime call failed */
+    GS_ERR_DEVICE_TIMEOUT = -4,   /* a bounded device-side wait ran out (gs_stats.error_flags) */
+    GS_ERR_NO_SCENE = -5,         /* render before upload */
+    GS_ERR_BUDGET_REFUSED = -6,   /* GPS budget resize refused; the old budget is kept */
+    GS_ERR_NO_DEVICE = -7,        /* no usable CUDA device */
+    GS_ERR_TOO_LARGE = -8         /* size beyond a documented limit */
+} gs_status;
+
+/* src/renderer.h:58-64 SplatRenderMode */
+typedef enum gs_render_mode {
+    GS_MODE_ALPHA = 0,            /* AlphaBlendSorted */
+    GS_MODE_STOCHASTIC = 1,       /* StochasticSplats */
+    GS_MODE_GPS = 2               /* GaussianPointSplatting */
+} gs_render_mode;
+
+/* CameraUniforms, byte for byte (src/camera.h:23-38): 40 floats, 160 bytes. */
+typedef struct gs_camera {
+    float view[16];
+    float proj[16];
+    float viewport[2];
+    float orthographic;
+    float persp_focal;
+    float ortho_focal;
+    float clip_y_sign;
+    float clip_z_01;
+    float pad[1];
+} gs_camera;
+
+/* Renderer knobs of the splatting path: the Renderer fields of
+ * src/renderer.h:121-247 that the path reads, with the defaults of
+ * renderer_init (src/renderer.cpp:588-599). */
+typedef struct gs_knobs {
+    int32_t render_mode;                      /* gs_render_mode; default GS_MODE_GPS */
+    int32_t sh_degree;                        /* 0..3; default 3 */
+    float sh_lod_distance;                    /* <= 0 disables; default 0 */
+    uint32_t gps_supersample_factor;          /* 1..4; default 2 */
+    uint32_t stochastic_samples_per_frame;    /* 1..16; default 1 */
+    uint32_t stochastic_taa_current_samples;  /* 1..16; default 4 */
+    int32_t stochastic_accumulation_enabled;  /* default 1 */
+    int32_t stochastic_taa_enabled;           /* default 1 */
+    int32_t black_background;                 /* default 0 (background 0.1) */
+    int32_t splat_diagnostics_enabled;        /* default 0 */
+    int32_t linear_color;                     /* 1: float sample target and linear GPS colour
+                                                 (gsanim 0.3 path); 0: RGBA8 sample target */
+    int32_t write_invisible_records;          /* 1: also write the reference's record for culled
+                                                 Gaussians (debug/parity); default 0 */
+    int32_t reserved[4];
+} gs_knobs;
+
+/* Per-frame statistics (the reference's SplatDiagnostics, src/renderer.h:28-38,
+ * and GPS work statistics, src/renderer.cpp:2038-2055). */
+typedef struct gs_stats {
+    uint32_t gaussian_count;
+    uint32_t visible_count;
+    uint32_t tile_entries;               /* (16x16 tile, splat) pairs of the last frame */
+    uint32_t tile_overflow;              /* entries that did not fit (frame re-rendered by gs_render_host) */
+    uint32_t diagnostics[8];             /* shaders/cull.glsl:296-318 counters, if enabled */
+    uint32_t gps_requested_work_items;
+    uint32_t gps_budget_exhausted;
+    uint32_t gps_max_work_items;
+    uint32_t sample_count;               /* accumulated samples (stochastic / GPS) */
+    uint32_t frame_seed;
+    uint32_t error_flags;                /* device error bits (bounded waits that ran out) */
+    uint32_t kernel_launches;            /* kernels launched by the last gs_render */
+    uint32_t reserved[5];
+} gs_stats;
+
+/* gs_debug_read selectors (reference buffers, src/renderer.cpp:922-1058). */
+typedef enum gs_debug_buffer {
+    GS_DEBUG_IDS = 0,        /* uint32[N] unsorted ids (idx or 0xFFFFFFFF), after cull */
+    GS_DEBUG_KEYS = 1,       /* uint32[N] depth keys (0xFFFFFFFF for culled), after cull */
+    GS_DEBUG_PROJECTED = 2,  /* float[N*16] CullProjectedSplatData */
+    GS_DEBUG_SORTED_IDS = 3, /* uint32[N] ids after the depth sort (culled tail = 0xFFFFFFFF) */
+    GS_DEBUG_SORTED_KEYS = 4,/* uint32[N] keys after the depth sort */
+    GS_DEBUG_ACCUM = 5,      /* float[W*H*4] accumulation image (stochastic / GPS), top row first */
+    GS_DEBUG_SAMPLE = 6,     /* float[W*H*4] last stochastic/GPS sample, top row first */
+    GS_DEBUG_DEPTH = 7       /* float[W*H] last sample's window depth, top row first */
+} gs_debug_buffer;
+
+typedef struct gs_ctx gs_ctx;
+
+/* renderer_init (src/renderer.h:249): create a context on `device`, issuing
+ * work on `stream` (cudaStream_t, may be NULL).  Knobs get the reference
+ * defaults. */
+int gs_create(gs_ctx** out, int device, void* stream);
+
+/* renderer_destroy (src/renderer.h:266). Accepts NULL. */
+void gs_destroy(gs_ctx* ctx);
+
+/* Renderer fields set by the caller (src/main.cpp:341-387). */
+int gs_get_knobs(const gs_ctx* ctx, gs_knobs* out);
+int gs_set_knobs(gs_ctx* ctx, const gs_knobs* knobs);
+int gs_set_mode(gs_ctx* ctx, int render_mode);
+
+/* renderer_upload_gaussians (src/renderer.h:250): copy `count` GpuGaussian
+ * rows (64 floats = 256 bytes each, src/gaussian.h:63-73) from host memory.
+ * The caller keeps ownership of `rows`.  Replaces any previous scene. */
+int gs_upload_rows(gs_ctx* ctx, const float* rows, uint64_t count);
+
+/* As gs_upload_rows, from device memory (stream-ordered copy). */
+int gs_upload_rows_device(gs_ctx* ctx, const float* rows_dev, uint64_t count);
+
+/* renderer_set_gps_work_budget (src/renderer.h:252): replace only the GPS work
+ * buffer; on failure the old budget and buffer are kept
+ * (src/renderer.cpp:1076-1123). */
+int gs_set_gps_budget(gs_ctx* ctx, uint32_t max_work_items);
+
+/* renderer_reset_stochastic_accumulation (src/renderer.h:261). */
+int gs_reset_accumulation(gs_ctx* ctx);
+
+/* renderer_draw_frame (src/renderer.h:265), splatting path only: cull,
+ * (alpha) sort, then composite / stochastic / GPS according to the mode, into
+ * caller-owned device memory `rgba16f_out` (width*height*4 halves, top row
+ * first; width/height = round(cam->viewport)).  `cam` is host memory. */
+int gs_render(gs_ctx* ctx, const gs_camera* cam, void* rgba16f_out);
+
+/* gs_render into host memory: includes the host->device camera copy and the
+ * device->host image copy, and waits for them. */
+int gs_render_host(gs_ctx* ctx, const gs_camera* cam, uint16_t* rgba16f_out_host);
+
+/* Statistics of the last frame (synchronises). */
+int gs_read_stats(gs_ctx* ctx, gs_stats* out);
+
+/* Copy a reference-layout buffer of the last frame to host memory (synchronises). */
+int gs_debug_read(gs_ctx* ctx, int which, void* host_dst, uint64_t bytes);
+
+/* Per-stage device timing.  enable != 0 records CUDA events around each stage
+ * of every following frame on the context's stream and accumulates them;
+ * gs_stage_times reads (and with reset != 0 clears) the totals in ms, one per
+ * stage in the order of gs_stage_names().  Returns the number of stages. */
+int gs_profile_enable(gs_ctx* ctx, int enable);
+int gs_stage_times(gs_ctx* ctx, float* ms_out, uint32_t* launches_out, int max_stages, int reset);
+const char* gs_stage_names(void);   /* comma-separated */
+
+const char* gs_status_str(int status);
+const char* gs_last_error(const gs_ctx* ctx);
+
+/* ---- host helpers (no GPU) ---------------------------------------------- */
+
+/* CameraUniforms of the reference fly camera: camera_get_view_matrix /
+ * camera_get_proj_matrix (src/camera.cpp:137-245) and the uniform setup of
+ * src/main.cpp:1264-1281 (persp_focal = H/2/tan(fov/2), ortho_focal =
+ * H/(2 ortho_size), GL clip conventions unless webgpu != 0). */
+int gs_camera_uniforms(const float position[3], float yaw, float pitch, float fov_y, float near_plane,
+                       float far_plane, int z_up, float ortho_size, float ortho_blend, int width,
+                       int height, int webgpu, gs_camera* out);
+
+/* Load a binary little-endian 3DGS PLY into GpuGaussian rows with the
+ * reference loader's transforms (src/gaussian_loader_ply.cpp:14-228 and
+ * pack_gpu_gaussians, src/gaussian.cpp:53-73).  With rows == NULL returns the
+ * vertex count; otherwise fills min(count, capacity) rows.  < 0 on error. */
+int64_t gs_load_ply(const char* path, float* rows, uint64_t capacity);
+
+/* The same transforms on raw PLY-layout attributes already in memory:
+ * raw is count x 59 floats in the order x y z, f_dc_0..2, f_rest_0..44,
+ * opacity, scale_0..2, rot_0..3 (the 3DGS property order). */
+int gs_pack_raw(const float* raw, uint64_t count, float* rows);
+
+/* ---- stage-level entry points (device pointers, stream-ordered) ---------- */
+
+/* Scratch bytes gs_sort_pairs needs for n pairs. */
+size_t gs_sort_pairs_scratch_bytes(uint32_t n);
+
+/* Stable ascending radix sort of (key, value) pairs on key bits
+ * [begin_bit, end_bit): the order of the reference's 8-bit LSD passes
+ * (shaders/sort.glsl:26-163, driven by src/renderer.cpp:1873-1962).
+ * keys_in/vals_in are left unchanged; results go to keys_out/vals_out.
+ * scratch: device memory of gs_sort_pairs_scratch_bytes(n) bytes. */
+int gs_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                  uint32_t* vals_out, uint32_t n, int begin_bit, int end_bit, void* scratch,
+                  size_t scratch_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GS_API_H */

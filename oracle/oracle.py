@@ -1,0 +1,231 @@
+"""ctypes wrapper around the CPU oracle (liboracle.so) and the reference's own
+CPU code (_ref/libgsref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, always as the checker.  The product package
+(gamesplat_b200) never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+SENTINEL = 0xFFFFFFFF
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+class OcCamera(C.Structure):
+    """Byte-for-byte CameraUniforms (src/camera.h:23-38)."""
+
+    _fields_ = [
+        ("view", C.c_float * 16),
+        ("proj", C.c_float * 16),
+        ("viewport", C.c_float * 2),
+        ("orthographic", C.c_float),
+        ("persp_focal", C.c_float),
+        ("ortho_focal", C.c_float),
+        ("clip_y_sign", C.c_float),
+        ("clip_z_01", C.c_float),
+        ("pad", C.c_float * 1),
+    ]
+
+
+def camera_struct(cam: np.ndarray) -> OcCamera:
+    """40-float CameraUniforms array -> OcCamera."""
+    cam = np.ascontiguousarray(cam, dtype=np.float32)
+    assert cam.shape == (40,)
+    s = OcCamera()
+    C.memmove(C.addressof(s), cam.ctypes.data, 160)
+    return s
+
+
+_lib = None
+_ref = None
+
+
+def build() -> None:
+    """Compile liboracle.so (and _ref/libgsref.so when the reference tree is present)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            build()
+        L = C.CDLL(str(path))
+        L.oc_logf.restype = C.c_float
+        L.oc_logf.argtypes = [C.c_float]
+        L.oc_expf.restype = C.c_float
+        L.oc_expf.argtypes = [C.c_float]
+        L.oc_sincosf.restype = None
+        L.oc_sincosf.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.oc_dilog.restype = C.c_float
+        L.oc_dilog.argtypes = [C.c_float]
+        L.oc_inv_dilog.restype = C.c_float
+        L.oc_inv_dilog.argtypes = [C.c_float]
+        L.oc_cull.restype = None
+        L.oc_cull.argtypes = [_f32p, C.c_uint32, C.POINTER(OcCamera), C.c_int, C.c_float, C.c_int,
+                              _u32p, _u32p, _f32p, C.POINTER(C.c_uint32), _u32p]
+        L.oc_sort_pairs.restype = None
+        L.oc_sort_pairs.argtypes = [_u32p, _u32p, C.c_uint32, _u32p, _u32p]
+        L.oc_quad_rect.restype = C.c_int
+        L.oc_quad_rect.argtypes = [_f32p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                   C.c_int, C.c_int, _i32p]
+        L.oc_composite_alpha.restype = C.c_uint64
+        L.oc_composite_alpha.argtypes = [_u32p, C.c_uint32, _f32p, C.c_int, C.c_int, C.c_float, C.c_float,
+                                         C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, _f32p]
+        L.oc_stochastic_sample.restype = C.c_uint64
+        L.oc_stochastic_sample.argtypes = [_u32p, C.c_uint32, _f32p, C.c_int, C.c_int, C.c_float, C.c_float,
+                                           C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                           _f32p, _f32p]
+        L.oc_gps_frame.restype = None
+        L.oc_gps_frame.argtypes = [_u32p, C.c_uint32, _f32p, C.c_int, C.c_int, C.c_int, C.c_uint32,
+                                   C.c_float, C.c_int, C.c_float, C.c_float, _f32p, _f32p, _u32p]
+        L.oc_accum.restype = None
+        L.oc_accum.argtypes = [_f32p, _f32p, C.c_float, C.c_uint64, _f32p]
+        L.oc_taa.restype = None
+        L.oc_taa.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p,
+                             _f32p, _f32p, C.c_float, C.c_float, _f32p, _f32p]
+        L.oc_halton.restype = C.c_float
+        L.oc_halton.argtypes = [C.c_uint32, C.c_uint32]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return (HERE / "_ref" / "libgsref.so").exists()
+
+
+def ref():
+    """The reference's own CPU code (compiled from the reference sources)."""
+    global _ref
+    if _ref is None:
+        path = HERE / "_ref" / "libgsref.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (needs the reference sources)")
+        R = C.CDLL(str(path))
+        R.ref_load_ply_rows.restype = C.c_uint32
+        R.ref_load_ply_rows.argtypes = [C.c_char_p, C.c_void_p, C.c_uint32]
+        R.ref_cull_sort_ply.restype = C.c_uint32
+        R.ref_cull_sort_ply.argtypes = [C.c_char_p, _f32p, _f32p, C.c_float, _u32p, _f32p, _u32p]
+        R.ref_camera_matrices.restype = None
+        R.ref_camera_matrices.argtypes = [_f32p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                          C.c_int, C.c_float, C.c_float, C.c_float, _f32p, _f32p]
+        _ref = R
+    return _ref
+
+
+# --------------------------------------------------------------------------
+# numpy-level helpers
+# --------------------------------------------------------------------------
+def cull(rows: np.ndarray, cam: np.ndarray, sh_degree: int = 3, sh_lod_distance: float = 0.0,
+         collect_stats: bool = True):
+    rows = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1, 64)
+    n = rows.shape[0]
+    ids = np.empty(n, np.uint32)
+    keys = np.empty(n, np.uint32)
+    proj = np.empty((n, 16), np.float32)
+    vc = C.c_uint32(0)
+    diag = np.zeros(8, np.uint32)
+    cs = camera_struct(cam)
+    lib().oc_cull(rows.reshape(-1), n, C.byref(cs), int(sh_degree), float(sh_lod_distance),
+                  int(bool(collect_stats)), ids, keys, proj.reshape(-1), C.byref(vc), diag)
+    return ids, keys, proj, int(vc.value), diag
+
+
+def sort_pairs(keys: np.ndarray, ids: np.ndarray):
+    keys = np.ascontiguousarray(keys, dtype=np.uint32)
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    ko = np.empty_like(keys)
+    io = np.empty_like(ids)
+    lib().oc_sort_pairs(keys, ids, keys.size, ko, io)
+    return ko, io
+
+
+def composite_alpha(sorted_ids: np.ndarray, projected: np.ndarray, width: int, height: int,
+                    cam: np.ndarray | None = None, bg: float = 0.0, jitter=(0.0, 0.0),
+                    fp16_per_blend: bool = False):
+    vp_w, vp_h, ysign = _vp(cam, width, height)
+    out = np.empty((height, width, 4), np.float32)
+    sorted_ids = np.ascontiguousarray(sorted_ids, dtype=np.uint32)
+    frags = lib().oc_composite_alpha(sorted_ids, sorted_ids.size, np.ascontiguousarray(projected, np.float32).reshape(-1),
+                                     width, height, vp_w, vp_h, ysign, float(bg), float(jitter[0]),
+                                     float(jitter[1]), int(bool(fp16_per_blend)), out.reshape(-1))
+    return out, int(frags)
+
+
+def stochastic_sample(ids: np.ndarray, projected: np.ndarray, width: int, height: int, frame_seed: float,
+                      cam: np.ndarray | None = None, bg: float = 0.0, jitter=(0.0, 0.0), rgba8: bool = True):
+    vp_w, vp_h, ysign = _vp(cam, width, height)
+    out = np.empty((height, width, 4), np.float32)
+    depth = np.empty((height, width), np.float32)
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    kept = lib().oc_stochastic_sample(ids, ids.size, np.ascontiguousarray(projected, np.float32).reshape(-1),
+                                      width, height, vp_w, vp_h, ysign, float(bg), float(jitter[0]),
+                                      float(jitter[1]), float(frame_seed), int(bool(rgba8)),
+                                      out.reshape(-1), depth.reshape(-1))
+    return out, depth, int(kept)
+
+
+def gps_frame(ids: np.ndarray, projected: np.ndarray, width: int, height: int, supersample: int,
+              max_work_items: int, frame_seed: float, clip_z_01: float = 0.0, linear_color: bool = False,
+              bg: float = 0.0):
+    out = np.empty((height, width, 4), np.float32)
+    depth = np.empty((height, width), np.float32)
+    stats = np.zeros(2, np.uint32)
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    lib().oc_gps_frame(ids, ids.size, np.ascontiguousarray(projected, np.float32).reshape(-1), width, height,
+                       int(supersample), int(max_work_items), float(clip_z_01), int(bool(linear_color)),
+                       float(frame_seed), float(bg), out.reshape(-1), depth.reshape(-1), stats)
+    return out, depth, int(stats[0]), int(stats[1])
+
+
+def accum(sample: np.ndarray, history: np.ndarray, n: float):
+    sample = np.ascontiguousarray(sample, np.float32)
+    history = np.ascontiguousarray(history, np.float32)
+    out = np.empty_like(sample)
+    lib().oc_accum(sample.reshape(-1), history.reshape(-1), float(n), sample.size, out.reshape(-1))
+    return out
+
+
+def taa(cur_color, cur_depth, hist_color, hist_xyz, inv_view, prev_view, viewport_ortho, focal_clip,
+        prev_focal_clip, proj_z, history_valid: float, view_changed: float):
+    h, w = cur_depth.shape
+    oc = np.empty((h, w, 4), np.float32)
+    ox = np.empty((h, w, 4), np.float32)
+    f = lambda a: np.ascontiguousarray(a, np.float32).reshape(-1)  # noqa: E731
+    lib().oc_taa(f(cur_color), f(cur_depth), f(hist_color), f(hist_xyz), w, h, f(inv_view), f(prev_view),
+                 f(viewport_ortho), f(focal_clip), f(prev_focal_clip), f(proj_z), float(history_valid),
+                 float(view_changed), oc.reshape(-1), ox.reshape(-1))
+    return oc, ox
+
+
+def quad_rect(projected16: np.ndarray, width: int, height: int, cam=None, jitter=(0.0, 0.0)):
+    vp_w, vp_h, ysign = _vp(cam, width, height)
+    rect = np.zeros(4, np.int32)
+    ok = lib().oc_quad_rect(np.ascontiguousarray(projected16, np.float32), float(jitter[0]), float(jitter[1]),
+                            vp_w, vp_h, ysign, width, height, rect)
+    return bool(ok), rect
+
+
+def _vp(cam, width, height):
+    if cam is None:
+        return float(width), float(height), 1.0
+    cam = np.asarray(cam, np.float32)
+    return float(cam[32]), float(cam[33]), float(cam[37])
+
+
+def to_f16(img: np.ndarray) -> np.ndarray:
+    """Round an FP32 image to RGBA16F (round-to-nearest-even), once."""
+    return img.astype(np.float16)

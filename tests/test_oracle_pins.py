@@ -1,0 +1,164 @@
+"""CPU tests: pin the oracle (and the host helpers of libgs_cuda.so) against
+the reference's own CPU code, through the committed golden fixture
+tests/golden/ref_small.npz (made by tests/golden/make_golden.py from
+src/gaussian.cpp, src/gaussian_loader_ply.cpp and src/camera.cpp) and, where
+the reference sources are present, against oracle/_ref live."""
+from __future__ import annotations
+
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gamesplat_b200 import renderer as R
+from gamesplat_b200 import scene
+from oracle import oracle as O
+
+GOLDEN = Path(__file__).with_name("golden") / "ref_small.npz"
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(GOLDEN)
+
+
+def _cam_from_pose(meta):
+    px, py, pz, yaw, pitch, fov, w, h, zup, ob = meta
+    return R.camera_uniforms((px, py, pz), yaw, pitch, int(w), int(h), fov_y=fov, z_up=bool(zup),
+                             ortho_blend=ob)
+
+
+def test_pack_raw_matches_reference_loader(golden):
+    rows = R.pack_raw(golden["raw"])
+    assert np.array_equal(rows.view(np.uint32), golden["rows"].view(np.uint32))
+
+
+def test_ply_loader_matches_reference_loader(golden, tmp_path):
+    ply = tmp_path / "g.ply"
+    scene.write_ply(str(ply), golden["raw"])
+    rows = R.load_ply(str(ply))
+    assert np.array_equal(rows.view(np.uint32), golden["rows"].view(np.uint32))
+
+
+def test_camera_uniforms_match_reference_camera(golden):
+    for k, meta in enumerate(golden["poses"]):
+        cam = _cam_from_pose(meta)
+        assert np.array_equal(cam[:16].view(np.uint32), golden["view"][k].view(np.uint32)), k
+        assert np.array_equal(cam[16:32].view(np.uint32), golden["proj"][k].view(np.uint32)), k
+        w, h = meta[6], meta[7]
+        assert cam[32] == w and cam[33] == h
+        # persp_focal = H/2/tan(fov/2) (src/main.cpp:1272)
+        assert cam[35] == np.float32((np.float32(1.0) / np.tan(np.float32(meta[5]) * np.float32(0.5))) * np.float32(h) * np.float32(0.5))
+        assert cam[37] == 1.0 and cam[38] == 0.0
+
+
+def test_oracle_cull_matches_reference_cull(golden):
+    """Visible set and depth keys of oracle cull == reference cull_gaussians."""
+    for k, meta in enumerate(golden["poses"]):
+        cam = _cam_from_pose(meta)
+        ids, keys, proj, vc, diag = O.cull(golden["rows"], cam)
+        vis = np.nonzero(ids != O.SENTINEL)[0].astype(np.uint32)
+        assert vc == vis.size
+        assert np.array_equal(vis, golden[f"visible_{k}"]), k
+        ref_keys = (np.uint32(0xFFFFFFFF) - golden[f"depths_{k}"].view(np.uint32)).astype(np.uint32)
+        assert np.array_equal(keys[vis], ref_keys), k
+        # culled entries keep the cull_reset sentinels (shaders/cull.glsl:469-472)
+        assert np.all(keys[ids == O.SENTINEL] == O.SENTINEL)
+
+
+def test_oracle_sort_matches_reference_sort_modulo_ties(golden):
+    """oracle sort == reference sort_gaussians reversed, except that the
+    reference CPU sort orders equal keys by descending index while the GPU
+    shader sort keeps ascending index (stable)."""
+    for k, meta in enumerate(golden["poses"]):
+        cam = _cam_from_pose(meta)
+        ids, keys, proj, vc, diag = O.cull(golden["rows"], cam)
+        ks, si = O.sort_pairs(keys, ids)
+        si = si[:vc]
+        ref_back_to_front = golden[f"sorted_{k}"]
+        assert ref_back_to_front.size == vc
+        # same multiset per key group, and keys ascending = depth descending
+        assert np.all(np.diff(ks[:vc].astype(np.int64)) >= 0)
+        ref_keys = keys[ref_back_to_front]
+        assert np.array_equal(np.sort(ref_keys), ks[:vc])
+        # identical ordering when ties are broken the same way
+        order = np.lexsort((ref_back_to_front, ref_keys))
+        assert np.array_equal(ref_back_to_front[order], si)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference sources not present")
+def test_oracle_cull_sort_live_reference_config0(tmp_path):
+    raw = scene.small_scene(0, 100_000)
+    ply = tmp_path / "s.ply"
+    scene.write_ply(str(ply), raw)
+    rows = R.load_ply(str(ply))
+    pos, yaw, pitch = scene.small_camera_pose()
+    cam = R.camera_uniforms(pos, yaw, pitch, 1280, 720)
+    ids, keys, proj, vc, diag = O.cull(rows, cam)
+    n = rows.shape[0]
+    vis = np.empty(n, np.uint32)
+    dep = np.empty(n, np.float32)
+    srt = np.empty(n, np.uint32)
+    rvc = O.ref().ref_cull_sort_ply(str(ply).encode(), cam[:16].copy(), cam[16:32].copy(), 0.0, vis, dep, srt)
+    assert rvc == vc
+    mask = ids != O.SENTINEL
+    assert np.array_equal(np.nonzero(mask)[0].astype(np.uint32), vis[:rvc])
+    assert np.array_equal(keys[mask], (np.uint32(0xFFFFFFFF) - dep[:rvc].view(np.uint32)).astype(np.uint32))
+
+
+def test_oracle_sort_is_stable_radix():
+    rng = np.random.default_rng(3)
+    keys = rng.integers(0, 1 << 12, size=5000, dtype=np.uint32) * np.uint32(0x10001)
+    ids = np.arange(5000, dtype=np.uint32)
+    ks, si = O.sort_pairs(keys, ids)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(si, ids[order]) and np.array_equal(ks, keys[order])
+
+
+def _ulps(a, b):
+    a = np.asarray(a, np.float32).view(np.int32).astype(np.int64)
+    b = np.asarray(b, np.float32).view(np.int32).astype(np.int64)
+    return np.abs(a - b)
+
+
+def test_deterministic_log_exp_sincos_error_bounds():
+    L = O.lib()
+    rng = np.random.default_rng(0)
+    xs = np.concatenate([rng.uniform(1e-6, 50, 4000), np.exp(rng.uniform(-80, 80, 4000)), [1.0, 0.5, 2.0]])
+    xs = xs.astype(np.float32)
+    got = np.array([L.oc_logf(float(x)) for x in xs], np.float32)
+    ref = np.log(xs.astype(np.float64)).astype(np.float32)
+    assert _ulps(got, ref).max() <= 2
+    ys = rng.uniform(-80, 80, 4000).astype(np.float32)
+    got = np.array([L.oc_expf(float(y)) for y in ys], np.float32)
+    ref = np.exp(ys.astype(np.float64)).astype(np.float32)
+    assert _ulps(got, ref).max() <= 2
+    zs = rng.uniform(0, 2 * math.pi, 4000).astype(np.float32)
+    import ctypes as C
+
+    s = C.c_float()
+    c = C.c_float()
+    gs_, gc = [], []
+    for z in zs:
+        L.oc_sincosf(float(z), C.byref(s), C.byref(c))
+        gs_.append(s.value)
+        gc.append(c.value)
+    assert np.abs(np.array(gs_) - np.sin(zs.astype(np.float64))).max() < 2e-7
+    assert np.abs(np.array(gc) - np.cos(zs.astype(np.float64))).max() < 2e-7
+    assert L.oc_logf(0.0) == -math.inf and L.oc_expf(-200.0) == 0.0
+
+
+def test_composite_fp16_rounding_gap_is_small():
+    """Report-mode check: FP32 blending (round once) vs per-blend fp16
+    rounding on the small workload differ by a bounded amount."""
+    raw = scene.small_scene(0, 20_000)
+    rows = R.pack_raw(raw)
+    cam = R.camera_uniforms(*scene.small_camera_pose(), 320, 180)
+    ids, keys, proj, vc, _ = O.cull(rows, cam)
+    _, si = O.sort_pairs(keys, ids)
+    a, fa = O.composite_alpha(si, proj, 320, 180, cam)
+    b, fb = O.composite_alpha(si, proj, 320, 180, cam, fp16_per_blend=True)
+    assert fa == fb > 0
+    gap = np.abs(a.astype(np.float16).astype(np.float32) - b).max()
+    assert gap < 0.05
