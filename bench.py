@@ -1,0 +1,355 @@
+"""Benchmark of the per-frame splatting path on B200.
+
+Workload (the one the headline metric is quoted on): 3M SH3 Gaussians
+("room3m": 256 clusters + 6 room planes, seed 1), 1920x1080, 120-frame orbit
+at radius 6 m, sorted-alpha mode, RGBA16F output.  One step = one frame of
+the orbit (cull/SH/project -> depth sort -> bin -> tile sort -> raster).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Timing: W untimed frames, then K frames between CUDA events on the render
+stream, barrier + synchronize on both sides, max over ranks.  The scene rows
+(768 MB) are larger than L2, so no L2 flush is inserted.  Multi-GPU runs are
+replicas (each rank renders its own orbit frames; no collective on the data
+path), value = total frames / max time.  `e2e` re-times K frames through
+gs_render_host (camera host->device, image device->host each frame).
+The reference arm (--impl reference) times the CPU oracle port of the same
+frame on all host cores (the reference's own CPU code covers only cull +
+sort; its cull+sort timing is reported beside it).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "1080p fps at 3M splats: sorted-alpha vs denoised stochastic @PSNR≥40dB"
+WIDTH, HEIGHT, FRAMES = 1920, 1080, 120
+WORKLOAD = "room3m_sh3_1080p_orbit120_sorted_alpha"
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def orbit_cameras(width=WIDTH, height=HEIGHT):
+    from gamesplat_b200 import renderer as R
+    from gamesplat_b200 import scene
+
+    return [R.camera_uniforms(*scene.orbit_pose(k, FRAMES), width, height) for k in range(FRAMES)]
+
+
+def make_rows(n=3_000_000):
+    from gamesplat_b200 import renderer as R
+    from gamesplat_b200 import scene
+
+    raw = scene.room_scene(1, n)
+    rows = R.pack_raw(raw)
+    del raw
+    return rows
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def cpu_frame(rows, cam, threads=None):
+    """One oracle frame (cull + sort + composite) on the host; seconds."""
+    from oracle import oracle as O
+
+    t = time.perf_counter()
+    ids, keys, proj, vc, _ = O.cull(rows, cam, collect_stats=False)
+    _, si = O.sort_pairs(keys, ids)
+    O.composite_alpha(si, proj, WIDTH, HEIGHT, cam, bg=0.0)
+    return time.perf_counter() - t
+
+
+def cpu_reference_cull_sort(rows_path, cam):
+    """The reference's own CPU cull_gaussians + sort_gaussians (single thread)."""
+    from oracle import oracle as O
+
+    n = 3_000_000
+    vis = np.empty(n, np.uint32)
+    dep = np.empty(n, np.float32)
+    srt = np.empty(n, np.uint32)
+    t = time.perf_counter()
+    O.ref().ref_cull_sort_ply(str(rows_path).encode(), cam[:16].copy(), cam[16:32].copy(), 0.0, vis, dep, srt)
+    return time.perf_counter() - t
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args.gpus)
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    rows = make_rows()
+    cams = orbit_cameras()
+    for i in range(args.warmup):
+        cpu_frame(rows, cams[i % FRAMES])
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        cpu_frame(rows, cams[(args.warmup + i) % FRAMES])
+    dt = time.perf_counter() - t0
+    fps = args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded room3m scene, orbit cameras)",
+        "config": {"workload": WORKLOAD, "gaussians": 3_000_000, "width": WIDTH, "height": HEIGHT,
+                   "l2": "inputs larger than L2 (768 MB of rows)"},
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full frames of the orbit, oracle cull+SH+sort+composite, "
+                                   f"OpenMP on {cores} threads"},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from gamesplat_b200 import Renderer
+
+    rows = make_rows(args.gaussians)
+    n = rows.shape[0]
+    cams = orbit_cameras()
+    stream = torch.cuda.Stream()
+    r = Renderer(local, stream=stream.cuda_stream)
+    r.set(splat_render_mode="alpha", black_background=1)
+    r.upload_gaussians(rows)
+    out = torch.empty(WIDTH * HEIGHT * 4, dtype=torch.float16, device="cuda")
+
+    def frame(i):
+        return cams[(rank + i * world) % FRAMES]
+
+    # untimed warm-up (also sizes the tile-entry buffers via the host path)
+    r.draw_frame(frame(0))
+    for i in range(args.warmup):
+        r.draw_frame(frame(i), out_ptr=out.data_ptr())
+    stream.synchronize()
+    r.profile(True)
+    r.stage_times(reset=True)
+    launches_per_frame = r.stats().kernel_launches
+    sampler = ClockSampler(local) if rank == 0 else None
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    vis_sum = 0
+    for i in range(args.steps):
+        r.draw_frame(frame(args.warmup + i), out_ptr=out.data_ptr())
+    ev1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    ms = ev0.elapsed_time(ev1)
+    stages = r.stage_times(reset=True)
+    stats = r.stats()
+    r.profile(False)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if pg:
+        pg.all_reduce(ms_t, op=pg.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    fps = world * args.steps / (ms_max / 1000.0)
+
+    # visible count / entries averaged over the orbit for the roofline units
+    vis_counts = []
+    for i in range(min(args.steps, 8)):
+        r.draw_frame(frame(args.warmup + i), out_ptr=out.data_ptr())
+        vis_counts.append(r.stats().visible_count)
+    n_vis = float(np.mean(vis_counts))
+
+    # e2e through the public API with host buffers (gs_render_host)
+    e2e_fps = None
+    if not args.no_e2e:
+        host_img = np.empty((HEIGHT, WIDTH, 4), np.float16)
+        from gamesplat_b200 import _lib as L
+        from gamesplat_b200.renderer import camera_from_array
+        import ctypes as C
+
+        camsC = [camera_from_array(c) for c in cams]
+        for i in range(2):
+            L.lib().gs_render_host(r._ctx, C.byref(camsC[i]), host_img.ctypes.data)
+        barrier()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            st = L.lib().gs_render_host(r._ctx, C.byref(camsC[(rank + (args.warmup + i) * world) % FRAMES]),
+                                        host_img.ctypes.data)
+            L.check(st, "gs_render_host", r._ctx)
+        dt = time.perf_counter() - t0
+        dt_t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        if pg:
+            pg.all_reduce(dt_t, op=pg.ReduceOp.MAX)
+        e2e_fps = world * args.steps / float(dt_t.item())
+
+    r.destroy()
+    if pg:
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+
+    hbm_peak, tflops_peak, peak_src = load_peaks()
+    # dominant stage and its roofline (per launch = per frame)
+    per_frame = {k: v[0] / args.steps for k, v in stages.items() if v[0] > 0}
+    dominant = max(per_frame, key=per_frame.get)
+    # algorithmic bytes per frame (per-unit figures of the scope table):
+    #   cull: 16 N + 272 N_vis + 8 N; sort: 68 N_vis (compacted sort length)
+    alg = {
+        "cull": 16.0 * n + 272.0 * n_vis + 8.0 * n,
+        "sort": 68.0 * n_vis,
+    }
+    roof_stage = dominant if dominant in alg else "cull"
+    achieved = alg[roof_stage] / (per_frame[roof_stage] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": roof_stage, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg[roof_stage]}
+    hbm_stages = {}
+    for k in alg:
+        if k in per_frame:
+            a = alg[k] / (per_frame[k] / 1000.0) / 1e9
+            hbm_stages[k] = {"ms": per_frame[k], "achieved_gbs": a, "frac": a / hbm_peak}
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        cores = os.cpu_count() or 1
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+        t = cpu_frame(rows, cams[0])
+        cpu = {"value": 1.0 / t, "unit": "frames/s", "cores": cores, "kind": "port",
+               "sample": f"1 full frame (orbit frame 0), oracle cull+SH+sort+composite on {cores} threads"}
+
+    line = {
+        "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded room3m scene: 3M SH3 Gaussians, 120-frame orbit cameras)",
+        "config": {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT, "mode": "alpha",
+                   "output": "RGBA16F", "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (768 MB of rows), no flush"},
+        "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": 160,
+                "d2h_bytes_per_step": WIDTH * HEIGHT * 8},
+        "gpu_launches": int(launches_per_frame) * args.steps,
+        "roofline": roofline,
+        "stages_ms_per_frame": per_frame,
+        "hbm_stages": hbm_stages,
+        "visible_per_frame": n_vis,
+        "tile_entries_last_frame": int(stats.tile_entries),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gaussians", type=int, default=3_000_000,
+                    help="scene size (the benchmark workload is 3M; smaller only for profiling captures)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -2,8 +2,11 @@
 // shader and fixed-function blender (shaders/splat.glsl:39-145,
 // src/renderer.cpp:266-320, 1687-1720).
 //
-// One CTA per 16x16 pixel tile, one pixel per thread (GL window coordinates,
-// row 0 at the bottom; the image is written top row first).  The tile's
+// One CTA per 16x16 pixel tile, one pixel per thread, each warp an 8x4 pixel
+// block (GL window coordinates, row 0 at the bottom; the image is written
+// top row first).  Control flow is warp-uniform: lanes never diverge around
+// the per-splat loop (per-pixel work is predicated), a warp skips splats whose
+// rectangle misses its block and leaves the loop when all its pixels are done.  The tile's
 // depth-ordered splat list is walked front to back (reverse of the
 // reference's back-to-front draw order, so equal depth keys are visited in
 // descending splat index, which reproduces "later instance on top").
@@ -63,10 +66,13 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     __shared__ __align__(128) RasterRecord s_rec[2][kBatch];
     __shared__ __align__(8) uint64_t s_bar[2];
 
+    // Each warp owns an 8x4 pixel block of the 16x16 tile (2 x 4 blocks), so
+    // a warp-uniform rectangle test can skip splats that miss its block.
     const uint32_t tile = blockIdx.x;
     const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
-    const int px = tx * kTileW + (int)(threadIdx.x % kTileW);
-    const int py = ty * kTileH + (int)(threadIdx.x / kTileW);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bx0 = tx * kTileW + (warp & 1) * 8, by0 = ty * kTileH + (warp >> 1) * 4;
+    const int px = bx0 + (lane & 7), py = by0 + (lane >> 3);
     const bool inside = px < p.width && py < p.height;
     const uint2 range = p.tile_ranges[tile];
     const uint32_t n = range.y > range.x ? range.y - range.x : 0u;
@@ -106,44 +112,57 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         if (b & 1) phase1 ^= 1u; else phase0 ^= 1u;
         const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
         const RasterRecord* recs = s_rec[b & 1];
-        if (!done && !failed) {
-            for (uint32_t j = 0; j < cnt; ++j) {
-                const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
-                const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
-                const uint4 q2 = reinterpret_cast<const uint4*>(recs + j)[2];
-                if (kMode == 1 && S.best_id != 0xFFFFFFFFu) {
-                    const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
-                    if (q3.x > S.best_d24 + kDepthMargin) { done = true; break; }
-                }
-                const uint32_t i0 = q2.z & 0xFFFFu, i1 = q2.z >> 16, j0 = q2.w & 0xFFFFu, j1 = q2.w >> 16;
-                if ((uint32_t)(px - (int)i0) >= i1 - i0 || (uint32_t)(py - (int)j0) >= j1 - j0) continue;
-                const float dx = sub(fcx, q0.x), dy = sub(fcy, q0.y);
-                const float power = splat_power(dx, dy, q0.z, q0.w, q1.x);
-                if (!(power <= 0.0f) || power < q1.z) continue;
-                if (kMode == 0) {
+        // Warp-uniform control flow only: every lane walks the same records;
+        // per-pixel work is predicated on `live`.
+        bool warp_done = __all_sync(0xffffffffu, done || failed);
+        for (uint32_t j = 0; j < cnt && !warp_done; ++j) {
+            const uint4 q2 = reinterpret_cast<const uint4*>(recs + j)[2];
+            const int i0 = (int)(q2.z & 0xFFFFu), i1 = (int)(q2.z >> 16);
+            const int j0 = (int)(q2.w & 0xFFFFu), j1 = (int)(q2.w >> 16);
+            // warp block [bx0, bx0+8) x [by0, by0+4) vs splat rect (uniform)
+            if (i1 <= bx0 || i0 >= bx0 + 8 || j1 <= by0 || j0 >= by0 + 4) continue;
+            const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
+            const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
+            if (kMode == 1) {
+                const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
+                // stop once this splat is beyond every lane's kept depth
+                const bool beyond = done || (S.best_id != 0xFFFFFFFFu && q3.x > S.best_d24 + kDepthMargin);
+                if (S.best_id != 0xFFFFFFFFu && q3.x > S.best_d24 + kDepthMargin) done = true;
+                if (__all_sync(0xffffffffu, beyond)) { warp_done = true; break; }
+            }
+            const bool in_rect = px >= i0 && px < i1 && py >= j0 && py < j1;
+            const float dx = sub(fcx, q0.x), dy = sub(fcy, q0.y);
+            const float power = splat_power(dx, dy, q0.z, q0.w, q1.x);
+            const bool live = !done && !failed && in_rect && (power <= 0.0f) && !(power < q1.z);
+            if (kMode == 0) {
+                if (live) {
                     const float alpha = fminf(q1.y * __expf(power), 0.99f);
                     const float w = alpha * A.T;
                     A.c0 = fmaf(w, q1.w, A.c0);
                     A.c1 = fmaf(w, __uint_as_float(q2.x), A.c1);
                     A.c2 = fmaf(w, __uint_as_float(q2.y), A.c2);
                     A.T = A.T * (1.0f - alpha);
-                    if (A.T < kTransmittanceMin) { done = true; break; }
-                } else {
-                    const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
-                    const uint32_t z24 = q3.x, id = q3.y;
-                    if (!(z24 < S.best_d24 || (z24 == S.best_d24 && id < S.best_id))) continue;
+                    done = A.T < kTransmittanceMin;
+                }
+                if (__all_sync(0xffffffffu, done || failed)) { warp_done = true; break; }
+            } else {
+                const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
+                const uint32_t z24 = q3.x, id = q3.y;
+                const bool better = z24 < S.best_d24 || (z24 == S.best_d24 && id < S.best_id);
+                if (live && better) {
                     const float alpha = g_min(mul(q1.y, det_expf(power)), 0.99f);
                     const float rnd = hash13(fcx, fcy, __uint_as_float(q3.z));
-                    if (rnd >= alpha) continue;
-                    S.best_d24 = z24;
-                    S.best_id = id;
-                    S.r = q1.w;
-                    S.g = __uint_as_float(q2.x);
-                    S.b = __uint_as_float(q2.y);
+                    if (rnd < alpha) {
+                        S.best_d24 = z24;
+                        S.best_id = id;
+                        S.r = q1.w;
+                        S.g = __uint_as_float(q2.x);
+                        S.b = __uint_as_float(q2.y);
+                    }
                 }
             }
         }
-        const int all_done = __syncthreads_and(done || failed);
+        const int all_done = __syncthreads_and(warp_done || done || failed);
         if (all_done) {
             if (b + 1 < nb) {
                 const uint32_t ph2 = ((b + 1) & 1) ? phase1 : phase0;
