@@ -210,6 +210,20 @@ int gs_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* ke
                   uint32_t* vals_out, uint32_t n, int begin_bit, int end_bit, void* scratch,
                   size_t scratch_bytes, void* stream);
 
+/* gs_sort_pairs without any allocation; no counterpart in the reference.
+ * For callers that cannot allocate device memory through this library: a
+ * real-time render loop where cudaMalloc/cudaFree would synchronise the device
+ * mid-frame, or a host engine whose memory manager owns every device
+ * allocation.  The caller passes inputs and outputs; the scratch is a fixed
+ * array of about 10 MiB in the library's device memory, held on every GPU that
+ * loads the library until exit, so n is limited to 1,048,576 pairs
+ * (GS_ERR_TOO_LARGE beyond).  The first call on a device, with that device
+ * current, looks up the array's device address; make it before any stream
+ * capture.  Every call shares the array (each clears what must start at zero);
+ * calls that overlap on the GPU race, so serialise them. */
+int gs_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                          uint32_t* vals_out, uint32_t n, int begin_bit, int end_bit, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
