@@ -223,6 +223,14 @@ __device__ __forceinline__ u64 ld_acquire64(const u64* p) {
     asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
+// Look-backs only read the status words themselves (no data published with
+// them), so relaxed GPU-scope loads of the atomically written 64-bit words
+// suffice and several can be in flight at once.
+__device__ __forceinline__ u64 ld_relaxed64(const u64* p) {
+    u64 v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ u64 status_word(uint32_t epoch, uint32_t flag, uint32_t value) {
     return ((u64)epoch << 32) | (u64)(flag | (value & kValMask));
 }
@@ -247,6 +255,76 @@ __device__ __forceinline__ uint32_t lookback(const u64* status, uint32_t stride,
         excl += lo & kValMask;
         if (flag == kFlagInc) break;
         --j;
+    }
+    return excl;
+}
+
+// Single-thread look-back that reads 8 predecessor words per step
+// (independent loads), then consumes them nearest first until an inclusive
+// prefix; an unpublished word is re-polled (bounded) before continuing.
+__device__ __forceinline__ uint32_t lookback_vec(const u64* status, size_t stride, uint32_t tile, uint32_t epoch,
+                                                 bool* timed_out) {
+    uint32_t excl = 0;
+    long long j = (long long)tile - 1;
+    uint32_t spins = 0;
+    while (j >= 0) {
+        u64 w[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            w[k] = (j - k >= 0) ? ld_relaxed64(status + (size_t)(j - k) * stride) : status_word(epoch, kFlagInc, 0);
+        int k = 0;
+        bool found = false;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (k != q || found) continue;
+            const uint32_t lo = (uint32_t)w[q];
+            const uint32_t flag = lo & ~kValMask;
+            if ((uint32_t)(w[q] >> 32) != epoch || flag == 0u) continue;  // not published yet
+            excl += lo & kValMask;
+            ++k;
+            if (flag == kFlagInc) found = true;
+        }
+        if (found) return excl;
+        j -= k;
+        if (k < 8) {  // word j is not published yet: wait for it
+            if (++spins > kSpinLimit) { *timed_out = true; return excl; }
+            if (spins > 64) __nanosleep(32);
+        }
+    }
+    return excl;
+}
+
+// Warp-cooperative look-back: all 32 lanes read a window of 32 predecessors
+// at once, the nearest inclusive word is found by ballot and the aggregates
+// after it are summed with a warp reduction.  Every lane returns the same
+// exclusive prefix.  Bounded like lookback().
+__device__ __forceinline__ uint32_t lookback_warp(const u64* status, uint32_t tile, uint32_t epoch,
+                                                  bool* timed_out) {
+    const int lane = threadIdx.x & 31;
+    uint32_t excl = 0;
+    long long end = (long long)tile;  // window = [end - 32, end)
+    uint32_t spins = 0;
+    while (end > 0) {
+        const long long j = end - 32 + lane;
+        uint32_t flag = kFlagInc, val = 0;   // before tile 0: an inclusive zero
+        if (j >= 0) {
+            for (;;) {
+                const u64 w = ld_relaxed64(status + j);
+                flag = (uint32_t)w & ~kValMask;
+                val = (uint32_t)w & kValMask;
+                if ((uint32_t)(w >> 32) == epoch && flag != 0u) break;
+                if (++spins > kSpinLimit) { *timed_out = true; flag = kFlagInc; val = 0; break; }
+                if (spins > 64) __nanosleep(32);
+            }
+        }
+        const uint32_t inc = __ballot_sync(0xffffffffu, flag == kFlagInc);
+        if (inc) {
+            const int h = 31 - __clz(inc);   // nearest inclusive in the window
+            excl += __reduce_add_sync(0xffffffffu, lane >= h ? val : 0u);
+            break;
+        }
+        excl += __reduce_add_sync(0xffffffffu, val);
+        end -= 32;
     }
     return excl;
 }

@@ -16,6 +16,8 @@
 //     all-equal (0xFFFFFFFF, 0xFFFFFFFF) pairs, so the result is identical).
 // Arithmetic follows the GLSL operand order with unfused intrinsics so the
 // keys, cull mask and projected records match the CPU oracle bit for bit.
+#include <algorithm>
+
 #include "gs_common.cuh"
 #include "gs_internal.h"
 
@@ -23,8 +25,7 @@ namespace gs {
 
 constexpr int kStageStride = 17;  // float4 per staged row (16 + 1 pad)
 constexpr int kCullWarps = kCullThreads / 32;
-constexpr size_t kCullSmem = (size_t)kCullWarps * 32 * kStageStride * sizeof(float4) +
-                             2 * (size_t)kCullTile * sizeof(uint32_t);
+constexpr size_t kCullSmem = (size_t)kCullWarps * 2 * 32 * kStageStride * sizeof(float4);  // double-buffered
 
 struct CamRegs {
     float V[16];
@@ -203,164 +204,199 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
     out[3] = make_float4(a, mul(b, cam.ysign), c, det);
 }
 
-__global__ void __launch_bounds__(kCullThreads, 2) cull_kernel(CullParams p, int nchunks) {
-    extern __shared__ float4 smem4[];
-    float4* stage = smem4;
-    uint32_t* s_keys = reinterpret_cast<uint32_t*>(stage + kCullWarps * 32 * kStageStride);
-    uint32_t* s_ids = s_keys + kCullTile;
-    __shared__ int vis_list[kCullWarps][32];
-    __shared__ uint32_t seg_count[kCullRounds * kCullWarps];
-    __shared__ uint32_t seg_off[kCullRounds * kCullWarps];
-    __shared__ uint32_t s_tile, s_excl, s_total;
-    static_assert(kCullRounds * kCullWarps == 32, "one warp scans the segments");
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int kPending>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(kPending) : "memory");
+}
 
+// Issue the async copies of chunks 1..kChunks-1 of the visible rows of one
+// 32-row round into `stage` (consecutive lanes -> consecutive 16-B chunks).
+template <int kChunks>
+__device__ __forceinline__ void stage_round(const float4* rows, uint32_t wbase, uint32_t mask, const uint8_t* list,
+                                            float4* stage, int lane) {
+    constexpr int per = kChunks - 1;
+    const int total = __popc(mask) * per;
+    for (int u = lane; u < total; u += 32) {
+        const int v = u / per;
+        const int ch = 1 + (u - v * per);
+        const int rl = list[v];
+        cp_async16(&stage[rl * kStageStride + ch], rows + (size_t)(wbase + rl) * 16 + ch);
+    }
+}
+
+// Every warp is independent: it takes 128-Gaussian warp tiles in ticket
+// order, stages round r+1's visible rows while it projects round r, and
+// places its visible (key, id) pairs with a warp-level decoupled look-back.
+template <int kChunks>  // 16-byte chunks of a row the SH degree needs: 4, 7, 10 or 16
+__global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
+    extern __shared__ float4 smem4[];
+    __shared__ uint8_t vis_list[kCullWarps][kCullRounds][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float4* stage0 = smem4 + (size_t)warp * 2 * 32 * kStageStride;
+    float4* stage1 = stage0 + 32 * kStageStride;
     const uint32_t num_tiles = (p.n + kCullTile - 1) / kCullTile;
     CamRegs cam;
     load_cam(p.cam, cam);
-    float4* warp_stage = stage + warp * 32 * kStageStride;
-    float4* my_stage = warp_stage + lane * kStageStride;
+    const uint32_t lt = (1u << lane) - 1u;
 
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&p.fc->cull_ticket, 1u);
-        __syncthreads();
-        const uint32_t tile = s_tile;
+        uint32_t tile = 0;
+        if (lane == 0) tile = atomicAdd(&p.fc->cull_ticket, 1u);
+        tile = __shfl_sync(0xffffffffu, tile, 0);
         if (tile >= num_tiles) break;
         const uint32_t base = tile * kCullTile;
 
-        for (int round = 0; round < kCullRounds; ++round) {
-            const uint32_t wbase = base + round * kCullThreads + warp * 32;
-            const uint32_t g = wbase + lane;
-            const bool valid = g < p.n;
-            float4 c0 = valid ? __ldg(p.rows + (size_t)g * 16) : make_float4(0.f, 0.f, 0.f, 0.f);
-            // p_view = view * vec4(position, 1.0)
-            float vx = add(add(add(mul(cam.V[0], c0.x), mul(cam.V[4], c0.y)), mul(cam.V[8], c0.z)), cam.V[12]);
-            float vy = add(add(add(mul(cam.V[1], c0.x), mul(cam.V[5], c0.y)), mul(cam.V[9], c0.z)), cam.V[13]);
-            float vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
-            bool visible = valid && (vz <= -0.2f);
+        float4 c0[kCullRounds];
+#pragma unroll
+        for (int r = 0; r < kCullRounds; ++r) {
+            const uint32_t g = base + r * 32 + lane;
+            c0[r] = g < p.n ? __ldg(p.rows + (size_t)g * 16) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        float vx[kCullRounds], vy[kCullRounds], vz[kCullRounds];
+        uint32_t mask[kCullRounds];
+#pragma unroll
+        for (int r = 0; r < kCullRounds; ++r) {
+            const uint32_t g = base + r * 32 + lane;
+            // p_view = view * vec4(position, 1.0)  (shaders/cull.glsl:209-220)
+            vx[r] = add(add(add(mul(cam.V[0], c0[r].x), mul(cam.V[4], c0[r].y)), mul(cam.V[8], c0[r].z)), cam.V[12]);
+            vy[r] = add(add(add(mul(cam.V[1], c0[r].x), mul(cam.V[5], c0[r].y)), mul(cam.V[9], c0[r].z)), cam.V[13]);
+            vz[r] = add(add(add(mul(cam.V[2], c0[r].x), mul(cam.V[6], c0[r].y)), mul(cam.V[10], c0[r].z)), cam.V[14]);
+            bool visible = g < p.n && (vz[r] <= -0.2f);
             if (visible) {
-                float inv_z = dv(-1.0f, vz);
-                float ndc_x = add(mul(mul(mul(cam.P0, vx), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P0, vx), cam.ortho));
-                float ndc_y = add(mul(mul(mul(cam.P5, vy), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P5, vy), cam.ortho));
+                float inv_z = dv(-1.0f, vz[r]);
+                float ndc_x = add(mul(mul(mul(cam.P0, vx[r]), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P0, vx[r]), cam.ortho));
+                float ndc_y = add(mul(mul(mul(cam.P5, vy[r]), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P5, vy[r]), cam.ortho));
                 visible = fabsf(ndc_x) <= 1.3f && fabsf(ndc_y) <= 1.3f;
             }
-            const uint32_t mask = __ballot_sync(0xffffffffu, visible);
-            const int nvis = __popc(mask);
-            const int pos = __popc(mask & ((1u << lane) - 1u));
-            if (visible) vis_list[warp][pos] = lane;
-            __syncwarp();
-            // Coalesced 128-bit loads of the visible rows' chunks 1..nchunks-1.
-            const int per = nchunks - 1;
-            const int total = nvis * per;
-            for (int u = lane; u < total; u += 32) {
-                int v = u / per;
-                int ch = 1 + (u - v * per);
-                int rl = vis_list[warp][v];
-                warp_stage[rl * kStageStride + ch] = __ldg(p.rows + (size_t)(wbase + rl) * 16 + ch);
+            mask[r] = __ballot_sync(0xffffffffu, visible);
+            if (visible) vis_list[warp][r][__popc(mask[r] & lt)] = (uint8_t)lane;
+        }
+        __syncwarp();
+        stage_round<kChunks>(p.rows, base, mask[0], vis_list[warp][0], stage0, lane);
+        cp_async_commit();
+        // The tile's visible count is known now: publish it before projecting.
+        uint32_t total = 0;
+#pragma unroll
+        for (int r = 0; r < kCullRounds; ++r) total += __popc(mask[r]);
+        if (lane == 0)
+            st_release64(p.status + tile, status_word(p.epoch, tile == 0 ? kFlagInc : kFlagAgg, total));
+
+        uint32_t keys[kCullRounds];
+        uint32_t d0 = 0, d2 = 0, d3 = 0, d4 = 0, d6 = 0, d7 = 0, m1 = 0, m5 = 0;
+#pragma unroll
+        for (int r = 0; r < kCullRounds; ++r) {
+            float4* cur = (r & 1) ? stage1 : stage0;
+            if (r + 1 < kCullRounds) {
+                stage_round<kChunks>(p.rows, base + (r + 1) * 32, mask[r + 1], vis_list[warp][r + 1],
+                                     (r & 1) ? stage0 : stage1, lane);
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
             }
             __syncwarp();
-            float qa = 0.0f, gp = 0.0f;
+            const uint32_t g = base + r * 32 + lane;
+            const bool visible = (mask[r] >> lane) & 1u;
+            keys[r] = 0u;
             if (visible) {
                 float4 rec[4];
-                project_visible(my_stage, c0, vx, vy, vz, cam, p.sh_degree, p.sh_lod_distance, rec, &qa, &gp);
+                float qa, gp;
+                project_visible(cur + lane * kStageStride, c0[r], vx[r], vy[r], vz[r], cam, p.sh_degree,
+                                p.sh_lod_distance, rec, &qa, &gp);
                 float4* dst = p.projected + (size_t)g * 4;
                 dst[0] = rec[0];
                 dst[1] = rec[1];
                 dst[2] = rec[2];
                 dst[3] = rec[3];
-                const int seg = round * kCullWarps + warp;
-                s_keys[seg * 32 + pos] = 0xFFFFFFFFu - __float_as_uint(g_max(-vz, 0.0f));
-                s_ids[seg * 32 + pos] = g;
-            } else if (valid && p.write_invisible) {
+                keys[r] = 0xFFFFFFFFu - __float_as_uint(g_max(-vz[r], 0.0f));
+                if (p.collect_stats) {
+                    // shaders/cull.glsl:296-318
+                    const uint32_t qpx = g_f2u_sat(g_min(g_max(0.0f, qa), 4294967295.0f));
+                    const uint32_t gpx = g_f2u_sat(g_min(ceilf(gp), 4294967295.0f));
+                    d0 += (uint32_t)(qpx + 1023u) >> 10u;
+                    m1 = max(m1, qpx);
+                    d2 += qpx > 1024u;
+                    d3 += qpx > 16384u;
+                    d4 += (uint32_t)(gpx + 1023u) >> 10u;
+                    m5 = max(m5, gpx);
+                    d6 += gpx > 1024u;
+                    d7 += gpx > 16384u;
+                }
+            } else if (g < p.n && p.write_invisible) {
                 float4* dst = p.projected + (size_t)g * 4;
                 dst[0] = make_float4(0.f, 0.f, 0.f, 0.f);
                 dst[1] = make_float4(0.f, 0.f, 0.f, 0.f);
                 dst[2] = make_float4(1.f, 0.f, 1.f, 1.f);
                 dst[3] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            if (p.collect_stats && mask) {
-                // shaders/cull.glsl:296-318, warp-aggregated.
-                uint32_t qpx = visible ? g_f2u_sat(g_min(g_max(0.0f, qa), 4294967295.0f)) : 0u;
-                uint32_t gpx = visible ? g_f2u_sat(g_min(ceilf(gp), 4294967295.0f)) : 0u;
-                uint32_t d0 = visible ? ((uint32_t)(qpx + 1023u) >> 10u) : 0u;
-                uint32_t d4 = visible ? ((uint32_t)(gpx + 1023u) >> 10u) : 0u;
-                uint32_t s0 = __reduce_add_sync(0xffffffffu, d0);
-                uint32_t m1 = __reduce_max_sync(0xffffffffu, qpx);
-                uint32_t s2 = __reduce_add_sync(0xffffffffu, (uint32_t)(visible && qpx > 1024u));
-                uint32_t s3 = __reduce_add_sync(0xffffffffu, (uint32_t)(visible && qpx > 16384u));
-                uint32_t s4 = __reduce_add_sync(0xffffffffu, d4);
-                uint32_t m5 = __reduce_max_sync(0xffffffffu, gpx);
-                uint32_t s6 = __reduce_add_sync(0xffffffffu, (uint32_t)(visible && gpx > 1024u));
-                uint32_t s7 = __reduce_add_sync(0xffffffffu, (uint32_t)(visible && gpx > 16384u));
-                if (lane == 0) {
-                    atomicAdd(&p.fc->diag[0], s0);
-                    atomicMax(&p.fc->diag[1], m1);
-                    atomicAdd(&p.fc->diag[2], s2);
-                    atomicAdd(&p.fc->diag[3], s3);
-                    atomicAdd(&p.fc->diag[4], s4);
-                    atomicMax(&p.fc->diag[5], m5);
-                    atomicAdd(&p.fc->diag[6], s6);
-                    atomicAdd(&p.fc->diag[7], s7);
-                }
-            }
-            if (lane == 0) seg_count[round * kCullWarps + warp] = (uint32_t)nvis;
             __syncwarp();
         }
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t cnt = seg_count[lane];
-            uint32_t x = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            seg_off[lane] = x - cnt;
-            uint32_t total = __shfl_sync(0xffffffffu, x, 31);
+        if (p.collect_stats) {
+            const uint32_t s0 = __reduce_add_sync(0xffffffffu, d0), s2 = __reduce_add_sync(0xffffffffu, d2);
+            const uint32_t s3 = __reduce_add_sync(0xffffffffu, d3), s4 = __reduce_add_sync(0xffffffffu, d4);
+            const uint32_t s6 = __reduce_add_sync(0xffffffffu, d6), s7 = __reduce_add_sync(0xffffffffu, d7);
+            const uint32_t x1 = __reduce_max_sync(0xffffffffu, m1), x5 = __reduce_max_sync(0xffffffffu, m5);
             if (lane == 0) {
-                u64* st = p.status + tile;
-                uint32_t excl = 0;
-                if (tile == 0) {
-                    st_release64(st, status_word(p.epoch, kFlagInc, total));
-                } else {
-                    st_release64(st, status_word(p.epoch, kFlagAgg, total));
-                    bool to = false;
-                    excl = lookback(p.status, 1, tile, p.epoch, &to);
-                    if (to) atomicOr(&p.fc->error_flags, kErrCullLookback);
-                    st_release64(st, status_word(p.epoch, kFlagInc, excl + total));
-                }
-                s_excl = excl;
-                s_total = total;
-                if (tile == num_tiles - 1) p.fc->visible_count = excl + total;
+                if (s0) atomicAdd(&p.fc->diag[0], s0);
+                if (x1) atomicMax(&p.fc->diag[1], x1);
+                if (s2) atomicAdd(&p.fc->diag[2], s2);
+                if (s3) atomicAdd(&p.fc->diag[3], s3);
+                if (s4) atomicAdd(&p.fc->diag[4], s4);
+                if (x5) atomicMax(&p.fc->diag[5], x5);
+                if (s6) atomicAdd(&p.fc->diag[6], s6);
+                if (s7) atomicAdd(&p.fc->diag[7], s7);
             }
         }
-        __syncthreads();
-        const uint32_t excl = s_excl;
-        for (int slot = threadIdx.x; slot < kCullTile; slot += kCullThreads) {
-            int seg = slot >> 5, k = slot & 31;
-            if ((uint32_t)k < seg_count[seg]) {
-                uint32_t o = excl + seg_off[seg] + (uint32_t)k;
-                p.keys_out[o] = s_keys[slot];
-                p.ids_out[o] = s_ids[slot];
+        // Warp-level ordered compaction (decoupled look-back over warp tiles).
+        uint32_t excl = 0;
+        if (tile > 0) {
+            bool to = false;
+            excl = lookback_warp(p.status, tile, p.epoch, &to);
+            if (lane == 0) {
+                if (to) atomicOr(&p.fc->error_flags, kErrCullLookback);
+                st_release64(p.status + tile, status_word(p.epoch, kFlagInc, excl + total));
             }
         }
-        __syncthreads();
+        if (lane == 0 && tile == num_tiles - 1) p.fc->visible_count = excl + total;
+        uint32_t before = 0;
+#pragma unroll
+        for (int r = 0; r < kCullRounds; ++r) {
+            if ((mask[r] >> lane) & 1u) {
+                const uint32_t o = excl + before + __popc(mask[r] & lt);
+                p.keys_out[o] = keys[r];
+                p.ids_out[o] = base + r * 32 + lane;
+            }
+            before += __popc(mask[r]);
+        }
     }
 }
 
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(cull_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         attr_set = true;
     }
-    static const int chunks_for_degree[4] = {4, 7, 10, 16};
     int deg = p.sh_degree < 0 ? 0 : (p.sh_degree > 3 ? 3 : p.sh_degree);
     uint32_t tiles = (p.n + kCullTile - 1) / kCullTile;
-    uint32_t grid = num_sms * 2;
-    if (grid > tiles) grid = tiles;
+    uint32_t warps = num_sms * 3 * kCullWarps;
+    uint32_t grid = (std::min(warps, tiles) + kCullWarps - 1) / kCullWarps;
     if (grid == 0) return 0;
-    cull_kernel<<<grid, kCullThreads, kCullSmem, s>>>(p, chunks_for_degree[deg]);
+    switch (deg) {
+        case 0: cull_kernel<4><<<grid, kCullThreads, kCullSmem, s>>>(p); break;
+        case 1: cull_kernel<7><<<grid, kCullThreads, kCullSmem, s>>>(p); break;
+        case 2: cull_kernel<10><<<grid, kCullThreads, kCullSmem, s>>>(p); break;
+        default: cull_kernel<16><<<grid, kCullThreads, kCullSmem, s>>>(p); break;
+    }
     return 1;
 }
 

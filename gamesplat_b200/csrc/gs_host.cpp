@@ -739,7 +739,7 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
     GS_CUDA(c, dalloc(&c->cull_status, cull_tiles * sizeof(unsigned long long)));
     c->sort_status_stride = gs::sort_status_words(n);
     GS_CUDA(c, dalloc(&c->sort_status, c->sort_status_stride * 4 * sizeof(unsigned long long)));
-    const size_t bin_tiles = ((size_t)n + gs::kBinThreads - 1) / gs::kBinThreads;
+    const size_t bin_tiles = ((size_t)n + gs::kBinTile - 1) / gs::kBinTile;
     GS_CUDA(c, dalloc(&c->bin_status, bin_tiles * sizeof(unsigned long long)));
     GS_CUDA(c, cudaMemsetAsync(c->cull_status, 0, cull_tiles * 8, c->stream));
     GS_CUDA(c, cudaMemsetAsync(c->sort_status, 0, c->sort_status_stride * 4 * 8, c->stream));

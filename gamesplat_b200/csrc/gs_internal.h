@@ -59,13 +59,16 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // keys per CTA tile
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 
-// Cull configuration: 256 threads, 4 rounds of 256 Gaussians per CTA tile.
-constexpr int kCullThreads = 256;
+// Cull configuration: 128-thread CTAs; each warp works alone on 128-Gaussian
+// warp tiles (4 rounds of 32), which are the units of the look-back.
+constexpr int kCullThreads = 128;
 constexpr int kCullRounds = 4;
-constexpr int kCullTile = kCullThreads * kCullRounds;
+constexpr int kCullTile = 32 * kCullRounds;
 
-// Binning configuration.
+// Binning configuration: 4 sorted splats per thread, 1024 per CTA tile.
 constexpr int kBinThreads = 256;
+constexpr int kBinItems = 4;
+constexpr int kBinTile = kBinThreads * kBinItems;
 constexpr int kTileW = 16;
 constexpr int kTileH = 16;
 
@@ -75,8 +78,8 @@ struct __align__(16) RasterRecord {
     float cx, cy, conic_x, conic_2y;     // centre (+jitter), conic.x, 2*conic.y
     float conic_z, opacity, cutoff, r;   // cutoff = log((1/255)/max(opacity,1e-8))
     float g, b;
-    uint32_t rect_x;                     // i0 | i1 << 16  (covered pixel columns)
-    uint32_t rect_y;                     // j0 | j1 << 16  (covered pixel rows, GL order)
+    uint32_t rect_x;                     // i0 | i1 << 16  (candidate pixel columns: quad coverage
+    uint32_t rect_y;                     // j0 | j1 << 16   intersected with the alpha >= 1/255 box, GL rows)
     uint32_t depth24;                    // window depth as D24 (stochastic depth test)
     uint32_t splat_id;                   // original Gaussian index
     float hash_z;                        // float(splat_id) + frame_seed

@@ -2,7 +2,7 @@
 // shader and fixed-function blender (shaders/splat.glsl:39-145,
 // src/renderer.cpp:266-320, 1687-1720).
 //
-// One CTA per 16x16 pixel tile, one pixel per thread, each warp an 8x4 pixel
+// One CTA per 16x16 pixel tile, two pixels per thread, each warp an 8x8 pixel
 // block (GL window coordinates, row 0 at the bottom; the image is written
 // top row first).  Control flow is warp-uniform: lanes never diverge around
 // the per-splat loop (per-pixel work is predicated), a warp skips splats whose
@@ -36,7 +36,7 @@
 
 namespace gs {
 
-constexpr int kRasterThreads = kTileW * kTileH;
+constexpr int kRasterThreads = kTileW * kTileH / 2;   // two pixels per thread
 constexpr int kBatch = 128;
 constexpr float kTransmittanceMin = 1.0f / 8192.0f;
 constexpr uint32_t kDepthMargin = 8;
@@ -61,19 +61,80 @@ struct StochState {
     float r, g, b;
 };
 
+// Per-pixel compositing state and the per-pixel step of each mode.
+__device__ __forceinline__ void alpha_step(AlphaState& A, bool& done, float power, float opacity, float r, float g,
+                                           float b) {
+    const float alpha = fminf(opacity * __expf(power), 0.99f);
+    const float w = alpha * A.T;
+    A.c0 = fmaf(w, r, A.c0);
+    A.c1 = fmaf(w, g, A.c1);
+    A.c2 = fmaf(w, b, A.c2);
+    A.T = A.T * (1.0f - alpha);
+    done = A.T < kTransmittanceMin;
+}
+
+__device__ __forceinline__ void stoch_step(StochState& S, float power, float opacity, float fcx, float fcy,
+                                           float hz, uint32_t z24, uint32_t id, float r, float g, float b) {
+    const float alpha = g_min(mul(opacity, det_expf(power)), 0.99f);
+    const float rnd = hash13(fcx, fcy, hz);
+    if (rnd < alpha) {
+        S.best_d24 = z24;
+        S.best_id = id;
+        S.r = r;
+        S.g = g;
+        S.b = b;
+    }
+}
+
+__device__ __forceinline__ void write_pixel_alpha(const RasterParams& p, int px, int py, const AlphaState& A) {
+    const size_t o = (size_t)(p.height - 1 - py) * p.width + px;
+    const float r = fmaf(A.T, p.bg, A.c0), g = fmaf(A.T, p.bg, A.c1), b = fmaf(A.T, p.bg, A.c2);
+    const float a = 1.0f - A.T;
+    __half2 h01 = __floats2half2_rn(r, g), h23 = __floats2half2_rn(b, a);
+    uint2 packed;
+    packed.x = *reinterpret_cast<uint32_t*>(&h01);
+    packed.y = *reinterpret_cast<uint32_t*>(&h23);
+    reinterpret_cast<uint2*>(p.out_rgba16f)[o] = packed;
+}
+
+__device__ __forceinline__ void write_pixel_stoch(const RasterParams& p, int px, int py, const StochState& S) {
+    const size_t o = (size_t)(p.height - 1 - py) * p.width + px;
+    float4 c;
+    if (S.best_id == 0xFFFFFFFFu) c = make_float4(p.bg, p.bg, p.bg, 0.0f);
+    else c = make_float4(S.r, S.g, S.b, 1.0f);
+    if (p.rgba8) {
+        c.x = rintf(g_clamp(c.x, 0.0f, 1.0f) * 255.0f) / 255.0f;
+        c.y = rintf(g_clamp(c.y, 0.0f, 1.0f) * 255.0f) / 255.0f;
+        c.z = rintf(g_clamp(c.z, 0.0f, 1.0f) * 255.0f) / 255.0f;
+        c.w = rintf(g_clamp(c.w, 0.0f, 1.0f) * 255.0f) / 255.0f;
+    }
+    if (p.out_rgba32f) p.out_rgba32f[o] = c;
+    if (p.out_depth) p.out_depth[o] = (float)S.best_d24 / 16777215.0f;
+    if (p.out_rgba16f) {
+        __half2 h01 = __floats2half2_rn(c.x, c.y), h23 = __floats2half2_rn(c.z, c.w);
+        uint2 packed;
+        packed.x = *reinterpret_cast<uint32_t*>(&h01);
+        packed.y = *reinterpret_cast<uint32_t*>(&h23);
+        reinterpret_cast<uint2*>(p.out_rgba16f)[o] = packed;
+    }
+}
+
+// One CTA of 128 threads per 16x16 tile; warp w owns the 8x8 block
+// (w & 1, w >> 1); lane l shades pixels (l & 7, l >> 3) and (l & 7, (l >> 3) + 4)
+// of it: the two pixels share a column, hence dx, the column test and the
+// first term of the Gaussian exponent.
 template <int kMode>  // 0 = alpha, 1 = stochastic
 __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) {
     __shared__ __align__(128) RasterRecord s_rec[2][kBatch];
     __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint8_t s_mask[kBatch];
 
-    // Each warp owns an 8x4 pixel block of the 16x16 tile (2 x 4 blocks), so
-    // a warp-uniform rectangle test can skip splats that miss its block.
     const uint32_t tile = blockIdx.x;
     const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bx0 = tx * kTileW + (warp & 1) * 8, by0 = ty * kTileH + (warp >> 1) * 4;
-    const int px = bx0 + (lane & 7), py = by0 + (lane >> 3);
-    const bool inside = px < p.width && py < p.height;
+    const int bx0 = tx * kTileW + (warp & 1) * 8, by0 = ty * kTileH + (warp >> 1) * 8;
+    const int px = bx0 + (lane & 7), py0 = by0 + (lane >> 3), py1 = py0 + 4;
+    const bool in0 = px < p.width && py0 < p.height, in1 = px < p.width && py1 < p.height;
     const uint2 range = p.tile_ranges[tile];
     const uint32_t n = range.y > range.x ? range.y - range.x : 0u;
     const uint32_t* __restrict__ vals = p.tile_plan->vfinal;
@@ -85,10 +146,10 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     }
     __syncthreads();
 
-    const float fcx = (float)px + 0.5f, fcy = (float)py + 0.5f;
-    AlphaState A = {1.0f, 0.0f, 0.0f, 0.0f};
-    StochState S = {16777215u, 0xFFFFFFFFu, 0.0f, 0.0f, 0.0f};
-    bool done = !inside;
+    const float fcx = (float)px + 0.5f, fcy0 = (float)py0 + 0.5f, fcy1 = (float)py1 + 0.5f;
+    AlphaState A0 = {1.0f, 0.0f, 0.0f, 0.0f}, A1 = A0;
+    StochState S0 = {16777215u, 0xFFFFFFFFu, 0.0f, 0.0f, 0.0f}, S1 = S0;
+    bool done0 = !in0, done1 = !in1;
     bool failed = false;
     const uint32_t nb = (n + kBatch - 1) / kBatch;
     uint32_t phase0 = 0, phase1 = 0;
@@ -112,57 +173,63 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         if (b & 1) phase1 ^= 1u; else phase0 ^= 1u;
         const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
         const RasterRecord* recs = s_rec[b & 1];
-        // Warp-uniform control flow only: every lane walks the same records;
-        // per-pixel work is predicated on `live`.
-        bool warp_done = __all_sync(0xffffffffu, done || failed);
-        for (uint32_t j = 0; j < cnt && !warp_done; ++j) {
-            const uint4 q2 = reinterpret_cast<const uint4*>(recs + j)[2];
+        // Which of the four 8x8 warp blocks each staged splat's rectangle
+        // touches (one thread per record); warps then visit only their own.
+        if (threadIdx.x < cnt) {
+            const uint4 q2 = reinterpret_cast<const uint4*>(recs + threadIdx.x)[2];
             const int i0 = (int)(q2.z & 0xFFFFu), i1 = (int)(q2.z >> 16);
             const int j0 = (int)(q2.w & 0xFFFFu), j1 = (int)(q2.w >> 16);
-            // warp block [bx0, bx0+8) x [by0, by0+4) vs splat rect (uniform)
-            if (i1 <= bx0 || i0 >= bx0 + 8 || j1 <= by0 || j0 >= by0 + 4) continue;
-            const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
-            const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
-            if (kMode == 1) {
-                const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
-                // stop once this splat is beyond every lane's kept depth
-                const bool beyond = done || (S.best_id != 0xFFFFFFFFu && q3.x > S.best_d24 + kDepthMargin);
-                if (S.best_id != 0xFFFFFFFFu && q3.x > S.best_d24 + kDepthMargin) done = true;
-                if (__all_sync(0xffffffffu, beyond)) { warp_done = true; break; }
-            }
-            const bool in_rect = px >= i0 && px < i1 && py >= j0 && py < j1;
-            const float dx = sub(fcx, q0.x), dy = sub(fcy, q0.y);
-            const float power = splat_power(dx, dy, q0.z, q0.w, q1.x);
-            const bool live = !done && !failed && in_rect && (power <= 0.0f) && !(power < q1.z);
-            if (kMode == 0) {
-                if (live) {
-                    const float alpha = fminf(q1.y * __expf(power), 0.99f);
-                    const float w = alpha * A.T;
-                    A.c0 = fmaf(w, q1.w, A.c0);
-                    A.c1 = fmaf(w, __uint_as_float(q2.x), A.c1);
-                    A.c2 = fmaf(w, __uint_as_float(q2.y), A.c2);
-                    A.T = A.T * (1.0f - alpha);
-                    done = A.T < kTransmittanceMin;
-                }
-                if (__all_sync(0xffffffffu, done || failed)) { warp_done = true; break; }
-            } else {
-                const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
-                const uint32_t z24 = q3.x, id = q3.y;
-                const bool better = z24 < S.best_d24 || (z24 == S.best_d24 && id < S.best_id);
-                if (live && better) {
-                    const float alpha = g_min(mul(q1.y, det_expf(power)), 0.99f);
-                    const float rnd = hash13(fcx, fcy, __uint_as_float(q3.z));
-                    if (rnd < alpha) {
-                        S.best_d24 = z24;
-                        S.best_id = id;
-                        S.r = q1.w;
-                        S.g = __uint_as_float(q2.x);
-                        S.b = __uint_as_float(q2.y);
-                    }
+            const int x0 = tx * kTileW, y0 = ty * kTileH;
+            const uint32_t cols = (uint32_t)(i0 < x0 + 8 && i1 > x0) | ((uint32_t)(i0 < x0 + 16 && i1 > x0 + 8) << 1);
+            const uint32_t rows = (uint32_t)(j0 < y0 + 8 && j1 > y0) | ((uint32_t)(j0 < y0 + 16 && j1 > y0 + 8) << 1);
+            // block w = (w & 1, w >> 1): bit w set iff its column and row halves are covered
+            s_mask[threadIdx.x] = (uint8_t)((cols & (rows & 1u ? 3u : 0u)) | ((cols & (rows & 2u ? 3u : 0u)) << 2));
+        }
+        __syncthreads();
+        // Warp-uniform control flow only; per-pixel work is predicated.
+        bool warp_done = __all_sync(0xffffffffu, (done0 && done1) || failed);
+        for (uint32_t c = 0; c < cnt && !warp_done; c += 32) {
+            const bool mine = c + lane < cnt && ((s_mask[c + lane] >> warp) & 1u);
+            uint32_t todo = __ballot_sync(0xffffffffu, mine);
+            while (todo) {
+                const uint32_t j = c + (uint32_t)(__ffs(todo) - 1);
+                todo &= todo - 1u;
+                const uint4 q2 = reinterpret_cast<const uint4*>(recs + j)[2];
+                const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
+                const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
+                const int i0 = (int)(q2.z & 0xFFFFu), i1 = (int)(q2.z >> 16);
+                const int j0 = (int)(q2.w & 0xFFFFu), j1 = (int)(q2.w >> 16);
+                const bool colx = px >= i0 && px < i1;
+                // splat_power() evaluated for both pixels with the shared first term
+                const float dx = sub(fcx, q0.x);
+                const float t0 = mul(mul(q0.z, dx), dx);
+                const float dy0 = sub(fcy0, q0.y), dy1 = sub(fcy1, q0.y);
+                const float pw0 = mul(-0.5f, add(add(t0, mul(mul(q0.w, dx), dy0)), mul(mul(q1.x, dy0), dy0)));
+                const float pw1 = mul(-0.5f, add(add(t0, mul(mul(q0.w, dx), dy1)), mul(mul(q1.x, dy1), dy1)));
+                const bool live0 = !done0 && colx && py0 >= j0 && py0 < j1 && (pw0 <= 0.0f) && !(pw0 < q1.z);
+                const bool live1 = !done1 && colx && py1 >= j0 && py1 < j1 && (pw1 <= 0.0f) && !(pw1 < q1.z);
+                if (kMode == 0) {
+                    const float g = __uint_as_float(q2.x), bb = __uint_as_float(q2.y);
+                    if (live0) alpha_step(A0, done0, pw0, q1.y, q1.w, g, bb);
+                    if (live1) alpha_step(A1, done1, pw1, q1.y, q1.w, g, bb);
+                    if (__all_sync(0xffffffffu, (done0 && done1) || failed)) { warp_done = true; break; }
+                } else {
+                    const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
+                    const uint32_t z24 = q3.x, id = q3.y;
+                    // a pixel stops once splats are beyond its kept depth (+ margin)
+                    if (S0.best_id != 0xFFFFFFFFu && z24 > S0.best_d24 + kDepthMargin) done0 = true;
+                    if (S1.best_id != 0xFFFFFFFFu && z24 > S1.best_d24 + kDepthMargin) done1 = true;
+                    if (__all_sync(0xffffffffu, (done0 && done1) || failed)) { warp_done = true; break; }
+                    const bool b0 = z24 < S0.best_d24 || (z24 == S0.best_d24 && id < S0.best_id);
+                    const bool b1 = z24 < S1.best_d24 || (z24 == S1.best_d24 && id < S1.best_id);
+                    const float g = __uint_as_float(q2.x), bb = __uint_as_float(q2.y);
+                    const float hz = __uint_as_float(q3.z);
+                    if (live0 && !done0 && b0) stoch_step(S0, pw0, q1.y, fcx, fcy0, hz, z24, id, q1.w, g, bb);
+                    if (live1 && !done1 && b1) stoch_step(S1, pw1, q1.y, fcx, fcy1, hz, z24, id, q1.w, g, bb);
                 }
             }
         }
-        const int all_done = __syncthreads_and(warp_done || done || failed);
+        const int all_done = __syncthreads_and(warp_done || (done0 && done1) || failed);
         if (all_done) {
             if (b + 1 < nb) {
                 const uint32_t ph2 = ((b + 1) & 1) ? phase1 : phase0;
@@ -172,35 +239,12 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         }
     }
     if (failed) atomicOr(&p.fc->error_flags, kErrRasterWait);
-    if (!inside) return;
-    const size_t o = (size_t)(p.height - 1 - py) * p.width + px;
     if (kMode == 0) {
-        const float r = fmaf(A.T, p.bg, A.c0), g = fmaf(A.T, p.bg, A.c1), b = fmaf(A.T, p.bg, A.c2);
-        const float a = 1.0f - A.T;
-        __half2 h01 = __floats2half2_rn(r, g), h23 = __floats2half2_rn(b, a);
-        uint2 packed;
-        packed.x = *reinterpret_cast<uint32_t*>(&h01);
-        packed.y = *reinterpret_cast<uint32_t*>(&h23);
-        reinterpret_cast<uint2*>(p.out_rgba16f)[o] = packed;
+        if (in0) write_pixel_alpha(p, px, py0, A0);
+        if (in1) write_pixel_alpha(p, px, py1, A1);
     } else {
-        float4 c;
-        if (S.best_id == 0xFFFFFFFFu) c = make_float4(p.bg, p.bg, p.bg, 0.0f);
-        else c = make_float4(S.r, S.g, S.b, 1.0f);
-        if (p.rgba8) {
-            c.x = rintf(g_clamp(c.x, 0.0f, 1.0f) * 255.0f) / 255.0f;
-            c.y = rintf(g_clamp(c.y, 0.0f, 1.0f) * 255.0f) / 255.0f;
-            c.z = rintf(g_clamp(c.z, 0.0f, 1.0f) * 255.0f) / 255.0f;
-            c.w = rintf(g_clamp(c.w, 0.0f, 1.0f) * 255.0f) / 255.0f;
-        }
-        if (p.out_rgba32f) p.out_rgba32f[o] = c;
-        if (p.out_depth) p.out_depth[o] = (float)S.best_d24 / 16777215.0f;
-        if (p.out_rgba16f) {
-            __half2 h01 = __floats2half2_rn(c.x, c.y), h23 = __floats2half2_rn(c.z, c.w);
-            uint2 packed;
-            packed.x = *reinterpret_cast<uint32_t*>(&h01);
-            packed.y = *reinterpret_cast<uint32_t*>(&h23);
-            reinterpret_cast<uint2*>(p.out_rgba16f)[o] = packed;
-        }
+        if (in0) write_pixel_stoch(p, px, py0, S0);
+        if (in1) write_pixel_stoch(p, px, py1, S1);
     }
 }
 

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
         } else {
             st_release64(st, status_word(p.epoch, kFlagAgg, tile_count));
             bool to = false;
-            gexcl = lookback(status + d, kRadix, tile, p.epoch, &to);
+            gexcl = lookback_vec(status + d, kRadix, tile, p.epoch, &to);
             if (to) atomicOr(p.error_flags, kErrSortLookback);
             st_release64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
         }
