@@ -95,8 +95,10 @@ __device__ __forceinline__ void emit(const BinParams& p, uint32_t o, uint32_t s,
         const uint32_t e = o + k;
         if (e < p.entry_cap) {
             const int ty = ty0 + (int)(k / (uint32_t)w), tx = tx0 + (int)(k % (uint32_t)w);
-            p.entry_keys[e] = (uint32_t)(ty * p.tiles_x + tx);
+            const uint32_t t = (uint32_t)(ty * p.tiles_x + tx);
+            p.entry_keys[e] = t;
             p.entry_vals[e] = s;
+            atomicAdd(&p.tile_count[t], 1u);
         }
     }
 }
@@ -183,16 +185,38 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
     }
 }
 
-__global__ void tile_ranges_kernel(const SortPlan* plan, const FrameCounters* fc, uint2* ranges,
-                                   uint32_t num_tiles) {
-    const uint32_t E = fc->tile_entries;
-    const uint32_t* keys = plan->kfinal;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        uint32_t k = keys[e];
-        if (k >= num_tiles) continue;  // only after a failed (timed-out) sort
-        if (e == 0 || keys[e - 1] != k) ranges[k].x = e;
-        if (e == E - 1 || keys[e + 1] != k) ranges[k].y = e + 1;
+// From the per-tile entry counts (one CTA): each tile's [start, end) in the
+// tile-sorted entry array (exclusive scan over tiles) and the digit
+// histograms of the tile-sort passes.  After an entry-buffer overflow the
+// frame is invalid: every range is left empty.
+constexpr int kPlanThreads = 1024;
+__global__ void __launch_bounds__(kPlanThreads) tile_plan_kernel(const uint32_t* __restrict__ tile_count,
+                                                                 uint32_t num_tiles, int npasses,
+                                                                 const FrameCounters* fc, uint2* ranges,
+                                                                 uint32_t* tile_hist) {
+    __shared__ uint32_t s_hist[4][256];
+    __shared__ uint32_t warp_tmp[33];
+    for (int i = threadIdx.x; i < 4 * 256; i += kPlanThreads) (&s_hist[0][0])[i] = 0u;
+    __syncthreads();
+    const bool overflow = fc->tile_overflow != 0u;
+    const uint32_t per = (num_tiles + kPlanThreads - 1) / kPlanThreads;
+    const uint32_t t0 = threadIdx.x * per;
+    uint32_t sum = 0;
+    for (uint32_t t = t0; t < t0 + per && t < num_tiles; ++t) {
+        const uint32_t c = tile_count[t];
+        sum += c;
+        for (int ps = 0; ps < npasses; ++ps)
+            if (c) atomicAdd(&s_hist[ps][(t >> (8 * ps)) & 255u], c);
     }
+    uint32_t total;
+    uint32_t run = block_excl_scan(sum, warp_tmp, &total);
+    for (uint32_t t = t0; t < t0 + per && t < num_tiles; ++t) {
+        const uint32_t c = tile_count[t];
+        ranges[t] = overflow ? make_uint2(0u, 0u) : make_uint2(run, run + c);
+        run += c;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < npasses * 256; i += kPlanThreads) tile_hist[i] = (&s_hist[0][0])[i];
 }
 
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s) {
@@ -204,12 +228,10 @@ int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_
     return 1;
 }
 
-int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
-                       uint32_t num_tiles, uint32_t num_sms, cudaStream_t s) {
-    uint32_t grid = (entry_cap + 255) / 256;
-    if (grid > num_sms * 8) grid = num_sms * 8;
-    if (grid == 0) grid = 1;
-    tile_ranges_kernel<<<grid, 256, 0, s>>>(tile_plan, fc, ranges, num_tiles);
+int launch_tile_plan(const uint32_t* tile_count, uint32_t num_tiles, int tile_bits, const FrameCounters* fc,
+                     uint2* ranges, uint32_t* tile_hist, cudaStream_t s) {
+    const int npasses = (tile_bits + 7) / 8;
+    tile_plan_kernel<<<1, kPlanThreads, 0, s>>>(tile_count, num_tiles, npasses, fc, ranges, tile_hist);
     return 1;
 }
 

@@ -230,6 +230,35 @@ __device__ __forceinline__ void stage_round(const float4* rows, uint32_t wbase, 
     }
 }
 
+// gsanim int8 appearance deltas applied in place to a staged row
+// (shaders/cull.glsl:125-164): DC slots 12..14 are j = 0..2, the SH slot
+// 16 + 3k + c is j = 3 + 15c + k; state s >= 1 adds q * scale[j] with q the
+// int8 at ((s-1) * n + row) * 48 + j; two states blend with the weight.
+__device__ __forceinline__ float anim_coeff(const CullParams& p, float base, uint32_t row, int j, int state) {
+    if (state == 0) return base;
+    const size_t off = ((size_t)(state - 1) * p.n + row) * 48u + (size_t)j;
+    return add(base, mul((float)p.anim_deltas[off], __ldg(p.anim_scales + j)));
+}
+
+__device__ void animate_row(const CullParams& p, uint32_t row, float4* staged, float4& c3) {
+    float* f = reinterpret_cast<float*>(staged);
+    float dc[3] = {c3.x, c3.y, c3.z};
+    for (int slot = 12; slot < 61; ++slot) {
+        if (slot == 15) continue;
+        const int j = slot < 15 ? slot - 12 : 3 + ((slot - 16) % 3) * 15 + (slot - 16) / 3;
+        const float base = slot < 15 ? dc[slot - 12] : f[slot];
+        float v = anim_coeff(p, base, row, j, p.anim_state_a);
+        if (p.anim_weight > 0.0f) {
+            const float bb = anim_coeff(p, base, row, j, p.anim_state_b);
+            v = add(mul(sub(1.0f, p.anim_weight), v), mul(p.anim_weight, bb));
+        }
+        if (slot < 15) dc[slot - 12] = v;
+        else f[slot] = v;
+    }
+    c3 = make_float4(dc[0], dc[1], dc[2], c3.w);
+    staged[3] = c3;
+}
+
 // Every warp is independent: it takes 128-Gaussian warp tiles in ticket
 // order, stages round r+1's visible rows while it projects round r, and
 // places its visible (key, id) pairs with a warp-level decoupled look-back.
@@ -237,6 +266,9 @@ template <int kChunks>  // 16-byte chunks of a row the SH degree needs: 4, 7, 10
 __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
     extern __shared__ float4 smem4[];
     __shared__ uint8_t vis_list[kCullWarps][kCullRounds][32];
+    __shared__ uint32_t s_hist[4][256];   // digit histograms of the emitted keys (for the depth sort)
+    for (int i = threadIdx.x; i < 4 * 256; i += kCullThreads) (&s_hist[0][0])[i] = 0u;
+    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float4* stage0 = smem4 + (size_t)warp * 2 * 32 * kStageStride;
     float4* stage1 = stage0 + 32 * kStageStride;
@@ -244,6 +276,8 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
     CamRegs cam;
     load_cam(p.cam, cam);
     const uint32_t lt = (1u << lane) - 1u;
+    const bool animated = p.anim_deltas != nullptr &&
+                          (p.anim_state_a != 0 || (p.anim_weight > 0.0f && p.anim_state_b != 0));
 
     for (;;) {
         uint32_t tile = 0;
@@ -307,6 +341,10 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
             if (visible) {
                 float4 rec[4];
                 float qa, gp;
+                if (animated) {
+                    float4 c3 = cur[lane * kStageStride + 3];
+                    animate_row(p, g, cur + lane * kStageStride, c3);
+                }
                 project_visible(cur + lane * kStageStride, c0[r], vx[r], vy[r], vz[r], cam, p.sh_degree,
                                 p.sh_lod_distance, rec, &qa, &gp);
                 float4* dst = p.projected + (size_t)g * 4;
@@ -371,9 +409,16 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
                 const uint32_t o = excl + before + __popc(mask[r] & lt);
                 p.keys_out[o] = keys[r];
                 p.ids_out[o] = base + r * 32 + lane;
+#pragma unroll
+                for (int ps = 0; ps < 4; ++ps) atomicAdd(&s_hist[ps][(keys[r] >> (8 * ps)) & 255u], 1u);
             }
             before += __popc(mask[r]);
         }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * 256; i += kCullThreads) {
+        const uint32_t c = (&s_hist[0][0])[i];
+        if (c) atomicAdd(p.key_hist + i, c);
     }
 }
 
@@ -387,6 +432,7 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
         attr_set = true;
     }
     int deg = p.sh_degree < 0 ? 0 : (p.sh_degree > 3 ? 3 : p.sh_degree);
+    if (p.anim_deltas) deg = 3;   // the delta pass touches every SH slot of the staged row
     uint32_t tiles = (p.n + kCullTile - 1) / kCullTile;
     uint32_t warps = num_sms * 3 * kCullWarps;
     uint32_t grid = (std::min(warps, tiles) + kCullWarps - 1) / kCullWarps;

@@ -76,7 +76,15 @@ struct gs_ctx {
     uint32_t* depth_hist = nullptr;
     uint32_t* tile_hist = nullptr;
     uint2* tile_ranges = nullptr;
+    uint32_t* tile_count = nullptr;
     uint32_t tiles_cap = 0;
+
+    // gsanim appearance deltas (renderer animation buffer, src/renderer.cpp:824-841)
+    int8_t* anim_deltas = nullptr;
+    float* anim_scales = nullptr;
+    uint32_t anim_states = 0;     // delta states (state 0 = the uploaded rows)
+    int anim_a = 0, anim_b = 0;
+    float anim_w = 0.0f;
 
     // camera
     gs_camera* d_cam = nullptr;
@@ -160,6 +168,11 @@ void release_scene(gs_ctx* c) {
     dfree(c->bin_status);
     dfree(c->tsort_status);
     gs::release_gps_scene(c->gps);
+    dfree(c->anim_deltas);
+    dfree(c->anim_scales);
+    c->anim_states = 0;
+    c->anim_a = c->anim_b = 0;
+    c->anim_w = 0.0f;
     c->n = 0;
     c->entry_cap = 0;
 }
@@ -240,7 +253,7 @@ int ensure_targets(gs_ctx* c, int w, int h) {
     if (c->width == w && c->height == h && c->ctrl) return GS_OK;
     release_targets(c);
     c->tiles_cap = (uint32_t)(tx * ty);
-    // control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges
+    // control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges | tile counts
     size_t off = 0;
     auto place = [&](size_t bytes) {
         size_t o = off;
@@ -253,6 +266,7 @@ int ensure_targets(gs_ctx* c, int w, int h) {
     size_t o_dh = place(4 * 256 * 4);
     size_t o_th = place(4 * 256 * 4);
     size_t o_tr = place((size_t)c->tiles_cap * sizeof(uint2));
+    size_t o_tc = place((size_t)c->tiles_cap * sizeof(uint32_t));
     c->ctrl_bytes = off;
     GS_CUDA(c, dalloc(reinterpret_cast<char**>(&c->ctrl), c->ctrl_bytes));
     char* base = static_cast<char*>(c->ctrl);
@@ -262,6 +276,7 @@ int ensure_targets(gs_ctx* c, int w, int h) {
     c->depth_hist = reinterpret_cast<uint32_t*>(base + o_dh);
     c->tile_hist = reinterpret_cast<uint32_t*>(base + o_th);
     c->tile_ranges = reinterpret_cast<uint2*>(base + o_tr);
+    c->tile_count = reinterpret_cast<uint32_t*>(base + o_tc);
     GS_CUDA(c, cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream));
     GS_CUDA(c, dalloc(&c->out16, (size_t)w * h * 8));
     c->width = w;
@@ -318,6 +333,14 @@ void run_cull(gs_ctx* c) {
     p.ids_out = c->ids[1];
     p.status = c->cull_status;
     p.epoch = c->epoch;
+    p.key_hist = c->depth_hist;
+    if (c->anim_deltas) {
+        p.anim_deltas = c->anim_deltas;
+        p.anim_scales = c->anim_scales;
+        p.anim_state_a = c->anim_a;
+        p.anim_state_b = c->anim_b;
+        p.anim_weight = c->anim_w;
+    }
     p.fc = c->fc;
     sc.add(gs::launch_cull(p, c->num_sms, c->stream));
 }
@@ -336,7 +359,8 @@ void run_depth_sort(gs_ctx* c) {
     p.count_cap = c->n;
     p.begin_bit = 0;
     p.end_bit = 32;
-    p.hist = c->depth_hist;
+    p.hist = c->depth_hist;   // accumulated by the cull kernel
+    p.hist_ready = 1;
     p.plan = c->depth_plan;
     p.status = c->sort_status;
     p.status_stride = c->sort_status_stride;
@@ -351,7 +375,7 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         StageScope sc(c, ST_BIN);
         if (reset_ranges) {
             // A second pass in the same frame: clear ranges, counters and the tile-sort plan.
-            cudaMemsetAsync(c->tile_ranges, 0, (size_t)c->tiles_cap * sizeof(uint2), c->stream);
+            cudaMemsetAsync(c->tile_count, 0, (size_t)c->tiles_cap * sizeof(uint32_t), c->stream);
             cudaMemsetAsync(c->tile_plan, 0, sizeof(SortPlan), c->stream);
             cudaMemsetAsync(c->tile_hist, 0, 4 * 256 * 4, c->stream);
             // bin_ticket, tile_entries, tile_overflow are adjacent in FrameCounters.
@@ -374,10 +398,13 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         p.entry_keys = c->ekeys[1];
         p.entry_vals = c->evals[1];
         p.entry_cap = c->entry_cap;
+        p.tile_count = c->tile_count;
         p.status = c->bin_status;
         p.epoch = c->epoch;
         p.fc = c->fc;
         sc.add(gs::launch_bin(p, c->n, c->num_sms, c->stream));
+        sc.add(gs::launch_tile_plan(c->tile_count, c->tiles_cap, entry_bits(c->tiles_cap), c->fc, c->tile_ranges,
+                                    c->tile_hist, c->stream));
     }
     {
         StageScope sc(c, ST_TILE_SORT);
@@ -393,15 +420,14 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         p.count_cap = c->entry_cap;
         p.begin_bit = 0;
         p.end_bit = entry_bits(c->tiles_cap);
-        p.hist = c->tile_hist;
+        p.hist = c->tile_hist;    // from the per-tile counts
+        p.hist_ready = 1;
         p.plan = c->tile_plan;
         p.status = c->tsort_status;
         p.status_stride = c->tsort_status_stride;
         p.epoch = c->epoch;
         p.error_flags = &c->fc->error_flags;
         sc.add(gs::launch_sort(p, c->num_sms, c->stream));
-        sc.add(gs::launch_tile_ranges(c->tile_plan, c->fc, c->entry_cap, c->tile_ranges, c->tiles_cap, c->num_sms,
-                                       c->stream));
     }
 }
 
@@ -760,6 +786,41 @@ int gs_upload_rows(gs_ctx* c, const float* rows, uint64_t count) {
 
 int gs_upload_rows_device(gs_ctx* c, const float* rows, uint64_t count) {
     return upload_common(c, rows, count, cudaMemcpyDeviceToDevice);
+}
+
+int gs_upload_anim(gs_ctx* c, const int8_t* deltas, uint32_t num_states, const float* scales) {
+    if (!c || (num_states && (!deltas || !scales))) return GS_ERR_BAD_ARG;
+    if (!c->n) return fail(c, GS_ERR_NO_SCENE, "upload the Gaussians before their animation");
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    dfree(c->anim_deltas);
+    dfree(c->anim_scales);
+    c->anim_states = 0;
+    c->anim_a = c->anim_b = 0;
+    c->anim_w = 0.0f;
+    if (num_states == 0) return GS_OK;
+    const size_t bytes = (size_t)num_states * c->n * 48u;
+    GS_CUDA(c, dalloc(&c->anim_deltas, bytes));
+    GS_CUDA(c, dalloc(&c->anim_scales, 48 * sizeof(float)));
+    GS_CUDA(c, cudaMemcpyAsync(c->anim_deltas, deltas, bytes, cudaMemcpyHostToDevice, c->stream));
+    GS_CUDA(c, cudaMemcpyAsync(c->anim_scales, scales, 48 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->anim_states = num_states;
+    gs_reset_accumulation(c);
+    return GS_OK;
+}
+
+int gs_set_anim_state(gs_ctx* c, int state_a, int state_b, float weight) {
+    if (!c) return GS_ERR_BAD_ARG;
+    if (state_a < 0 || state_b < 0 || (uint32_t)state_a > c->anim_states || (uint32_t)state_b > c->anim_states ||
+        !(weight >= 0.0f && weight <= 1.0f))
+        return fail(c, GS_ERR_BAD_ARG, "animation state out of range");
+    // src/renderer.cpp:2148-2161: a changed sample resets accumulation
+    if (state_a != c->anim_a || state_b != c->anim_b || weight != c->anim_w) gs_reset_accumulation(c);
+    c->anim_a = state_a;
+    c->anim_b = state_b;
+    c->anim_w = weight;
+    return GS_OK;
 }
 
 int gs_set_gps_budget(gs_ctx* c, uint32_t max_work_items) {

@@ -100,6 +100,12 @@ struct CullParams {
     uint32_t* ids_out;           // compacted visible ids
     unsigned long long* status;  // per-tile look-back words (epoch-tagged)
     uint32_t epoch;
+    uint32_t* key_hist;          // 4 x 256 digit histograms of the emitted keys (zeroed per frame)
+    // gsanim int8 appearance deltas (shaders/cull.glsl:125-164); null = none
+    const int8_t* anim_deltas;   // [(state-1) * n + row] * 48 + j
+    const float* anim_scales;    // 48 (device)
+    int anim_state_a, anim_state_b;
+    float anim_weight;
     FrameCounters* fc;
 };
 
@@ -113,6 +119,7 @@ struct SortParams {
     uint32_t count_cap;          // capacity (grid sizing)
     int begin_bit, end_bit;
     uint32_t* hist;              // 4 x 256 digit histograms (zeroed before the sort)
+    int hist_ready;              // 1: the producer of the keys already filled `hist`
     SortPlan* plan;              // zeroed before the sort
     unsigned long long* status;  // per pass: tiles x 256 look-back words (epoch-tagged)
     size_t status_stride;        // words per pass
@@ -131,6 +138,7 @@ struct BinParams {
     uint32_t* entry_keys;            // tile id per entry
     uint32_t* entry_vals;            // sorted position per entry
     uint32_t entry_cap;
+    uint32_t* tile_count;            // entries written per screen tile (zeroed per pass)
     unsigned long long* status;      // per-CTA-tile look-back words (epoch-tagged)
     uint32_t epoch;
     FrameCounters* fc;
@@ -154,8 +162,9 @@ struct RasterParams {
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s);
-int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
-                       uint32_t num_tiles, uint32_t num_sms, cudaStream_t s);
+// Tile ranges and tile-sort digit histograms from the per-tile entry counts.
+int launch_tile_plan(const uint32_t* tile_count, uint32_t num_tiles, int tile_bits, const FrameCounters* fc,
+                     uint2* ranges, uint32_t* tile_hist, cudaStream_t s);
 int launch_raster_alpha(const RasterParams& p, cudaStream_t s);
 int launch_raster_stochastic(const RasterParams& p, cudaStream_t s);
 

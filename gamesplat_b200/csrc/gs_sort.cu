@@ -6,16 +6,18 @@
 // order.  Structure:
 //   1. sort_hist_kernel   - one read of the keys builds the digit histograms
 //                           of every pass (warp-private shared histograms);
-//   2. sort_plan_kernel   - exclusive digit offsets; passes whose digit is the
-//                           same for all keys are skipped (identity for a
-//                           stable sort); ping-pong assignment of active passes;
-//   3. sort_pass_kernel   - per pass, persistent CTAs take 4096-key tiles in
+//      (skipped when the producer of the keys already accumulated them);
+//   2. sort_pass_kernel   - every CTA derives the pass plan from the
+//                           histograms (passes whose digit is the same for all
+//                           keys are skipped: identity for a stable sort;
+//                           ping-pong assignment of the active passes), then
+//                           persistent CTAs take 4096-key tiles in
 //                           ticket order, rank keys with warp match/ballot
-//                           (__match_any_sync), publish per-digit counts and
+//                           (__match_any_sync), publish per-digit counts,
+//                           reorder the tile by digit in shared memory, then
 //                           resolve their global offsets by decoupled
-//                           look-back (bounded spin), reorder the tile by digit
-//                           in shared memory and write runs coalesced;
-//   4. sort_copy_kernel   - only when the caller needs the result in a given
+//                           look-back (bounded spin) and write runs coalesced;
+//   3. sort_copy_kernel   - only when the caller needs the result in a given
 //                           buffer and every pass was skipped.
 // Element counts are read on the device, so nothing here synchronises with
 // the host.
@@ -74,50 +76,62 @@ __global__ void __launch_bounds__(kSortThreads) sort_hist_kernel(SortParams p, i
     }
 }
 
-__global__ void __launch_bounds__(kSortThreads) sort_plan_kernel(SortParams p, int npasses) {
-    __shared__ uint32_t scan_tmp[33];
-    __shared__ uint32_t s_active[4];
-    const uint32_t n = p.count_ptr ? *p.count_ptr : p.count_cap;
-    const int t = threadIdx.x;
+// Pass plan, recomputed by every CTA of every pass kernel from the digit
+// histograms: a pass is skipped when one digit holds every key (a stable sort
+// by a constant digit is the identity); active passes ping-pong between the
+// writable buffers (with land_in_buf0 the last one writes buffer 0).
+struct PassIO {
+    const uint32_t* kin;
+    const uint32_t* vin;
+    uint32_t* kout;
+    uint32_t* vout;
+    const uint32_t* kfinal;
+    const uint32_t* vfinal;
+    bool active;
+    bool copy_needed;
+};
+
+__device__ PassIO plan_passes(const SortParams& p, int npasses, int pass, uint32_t n, uint32_t* s_act) {
     for (int ps = 0; ps < npasses; ++ps) {
-        uint32_t c = p.hist[ps * kRadix + t];
-        int all_in_one = __syncthreads_or(c == n);
-        uint32_t total;
-        uint32_t excl = block_excl_scan(c, scan_tmp, &total);
-        p.hist[ps * kRadix + t] = excl;
-        if (t == 0) s_active[ps] = all_in_one ? 0u : 1u;
+        const int trivial = __syncthreads_or(p.hist[ps * kRadix + threadIdx.x] == n);
+        if (threadIdx.x == 0) s_act[ps] = trivial ? 0u : 1u;
     }
     __syncthreads();
-    if (t == 0) {
-        SortPlan* pl = p.plan;
-        int m = 0;
-        for (int ps = 0; ps < npasses; ++ps) m += (int)s_active[ps];
-        const uint32_t* kcur = p.keys_in;
-        const uint32_t* vcur = p.vals_in;
-        // Destination of the j-th active pass (j = 0..m-1): with land_in_buf0
-        // the last one writes buffer 0, alternating backwards; otherwise the
-        // first writes buffer 0, alternating forwards.
-        int j = 0;
-        for (int ps = 0; ps < 4; ++ps) {
-            pl->active[ps] = (ps < npasses) ? s_active[ps] : 0u;
-            if (!pl->active[ps]) continue;
-            int dst = p.land_in_buf0 ? ((m - 1 - j) & 1) : (j & 1);
-            pl->kin[ps] = kcur;
-            pl->vin[ps] = vcur;
-            pl->kout[ps] = p.keys_buf[dst];
-            pl->vout[ps] = p.vals_buf[dst];
-            kcur = p.keys_buf[dst];
-            vcur = p.vals_buf[dst];
-            ++j;
+    int m = 0;
+    for (int ps = 0; ps < npasses; ++ps) m += (int)s_act[ps];
+    PassIO io{};
+    const uint32_t* kcur = p.keys_in;
+    const uint32_t* vcur = p.vals_in;
+    int j = 0;
+    for (int ps = 0; ps < npasses; ++ps) {
+        if (!s_act[ps]) continue;
+        const int dst = p.land_in_buf0 ? ((m - 1 - j) & 1) : (j & 1);
+        if (ps == pass) {
+            io.kin = kcur;
+            io.vin = vcur;
+            io.kout = p.keys_buf[dst];
+            io.vout = p.vals_buf[dst];
         }
-        pl->copy_needed = (p.land_in_buf0 && m == 0) ? 1u : 0u;
-        pl->kfinal = pl->copy_needed ? p.keys_buf[0] : kcur;
-        pl->vfinal = pl->copy_needed ? p.vals_buf[0] : vcur;
+        kcur = p.keys_buf[dst];
+        vcur = p.vals_buf[dst];
+        ++j;
+    }
+    io.active = s_act[pass] != 0u;
+    io.copy_needed = p.land_in_buf0 && m == 0;
+    io.kfinal = io.copy_needed ? p.keys_buf[0] : kcur;
+    io.vfinal = io.copy_needed ? p.vals_buf[0] : vcur;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        SortPlan* pl = p.plan;
+        for (int ps = 0; ps < 4; ++ps) pl->active[ps] = ps < npasses ? s_act[ps] : 0u;
+        pl->kfinal = io.kfinal;
+        pl->vfinal = io.vfinal;
+        pl->copy_needed = io.copy_needed ? 1u : 0u;
         pl->count = n;
     }
+    return io;
 }
 
-__global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p, int pass) {
+__global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p, int pass, int npasses) {
     __shared__ uint32_t s_keys[kSortTile];
     __shared__ uint32_t s_vals[kSortTile];
     __shared__ uint32_t warp_hist[kSortWarps][kRadix];
@@ -125,24 +139,27 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
     __shared__ uint32_t s_global_base[kRadix];
     __shared__ uint32_t scan_tmp[33];
     __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_act[4];
 
-    SortPlan* pl = p.plan;
-    if (!pl->active[pass]) return;
-    const uint32_t n = pl->count;
-    const uint32_t* __restrict__ kin = pl->kin[pass];
-    const uint32_t* __restrict__ vin = pl->vin[pass];
-    uint32_t* __restrict__ kout = pl->kout[pass];
-    uint32_t* __restrict__ vout = pl->vout[pass];
+    const uint32_t n = p.count_ptr ? *p.count_ptr : p.count_cap;
+    const PassIO io = plan_passes(p, npasses, pass, n, s_act);
+    if (!io.active) return;
+    const uint32_t* __restrict__ kin = io.kin;
+    const uint32_t* __restrict__ vin = io.vin;
+    uint32_t* __restrict__ kout = io.kout;
+    uint32_t* __restrict__ vout = io.vout;
     const int shift = p.begin_bit + pass * kRadixBits;
     const uint32_t dmask = (1u << min(kRadixBits, p.end_bit - shift)) - 1u;
-    const uint32_t* gdigit = p.hist + pass * kRadix;
     u64* status = p.status + (size_t)pass * p.status_stride;
     const uint32_t num_tiles = (n + kSortTile - 1) / kSortTile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
+    // global start of this thread's digit (exclusive scan of the histogram)
+    uint32_t digit_total;
+    const uint32_t gdigit = block_excl_scan(p.hist[pass * kRadix + threadIdx.x], scan_tmp, &digit_total);
 
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&pl->ticket[pass], 1u);
+        if (threadIdx.x == 0) s_tile = atomicAdd(&p.plan->ticket[pass], 1u);
         for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&warp_hist[0][0])[i] = 0u;
         __syncthreads();
         const uint32_t tile = s_tile;
@@ -186,23 +203,13 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
         }
         const uint32_t tile_count = run;
         u64* st = status + (size_t)tile * kRadix + d;
-        uint32_t gexcl;
-        if (tile == 0) {
-            gexcl = gdigit[d];
-            st_release64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
-        } else {
-            st_release64(st, status_word(p.epoch, kFlagAgg, tile_count));
-            bool to = false;
-            gexcl = lookback_vec(status + d, kRadix, tile, p.epoch, &to);
-            if (to) atomicOr(p.error_flags, kErrSortLookback);
-            st_release64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
-        }
+        if (tile == 0) st_release64(st, status_word(p.epoch, kFlagInc, gdigit + tile_count));
+        else st_release64(st, status_word(p.epoch, kFlagAgg, tile_count));
+        // Reorder the tile by digit in shared memory while predecessors publish.
         uint32_t total;
-        uint32_t lstart = block_excl_scan(tile_count, scan_tmp, &total);
+        const uint32_t lstart = block_excl_scan(tile_count, scan_tmp, &total);
         s_local_start[d] = lstart;
-        s_global_base[d] = gexcl - lstart;
         __syncthreads();
-        // Reorder the tile by digit in shared memory.
 #pragma unroll
         for (int k = 0; k < kSortItems; ++k) {
             uint32_t idx = wbase + k * 32 + lane;
@@ -213,6 +220,15 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
                 s_vals[lp] = val[k];
             }
         }
+        // Global offset of each digit's run: decoupled look-back.
+        uint32_t gexcl = gdigit;
+        if (tile > 0) {
+            bool to = false;
+            gexcl = lookback_vec(status + d, kRadix, tile, p.epoch, &to);
+            if (to) atomicOr(p.error_flags, kErrSortLookback);
+            st_release64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
+        }
+        s_global_base[d] = gexcl - lstart;
         __syncthreads();
         const uint32_t nvalid = min((uint32_t)kSortTile, n - base);
         for (uint32_t i = threadIdx.x; i < nvalid; i += kSortThreads) {
@@ -248,17 +264,17 @@ int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s) {
     const int npasses = sort_passes(p.begin_bit, p.end_bit);
     int launches = 0;
     uint32_t tiles_cap = (p.count_cap + kSortTile - 1) / kSortTile;
-    uint32_t hist_grid = num_sms * 2;
-    uint32_t hist_need = (p.count_cap / 4 + kSortThreads - 1) / kSortThreads;
-    if (hist_grid > hist_need) hist_grid = hist_need > 0 ? hist_need : 1;
-    sort_hist_kernel<<<hist_grid, kSortThreads, 0, s>>>(p, npasses);
-    ++launches;
-    sort_plan_kernel<<<1, kSortThreads, 0, s>>>(p, npasses);
-    ++launches;
+    if (!p.hist_ready) {
+        uint32_t hist_grid = num_sms * 2;
+        uint32_t hist_need = (p.count_cap / 4 + kSortThreads - 1) / kSortThreads;
+        if (hist_grid > hist_need) hist_grid = hist_need > 0 ? hist_need : 1;
+        sort_hist_kernel<<<hist_grid, kSortThreads, 0, s>>>(p, npasses);
+        ++launches;
+    }
     uint32_t pass_grid = num_sms * (uint32_t)g_pass_blocks_per_sm;
     if (pass_grid > tiles_cap) pass_grid = tiles_cap > 0 ? tiles_cap : 1;
     for (int ps = 0; ps < npasses; ++ps) {
-        sort_pass_kernel<<<pass_grid, kSortThreads, 0, s>>>(p, ps);
+        sort_pass_kernel<<<pass_grid, kSortThreads, 0, s>>>(p, ps, npasses);
         ++launches;
     }
     if (p.land_in_buf0) {

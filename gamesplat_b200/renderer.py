@@ -139,6 +139,19 @@ class Renderer:
         L.check(L.lib().gs_upload_rows_device(self._ctx, C.c_void_p(ptr), count), "gs_upload_rows_device",
                 self._ctx)
 
+    def upload_animation(self, deltas: np.ndarray, scales: np.ndarray) -> None:
+        """gsanim int8 appearance deltas: (states, N, 48) int8 and 48 float32 scales."""
+        deltas = np.ascontiguousarray(deltas, dtype=np.int8)
+        scales = np.ascontiguousarray(scales, dtype=np.float32)
+        if deltas.ndim != 3 or deltas.shape[2] != 48 or scales.shape != (48,):
+            raise ValueError("deltas must be (states, N, 48) int8 and scales 48 float32")
+        L.check(L.lib().gs_upload_anim(self._ctx, deltas.ctypes.data, deltas.shape[0], scales.ctypes.data),
+                "gs_upload_anim", self._ctx)
+
+    def set_animation_state(self, state_a: int, state_b: int = 0, weight: float = 0.0) -> None:
+        L.check(L.lib().gs_set_anim_state(self._ctx, int(state_a), int(state_b), float(weight)),
+                "gs_set_anim_state", self._ctx)
+
     def set_gps_work_budget(self, max_work_items: int) -> bool:
         st = L.lib().gs_set_gps_budget(self._ctx, int(max_work_items))
         if st == L.GS_ERR_BUDGET_REFUSED:

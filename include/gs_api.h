@@ -140,6 +140,20 @@ int gs_upload_rows(gs_ctx* ctx, const float* rows, uint64_t count);
 /* As gs_upload_rows, from device memory (stream-ordered copy). */
 int gs_upload_rows_device(gs_ctx* ctx, const float* rows_dev, uint64_t count);
 
+/* gsanim appearance states (the renderer's animation buffer,
+ * src/renderer.cpp:824-841, decoded by shaders/cull.glsl:125-164):
+ * `deltas` holds num_states x N x 48 int8 values (state-major, row, then
+ * coefficient j: 0..2 = DC, 3 + 15c + k = SH coefficient k of channel c);
+ * state s >= 1 adds deltas[s-1][row][j] * scales[j] to the uploaded row's
+ * coefficient, state 0 is the row itself.  Upload after gs_upload_rows;
+ * num_states = 0 removes the animation.  Copies; the caller keeps ownership. */
+int gs_upload_anim(gs_ctx* ctx, const int8_t* deltas, uint32_t num_states, const float* scales);
+
+/* The renderer's animation_state_a / animation_state_b / animation_weight
+ * (src/renderer.cpp:2148-2161, from gsanim_sample): the coefficients are
+ * (1 - weight) * state_a + weight * state_b.  A change resets accumulation. */
+int gs_set_anim_state(gs_ctx* ctx, int state_a, int state_b, float weight);
+
 /* renderer_set_gps_work_budget (src/renderer.h:252): replace only the GPS work
  * buffer; on failure the old budget and buffer are kept
  * (src/renderer.cpp:1076-1123). */

@@ -145,6 +145,39 @@ static inline void sh_add(float* res, float w, const float* sh) {
     res[2] = res[2] + w * sh[2];
 }
 
+/* gsanim int8 appearance deltas (shaders/cull.glsl:125-164): state 0 is the
+ * base row; state s >= 1 adds q * scale[j] with q the int8 at
+ * ((s-1) * N + row) * 48 + j, j = 0..2 for the DC slots 12..14 and
+ * 3 + channel*15 + k for the SH slot 16 + 3k + channel. */
+typedef struct oc_anim {
+    const int8_t* deltas;
+    uint32_t count;           /* rows per state (N) */
+    const float* scales;      /* 48 */
+    int state_a, state_b;
+    float weight;
+} oc_anim;
+
+static inline float anim_coeff(const oc_anim* a, float base, uint32_t row, int j, int state) {
+    if (state == 0) return base;
+    uint64_t off = ((uint64_t)(state - 1) * a->count + row) * 48u + (uint64_t)j;
+    int q = (int)a->deltas[off];
+    return base + (float)q * a->scales[j];
+}
+
+static void anim_row(const oc_anim* a, uint32_t row, const float* in, float* out) {
+    memcpy(out, in, 64 * sizeof(float));
+    for (int slot = 12; slot < 61; ++slot) {
+        if (slot == 15) continue;
+        int j = slot < 15 ? slot - 12 : 3 + ((slot - 16) % 3) * 15 + (slot - 16) / 3;
+        float v = anim_coeff(a, in[slot], row, j, a->state_a);
+        if (a->weight > 0.0f) {
+            float b = anim_coeff(a, in[slot], row, j, a->state_b);
+            v = (1.0f - a->weight) * v + a->weight * b;
+        }
+        out[slot] = v;
+    }
+}
+
 static void cull_one(const float* r, uint32_t idx, const oc_camera* cam, int sh_degree,
                      float sh_lod_distance, int collect_stats, uint32_t* ids, uint32_t* keys,
                      float* out, uint32_t* visible_count, uint32_t* diag) {
@@ -305,15 +338,32 @@ static void cull_one(const float* r, uint32_t idx, const oc_camera* cam, int sh_
     out[12] = a; out[13] = b * cam->clip_y_sign; out[14] = c; out[15] = det;
 }
 
-void oc_cull(const float* rows, uint32_t n, const oc_camera* cam, int sh_degree,
-             float sh_lod_distance, int collect_stats, uint32_t* ids, uint32_t* keys,
-             float* projected, uint32_t* visible_count, uint32_t* diag) {
+void oc_cull_anim(const float* rows, uint32_t n, const oc_camera* cam, int sh_degree,
+                  float sh_lod_distance, int collect_stats, const int8_t* deltas, const float* scales,
+                  int state_a, int state_b, float weight, uint32_t* ids, uint32_t* keys,
+                  float* projected, uint32_t* visible_count, uint32_t* diag) {
     *visible_count = 0;
     for (int k = 0; k < 8; ++k) diag[k] = 0;
     for (uint32_t i = 0; i < n; ++i) { ids[i] = OC_SENTINEL; keys[i] = OC_SENTINEL; }
-    for (uint32_t i = 0; i < n; ++i)
-        cull_one(rows + (size_t)i * 64, i, cam, sh_degree, sh_lod_distance, collect_stats, ids, keys,
+    oc_anim a = {deltas, n, scales, state_a, state_b, weight};
+    const int animated = deltas != NULL && (state_a != 0 || (weight > 0.0f && state_b != 0));
+    float tmp[64];
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* row = rows + (size_t)i * 64;
+        if (animated) {
+            anim_row(&a, i, row, tmp);
+            row = tmp;
+        }
+        cull_one(row, i, cam, sh_degree, sh_lod_distance, collect_stats, ids, keys,
                  projected + (size_t)i * 16, visible_count, diag);
+    }
+}
+
+void oc_cull(const float* rows, uint32_t n, const oc_camera* cam, int sh_degree,
+             float sh_lod_distance, int collect_stats, uint32_t* ids, uint32_t* keys,
+             float* projected, uint32_t* visible_count, uint32_t* diag) {
+    oc_cull_anim(rows, n, cam, sh_degree, sh_lod_distance, collect_stats, NULL, NULL, 0, 0, 0.0f, ids, keys,
+                 projected, visible_count, diag);
 }
 
 /* ------------------------------------------------------------------------ */

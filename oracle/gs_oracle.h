@@ -58,6 +58,15 @@ void oc_cull(const float* rows, uint32_t n, const oc_camera* cam, int sh_degree,
              float sh_lod_distance, int collect_stats, uint32_t* ids, uint32_t* keys,
              float* projected, uint32_t* visible_count, uint32_t* diag);
 
+/* oc_cull with gsanim int8 appearance deltas applied to the DC and SH
+ * coefficients (shaders/cull.glsl:125-164): deltas[((s-1)*n + row)*48 + j],
+ * scales[48], states a/b and blend weight as in the renderer's
+ * animation_state_a/b and animation_weight. */
+void oc_cull_anim(const float* rows, uint32_t n, const oc_camera* cam, int sh_degree,
+                  float sh_lod_distance, int collect_stats, const int8_t* deltas, const float* scales,
+                  int state_a, int state_b, float weight, uint32_t* ids, uint32_t* keys,
+                  float* projected, uint32_t* visible_count, uint32_t* diag);
+
 /* Stable ascending LSD radix sort (8-bit digits, 4 passes) of (key, id) pairs,
  * the order shaders/sort.glsl:26-163 produces. */
 void oc_sort_pairs(const uint32_t* keys_in, const uint32_t* ids_in, uint32_t n,

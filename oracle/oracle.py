@@ -77,6 +77,10 @@ def lib():
         L.oc_cull.restype = None
         L.oc_cull.argtypes = [_f32p, C.c_uint32, C.POINTER(OcCamera), C.c_int, C.c_float, C.c_int,
                               _u32p, _u32p, _f32p, C.POINTER(C.c_uint32), _u32p]
+        L.oc_cull_anim.restype = None
+        L.oc_cull_anim.argtypes = [_f32p, C.c_uint32, C.POINTER(OcCamera), C.c_int, C.c_float, C.c_int,
+                                   C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
+                                   _u32p, _u32p, _f32p, C.POINTER(C.c_uint32), _u32p]
         L.oc_sort_pairs.restype = None
         L.oc_sort_pairs.argtypes = [_u32p, _u32p, C.c_uint32, _u32p, _u32p]
         L.oc_quad_rect.restype = C.c_int
@@ -141,6 +145,25 @@ def cull(rows: np.ndarray, cam: np.ndarray, sh_degree: int = 3, sh_lod_distance:
     cs = camera_struct(cam)
     lib().oc_cull(rows.reshape(-1), n, C.byref(cs), int(sh_degree), float(sh_lod_distance),
                   int(bool(collect_stats)), ids, keys, proj.reshape(-1), C.byref(vc), diag)
+    return ids, keys, proj, int(vc.value), diag
+
+
+def cull_anim(rows: np.ndarray, cam: np.ndarray, deltas: np.ndarray, scales: np.ndarray, state_a: int,
+              state_b: int = 0, weight: float = 0.0, sh_degree: int = 3):
+    """oc_cull with gsanim int8 deltas (deltas: (states, N, 48) int8, scales: 48 float32)."""
+    rows = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1, 64)
+    n = rows.shape[0]
+    deltas = np.ascontiguousarray(deltas, dtype=np.int8)
+    scales = np.ascontiguousarray(scales, dtype=np.float32)
+    ids = np.empty(n, np.uint32)
+    keys = np.empty(n, np.uint32)
+    proj = np.empty((n, 16), np.float32)
+    vc = C.c_uint32(0)
+    diag = np.zeros(8, np.uint32)
+    cs = camera_struct(cam)
+    lib().oc_cull_anim(rows.reshape(-1), n, C.byref(cs), int(sh_degree), 0.0, 1, deltas.ctypes.data,
+                       scales.ctypes.data, int(state_a), int(state_b), float(weight), ids, keys, proj.reshape(-1),
+                       C.byref(vc), diag)
     return ids, keys, proj, int(vc.value), diag
 
 
