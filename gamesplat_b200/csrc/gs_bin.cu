@@ -9,6 +9,11 @@
 // in s order at offsets found by a decoupled look-back over CTA tiles, so a
 // stable sort on the tile id alone keeps each tile's list in depth order.
 //
+// The CTA tile's entries are written by a load-balanced expansion (entry e
+// finds its splat by binary search over the CTA's offsets), so the stores are
+// coalesced however many tiles a splat covers; the tile ids' digit
+// histograms for the tile sort are accumulated on the way.
+//
 // Tile selection is conservative: the covered rectangle is intersected with
 // the bounding box of the ellipse where the Gaussian's alpha reaches 1/255
 // (power >= cutoff), widened by a pixel; per-pixel coverage and discards are
@@ -87,71 +92,78 @@ __device__ __forceinline__ BinItem bin_one(const BinParams& p, uint32_t s, uint3
     return it;
 }
 
-__device__ __forceinline__ void emit(const BinParams& p, uint32_t o, uint32_t s, int tx0, int tx1, int ty0, int ty1,
-                                     uint32_t first, uint32_t step) {
-    const int w = tx1 - tx0 + 1;
-    const uint32_t cnt = (uint32_t)(w * (ty1 - ty0 + 1));
-    for (uint32_t k = first; k < cnt; k += step) {
-        const uint32_t e = o + k;
-        if (e < p.entry_cap) {
-            const int ty = ty0 + (int)(k / (uint32_t)w), tx = tx0 + (int)(k % (uint32_t)w);
-            const uint32_t t = (uint32_t)(ty * p.tiles_x + tx);
-            p.entry_keys[e] = t;
-            p.entry_vals[e] = s;
-            atomicAdd(&p.tile_count[t], 1u);
-        }
-    }
-}
-
 __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
     __shared__ uint32_t scan_tmp[33];
-    __shared__ uint32_t s_tile, s_excl;
+    __shared__ uint32_t s_tile, s_excl, s_total;
+    __shared__ uint32_t s_off[kBinTile];    // exclusive entry offset of each splat in the CTA tile
+    __shared__ uint32_t s_org[kBinTile];    // tx0 | ty0 << 16 of its tile rectangle
+    __shared__ uint16_t s_w[kBinTile];      // width of its tile rectangle (tiles)
+    __shared__ uint32_t s_hist[3][256];     // tile-id digit histograms for the tile sort
     const uint32_t n_vis = p.fc->visible_count;
     const uint32_t num_tiles = (n_vis + kBinTile - 1) / kBinTile;
     const uint32_t* __restrict__ sorted_ids = p.depth_plan->vfinal;
     const float* camf = reinterpret_cast<const float*>(p.cam);
     const float vp_w = __ldg(camf + 32), vp_h = __ldg(camf + 33), ysign = __ldg(camf + 37);
-    const int lane = threadIdx.x & 31;
+    const int t = threadIdx.x;
+    for (int i = t; i < 3 * 256; i += kBinThreads) (&s_hist[0][0])[i] = 0u;
 
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&p.fc->bin_ticket, 1u);
+        if (t == 0) s_tile = atomicAdd(&p.fc->bin_ticket, 1u);
         __syncthreads();
         const uint32_t tile = s_tile;
         if (tile >= num_tiles) break;
-        // Items are blocked per thread (s = base + 4t + i) so that each
-        // thread's entries are contiguous and in s order.
-        const uint32_t sbase = tile * kBinTile + threadIdx.x * kBinItems;
+        const uint32_t base = tile * kBinTile;
+        // Splats striped over threads (coalesced id loads and record writes).
         uint32_t ids[kBinItems];
 #pragma unroll
-        for (int i = 0; i < kBinItems; ++i) ids[i] = sbase + i < n_vis ? sorted_ids[sbase + i] : kSentinel;
-        BinItem it[kBinItems];
-        uint32_t count = 0;
+        for (int i = 0; i < kBinItems; ++i) {
+            const uint32_t s = base + i * kBinThreads + t;
+            ids[i] = s < n_vis ? sorted_ids[s] : kSentinel;
+        }
 #pragma unroll
         for (int i = 0; i < kBinItems; ++i) {
-            it[i] = ids[i] != kSentinel ? bin_one(p, sbase + i, ids[i], vp_w, vp_h, ysign)
-                                        : BinItem{0u, 0, -1, 0, -1};
-            count += it[i].count;
+            const uint32_t s = base + i * kBinThreads + t;
+            const BinItem it = ids[i] != kSentinel ? bin_one(p, s, ids[i], vp_w, vp_h, ysign)
+                                                   : BinItem{0u, 0, -1, 0, -1};
+            const int slot = i * kBinThreads + t;
+            s_off[slot] = it.count;
+            s_org[slot] = (uint32_t)it.tx0 | ((uint32_t)it.ty0 << 16);
+            s_w[slot] = (uint16_t)(it.tx1 - it.tx0 + 1);
+        }
+        __syncthreads();
+        // Exclusive scan of the counts in splat order (blocked: 4 per thread).
+        uint32_t c[kBinItems], sum = 0;
+#pragma unroll
+        for (int k = 0; k < kBinItems; ++k) {
+            c[k] = s_off[t * kBinItems + k];
+            sum += c[k];
         }
         uint32_t total;
-        const uint32_t local = block_excl_scan(count, scan_tmp, &total);
-        if (threadIdx.x < 32) {
+        uint32_t run = block_excl_scan(sum, scan_tmp, &total);
+#pragma unroll
+        for (int k = 0; k < kBinItems; ++k) {
+            s_off[t * kBinItems + k] = run;
+            run += c[k];
+        }
+        if (t < 32) {
             // warp 0: publish the tile count, resolve the prefix by a
             // warp-cooperative look-back, publish the inclusive prefix
             u64* st = p.status + tile;
             uint32_t excl = 0;
             if (tile == 0) {
-                if (threadIdx.x == 0) st_release64(st, status_word(p.epoch, kFlagInc, total));
+                if (t == 0) st_release64(st, status_word(p.epoch, kFlagInc, total));
             } else {
-                if (threadIdx.x == 0) st_release64(st, status_word(p.epoch, kFlagAgg, total));
+                if (t == 0) st_release64(st, status_word(p.epoch, kFlagAgg, total));
                 bool to = false;
                 excl = lookback_warp(p.status, tile, p.epoch, &to);
-                if (threadIdx.x == 0) {
+                if (t == 0) {
                     if (to) atomicOr(&p.fc->error_flags, kErrBinLookback);
                     st_release64(st, status_word(p.epoch, kFlagInc, excl + total));
                 }
             }
-            if (threadIdx.x == 0) {
+            if (t == 0) {
                 s_excl = excl;
+                s_total = total;
                 if (tile == num_tiles - 1) {
                     const uint32_t e = excl + total;
                     p.fc->tile_entries = e < p.entry_cap ? e : p.entry_cap;
@@ -161,62 +173,48 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
             }
         }
         __syncthreads();
-        // Entries: small splats by their own thread, splats covering many
-        // tiles by the whole warp.
-        uint32_t o = s_excl + local;
-        constexpr uint32_t kBig = 8;
-#pragma unroll
-        for (int i = 0; i < kBinItems; ++i) {
-            const bool big = it[i].count > kBig;
-            if (!big && it[i].count) emit(p, o, sbase + i, it[i].tx0, it[i].tx1, it[i].ty0, it[i].ty1, 0u, 1u);
-            uint32_t bigmask = __ballot_sync(0xffffffffu, big);
-            while (bigmask) {
-                const int l = __ffs(bigmask) - 1;
-                bigmask &= bigmask - 1;
-                const uint32_t lo = __shfl_sync(0xffffffffu, o, l);
-                const uint32_t ls = __shfl_sync(0xffffffffu, sbase + i, l);
-                const int a = __shfl_sync(0xffffffffu, it[i].tx0, l), b = __shfl_sync(0xffffffffu, it[i].tx1, l);
-                const int c = __shfl_sync(0xffffffffu, it[i].ty0, l), d = __shfl_sync(0xffffffffu, it[i].ty1, l);
-                emit(p, lo, ls, a, b, c, d, (uint32_t)lane, 32u);
+        // Load-balanced expansion: entry e of the CTA tile belongs to the last
+        // splat whose offset is <= e (binary search over s_off).
+        const uint32_t excl = s_excl, cta_total = s_total;
+        for (uint32_t e = t; e < cta_total; e += kBinThreads) {
+            int lo = 0, hi = kBinTile - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_off[mid] <= e) lo = mid;
+                else hi = mid - 1;
             }
-            o += it[i].count;
+            const uint32_t k = e - s_off[lo];
+            const uint32_t w = s_w[lo], org = s_org[lo];
+            const uint32_t ty = (org >> 16) + k / w, tx = (org & 0xFFFFu) + k % w;
+            const uint32_t tid = ty * (uint32_t)p.tiles_x + tx;
+            const uint32_t o = excl + e;
+            if (o < p.entry_cap) {
+                p.entry_keys[o] = tid;
+                p.entry_vals[o] = base + (uint32_t)lo;
+                atomicAdd(&s_hist[0][tid & 255u], 1u);
+                atomicAdd(&s_hist[1][(tid >> 8) & 255u], 1u);
+                atomicAdd(&s_hist[2][(tid >> 16) & 255u], 1u);
+            }
         }
         __syncthreads();
     }
+    __syncthreads();
+    for (int i = t; i < 3 * 256; i += kBinThreads) {
+        const uint32_t c = (&s_hist[0][0])[i];
+        if (c) atomicAdd(p.tile_hist + i, c);
+    }
 }
 
-// From the per-tile entry counts (one CTA): each tile's [start, end) in the
-// tile-sorted entry array (exclusive scan over tiles) and the digit
-// histograms of the tile-sort passes.  After an entry-buffer overflow the
-// frame is invalid: every range is left empty.
-constexpr int kPlanThreads = 1024;
-__global__ void __launch_bounds__(kPlanThreads) tile_plan_kernel(const uint32_t* __restrict__ tile_count,
-                                                                 uint32_t num_tiles, int npasses,
-                                                                 const FrameCounters* fc, uint2* ranges,
-                                                                 uint32_t* tile_hist) {
-    __shared__ uint32_t s_hist[4][256];
-    __shared__ uint32_t warp_tmp[33];
-    for (int i = threadIdx.x; i < 4 * 256; i += kPlanThreads) (&s_hist[0][0])[i] = 0u;
-    __syncthreads();
-    const bool overflow = fc->tile_overflow != 0u;
-    const uint32_t per = (num_tiles + kPlanThreads - 1) / kPlanThreads;
-    const uint32_t t0 = threadIdx.x * per;
-    uint32_t sum = 0;
-    for (uint32_t t = t0; t < t0 + per && t < num_tiles; ++t) {
-        const uint32_t c = tile_count[t];
-        sum += c;
-        for (int ps = 0; ps < npasses; ++ps)
-            if (c) atomicAdd(&s_hist[ps][(t >> (8 * ps)) & 255u], c);
+__global__ void tile_ranges_kernel(const SortPlan* plan, const FrameCounters* fc, uint2* ranges,
+                                   uint32_t num_tiles) {
+    const uint32_t E = fc->tile_entries;
+    const uint32_t* keys = plan->kfinal;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const uint32_t k = keys[e];
+        if (k >= num_tiles) continue;  // only after a failed (timed-out) sort
+        if (e == 0 || keys[e - 1] != k) ranges[k].x = e;
+        if (e == E - 1 || keys[e + 1] != k) ranges[k].y = e + 1;
     }
-    uint32_t total;
-    uint32_t run = block_excl_scan(sum, warp_tmp, &total);
-    for (uint32_t t = t0; t < t0 + per && t < num_tiles; ++t) {
-        const uint32_t c = tile_count[t];
-        ranges[t] = overflow ? make_uint2(0u, 0u) : make_uint2(run, run + c);
-        run += c;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < npasses * 256; i += kPlanThreads) tile_hist[i] = (&s_hist[0][0])[i];
 }
 
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s) {
@@ -228,10 +226,12 @@ int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_
     return 1;
 }
 
-int launch_tile_plan(const uint32_t* tile_count, uint32_t num_tiles, int tile_bits, const FrameCounters* fc,
-                     uint2* ranges, uint32_t* tile_hist, cudaStream_t s) {
-    const int npasses = (tile_bits + 7) / 8;
-    tile_plan_kernel<<<1, kPlanThreads, 0, s>>>(tile_count, num_tiles, npasses, fc, ranges, tile_hist);
+int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
+                       uint32_t num_tiles, uint32_t num_sms, cudaStream_t s) {
+    uint32_t grid = (entry_cap + 255) / 256;
+    if (grid > num_sms * 8) grid = num_sms * 8;
+    if (grid == 0) grid = 1;
+    tile_ranges_kernel<<<grid, 256, 0, s>>>(tile_plan, fc, ranges, num_tiles);
     return 1;
 }
 

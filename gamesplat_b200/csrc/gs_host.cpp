@@ -76,7 +76,6 @@ struct gs_ctx {
     uint32_t* depth_hist = nullptr;
     uint32_t* tile_hist = nullptr;
     uint2* tile_ranges = nullptr;
-    uint32_t* tile_count = nullptr;
     uint32_t tiles_cap = 0;
 
     // gsanim appearance deltas (renderer animation buffer, src/renderer.cpp:824-841)
@@ -253,7 +252,7 @@ int ensure_targets(gs_ctx* c, int w, int h) {
     if (c->width == w && c->height == h && c->ctrl) return GS_OK;
     release_targets(c);
     c->tiles_cap = (uint32_t)(tx * ty);
-    // control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges | tile counts
+    // control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges
     size_t off = 0;
     auto place = [&](size_t bytes) {
         size_t o = off;
@@ -266,7 +265,6 @@ int ensure_targets(gs_ctx* c, int w, int h) {
     size_t o_dh = place(4 * 256 * 4);
     size_t o_th = place(4 * 256 * 4);
     size_t o_tr = place((size_t)c->tiles_cap * sizeof(uint2));
-    size_t o_tc = place((size_t)c->tiles_cap * sizeof(uint32_t));
     c->ctrl_bytes = off;
     GS_CUDA(c, dalloc(reinterpret_cast<char**>(&c->ctrl), c->ctrl_bytes));
     char* base = static_cast<char*>(c->ctrl);
@@ -276,7 +274,6 @@ int ensure_targets(gs_ctx* c, int w, int h) {
     c->depth_hist = reinterpret_cast<uint32_t*>(base + o_dh);
     c->tile_hist = reinterpret_cast<uint32_t*>(base + o_th);
     c->tile_ranges = reinterpret_cast<uint2*>(base + o_tr);
-    c->tile_count = reinterpret_cast<uint32_t*>(base + o_tc);
     GS_CUDA(c, cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream));
     GS_CUDA(c, dalloc(&c->out16, (size_t)w * h * 8));
     c->width = w;
@@ -375,7 +372,7 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         StageScope sc(c, ST_BIN);
         if (reset_ranges) {
             // A second pass in the same frame: clear ranges, counters and the tile-sort plan.
-            cudaMemsetAsync(c->tile_count, 0, (size_t)c->tiles_cap * sizeof(uint32_t), c->stream);
+            cudaMemsetAsync(c->tile_ranges, 0, (size_t)c->tiles_cap * sizeof(uint2), c->stream);
             cudaMemsetAsync(c->tile_plan, 0, sizeof(SortPlan), c->stream);
             cudaMemsetAsync(c->tile_hist, 0, 4 * 256 * 4, c->stream);
             // bin_ticket, tile_entries, tile_overflow are adjacent in FrameCounters.
@@ -398,13 +395,12 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         p.entry_keys = c->ekeys[1];
         p.entry_vals = c->evals[1];
         p.entry_cap = c->entry_cap;
-        p.tile_count = c->tile_count;
+        p.tile_hist = c->tile_hist;
         p.status = c->bin_status;
         p.epoch = c->epoch;
         p.fc = c->fc;
         sc.add(gs::launch_bin(p, c->n, c->num_sms, c->stream));
-        sc.add(gs::launch_tile_plan(c->tile_count, c->tiles_cap, entry_bits(c->tiles_cap), c->fc, c->tile_ranges,
-                                    c->tile_hist, c->stream));
+
     }
     {
         StageScope sc(c, ST_TILE_SORT);
@@ -420,7 +416,7 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         p.count_cap = c->entry_cap;
         p.begin_bit = 0;
         p.end_bit = entry_bits(c->tiles_cap);
-        p.hist = c->tile_hist;    // from the per-tile counts
+        p.hist = c->tile_hist;    // accumulated by the bin kernel
         p.hist_ready = 1;
         p.plan = c->tile_plan;
         p.status = c->tsort_status;
@@ -428,6 +424,8 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         p.epoch = c->epoch;
         p.error_flags = &c->fc->error_flags;
         sc.add(gs::launch_sort(p, c->num_sms, c->stream));
+        sc.add(gs::launch_tile_ranges(c->tile_plan, c->fc, c->entry_cap, c->tile_ranges, c->tiles_cap, c->num_sms,
+                                       c->stream));
     }
 }
 

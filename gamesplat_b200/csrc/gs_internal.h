@@ -138,7 +138,7 @@ struct BinParams {
     uint32_t* entry_keys;            // tile id per entry
     uint32_t* entry_vals;            // sorted position per entry
     uint32_t entry_cap;
-    uint32_t* tile_count;            // entries written per screen tile (zeroed per pass)
+    uint32_t* tile_hist;             // 3 x 256 digit histograms of the tile ids (zeroed per pass)
     unsigned long long* status;      // per-CTA-tile look-back words (epoch-tagged)
     uint32_t epoch;
     FrameCounters* fc;
@@ -162,9 +162,8 @@ struct RasterParams {
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s);
-// Tile ranges and tile-sort digit histograms from the per-tile entry counts.
-int launch_tile_plan(const uint32_t* tile_count, uint32_t num_tiles, int tile_bits, const FrameCounters* fc,
-                     uint2* ranges, uint32_t* tile_hist, cudaStream_t s);
+int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
+                       uint32_t num_tiles, uint32_t num_sms, cudaStream_t s);
 int launch_raster_alpha(const RasterParams& p, cudaStream_t s);
 int launch_raster_stochastic(const RasterParams& p, cudaStream_t s);
 
