@@ -98,6 +98,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu capture of the
+    benchmark workload (profiles/traffic_room3m_1080p.txt), or None."""
+    p = ROOT / "profiles" / "traffic_room3m_1080p.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) == 2 and parts[0] == kernel:
+            return int(parts[1])
+    return None
+
+
 def orbit_cameras(width=WIDTH, height=HEIGHT):
     from gamesplat_b200 import renderer as R
     from gamesplat_b200 import scene
@@ -191,7 +204,7 @@ def run_ours(args):
 
     world, rank, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    from gamesplat_b200 import Renderer
+    from gamesplat_b200 import Renderer, replicas
 
     rows = make_rows(args.gaussians)
     n = rows.shape[0]
@@ -203,7 +216,7 @@ def run_ours(args):
     out = torch.empty(WIDTH * HEIGHT * 4, dtype=torch.float16, device="cuda")
 
     def frame(i):
-        return cams[(rank + i * world) % FRAMES]
+        return cams[replicas.frame_index(rank, world, i, FRAMES)]
 
     # untimed warm-up (also sizes the tile-entry buffers via the host path)
     r.draw_frame(frame(0))
@@ -239,18 +252,21 @@ def run_ours(args):
     stages = r.stage_times(reset=True)
     stats = r.stats()
     r.profile(False)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if pg:
-        pg.all_reduce(ms_t, op=pg.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    fps = world * args.steps / (ms_max / 1000.0)
+    ms_max = replicas.reduce_max(ms, pg, "cuda")
+    fps = replicas.whole_job_rate(args.steps, world, ms_max / 1000.0)
 
-    # visible count / entries averaged over the orbit for the roofline units
-    vis_counts = []
+    # visible count and quad-area diagnostics over the timed frames' cameras
+    # (outside the timed region) for the roofline units
+    vis_counts, quad_frags = [], []
+    r.set(splat_diagnostics_enabled=1)
     for i in range(min(args.steps, 8)):
         r.draw_frame(frame(args.warmup + i), out_ptr=out.data_ptr())
-        vis_counts.append(r.stats().visible_count)
+        st_i = r.stats()
+        vis_counts.append(st_i.visible_count)
+        quad_frags.append(st_i.diagnostics[0] * 1024.0)   # shaders/cull.glsl:297-299 (kpix)
+    r.set(splat_diagnostics_enabled=0)
     n_vis = float(np.mean(vis_counts))
+    frags = float(np.mean(quad_frags))
 
     # e2e through the public API with host buffers (gs_render_host)
     e2e_fps = None
@@ -266,14 +282,12 @@ def run_ours(args):
         barrier()
         t0 = time.perf_counter()
         for i in range(args.steps):
-            st = L.lib().gs_render_host(r._ctx, C.byref(camsC[(rank + (args.warmup + i) * world) % FRAMES]),
+            st = L.lib().gs_render_host(r._ctx, C.byref(camsC[replicas.frame_index(rank, world, args.warmup + i,
+                                                                                    FRAMES)]),
                                         host_img.ctypes.data)
             L.check(st, "gs_render_host", r._ctx)
         dt = time.perf_counter() - t0
-        dt_t = torch.tensor([dt], dtype=torch.float64, device="cuda")
-        if pg:
-            pg.all_reduce(dt_t, op=pg.ReduceOp.MAX)
-        e2e_fps = world * args.steps / float(dt_t.item())
+        e2e_fps = replicas.whole_job_rate(args.steps, world, replicas.reduce_max(dt, pg, "cuda"))
 
     r.destroy()
     if pg:
@@ -291,11 +305,20 @@ def run_ours(args):
         "cull": 16.0 * n + 272.0 * n_vis + 8.0 * n,
         "sort": 68.0 * n_vis,
     }
-    roof_stage = dominant if dominant in alg else "cull"
+    # The roofline kernel is the HBM-bound cull; the raster (the dominant
+    # stage) is issue-bound and reported separately in fragments/s.
+    roof_stage = "cull"
     achieved = alg[roof_stage] / (per_frame[roof_stage] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": roof_stage, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": alg[roof_stage]}
+    traffic = profiled_traffic("cull_kernel") if n == 3_000_000 else None
+    roofline = {"bound": "hbm", "kernel": "cull_kernel", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg[roof_stage],
+                "traffic_source": "profiles/cull_kernel_room3m_1080p.md" if traffic else None}
+    raster = {"kernel": "raster_kernel<0>", "ms_per_frame": per_frame.get("raster"),
+              "share_of_frame": per_frame.get("raster", 0.0) / (ms_max / args.steps),
+              "bound": "instruction issue (ALU pipe)", "quad_fragments_per_frame": frags,
+              "reference_equivalent_fragments_per_s": frags / (per_frame["raster"] / 1000.0)
+              if per_frame.get("raster") else None}
     hbm_stages = {}
     for k in alg:
         if k in per_frame:
@@ -322,6 +345,8 @@ def run_ours(args):
                 "d2h_bytes_per_step": WIDTH * HEIGHT * 8},
         "gpu_launches": int(launches_per_frame) * args.steps,
         "roofline": roofline,
+        "dominant_stage": dominant,
+        "raster": raster,
         "stages_ms_per_frame": per_frame,
         "hbm_stages": hbm_stages,
         "visible_per_frame": n_vis,
