@@ -68,8 +68,9 @@ __device__ __forceinline__ BinItem bin_one(const BinParams& p, uint32_t s, uint3
     rec.conic_x = cd.x;
     rec.conic_2y = mul(2.0f, cd.y);
     rec.conic_z = cd.z;
-    rec.opacity = co.w;
-    rec.cutoff = cutoff;
+    rec.log2_opacity = log2f(co.w);
+    // cutoff <= 0 here; s_max = -2 cutoff is exact (cutoff is a normal float)
+    rec.s_max = cutoff == 0.0f ? __int_as_float(1) : mul(-2.0f, cutoff);
     rec.r = co.x;
     rec.g = co.y;
     rec.b = co.z;
@@ -82,7 +83,7 @@ __device__ __forceinline__ BinItem bin_one(const BinParams& p, uint32_t s, uint3
     rec.depth24 = (uint32_t)__float2int_rn(mul(g_clamp(zw, 0.0f, 1.0f), 16777215.0f));
     rec.splat_id = id;
     rec.hash_z = add((float)id, p.frame_seed);
-    rec.pad = 0u;
+    rec.opacity = co.w;
     float4* dst = reinterpret_cast<float4*>(p.records + s);
     const float4* src = reinterpret_cast<const float4*>(&rec);
     dst[0] = src[0];
@@ -151,14 +152,14 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
             u64* st = p.status + tile;
             uint32_t excl = 0;
             if (tile == 0) {
-                if (t == 0) st_release64(st, status_word(p.epoch, kFlagInc, total));
+                if (t == 0) st_relaxed64(st, status_word(p.epoch, kFlagInc, total));
             } else {
-                if (t == 0) st_release64(st, status_word(p.epoch, kFlagAgg, total));
+                if (t == 0) st_relaxed64(st, status_word(p.epoch, kFlagAgg, total));
                 bool to = false;
                 excl = lookback_warp(p.status, tile, p.epoch, &to);
                 if (t == 0) {
                     if (to) atomicOr(&p.fc->error_flags, kErrBinLookback);
-                    st_release64(st, status_word(p.epoch, kFlagInc, excl + total));
+                    st_relaxed64(st, status_word(p.epoch, kFlagInc, excl + total));
                 }
             }
             if (t == 0) {

@@ -215,13 +215,11 @@ constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1u;
 typedef unsigned long long u64;
 
-__device__ __forceinline__ void st_release64(u64* p, u64 v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ u64 ld_acquire64(const u64* p) {
-    u64 v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
+// Status words carry their whole message (flag + value); the data a tile
+// writes is read only by later kernels, so publishing needs no release
+// ordering, and a relaxed GPU-scope store avoids a memory barrier per tile.
+__device__ __forceinline__ void st_relaxed64(u64* p, u64 v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 // Look-backs only read the status words themselves (no data published with
 // them), so relaxed GPU-scope loads of the atomically written 64-bit words
@@ -233,30 +231,6 @@ __device__ __forceinline__ u64 ld_relaxed64(const u64* p) {
 }
 __device__ __forceinline__ u64 status_word(uint32_t epoch, uint32_t flag, uint32_t value) {
     return ((u64)epoch << 32) | (u64)(flag | (value & kValMask));
-}
-
-// Exclusive prefix of tile `tile` from its predecessors' status words
-// status[(tile-1)*stride], ... with a bounded spin.  Sets *timed_out if a wait
-// exceeded kSpinLimit (the result is then incomplete but the kernel ends).
-__device__ __forceinline__ uint32_t lookback(const u64* status, uint32_t stride, uint32_t tile, uint32_t epoch,
-                                             bool* timed_out) {
-    uint32_t excl = 0;
-    long long j = (long long)tile - 1;
-    uint32_t spins = 0;
-    while (j >= 0) {
-        u64 w = ld_acquire64(status + (size_t)j * stride);
-        uint32_t lo = (uint32_t)w;
-        uint32_t flag = lo & ~kValMask;
-        if ((uint32_t)(w >> 32) != epoch || flag == 0u) {
-            if (++spins > kSpinLimit) { *timed_out = true; break; }
-            if (spins > 64) __nanosleep(32);
-            continue;
-        }
-        excl += lo & kValMask;
-        if (flag == kFlagInc) break;
-        --j;
-    }
-    return excl;
 }
 
 // Single-thread look-back that reads 8 predecessor words per step

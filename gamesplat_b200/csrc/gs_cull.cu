@@ -20,6 +20,7 @@
 
 #include "gs_common.cuh"
 #include "gs_internal.h"
+#include "gs_tma.cuh"
 
 namespace gs {
 
@@ -204,30 +205,19 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
     out[3] = make_float4(a, mul(b, cam.ysign), c, det);
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
-                 "l"(gmem_src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int kPending>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(kPending) : "memory");
-}
-
-// Issue the async copies of chunks 1..kChunks-1 of the visible rows of one
-// 32-row round into `stage` (consecutive lanes -> consecutive 16-B chunks).
+// Stage the visible rows of one 32-row round: lane l copies the first
+// kChunks 16-byte chunks of row wbase + l (if visible) to stage row l with
+// one TMA bulk copy; completion is counted on `bar`.
 template <int kChunks>
-__device__ __forceinline__ void stage_round(const float4* rows, uint32_t wbase, uint32_t mask, const uint8_t* list,
-                                            float4* stage, int lane) {
-    constexpr int per = kChunks - 1;
-    const int total = __popc(mask) * per;
-    for (int u = lane; u < total; u += 32) {
-        const int v = u / per;
-        const int ch = 1 + (u - v * per);
-        const int rl = list[v];
-        cp_async16(&stage[rl * kStageStride + ch], rows + (size_t)(wbase + rl) * 16 + ch);
-    }
+__device__ __forceinline__ void stage_round(const float4* rows, uint32_t wbase, uint32_t mask, float4* stage,
+                                            uint64_t* bar, int lane) {
+    if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)__popc(mask) * (uint32_t)(kChunks * 16));
+    __syncwarp();
+    // order this lane's earlier generic accesses to its stage row (reads, and
+    // the in-place gsanim deltas) before the async-proxy refill
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if ((mask >> lane) & 1u)
+        bulk_g2s(stage + lane * kStageStride, rows + (size_t)(wbase + lane) * 16, (uint32_t)(kChunks * 16), bar);
 }
 
 // gsanim int8 appearance deltas applied in place to a staged row
@@ -260,24 +250,33 @@ __device__ void animate_row(const CullParams& p, uint32_t row, float4* staged, f
 }
 
 // Every warp is independent: it takes 128-Gaussian warp tiles in ticket
-// order, stages round r+1's visible rows while it projects round r, and
-// places its visible (key, id) pairs with a warp-level decoupled look-back.
+// order, tests visibility from the rows' first 16 bytes, stages round r+1's
+// visible rows (TMA bulk copies) while it projects round r, and places its
+// visible (key, id) pairs with a warp-level decoupled look-back.  The round
+// loop is not unrolled (one copy of the projection code: the SH degree 3 body
+// is large), so per-round values are picked out of small register arrays.
 template <int kChunks>  // 16-byte chunks of a row the SH degree needs: 4, 7, 10 or 16
 __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
     extern __shared__ float4 smem4[];
-    __shared__ uint8_t vis_list[kCullWarps][kCullRounds][32];
+    __shared__ __align__(8) uint64_t s_bar[kCullWarps][2];
     __shared__ uint32_t s_hist[4][256];   // digit histograms of the emitted keys (for the depth sort)
     for (int i = threadIdx.x; i < 4 * 256; i += kCullThreads) (&s_hist[0][0])[i] = 0u;
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float4* stage0 = smem4 + (size_t)warp * 2 * 32 * kStageStride;
-    float4* stage1 = stage0 + 32 * kStageStride;
+    if (lane == 0) {
+        mbar_init(&s_bar[warp][0], 1);
+        mbar_init(&s_bar[warp][1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    float4* const stage0 = smem4 + (size_t)warp * 2 * 32 * kStageStride;   // stage b at stage0 + b * 32 rows
+    uint32_t phase = 0;   // bit b: parity of the next completion of bar[b]
     const uint32_t num_tiles = (p.n + kCullTile - 1) / kCullTile;
     CamRegs cam;
     load_cam(p.cam, cam);
     const uint32_t lt = (1u << lane) - 1u;
     const bool animated = p.anim_deltas != nullptr &&
                           (p.anim_state_a != 0 || (p.anim_weight > 0.0f && p.anim_state_b != 0));
+    bool stage_failed = false;
 
     for (;;) {
         uint32_t tile = 0;
@@ -286,73 +285,71 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
         if (tile >= num_tiles) break;
         const uint32_t base = tile * kCullTile;
 
-        float4 c0[kCullRounds];
-#pragma unroll
-        for (int r = 0; r < kCullRounds; ++r) {
-            const uint32_t g = base + r * 32 + lane;
-            c0[r] = g < p.n ? __ldg(p.rows + (size_t)g * 16) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        float vx[kCullRounds], vy[kCullRounds], vz[kCullRounds];
         uint32_t mask[kCullRounds];
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) {
             const uint32_t g = base + r * 32 + lane;
+            const float4 c0 = g < p.n ? __ldg(p.rows + (size_t)g * 16) : make_float4(0.f, 0.f, 0.f, 0.f);
             // p_view = view * vec4(position, 1.0)  (shaders/cull.glsl:209-220)
-            vx[r] = add(add(add(mul(cam.V[0], c0[r].x), mul(cam.V[4], c0[r].y)), mul(cam.V[8], c0[r].z)), cam.V[12]);
-            vy[r] = add(add(add(mul(cam.V[1], c0[r].x), mul(cam.V[5], c0[r].y)), mul(cam.V[9], c0[r].z)), cam.V[13]);
-            vz[r] = add(add(add(mul(cam.V[2], c0[r].x), mul(cam.V[6], c0[r].y)), mul(cam.V[10], c0[r].z)), cam.V[14]);
-            bool visible = g < p.n && (vz[r] <= -0.2f);
+            const float vx = add(add(add(mul(cam.V[0], c0.x), mul(cam.V[4], c0.y)), mul(cam.V[8], c0.z)), cam.V[12]);
+            const float vy = add(add(add(mul(cam.V[1], c0.x), mul(cam.V[5], c0.y)), mul(cam.V[9], c0.z)), cam.V[13]);
+            const float vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
+            bool visible = g < p.n && (vz <= -0.2f);
             if (visible) {
-                float inv_z = dv(-1.0f, vz[r]);
-                float ndc_x = add(mul(mul(mul(cam.P0, vx[r]), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P0, vx[r]), cam.ortho));
-                float ndc_y = add(mul(mul(mul(cam.P5, vy[r]), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P5, vy[r]), cam.ortho));
+                float inv_z = dv(-1.0f, vz);
+                float ndc_x = add(mul(mul(mul(cam.P0, vx), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P0, vx), cam.ortho));
+                float ndc_y = add(mul(mul(mul(cam.P5, vy), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P5, vy), cam.ortho));
                 visible = fabsf(ndc_x) <= 1.3f && fabsf(ndc_y) <= 1.3f;
             }
             mask[r] = __ballot_sync(0xffffffffu, visible);
-            if (visible) vis_list[warp][r][__popc(mask[r] & lt)] = (uint8_t)lane;
         }
-        __syncwarp();
-        stage_round<kChunks>(p.rows, base, mask[0], vis_list[warp][0], stage0, lane);
-        cp_async_commit();
+        stage_round<kChunks>(p.rows, base, mask[0], stage0, &s_bar[warp][0], lane);
         // The tile's visible count is known now: publish it before projecting.
         uint32_t total = 0;
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) total += __popc(mask[r]);
         if (lane == 0)
-            st_release64(p.status + tile, status_word(p.epoch, tile == 0 ? kFlagInc : kFlagAgg, total));
+            st_relaxed64(p.status + tile, status_word(p.epoch, tile == 0 ? kFlagInc : kFlagAgg, total));
 
         uint32_t keys[kCullRounds];
         uint32_t d0 = 0, d2 = 0, d3 = 0, d4 = 0, d6 = 0, d7 = 0, m1 = 0, m5 = 0;
-#pragma unroll
+#pragma unroll 1
         for (int r = 0; r < kCullRounds; ++r) {
-            float4* cur = (r & 1) ? stage1 : stage0;
-            if (r + 1 < kCullRounds) {
-                stage_round<kChunks>(p.rows, base + (r + 1) * 32, mask[r + 1], vis_list[warp][r + 1],
-                                     (r & 1) ? stage0 : stage1, lane);
-                cp_async_commit();
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
+            uint32_t mr = mask[0], mnext = 0u;
+#pragma unroll
+            for (int k = 1; k < kCullRounds; ++k) {
+                if (r == k) mr = mask[k];
+                if (r + 1 == k) mnext = mask[k];
             }
-            __syncwarp();
+            const int b = r & 1;
+            if (r + 1 < kCullRounds)
+                stage_round<kChunks>(p.rows, base + (r + 1) * 32, mnext, stage0 + (b ^ 1) * 32 * kStageStride,
+                                     &s_bar[warp][b ^ 1], lane);
+            if (!mbar_wait_bounded(&s_bar[warp][b], (phase >> b) & 1u)) stage_failed = true;
+            phase ^= 1u << b;
+            float4* const cur = stage0 + b * 32 * kStageStride;
             const uint32_t g = base + r * 32 + lane;
-            const bool visible = (mask[r] >> lane) & 1u;
-            keys[r] = 0u;
+            const bool visible = (mr >> lane) & 1u;
+            uint32_t key = 0u;
             if (visible) {
                 float4 rec[4];
                 float qa, gp;
+                float4* row = cur + lane * kStageStride;
+                const float4 c0 = row[0];
+                const float vx = add(add(add(mul(cam.V[0], c0.x), mul(cam.V[4], c0.y)), mul(cam.V[8], c0.z)), cam.V[12]);
+                const float vy = add(add(add(mul(cam.V[1], c0.x), mul(cam.V[5], c0.y)), mul(cam.V[9], c0.z)), cam.V[13]);
+                const float vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
                 if (animated) {
-                    float4 c3 = cur[lane * kStageStride + 3];
-                    animate_row(p, g, cur + lane * kStageStride, c3);
+                    float4 c3 = row[3];
+                    animate_row(p, g, row, c3);
                 }
-                project_visible(cur + lane * kStageStride, c0[r], vx[r], vy[r], vz[r], cam, p.sh_degree,
-                                p.sh_lod_distance, rec, &qa, &gp);
+                project_visible(row, c0, vx, vy, vz, cam, p.sh_degree, p.sh_lod_distance, rec, &qa, &gp);
                 float4* dst = p.projected + (size_t)g * 4;
                 dst[0] = rec[0];
                 dst[1] = rec[1];
                 dst[2] = rec[2];
                 dst[3] = rec[3];
-                keys[r] = 0xFFFFFFFFu - __float_as_uint(g_max(-vz[r], 0.0f));
+                key = 0xFFFFFFFFu - __float_as_uint(g_max(-vz, 0.0f));
                 if (p.collect_stats) {
                     // shaders/cull.glsl:296-318
                     const uint32_t qpx = g_f2u_sat(g_min(g_max(0.0f, qa), 4294967295.0f));
@@ -373,6 +370,10 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
                 dst[2] = make_float4(1.f, 0.f, 1.f, 1.f);
                 dst[3] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
+#pragma unroll
+            for (int k = 0; k < kCullRounds; ++k)
+                if (r == k) keys[k] = key;
+            // every lane is done reading stage[b] before round r + 2 refills it
             __syncwarp();
         }
         if (p.collect_stats) {
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
             excl = lookback_warp(p.status, tile, p.epoch, &to);
             if (lane == 0) {
                 if (to) atomicOr(&p.fc->error_flags, kErrCullLookback);
-                st_release64(p.status + tile, status_word(p.epoch, kFlagInc, excl + total));
+                st_relaxed64(p.status + tile, status_word(p.epoch, kFlagInc, excl + total));
             }
         }
         if (lane == 0 && tile == num_tiles - 1) p.fc->visible_count = excl + total;
@@ -415,6 +416,7 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
             before += __popc(mask[r]);
         }
     }
+    if (stage_failed) atomicOr(&p.fc->error_flags, kErrCullStage);
     __syncthreads();
     for (int i = threadIdx.x; i < 4 * 256; i += kCullThreads) {
         const uint32_t c = (&s_hist[0][0])[i];

@@ -17,6 +17,7 @@ enum : uint32_t {
     kErrRasterWait = 1u << 3,
     kErrTileOverflow = 1u << 4,
     kErrGpsWait = 1u << 5,
+    kErrCullStage = 1u << 6,
 };
 
 // Small per-frame device control block.  Zeroed at the start of each frame
@@ -74,16 +75,22 @@ constexpr int kTileH = 16;
 
 // Raster record: one per visible splat in depth-sorted order, 64 bytes,
 // staged into shared memory by TMA bulk copies.
+//
+// The rasterizer tests the splat's quadratic form s = conic(d) (the power is
+// -0.5 s) instead of the power: "power <= 0 && !(power < cutoff)" holds
+// exactly when -kSMin <= s <= s_max, with s_max = -2 cutoff, or the smallest
+// subnormal when cutoff == 0 (multiplying by -0.5 is exact except for
+// subnormal s, and those cases are what the two bounds absorb).
 struct __align__(16) RasterRecord {
     float cx, cy, conic_x, conic_2y;     // centre (+jitter), conic.x, 2*conic.y
-    float conic_z, opacity, cutoff, r;   // cutoff = log((1/255)/max(opacity,1e-8))
+    float conic_z, log2_opacity, s_max, r;
     float g, b;
     uint32_t rect_x;                     // i0 | i1 << 16  (candidate pixel columns: quad coverage
     uint32_t rect_y;                     // j0 | j1 << 16   intersected with the alpha >= 1/255 box, GL rows)
     uint32_t depth24;                    // window depth as D24 (stochastic depth test)
     uint32_t splat_id;                   // original Gaussian index
     float hash_z;                        // float(splat_id) + frame_seed
-    uint32_t pad;
+    float opacity;
 };
 static_assert(sizeof(RasterRecord) == 64, "RasterRecord must be 64 bytes");
 

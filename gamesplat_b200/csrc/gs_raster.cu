@@ -5,22 +5,31 @@
 // One CTA per 16x16 pixel tile, two pixels per thread, each warp an 8x8 pixel
 // block (GL window coordinates, row 0 at the bottom; the image is written
 // top row first).  Control flow is warp-uniform: lanes never diverge around
-// the per-splat loop (per-pixel work is predicated), a warp skips splats whose
-// rectangle misses its block and leaves the loop when all its pixels are done.  The tile's
-// depth-ordered splat list is walked front to back (reverse of the
-// reference's back-to-front draw order, so equal depth keys are visited in
-// descending splat index, which reproduces "later instance on top").
-// Batches of 128 64-byte RasterRecords are staged into shared memory by TMA
-// 1-D bulk copies (cp.async.bulk, completion on an mbarrier), double
-// buffered so the next batch lands while the current one is composited.
+// the per-splat loop (per-pixel work is predicated or selected), a warp skips
+// splats whose rectangle misses its block and leaves the loop when all its
+// pixels are done.  The tile's depth-ordered splat list is walked front to
+// back (reverse of the reference's back-to-front draw order, so equal depth
+// keys are visited in descending splat index, which reproduces "later
+// instance on top").  Batches of 128 64-byte RasterRecords are staged into
+// shared memory by TMA 1-D bulk copies (cp.async.bulk, completion on an
+// mbarrier), double buffered so the next batch lands while the current one
+// is composited.  When a batch lands, one thread per record turns its pixel
+// rectangle into tile-relative column and row bit masks, so a pixel's
+// coverage test is one AND and one compare.
+//
+// The two pixels of a thread share a column; their arithmetic runs as packed
+// f32x2 operations (add/mul/fma .rn on float pairs, each element rounded like
+// the scalar operation), which halves the issue slots of the per-pixel math.
 //
 // Alpha mode: premultiplied "over" in FP32, front to back:
-//   C += T * alpha * rgb,  T *= 1 - alpha,  output (C + T*bg, 1 - T),
+//   C += T * alpha * rgb,  T -= T * alpha,  output (C + T*bg, 1 - T),
 // which equals the reference's back-to-front ONE / ONE_MINUS_SRC_ALPHA
-// blend into a (bg,bg,bg,0) target up to FP32 rounding.  A pixel stops once
-// T < 2^-13: the skipped remainder is below T * max(rgb, bg).  Coverage
-// (quad rectangle) and the two discards (power > 0, power < cutoff) are
-// evaluated bit-exactly like the CPU oracle; alpha uses the hardware exp.
+// blend into a (bg,bg,bg,0) target up to FP32 rounding.  A warp stops once
+// T < 2^-13 for all its pixels: the skipped remainder is below T * max(rgb, bg).
+// Coverage (quad rectangle) and the two discards (power > 0, power < cutoff)
+// are evaluated bit-exactly like the CPU oracle, on the quadratic form s with
+// the bounds of RasterRecord; alpha = min(2^(s * -0.5 log2(e) + log2(opacity)),
+// 0.99) uses the hardware exp2.
 //
 // Stochastic mode: a fragment is kept iff hash13(fragcoord, id + seed) <
 // alpha; the depth test (LESS, writes on) keeps the kept fragment with the
@@ -40,6 +49,7 @@ constexpr int kRasterThreads = kTileW * kTileH / 2;   // two pixels per thread
 constexpr int kBatch = 128;
 constexpr float kTransmittanceMin = 1.0f / 8192.0f;
 constexpr uint32_t kDepthMargin = 8;
+constexpr float kNegHalfLog2e = -0.72134752044448170368f;   // -0.5 / ln(2)
 
 __device__ __forceinline__ float hash13(float p0, float p1, float p2) {
     p0 = g_fract(mul(p0, 0.1031f));
@@ -52,30 +62,22 @@ __device__ __forceinline__ float hash13(float p0, float p1, float p2) {
     return g_fract(mul(add(p0, p1), p2));
 }
 
-struct AlphaState {
-    float T, c0, c1, c2;
-};
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
 
 struct StochState {
     uint32_t best_d24, best_id;
     float r, g, b;
 };
 
-// Per-pixel compositing state and the per-pixel step of each mode.
-__device__ __forceinline__ void alpha_step(AlphaState& A, bool& done, float power, float opacity, float r, float g,
-                                           float b) {
-    const float alpha = fminf(opacity * __expf(power), 0.99f);
-    const float w = alpha * A.T;
-    A.c0 = fmaf(w, r, A.c0);
-    A.c1 = fmaf(w, g, A.c1);
-    A.c2 = fmaf(w, b, A.c2);
-    A.T = A.T * (1.0f - alpha);
-    done = A.T < kTransmittanceMin;
-}
-
-__device__ __forceinline__ void stoch_step(StochState& S, float power, float opacity, float fcx, float fcy,
+__device__ __forceinline__ void stoch_step(StochState& S, float s, float opacity, float fcx, float fcy,
                                            float hz, uint32_t z24, uint32_t id, float r, float g, float b) {
-    const float alpha = g_min(mul(opacity, det_expf(power)), 0.99f);
+    const float alpha = g_min(mul(opacity, det_expf(mul(-0.5f, s))), 0.99f);
     const float rnd = hash13(fcx, fcy, hz);
     if (rnd < alpha) {
         S.best_d24 = z24;
@@ -86,15 +88,12 @@ __device__ __forceinline__ void stoch_step(StochState& S, float power, float opa
     }
 }
 
-__device__ __forceinline__ void write_pixel_alpha(const RasterParams& p, int px, int py, const AlphaState& A) {
-    const size_t o = (size_t)(p.height - 1 - py) * p.width + px;
-    const float r = fmaf(A.T, p.bg, A.c0), g = fmaf(A.T, p.bg, A.c1), b = fmaf(A.T, p.bg, A.c2);
-    const float a = 1.0f - A.T;
+__device__ __forceinline__ void write_rgba16f(uint16_t* out, size_t o, float r, float g, float b, float a) {
     __half2 h01 = __floats2half2_rn(r, g), h23 = __floats2half2_rn(b, a);
     uint2 packed;
     packed.x = *reinterpret_cast<uint32_t*>(&h01);
     packed.y = *reinterpret_cast<uint32_t*>(&h23);
-    reinterpret_cast<uint2*>(p.out_rgba16f)[o] = packed;
+    reinterpret_cast<uint2*>(out)[o] = packed;
 }
 
 __device__ __forceinline__ void write_pixel_stoch(const RasterParams& p, int px, int py, const StochState& S) {
@@ -110,13 +109,18 @@ __device__ __forceinline__ void write_pixel_stoch(const RasterParams& p, int px,
     }
     if (p.out_rgba32f) p.out_rgba32f[o] = c;
     if (p.out_depth) p.out_depth[o] = (float)S.best_d24 / 16777215.0f;
-    if (p.out_rgba16f) {
-        __half2 h01 = __floats2half2_rn(c.x, c.y), h23 = __floats2half2_rn(c.z, c.w);
-        uint2 packed;
-        packed.x = *reinterpret_cast<uint32_t*>(&h01);
-        packed.y = *reinterpret_cast<uint32_t*>(&h23);
-        reinterpret_cast<uint2*>(p.out_rgba16f)[o] = packed;
-    }
+    if (p.out_rgba16f) write_rgba16f(p.out_rgba16f, o, c.x, c.y, c.z, c.w);
+}
+
+// Tile-relative coverage of a record's pixel rectangle: column bits [15:0],
+// row bits [31:16] (bit k = tile column / GL row k).  Empty rectangles give 0.
+__device__ __forceinline__ uint32_t rect_bits(uint32_t rect_x, uint32_t rect_y, int x0, int y0) {
+    const int i0 = min(max((int)(rect_x & 0xFFFFu) - x0, 0), 16), i1 = min(max((int)(rect_x >> 16) - x0, 0), 16);
+    const int j0 = min(max((int)(rect_y & 0xFFFFu) - y0, 0), 16), j1 = min(max((int)(rect_y >> 16) - y0, 0), 16);
+    if (i1 <= i0 || j1 <= j0) return 0u;
+    const uint32_t cols = (1u << i1) - (1u << i0);
+    const uint32_t rows = (1u << j1) - (1u << j0);
+    return cols | (rows << 16);
 }
 
 // One CTA of 128 threads per 16x16 tile; warp w owns the 8x8 block
@@ -127,14 +131,18 @@ template <int kMode>  // 0 = alpha, 1 = stochastic
 __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) {
     __shared__ __align__(128) RasterRecord s_rec[2][kBatch];
     __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_bits[kBatch];
     __shared__ uint8_t s_mask[kBatch];
 
     const uint32_t tile = blockIdx.x;
     const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bx0 = tx * kTileW + (warp & 1) * 8, by0 = ty * kTileH + (warp >> 1) * 8;
-    const int px = bx0 + (lane & 7), py0 = by0 + (lane >> 3), py1 = py0 + 4;
+    const int x0 = tx * kTileW, y0 = ty * kTileH;
+    const int lx = (warp & 1) * 8 + (lane & 7), ly0 = (warp >> 1) * 8 + (lane >> 3), ly1 = ly0 + 4;
+    const int px = x0 + lx, py0 = y0 + ly0, py1 = y0 + ly1;
     const bool in0 = px < p.width && py0 < p.height, in1 = px < p.width && py1 < p.height;
+    // coverage bits a pixel needs: its tile column and its tile row
+    const uint32_t need0 = (1u << lx) | (1u << (16 + ly0)), need1 = (1u << lx) | (1u << (16 + ly1));
     const uint2 range = p.tile_ranges[tile];
     const uint32_t n = range.y > range.x ? range.y - range.x : 0u;
     const uint32_t* __restrict__ vals = p.tile_plan->vfinal;
@@ -147,9 +155,13 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     __syncthreads();
 
     const float fcx = (float)px + 0.5f, fcy0 = (float)py0 + 0.5f, fcy1 = (float)py1 + 0.5f;
-    AlphaState A0 = {1.0f, 0.0f, 0.0f, 0.0f}, A1 = A0;
+    const float2 fcy = make_float2(fcy0, fcy1);
+    // alpha state of the two pixels (x: pixel 0, y: pixel 1); pixels outside
+    // the image start "done" (T = 0) and are never written
+    float2 T = make_float2(in0 ? 1.0f : 0.0f, in1 ? 1.0f : 0.0f);
+    float2 C0 = f2(0.0f), C1 = f2(0.0f), C2 = f2(0.0f);
     StochState S0 = {16777215u, 0xFFFFFFFFu, 0.0f, 0.0f, 0.0f}, S1 = S0;
-    bool done0 = !in0, done1 = !in1;
+    bool sdone0 = !in0, sdone1 = !in1;
     bool failed = false;
     const uint32_t nb = (n + kBatch - 1) / kBatch;
     uint32_t phase0 = 0, phase1 = 0;
@@ -164,6 +176,10 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
             bulk_g2s(&s_rec[b & 1][threadIdx.x], p.records + s, (uint32_t)sizeof(RasterRecord), bar);
         }
     };
+    auto pixels_done = [&]() -> bool {
+        if (kMode == 0) return fmaxf(T.x, T.y) < kTransmittanceMin;
+        return sdone0 && sdone1;
+    };
 
     if (nb > 0) issue(0);
     for (uint32_t b = 0; b < nb; ++b) {
@@ -173,63 +189,66 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         if (b & 1) phase1 ^= 1u; else phase0 ^= 1u;
         const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
         const RasterRecord* recs = s_rec[b & 1];
-        // Which of the four 8x8 warp blocks each staged splat's rectangle
-        // touches (one thread per record); warps then visit only their own.
+        // Coverage bits of each staged record and which of the four 8x8 warp
+        // blocks it touches (one thread per record).
         if (threadIdx.x < cnt) {
-            const uint4 q2 = reinterpret_cast<const uint4*>(recs + threadIdx.x)[2];
-            const int i0 = (int)(q2.z & 0xFFFFu), i1 = (int)(q2.z >> 16);
-            const int j0 = (int)(q2.w & 0xFFFFu), j1 = (int)(q2.w >> 16);
-            const int x0 = tx * kTileW, y0 = ty * kTileH;
-            const uint32_t cols = (uint32_t)(i0 < x0 + 8 && i1 > x0) | ((uint32_t)(i0 < x0 + 16 && i1 > x0 + 8) << 1);
-            const uint32_t rows = (uint32_t)(j0 < y0 + 8 && j1 > y0) | ((uint32_t)(j0 < y0 + 16 && j1 > y0 + 8) << 1);
+            const uint2 rr = reinterpret_cast<const uint2*>(recs + threadIdx.x)[5];
+            const uint32_t bits = rect_bits(rr.x, rr.y, x0, y0);
+            s_bits[threadIdx.x] = bits;
+            const uint32_t c = (uint32_t)((bits & 0x00FFu) != 0u) | ((uint32_t)((bits & 0xFF00u) != 0u) << 1);
+            const uint32_t r = (uint32_t)((bits & 0x00FF0000u) != 0u) | ((uint32_t)((bits & 0xFF000000u) != 0u) << 1);
             // block w = (w & 1, w >> 1): bit w set iff its column and row halves are covered
-            s_mask[threadIdx.x] = (uint8_t)((cols & (rows & 1u ? 3u : 0u)) | ((cols & (rows & 2u ? 3u : 0u)) << 2));
+            s_mask[threadIdx.x] = (uint8_t)((c & (r & 1u ? 3u : 0u)) | ((c & (r & 2u ? 3u : 0u)) << 2));
         }
         __syncthreads();
         // Warp-uniform control flow only; per-pixel work is predicated.
-        bool warp_done = __all_sync(0xffffffffu, (done0 && done1) || failed);
+        bool warp_done = __any_sync(0xffffffffu, failed) || __all_sync(0xffffffffu, pixels_done());
         for (uint32_t c = 0; c < cnt && !warp_done; c += 32) {
             const bool mine = c + lane < cnt && ((s_mask[c + lane] >> warp) & 1u);
             uint32_t todo = __ballot_sync(0xffffffffu, mine);
             while (todo) {
                 const uint32_t j = c + (uint32_t)(__ffs(todo) - 1);
                 todo &= todo - 1u;
-                const uint4 q2 = reinterpret_cast<const uint4*>(recs + j)[2];
                 const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
                 const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
-                const int i0 = (int)(q2.z & 0xFFFFu), i1 = (int)(q2.z >> 16);
-                const int j0 = (int)(q2.w & 0xFFFFu), j1 = (int)(q2.w >> 16);
-                const bool colx = px >= i0 && px < i1;
-                // splat_power() evaluated for both pixels with the shared first term
+                const uint32_t bits = s_bits[j];
+                // splat_power()'s sum for both pixels with the shared first term
                 const float dx = sub(fcx, q0.x);
                 const float t0 = mul(mul(q0.z, dx), dx);
-                const float dy0 = sub(fcy0, q0.y), dy1 = sub(fcy1, q0.y);
-                const float pw0 = mul(-0.5f, add(add(t0, mul(mul(q0.w, dx), dy0)), mul(mul(q1.x, dy0), dy0)));
-                const float pw1 = mul(-0.5f, add(add(t0, mul(mul(q0.w, dx), dy1)), mul(mul(q1.x, dy1), dy1)));
-                const bool live0 = !done0 && colx && py0 >= j0 && py0 < j1 && (pw0 <= 0.0f) && !(pw0 < q1.z);
-                const bool live1 = !done1 && colx && py1 >= j0 && py1 < j1 && (pw1 <= 0.0f) && !(pw1 < q1.z);
+                const float m = mul(q0.w, dx);
+                const float2 dy = __fadd2_rn(fcy, f2(-q0.y));
+                const float2 sq = __fadd2_rn(__fadd2_rn(f2(t0), __fmul2_rn(f2(m), dy)),
+                                             __fmul2_rn(__fmul2_rn(f2(q1.x), dy), dy));
+                const bool live0 = (bits & need0) == need0 && sq.x >= -__int_as_float(1) && sq.x <= q1.z;
+                const bool live1 = (bits & need1) == need1 && sq.y >= -__int_as_float(1) && sq.y <= q1.z;
                 if (kMode == 0) {
-                    const float g = __uint_as_float(q2.x), bb = __uint_as_float(q2.y);
-                    if (live0) alpha_step(A0, done0, pw0, q1.y, q1.w, g, bb);
-                    if (live1) alpha_step(A1, done1, pw1, q1.y, q1.w, g, bb);
-                    if (__all_sync(0xffffffffu, (done0 && done1) || failed)) { warp_done = true; break; }
+                    const float2 q2 = reinterpret_cast<const float2*>(recs + j)[4];
+                    const float2 arg = __ffma2_rn(sq, f2(kNegHalfLog2e), f2(q1.y));
+                    const float a0 = live0 ? fminf(ex2_approx(arg.x), 0.99f) : 0.0f;
+                    const float a1 = live1 ? fminf(ex2_approx(arg.y), 0.99f) : 0.0f;
+                    const float2 w = __fmul2_rn(make_float2(a0, a1), T);
+                    C0 = __ffma2_rn(w, f2(q1.w), C0);
+                    C1 = __ffma2_rn(w, f2(q2.x), C1);
+                    C2 = __ffma2_rn(w, f2(q2.y), C2);
+                    T = __ffma2_rn(w, f2(-1.0f), T);
+                    if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
                 } else {
                     const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
                     const uint32_t z24 = q3.x, id = q3.y;
                     // a pixel stops once splats are beyond its kept depth (+ margin)
-                    if (S0.best_id != 0xFFFFFFFFu && z24 > S0.best_d24 + kDepthMargin) done0 = true;
-                    if (S1.best_id != 0xFFFFFFFFu && z24 > S1.best_d24 + kDepthMargin) done1 = true;
-                    if (__all_sync(0xffffffffu, (done0 && done1) || failed)) { warp_done = true; break; }
+                    if (S0.best_id != 0xFFFFFFFFu && z24 > S0.best_d24 + kDepthMargin) sdone0 = true;
+                    if (S1.best_id != 0xFFFFFFFFu && z24 > S1.best_d24 + kDepthMargin) sdone1 = true;
+                    if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
                     const bool b0 = z24 < S0.best_d24 || (z24 == S0.best_d24 && id < S0.best_id);
                     const bool b1 = z24 < S1.best_d24 || (z24 == S1.best_d24 && id < S1.best_id);
-                    const float g = __uint_as_float(q2.x), bb = __uint_as_float(q2.y);
-                    const float hz = __uint_as_float(q3.z);
-                    if (live0 && !done0 && b0) stoch_step(S0, pw0, q1.y, fcx, fcy0, hz, z24, id, q1.w, g, bb);
-                    if (live1 && !done1 && b1) stoch_step(S1, pw1, q1.y, fcx, fcy1, hz, z24, id, q1.w, g, bb);
+                    const float2 q2 = reinterpret_cast<const float2*>(recs + j)[4];
+                    const float hz = __uint_as_float(q3.z), op = __uint_as_float(q3.w);
+                    if (live0 && !sdone0 && b0) stoch_step(S0, sq.x, op, fcx, fcy0, hz, z24, id, q1.w, q2.x, q2.y);
+                    if (live1 && !sdone1 && b1) stoch_step(S1, sq.y, op, fcx, fcy1, hz, z24, id, q1.w, q2.x, q2.y);
                 }
             }
         }
-        const int all_done = __syncthreads_and(warp_done || (done0 && done1) || failed);
+        const int all_done = __syncthreads_and(warp_done || pixels_done() || failed);
         if (all_done) {
             if (b + 1 < nb) {
                 const uint32_t ph2 = ((b + 1) & 1) ? phase1 : phase0;
@@ -240,8 +259,12 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     }
     if (failed) atomicOr(&p.fc->error_flags, kErrRasterWait);
     if (kMode == 0) {
-        if (in0) write_pixel_alpha(p, px, py0, A0);
-        if (in1) write_pixel_alpha(p, px, py1, A1);
+        const size_t o0 = (size_t)(p.height - 1 - py0) * p.width + px;
+        const size_t o1 = (size_t)(p.height - 1 - py1) * p.width + px;
+        const float2 bg = f2(p.bg);
+        const float2 r = __ffma2_rn(T, bg, C0), g = __ffma2_rn(T, bg, C1), bb = __ffma2_rn(T, bg, C2);
+        if (in0) write_rgba16f(p.out_rgba16f, o0, r.x, g.x, bb.x, 1.0f - T.x);
+        if (in1) write_rgba16f(p.out_rgba16f, o1, r.y, g.y, bb.y, 1.0f - T.y);
     } else {
         if (in0) write_pixel_stoch(p, px, py0, S0);
         if (in1) write_pixel_stoch(p, px, py1, S1);

@@ -203,8 +203,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
         }
         const uint32_t tile_count = run;
         u64* st = status + (size_t)tile * kRadix + d;
-        if (tile == 0) st_release64(st, status_word(p.epoch, kFlagInc, gdigit + tile_count));
-        else st_release64(st, status_word(p.epoch, kFlagAgg, tile_count));
+        if (tile == 0) st_relaxed64(st, status_word(p.epoch, kFlagInc, gdigit + tile_count));
+        else st_relaxed64(st, status_word(p.epoch, kFlagAgg, tile_count));
         // Reorder the tile by digit in shared memory while predecessors publish.
         uint32_t total;
         const uint32_t lstart = block_excl_scan(tile_count, scan_tmp, &total);
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
             bool to = false;
             gexcl = lookback_vec(status + d, kRadix, tile, p.epoch, &to);
             if (to) atomicOr(p.error_flags, kErrSortLookback);
-            st_release64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
+            st_relaxed64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
         }
         s_global_base[d] = gexcl - lstart;
         __syncthreads();
