@@ -103,8 +103,7 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
     const uint32_t n_vis = p.fc->visible_count;
     const uint32_t num_tiles = (n_vis + kBinTile - 1) / kBinTile;
     const uint32_t* __restrict__ sorted_ids = p.depth_plan->vfinal;
-    const float* camf = reinterpret_cast<const float*>(p.cam);
-    const float vp_w = __ldg(camf + 32), vp_h = __ldg(camf + 33), ysign = __ldg(camf + 37);
+    const float vp_w = p.vp_w, vp_h = p.vp_h, ysign = p.clip_y_sign;
     const int t = threadIdx.x;
     for (int i = t; i < 3 * 256; i += kBinThreads) (&s_hist[0][0])[i] = 0u;
 

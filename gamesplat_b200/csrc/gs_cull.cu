@@ -24,6 +24,7 @@
 
 namespace gs {
 
+static_assert(kCullRounds == 4, "the round loop selects per-round values among four scalars");
 constexpr int kStageStride = 17;  // float4 per staged row (16 + 1 pad)
 constexpr int kCullWarps = kCullThreads / 32;
 constexpr size_t kCullSmem = (size_t)kCullWarps * 2 * 32 * kStageStride * sizeof(float4);  // double-buffered
@@ -35,21 +36,20 @@ struct CamRegs {
     float camw[3];
 };
 
-__device__ __forceinline__ void load_cam(const gs_camera* c, CamRegs& r) {
-    const float* f = reinterpret_cast<const float*>(c);
+__device__ __forceinline__ void load_cam(const gs_camera& c, CamRegs& r) {
 #pragma unroll
-    for (int k = 0; k < 16; ++k) r.V[k] = __ldg(f + k);
-    r.P0 = __ldg(f + 16 + 0);
-    r.P5 = __ldg(f + 16 + 5);
-    r.P10 = __ldg(f + 16 + 10);
-    r.P14 = __ldg(f + 16 + 14);
-    r.vpx = __ldg(f + 32);
-    r.vpy = __ldg(f + 33);
-    r.ortho = __ldg(f + 34);
-    r.fxp = __ldg(f + 35);
-    r.fxo = __ldg(f + 36);
-    r.ysign = __ldg(f + 37);
-    r.z01 = __ldg(f + 38);
+    for (int k = 0; k < 16; ++k) r.V[k] = c.view[k];
+    r.P0 = c.proj[0];
+    r.P5 = c.proj[5];
+    r.P10 = c.proj[10];
+    r.P14 = c.proj[14];
+    r.vpx = c.viewport[0];
+    r.vpy = c.viewport[1];
+    r.ortho = c.orthographic;
+    r.fxp = c.persp_focal;
+    r.fxo = c.ortho_focal;
+    r.ysign = c.clip_y_sign;
+    r.z01 = c.clip_z_01;
     // cam_pos_world = -transpose(W) * view[3].xyz (shaders/cull.glsl:323)
 #pragma unroll
     for (int rr = 0; rr < 3; ++rr) {
@@ -210,14 +210,15 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
 // one TMA bulk copy; completion is counted on `bar`.
 template <int kChunks>
 __device__ __forceinline__ void stage_round(const float4* rows, uint32_t wbase, uint32_t mask, float4* stage,
-                                            uint64_t* bar, int lane) {
+                                            uint64_t* bar, int lane, uint64_t policy) {
     if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)__popc(mask) * (uint32_t)(kChunks * 16));
     __syncwarp();
     // order this lane's earlier generic accesses to its stage row (reads, and
     // the in-place gsanim deltas) before the async-proxy refill
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if ((mask >> lane) & 1u)
-        bulk_g2s(stage + lane * kStageStride, rows + (size_t)(wbase + lane) * 16, (uint32_t)(kChunks * 16), bar);
+        bulk_g2s_hint(stage + lane * kStageStride, rows + (size_t)(wbase + lane) * 16, (uint32_t)(kChunks * 16), bar,
+                      policy);
 }
 
 // gsanim int8 appearance deltas applied in place to a staged row
@@ -277,23 +278,33 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
     const bool animated = p.anim_deltas != nullptr &&
                           (p.anim_state_a != 0 || (p.anim_weight > 0.0f && p.anim_state_b != 0));
     bool stage_failed = false;
+    const uint64_t stream_policy = l2_policy_evict_first();
 
-    for (;;) {
-        uint32_t tile = 0;
-        if (lane == 0) tile = atomicAdd(&p.fc->cull_ticket, 1u);
-        tile = __shfl_sync(0xffffffffu, tile, 0);
-        if (tile >= num_tiles) break;
-        const uint32_t base = tile * kCullTile;
-
-        uint32_t mask[kCullRounds];
+    auto take_ticket = [&]() -> uint32_t {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&p.fc->cull_ticket, 1u);
+        return __shfl_sync(0xffffffffu, t, 0);
+    };
+    // First 16 bytes (position, opacity) of the tile's 4 x 32 rows.
+    auto load_heads = [&](uint32_t t, float4* c0) {
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) {
-            const uint32_t g = base + r * 32 + lane;
-            const float4 c0 = g < p.n ? __ldg(p.rows + (size_t)g * 16) : make_float4(0.f, 0.f, 0.f, 0.f);
-            // p_view = view * vec4(position, 1.0)  (shaders/cull.glsl:209-220)
-            const float vx = add(add(add(mul(cam.V[0], c0.x), mul(cam.V[4], c0.y)), mul(cam.V[8], c0.z)), cam.V[12]);
-            const float vy = add(add(add(mul(cam.V[1], c0.x), mul(cam.V[5], c0.y)), mul(cam.V[9], c0.z)), cam.V[13]);
-            const float vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
+            const uint32_t g = t * kCullTile + r * 32 + lane;
+            c0[r] = g < p.n ? ldg_hint(p.rows + (size_t)g * 16, stream_policy) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    // Visibility masks of a tile (shaders/cull.glsl:209-232), then stage its
+    // round 0 into buffer 0 and publish its visible count as an aggregate.
+    auto begin_tile = [&](uint32_t t, const float4* c0, uint32_t& m0, uint32_t& m1, uint32_t& m2,
+                          uint32_t& m3) -> uint32_t {
+        uint32_t total = 0;
+#pragma unroll
+        for (int r = 0; r < kCullRounds; ++r) {
+            const uint32_t g = t * kCullTile + r * 32 + lane;
+            // p_view = view * vec4(position, 1.0)
+            const float vx = add(add(add(mul(cam.V[0], c0[r].x), mul(cam.V[4], c0[r].y)), mul(cam.V[8], c0[r].z)), cam.V[12]);
+            const float vy = add(add(add(mul(cam.V[1], c0[r].x), mul(cam.V[5], c0[r].y)), mul(cam.V[9], c0[r].z)), cam.V[13]);
+            const float vz = add(add(add(mul(cam.V[2], c0[r].x), mul(cam.V[6], c0[r].y)), mul(cam.V[10], c0[r].z)), cam.V[14]);
             bool visible = g < p.n && (vz <= -0.2f);
             if (visible) {
                 float inv_z = dv(-1.0f, vz);
@@ -301,30 +312,57 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
                 float ndc_y = add(mul(mul(mul(cam.P5, vy), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P5, vy), cam.ortho));
                 visible = fabsf(ndc_x) <= 1.3f && fabsf(ndc_y) <= 1.3f;
             }
-            mask[r] = __ballot_sync(0xffffffffu, visible);
+            const uint32_t m = __ballot_sync(0xffffffffu, visible);
+            if (r == 0) m0 = m;
+            if (r == 1) m1 = m;
+            if (r == 2) m2 = m;
+            if (r == 3) m3 = m;
+            total += __popc(m);
         }
-        stage_round<kChunks>(p.rows, base, mask[0], stage0, &s_bar[warp][0], lane);
-        // The tile's visible count is known now: publish it before projecting.
-        uint32_t total = 0;
-#pragma unroll
-        for (int r = 0; r < kCullRounds; ++r) total += __popc(mask[r]);
-        if (lane == 0)
-            st_relaxed64(p.status + tile, status_word(p.epoch, tile == 0 ? kFlagInc : kFlagAgg, total));
+        stage_round<kChunks>(p.rows, t * kCullTile, m0, stage0, &s_bar[warp][0], lane, stream_policy);
+        if (lane == 0) st_relaxed64(p.status + t, status_word(p.epoch, t == 0 ? kFlagInc : kFlagAgg, total));
+        return total;
+    };
 
-        uint32_t keys[kCullRounds];
+    // Tiles are software-pipelined: the next tile's ticket and row heads are
+    // fetched while this tile projects, and its visibility, round-0 staging
+    // and aggregate publish happen during this tile's last round.
+    float4 heads[kCullRounds];
+    uint32_t mask0 = 0u, mask1 = 0u, mask2 = 0u, mask3 = 0u;
+    uint32_t tile = take_ticket();
+    uint32_t total = 0;
+    if (tile < num_tiles) {
+        load_heads(tile, heads);
+        total = begin_tile(tile, heads, mask0, mask1, mask2, mask3);
+    }
+    while (tile < num_tiles) {
+        const uint32_t base = tile * kCullTile;
+        // next tile's ticket: requested now, read in round 1 (its latency is
+        // hidden behind round 0), its row heads loaded then for round 3
+        uint32_t ticket_raw = 0u;
+        if (lane == 0) ticket_raw = atomicAdd(&p.fc->cull_ticket, 1u);
+        uint32_t ntile = num_tiles;
+        uint32_t nmask0 = 0u, nmask1 = 0u, nmask2 = 0u, nmask3 = 0u;
+        uint32_t ntotal = 0;
+
+        uint32_t key0 = 0u, key1 = 0u, key2 = 0u, key3 = 0u;
         uint32_t d0 = 0, d2 = 0, d3 = 0, d4 = 0, d6 = 0, d7 = 0, m1 = 0, m5 = 0;
 #pragma unroll 1
         for (int r = 0; r < kCullRounds; ++r) {
-            uint32_t mr = mask[0], mnext = 0u;
-#pragma unroll
-            for (int k = 1; k < kCullRounds; ++k) {
-                if (r == k) mr = mask[k];
-                if (r + 1 == k) mnext = mask[k];
-            }
+            // scalar selects (no dynamically indexed arrays, which would live
+            // in local memory)
+            const uint32_t mr = r == 0 ? mask0 : r == 1 ? mask1 : r == 2 ? mask2 : mask3;
+            const uint32_t mnext = r == 0 ? mask1 : r == 1 ? mask2 : mask3;
             const int b = r & 1;
+            if (r == 1) {
+                ntile = __shfl_sync(0xffffffffu, ticket_raw, 0);
+                if (ntile < num_tiles) load_heads(ntile, heads);
+            }
             if (r + 1 < kCullRounds)
                 stage_round<kChunks>(p.rows, base + (r + 1) * 32, mnext, stage0 + (b ^ 1) * 32 * kStageStride,
-                                     &s_bar[warp][b ^ 1], lane);
+                                     &s_bar[warp][b ^ 1], lane, stream_policy);
+            else if (ntile < num_tiles)   // buffer 0 is free: round 2 is done
+                ntotal = begin_tile(ntile, heads, nmask0, nmask1, nmask2, nmask3);
             if (!mbar_wait_bounded(&s_bar[warp][b], (phase >> b) & 1u)) stage_failed = true;
             phase ^= 1u << b;
             float4* const cur = stage0 + b * 32 * kStageStride;
@@ -370,9 +408,10 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
                 dst[2] = make_float4(1.f, 0.f, 1.f, 1.f);
                 dst[3] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-#pragma unroll
-            for (int k = 0; k < kCullRounds; ++k)
-                if (r == k) keys[k] = key;
+            key0 = r == 0 ? key : key0;
+            key1 = r == 1 ? key : key1;
+            key2 = r == 2 ? key : key2;
+            key3 = r == 3 ? key : key3;
             // every lane is done reading stage[b] before round r + 2 refills it
             __syncwarp();
         }
@@ -406,15 +445,23 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
         uint32_t before = 0;
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) {
-            if ((mask[r] >> lane) & 1u) {
-                const uint32_t o = excl + before + __popc(mask[r] & lt);
-                p.keys_out[o] = keys[r];
+            const uint32_t mr = r == 0 ? mask0 : r == 1 ? mask1 : r == 2 ? mask2 : mask3;
+            if ((mr >> lane) & 1u) {
+                const uint32_t o = excl + before + __popc(mr & lt);
+                const uint32_t kr = r == 0 ? key0 : r == 1 ? key1 : r == 2 ? key2 : key3;
+                p.keys_out[o] = kr;
                 p.ids_out[o] = base + r * 32 + lane;
 #pragma unroll
-                for (int ps = 0; ps < 4; ++ps) atomicAdd(&s_hist[ps][(keys[r] >> (8 * ps)) & 255u], 1u);
+                for (int ps = 0; ps < 4; ++ps) atomicAdd(&s_hist[ps][(kr >> (8 * ps)) & 255u], 1u);
             }
-            before += __popc(mask[r]);
+            before += __popc(mr);
         }
+        tile = ntile;
+        total = ntotal;
+        mask0 = nmask0;
+        mask1 = nmask1;
+        mask2 = nmask2;
+        mask3 = nmask3;
     }
     if (stage_failed) atomicOr(&p.fc->error_flags, kErrCullStage);
     __syncthreads();

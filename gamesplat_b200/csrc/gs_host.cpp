@@ -86,8 +86,7 @@ struct gs_ctx {
     float anim_w = 0.0f;
 
     // camera
-    gs_camera* d_cam = nullptr;
-    gs_camera* h_cam = nullptr;   // pinned staging
+    gs_camera cam{};                 // the frame's camera (kernels take it by value)
     FrameCounters* h_fc = nullptr;  // pinned readback
     cudaEvent_t fc_event = nullptr;
     bool fc_pending = false;
@@ -300,8 +299,7 @@ int check_previous_frame(gs_ctx* c) {
 }
 
 void begin_frame(gs_ctx* c, const gs_camera* cam) {
-    std::memcpy(c->h_cam, cam, sizeof(gs_camera));
-    cudaMemcpyAsync(c->d_cam, c->h_cam, sizeof(gs_camera), cudaMemcpyHostToDevice, c->stream);
+    c->cam = *cam;
     cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream);
     ++c->epoch;
     if (c->epoch == 0) ++c->epoch;
@@ -320,7 +318,7 @@ void run_cull(gs_ctx* c) {
     gs::CullParams p{};
     p.rows = c->rows;
     p.n = c->n;
-    p.cam = c->d_cam;
+    p.cam = c->cam;
     p.sh_degree = std::max(0, std::min(3, c->knobs.sh_degree));
     p.sh_lod_distance = c->knobs.sh_lod_distance;
     p.collect_stats = c->knobs.splat_diagnostics_enabled ? 1 : 0;
@@ -383,7 +381,9 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         gs::BinParams p{};
         p.depth_plan = c->depth_plan;
         p.projected = c->projected;
-        p.cam = c->d_cam;
+        p.vp_w = c->cam.viewport[0];
+        p.vp_h = c->cam.viewport[1];
+        p.clip_y_sign = c->cam.clip_y_sign;
         p.jitter_x = jx;
         p.jitter_y = jy;
         p.frame_seed = seed;
@@ -676,9 +676,7 @@ int gs_create(gs_ctx** out, int device, void* stream) {
     c->knobs.splat_diagnostics_enabled = 0;
     c->knobs.linear_color = 0;
     c->knobs.write_invisible_records = 0;
-    if (cudaMalloc(reinterpret_cast<void**>(&c->d_cam), sizeof(gs_camera)) != cudaSuccess ||
-        cudaMallocHost(reinterpret_cast<void**>(&c->h_cam), sizeof(gs_camera)) != cudaSuccess ||
-        cudaMallocHost(reinterpret_cast<void**>(&c->h_fc), sizeof(FrameCounters)) != cudaSuccess ||
+    if (cudaMallocHost(reinterpret_cast<void**>(&c->h_fc), sizeof(FrameCounters)) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->fc_event, cudaEventDisableTiming) != cudaSuccess) {
         gs_destroy(c);
         return GS_ERR_OOM;
@@ -694,8 +692,6 @@ void gs_destroy(gs_ctx* c) {
     cudaStreamSynchronize(c->stream);
     release_scene(c);
     release_targets(c);
-    dfree(c->d_cam);
-    if (c->h_cam) cudaFreeHost(c->h_cam);
     if (c->h_fc) cudaFreeHost(c->h_fc);
     if (c->h_out16) cudaFreeHost(c->h_out16);
     if (c->fc_event) cudaEventDestroy(c->fc_event);

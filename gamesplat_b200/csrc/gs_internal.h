@@ -97,7 +97,7 @@ static_assert(sizeof(RasterRecord) == 64, "RasterRecord must be 64 bytes");
 struct CullParams {
     const float4* rows;          // N x 16 float4 (GpuGaussian)
     uint32_t n;
-    const gs_camera* cam;        // device copy of the frame's CameraUniforms
+    gs_camera cam;               // the frame's CameraUniforms, by value (constant-bank operands)
     int sh_degree;
     float sh_lod_distance;
     int collect_stats;
@@ -137,7 +137,7 @@ struct SortParams {
 struct BinParams {
     const SortPlan* depth_plan;      // sorted ids at depth_plan->vfinal
     const float4* projected;
-    const gs_camera* cam;
+    float vp_w, vp_h, clip_y_sign;   // CameraUniforms viewport and clip_y_sign of the frame
     float jitter_x, jitter_y;
     float frame_seed;
     int width, height, tiles_x, tiles_y;
