@@ -6,8 +6,10 @@
 // geometry and fill rule as the CPU oracle (gs::quad_rect), (b) writes a
 // 64-byte RasterRecord at position s, and (c) emits one (tile, s) entry per
 // 16x16 tile that can receive a non-discarded fragment.  Entries are written
-// in s order at offsets found by a decoupled look-back over CTA tiles, so a
-// stable sort on the tile id alone keeps each tile's list in depth order.
+// in descending s order (nearest splat first) at offsets found by a
+// decoupled look-back over CTA tiles, so a stable sort on the tile id alone
+// leaves each tile's list in front-to-back order, the order the rasterizer
+// walks.
 //
 // The CTA tile's entries are written by a load-balanced expansion (entry e
 // finds its splat by binary search over the CTA's offsets), so the stores are
@@ -112,17 +114,21 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
         __syncthreads();
         const uint32_t tile = s_tile;
         if (tile >= num_tiles) break;
-        const uint32_t base = tile * kBinTile;
+        // CTA tile b holds sorted positions top - 1, top - 2, ..., down to
+        // top - kBinTile (nearest splats first: their large footprints make
+        // the heavy tiles, which are then taken first instead of last).
+        const uint32_t top = n_vis - tile * kBinTile;
+        const uint32_t cnt = min((uint32_t)kBinTile, top);
         // Splats striped over threads (coalesced id loads and record writes).
         uint32_t ids[kBinItems];
 #pragma unroll
         for (int i = 0; i < kBinItems; ++i) {
-            const uint32_t s = base + i * kBinThreads + t;
-            ids[i] = s < n_vis ? sorted_ids[s] : kSentinel;
+            const uint32_t j = (uint32_t)(i * kBinThreads + t);
+            ids[i] = j < cnt ? sorted_ids[top - 1u - j] : kSentinel;
         }
 #pragma unroll
         for (int i = 0; i < kBinItems; ++i) {
-            const uint32_t s = base + i * kBinThreads + t;
+            const uint32_t s = top - 1u - (uint32_t)(i * kBinThreads + t);
             const BinItem it = ids[i] != kSentinel ? bin_one(p, s, ids[i], vp_w, vp_h, ysign)
                                                    : BinItem{0u, 0, -1, 0, -1};
             const int slot = i * kBinThreads + t;
@@ -190,7 +196,7 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
             const uint32_t o = excl + e;
             if (o < p.entry_cap) {
                 p.entry_keys[o] = tid;
-                p.entry_vals[o] = base + (uint32_t)lo;
+                p.entry_vals[o] = top - 1u - (uint32_t)lo;
                 atomicAdd(&s_hist[0][tid & 255u], 1u);
                 atomicAdd(&s_hist[1][(tid >> 8) & 255u], 1u);
                 atomicAdd(&s_hist[2][(tid >> 16) & 255u], 1u);

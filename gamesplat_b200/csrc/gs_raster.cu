@@ -7,13 +7,13 @@
 // top row first).  Control flow is warp-uniform: lanes never diverge around
 // the per-splat loop (per-pixel work is predicated or selected), a warp skips
 // splats whose rectangle misses its block and leaves the loop when all its
-// pixels are done.  The tile's depth-ordered splat list is walked front to
-// back (reverse of the reference's back-to-front draw order, so equal depth
-// keys are visited in descending splat index, which reproduces "later
-// instance on top").  Batches of 128 64-byte RasterRecords are staged into
-// shared memory by TMA 1-D bulk copies (cp.async.bulk, completion on an
-// mbarrier), double buffered so the next batch lands while the current one
-// is composited.  When a batch lands, one thread per record turns its pixel
+// pixels are done.  The tile's splat list (descending sorted position) is
+// walked front to back (reverse of the reference's back-to-front draw order,
+// so equal depth keys are visited in descending splat index, which
+// reproduces "later instance on top").  Batches of 128 64-byte RasterRecords
+// are staged into shared memory by TMA 1-D bulk copies (cp.async.bulk,
+// completion on an mbarrier), double buffered so the next batch lands while
+// the current one is composited.  When a batch lands, one thread per record turns its pixel
 // rectangle into tile-relative column and row bit masks, so a pixel's
 // coverage test is one AND and one compare.
 //
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         uint64_t* bar = &s_bar[b & 1];
         if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, cnt * (uint32_t)sizeof(RasterRecord));
         if (threadIdx.x < cnt) {
-            const uint32_t s = min(vals[range.y - 1 - (first + threadIdx.x)], p.record_cap - 1u);
+            const uint32_t s = min(vals[range.x + first + threadIdx.x], p.record_cap - 1u);
             bulk_g2s(&s_rec[b & 1][threadIdx.x], p.records + s, (uint32_t)sizeof(RasterRecord), bar);
         }
     };
