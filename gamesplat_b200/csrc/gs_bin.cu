@@ -102,6 +102,7 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
     __shared__ uint32_t s_org[kBinTile];    // tx0 | ty0 << 16 of its tile rectangle
     __shared__ uint16_t s_w[kBinTile];      // width of its tile rectangle (tiles)
     __shared__ uint32_t s_hist[3][256];     // tile-id digit histograms for the tile sort
+    __shared__ __align__(16) int32_t s_own[kBinChunk];   // owning splat of each entry of the current chunk
     const uint32_t n_vis = p.fc->visible_count;
     const uint32_t num_tiles = (n_vis + kBinTile - 1) / kBinTile;
     const uint32_t* __restrict__ sorted_ids = p.depth_plan->vfinal;
@@ -146,8 +147,10 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
         }
         uint32_t total;
         uint32_t run = block_excl_scan(sum, scan_tmp, &total);
+        uint32_t off[kBinItems];
 #pragma unroll
         for (int k = 0; k < kBinItems; ++k) {
+            off[k] = run;
             s_off[t * kBinItems + k] = run;
             run += c[k];
         }
@@ -179,30 +182,55 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
             }
         }
         __syncthreads();
-        // Load-balanced expansion: entry e of the CTA tile belongs to the last
-        // splat whose offset is <= e (binary search over s_off).
+        // Load-balanced expansion in chunks of kBinChunk entries: each
+        // non-empty splat marks its first entry with its index, and a
+        // block-wide prefix maximum turns the marks into the owning splat of
+        // every entry (the owner of the chunk's first entries carries over
+        // from the previous chunk).
         const uint32_t excl = s_excl, cta_total = s_total;
-        for (uint32_t e = t; e < cta_total; e += kBinThreads) {
-            int lo = 0, hi = kBinTile - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_off[mid] <= e) lo = mid;
-                else hi = mid - 1;
+        int32_t carry = -1;
+        for (uint32_t e0 = 0; e0 < cta_total; e0 += kBinChunk) {
+            for (int i = t; i < kBinChunk; i += kBinThreads) s_own[i] = -1;
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < kBinItems; ++k)
+                if (c[k] != 0u && off[k] - e0 < (uint32_t)kBinChunk) s_own[off[k] - e0] = t * kBinItems + k;
+            __syncthreads();
+            static_assert(kBinChunk == 8 * kBinThreads, "eight entries per thread in the prefix maximum");
+            int4* own4 = reinterpret_cast<int4*>(s_own) + 2 * t;
+            int4 a = own4[0], bq = own4[1];
+            a.y = max(a.y, a.x);
+            a.z = max(a.z, a.y);
+            a.w = max(a.w, a.z);
+            bq.x = max(bq.x, a.w);
+            bq.y = max(bq.y, bq.x);
+            bq.z = max(bq.z, bq.y);
+            bq.w = max(bq.w, bq.z);
+            const int32_t pre = max(block_excl_max(bq.w, reinterpret_cast<int32_t*>(scan_tmp)), carry);
+            own4[0] = make_int4(max(a.x, pre), max(a.y, pre), max(a.z, pre), max(a.w, pre));
+            own4[1] = make_int4(max(bq.x, pre), max(bq.y, pre), max(bq.z, pre), max(bq.w, pre));
+            __syncthreads();
+            const uint32_t n_here = min((uint32_t)kBinChunk, cta_total - e0);
+            for (uint32_t i = t; i < n_here; i += kBinThreads) {
+                const uint32_t e = e0 + i;
+                const int lo = s_own[i];
+                if (lo < 0) continue;   // unreachable: entry 0's owner always marks slot 0
+                const uint32_t k = e - s_off[lo];
+                const uint32_t w = s_w[lo], org = s_org[lo];
+                const uint32_t ty = (org >> 16) + k / w, tx = (org & 0xFFFFu) + k % w;
+                const uint32_t tid = ty * (uint32_t)p.tiles_x + tx;
+                const uint32_t o = excl + e;
+                if (o < p.entry_cap) {
+                    p.entry_keys[o] = tid;
+                    p.entry_vals[o] = top - 1u - (uint32_t)lo;
+                    atomicAdd(&s_hist[0][tid & 255u], 1u);
+                    atomicAdd(&s_hist[1][(tid >> 8) & 255u], 1u);
+                    atomicAdd(&s_hist[2][(tid >> 16) & 255u], 1u);
+                }
             }
-            const uint32_t k = e - s_off[lo];
-            const uint32_t w = s_w[lo], org = s_org[lo];
-            const uint32_t ty = (org >> 16) + k / w, tx = (org & 0xFFFFu) + k % w;
-            const uint32_t tid = ty * (uint32_t)p.tiles_x + tx;
-            const uint32_t o = excl + e;
-            if (o < p.entry_cap) {
-                p.entry_keys[o] = tid;
-                p.entry_vals[o] = top - 1u - (uint32_t)lo;
-                atomicAdd(&s_hist[0][tid & 255u], 1u);
-                atomicAdd(&s_hist[1][(tid >> 8) & 255u], 1u);
-                atomicAdd(&s_hist[2][(tid >> 16) & 255u], 1u);
-            }
+            carry = s_own[kBinChunk - 1];
+            __syncthreads();
         }
-        __syncthreads();
     }
     __syncthreads();
     for (int i = t; i < 3 * 256; i += kBinThreads) {

@@ -333,4 +333,35 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* warp_t
     return r;
 }
 
+// Block-wide exclusive prefix maximum of signed values (identity -1);
+// warp_tmp holds 33 words.  Every thread of the block must call it.
+__device__ __forceinline__ int32_t block_excl_max(int32_t v, int32_t* warp_tmp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    int32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    if (lane == 31) warp_tmp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int32_t w = lane < nwarps ? warp_tmp[lane] : -1;
+        int32_t ws = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, ws, o);
+            if (lane >= o) ws = max(ws, y);
+        }
+        // exclusive over warps: shift by one
+        const int32_t prev = __shfl_up_sync(0xffffffffu, ws, 1);
+        if (lane < nwarps) warp_tmp[lane] = lane == 0 ? -1 : prev;
+    }
+    __syncthreads();
+    const int32_t xin = __shfl_up_sync(0xffffffffu, x, 1);
+    const int32_t r = max(warp_tmp[warp], lane == 0 ? -1 : xin);
+    __syncthreads();
+    return r;
+}
+
 }  // namespace gs

@@ -70,6 +70,7 @@ constexpr int kCullTile = 32 * kCullRounds;
 constexpr int kBinThreads = 256;
 constexpr int kBinItems = 4;
 constexpr int kBinTile = kBinThreads * kBinItems;
+constexpr int kBinChunk = 2048;                 // entries expanded per round
 constexpr int kTileW = 16;
 constexpr int kTileH = 16;
 
