@@ -233,23 +233,26 @@ __device__ __forceinline__ u64 status_word(uint32_t epoch, uint32_t flag, uint32
     return ((u64)epoch << 32) | (u64)(flag | (value & kValMask));
 }
 
-// Single-thread look-back that reads 8 predecessor words per step
+// Single-thread look-back that reads W predecessor words per step
 // (independent loads), then consumes them nearest first until an inclusive
 // prefix; an unpublished word is re-polled (bounded) before continuing.
+// Sets *timed_out if a wait exceeded kSpinLimit (the result is then
+// incomplete but the kernel ends).
+template <int W>
 __device__ __forceinline__ uint32_t lookback_vec(const u64* status, size_t stride, uint32_t tile, uint32_t epoch,
                                                  bool* timed_out) {
     uint32_t excl = 0;
     long long j = (long long)tile - 1;
     uint32_t spins = 0;
     while (j >= 0) {
-        u64 w[8];
+        u64 w[W];
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
+        for (int k = 0; k < W; ++k)
             w[k] = (j - k >= 0) ? ld_relaxed64(status + (size_t)(j - k) * stride) : status_word(epoch, kFlagInc, 0);
         int k = 0;
         bool found = false;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < W; ++q) {
             if (k != q || found) continue;
             const uint32_t lo = (uint32_t)w[q];
             const uint32_t flag = lo & ~kValMask;
@@ -260,7 +263,7 @@ __device__ __forceinline__ uint32_t lookback_vec(const u64* status, size_t strid
         }
         if (found) return excl;
         j -= k;
-        if (k < 8) {  // word j is not published yet: wait for it
+        if (k < W) {  // word j is not published yet: wait for it
             if (++spins > kSpinLimit) { *timed_out = true; return excl; }
             if (spins > 64) __nanosleep(32);
         }
@@ -271,7 +274,7 @@ __device__ __forceinline__ uint32_t lookback_vec(const u64* status, size_t strid
 // Warp-cooperative look-back: all 32 lanes read a window of 32 predecessors
 // at once, the nearest inclusive word is found by ballot and the aggregates
 // after it are summed with a warp reduction.  Every lane returns the same
-// exclusive prefix.  Bounded like lookback().
+// exclusive prefix.  Bounded like lookback_vec().
 __device__ __forceinline__ uint32_t lookback_warp(const u64* status, uint32_t tile, uint32_t epoch,
                                                   bool* timed_out) {
     const int lane = threadIdx.x & 31;

@@ -290,7 +290,8 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) {
             const uint32_t g = t * kCullTile + r * 32 + lane;
-            c0[r] = g < p.n ? ldg_hint(p.rows + (size_t)g * 16, stream_policy) : make_float4(0.f, 0.f, 0.f, 0.f);
+            // default L2 policy: the row's bulk copy re-reads this sector soon
+            c0[r] = g < p.n ? __ldg(p.rows + (size_t)g * 16) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
     };
     // Visibility masks of a tile (shaders/cull.glsl:209-232), then stage its

@@ -57,6 +57,7 @@ struct SortPlan {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // keys per CTA tile
+constexpr int kSortLookback = 8;                       // look-back words read per step
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 

@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
         uint32_t gexcl = gdigit;
         if (tile > 0) {
             bool to = false;
-            gexcl = lookback_vec(status + d, kRadix, tile, p.epoch, &to);
+            gexcl = lookback_vec<kSortLookback>(status + d, kRadix, tile, p.epoch, &to);
             if (to) atomicOr(p.error_flags, kErrSortLookback);
             st_relaxed64(st, status_word(p.epoch, kFlagInc, gexcl + tile_count));
         }

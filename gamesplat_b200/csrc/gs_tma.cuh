@@ -77,13 +77,4 @@ __device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, uint32
         : "memory");
 }
 
-// 16-byte read-only global load with an L2 cache policy.
-__device__ __forceinline__ float4 ldg_hint(const float4* p, uint64_t policy) {
-    float4 v;
-    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-                 : "l"(p), "l"(policy));
-    return v;
-}
-
 }  // namespace gs
