@@ -192,9 +192,9 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         const uint32_t cnt = min((uint32_t)kBatch, n - first);
         uint64_t* bar = &s_bar[b & 1];
         if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, cnt * (uint32_t)sizeof(RasterRecord));
-        if (threadIdx.x < cnt) {
-            const uint32_t s = min(vals[range.x + first + threadIdx.x], p.record_cap - 1u);
-            bulk_g2s(&s_rec[b & 1][threadIdx.x], p.records + s, (uint32_t)sizeof(RasterRecord), bar);
+        for (uint32_t i = threadIdx.x; i < cnt; i += kRasterThreads) {
+            const uint32_t s = min(vals[range.x + first + i], p.record_cap - 1u);
+            bulk_g2s(&s_rec[b & 1][i], p.records + s, (uint32_t)sizeof(RasterRecord), bar);
         }
     };
     auto pixels_done = [&]() -> bool {
@@ -215,11 +215,11 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         // touches, minus those where the splat's ellipse q(d) <= s_max misses
         // every covered pixel centre (tested with a 2 % + 0.02 margin over
         // s_max, far above the rounding of q and of the exact per-pixel sum).
-        if (threadIdx.x < cnt) {
-            const RasterRecord* R = recs + threadIdx.x;
+        for (uint32_t i = threadIdx.x; i < cnt; i += kRasterThreads) {
+            const RasterRecord* R = recs + i;
             const uint2 rr = reinterpret_cast<const uint2*>(R)[5];
             const uint32_t bits = rect_bits(rr.x, rr.y, x0, y0);
-            s_bits[threadIdx.x] = bits;
+            s_bits[i] = bits;
             const uint32_t c = (uint32_t)((bits & 0x00FFu) != 0u) | ((uint32_t)((bits & 0xFF00u) != 0u) << 1);
             const uint32_t r = (uint32_t)((bits & 0x00FF0000u) != 0u) | ((uint32_t)((bits & 0xFF000000u) != 0u) << 1);
             // block w = (w & 1, w >> 1): bit w set iff its column and row halves are covered
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
                     if (m > thr) blocks &= ~(1u << w);
                 }
             }
-            s_mask[threadIdx.x] = (uint8_t)blocks;
+            s_mask[i] = (uint8_t)blocks;
         }
         __syncthreads();
         // Warp-uniform control flow only; per-pixel work is predicated.

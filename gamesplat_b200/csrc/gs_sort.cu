@@ -12,8 +12,9 @@
 //                           keys are skipped: identity for a stable sort;
 //                           ping-pong assignment of the active passes), then
 //                           persistent CTAs take 4096-key tiles in
-//                           ticket order, rank keys with warp match/ballot
-//                           (__match_any_sync), publish per-digit counts,
+//                           ticket order, rank keys within each warp (lanes
+//                           of equal digit found by per-bit ballots), publish
+//                           per-digit counts,
 //                           reorder the tile by digit in shared memory, then
 //                           resolve their global offsets by decoupled
 //                           look-back (bounded spin) and write runs coalesced;
@@ -135,7 +136,6 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
     __shared__ uint32_t s_keys[kSortTile];
     __shared__ uint32_t s_vals[kSortTile];
     __shared__ uint32_t warp_hist[kSortWarps][kRadix];
-    __shared__ uint32_t s_local_start[kRadix];
     __shared__ uint32_t s_global_base[kRadix];
     __shared__ uint32_t scan_tmp[33];
     __shared__ uint32_t s_tile;
@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
     uint32_t* __restrict__ kout = io.kout;
     uint32_t* __restrict__ vout = io.vout;
     const int shift = p.begin_bit + pass * kRadixBits;
-    const uint32_t dmask = (1u << min(kRadixBits, p.end_bit - shift)) - 1u;
+    const int nbits = min(kRadixBits, p.end_bit - shift);
+    const uint32_t dmask = (1u << nbits) - 1u;
     u64* status = p.status + (size_t)pass * p.status_stride;
     const uint32_t num_tiles = (n + kSortTile - 1) / kSortTile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -175,12 +176,25 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
             key[k] = ok ? kin[idx] : 0u;
             val[k] = ok ? vin[idx] : 0u;
         }
-        // Warp ranking in index order (item k, then lane).
+        // Warp ranking in index order (item k, then lane): the lanes holding a
+        // digit find each other; their leader reads and advances the warp's
+        // running count of that digit.
 #pragma unroll
         for (int k = 0; k < kSortItems; ++k) {
             uint32_t idx = wbase + k * 32 + lane;
             uint32_t d = (idx < n) ? digit_of(key[k], shift, dmask) : (uint32_t)kRadix;
-            uint32_t peers = __match_any_sync(0xffffffffu, d);
+            // Lanes with the same digit: one ballot per digit bit (plus one
+            // for validity).  Measured faster than __match_any_sync here.
+            const bool valid = d < (uint32_t)kRadix;
+            const uint32_t vb = __ballot_sync(0xffffffffu, valid);
+            uint32_t peers = valid ? vb : ~vb;
+#pragma unroll
+            for (int bit = 0; bit < kRadixBits; ++bit) {
+                if (bit < nbits) {
+                    const uint32_t bb = __ballot_sync(0xffffffffu, (d >> bit) & 1u);
+                    peers &= ((d >> bit) & 1u) ? bb : ~bb;
+                }
+            }
             int leader = __ffs(peers) - 1;
             uint32_t before = 0;
             if (lane == leader && d < (uint32_t)kRadix) {
@@ -192,30 +206,33 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
             __syncwarp();
         }
         __syncthreads();
-        // One thread per digit: tile count and per-warp exclusive offsets.
+        // One thread per digit: tile count, published at once; then every
+        // warp's start of the digit's run in the reordered tile.
         const uint32_t d = threadIdx.x;
-        uint32_t run = 0;
+        uint32_t c[kSortWarps], tile_count = 0;
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w) {
-            uint32_t c = warp_hist[w][d];
-            warp_hist[w][d] = run;
-            run += c;
+            c[w] = warp_hist[w][d];
+            tile_count += c[w];
         }
-        const uint32_t tile_count = run;
         u64* st = status + (size_t)tile * kRadix + d;
         if (tile == 0) st_relaxed64(st, status_word(p.epoch, kFlagInc, gdigit + tile_count));
         else st_relaxed64(st, status_word(p.epoch, kFlagAgg, tile_count));
-        // Reorder the tile by digit in shared memory while predecessors publish.
         uint32_t total;
         const uint32_t lstart = block_excl_scan(tile_count, scan_tmp, &total);
-        s_local_start[d] = lstart;
+        uint32_t run = lstart;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            warp_hist[w][d] = run;
+            run += c[w];
+        }
         __syncthreads();
+        // Reorder the tile by digit in shared memory while predecessors publish.
 #pragma unroll
         for (int k = 0; k < kSortItems; ++k) {
             uint32_t idx = wbase + k * 32 + lane;
             if (idx < n) {
-                uint32_t dk = digit_of(key[k], shift, dmask);
-                uint32_t lp = s_local_start[dk] + warp_hist[warp][dk] + rank[k];
+                const uint32_t lp = warp_hist[warp][digit_of(key[k], shift, dmask)] + rank[k];
                 s_keys[lp] = key[k];
                 s_vals[lp] = val[k];
             }
@@ -232,8 +249,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
         __syncthreads();
         const uint32_t nvalid = min((uint32_t)kSortTile, n - base);
         for (uint32_t i = threadIdx.x; i < nvalid; i += kSortThreads) {
-            uint32_t k = s_keys[i];
-            uint32_t o = s_global_base[digit_of(k, shift, dmask)] + i;
+            const uint32_t k = s_keys[i];
+            const uint32_t o = s_global_base[digit_of(k, shift, dmask)] + i;
             if (o < n) {  // always true unless a look-back wait ran out
                 kout[o] = k;
                 vout[o] = s_vals[i];
