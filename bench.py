@@ -289,6 +289,48 @@ def run_ours(args):
         dt = time.perf_counter() - t0
         e2e_fps = replicas.whole_job_rate(args.steps, world, replicas.reduce_max(dt, pg, "cuda"))
 
+    # The path's other render modes on the same scene and cameras, with the
+    # renderer's defaults (stochastic: TAA, 4 samples per frame; GPS:
+    # supersample 2, 16 Mi work items): secondary figures, not the headline.
+    modes = {}
+    if not args.no_modes:
+        nm = min(args.steps, 20)
+        for mode in ("stochastic", "gps"):
+            r.set(splat_render_mode=mode, black_background=1)
+            r.reset_stochastic_accumulation()
+            for i in range(3):
+                r.draw_frame(frame(i), out_ptr=out.data_ptr())
+            stream.synchronize()
+            r.profile(True)
+            r.stage_times(reset=True)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for i in range(nm):
+                r.draw_frame(frame(args.warmup + i), out_ptr=out.data_ptr())
+            e1.record(stream)
+            stream.synchronize()
+            mms = e0.elapsed_time(e1) / nm
+            st_m = {k: round(v[0] / nm, 4) for k, v in r.stage_times(reset=True).items() if v[0] > 0}
+            r.profile(False)
+            sm = r.stats()
+            entry = {"ms_per_frame": mms, "fps": 1000.0 / mms, "frames": nm, "stages_ms_per_frame": st_m}
+            if mode == "stochastic":
+                k = r.knobs()
+                entry["samples_per_frame"] = int(k.stochastic_taa_current_samples if k.stochastic_taa_enabled
+                                                 else k.stochastic_samples_per_frame)
+            else:
+                k = r.knobs()
+                ss = int(k.gps_supersample_factor)
+                work = min(int(sm.gps_requested_work_items), int(sm.gps_max_work_items))
+                gps_ms = st_m.get("gps", mms)
+                entry.update({"supersample": ss, "work_items_per_frame": work,
+                              "points_per_s": work * ss * ss / (gps_ms / 1000.0),
+                              "atomics_per_s": work * ss * ss / (gps_ms / 1000.0),
+                              "budget_exhausted": int(sm.gps_budget_exhausted)})
+            modes[mode] = entry
+        r.set(splat_render_mode="alpha", black_background=1)
+
     r.destroy()
     if pg:
         pg.destroy_process_group()
@@ -347,6 +389,7 @@ def run_ours(args):
         "roofline": roofline,
         "dominant_stage": dominant,
         "raster": raster,
+        "modes": modes or None,
         "stages_ms_per_frame": per_frame,
         "hbm_stages": hbm_stages,
         "visible_per_frame": n_vis,
@@ -365,6 +408,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-modes", action="store_true", help="skip the stochastic and GPS mode figures")
     ap.add_argument("--gaussians", type=int, default=3_000_000,
                     help="scene size (the benchmark workload is 3M; smaller only for profiling captures)")
     args = ap.parse_args()

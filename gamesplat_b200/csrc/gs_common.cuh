@@ -50,6 +50,7 @@ __device__ __forceinline__ uint32_t g_f2u_sat(float x) { return __float2uint_rz(
 constexpr float kLn2Hi = 0.693145751953125f;
 constexpr float kLn2Lo = 1.428606765330187e-06f;
 constexpr float kInvLn2 = 1.4426950216293335f;
+constexpr float kLn2f = 0.6931471805599453f;
 constexpr float kPio2Hi = 1.5707855224609375f;
 constexpr float kPio2Lo = 1.0804334124259185e-05f;
 constexpr float kTwoOverPi = 0.6366197466850281f;

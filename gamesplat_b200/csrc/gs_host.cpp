@@ -24,6 +24,7 @@
 
 #include "gs_internal.h"
 #include "gs_extra.h"
+#include "gs_display.h"
 
 using gs::FrameCounters;
 using gs::RasterRecord;
@@ -47,6 +48,11 @@ struct gs_ctx {
     uint32_t num_sms = 148;
     gs_knobs knobs{};
     std::string last_error;
+
+    // display transform LUT (gsanim 0.3 "layers" scenes)
+    uint16_t* display_lut = nullptr;
+    int lut_size = 0;
+    float lut_log2_min = 0.0f, lut_log2_max = 0.0f;
 
     // scene
     uint32_t n = 0;
@@ -692,6 +698,7 @@ void gs_destroy(gs_ctx* c) {
     cudaStreamSynchronize(c->stream);
     release_scene(c);
     release_targets(c);
+    dfree(c->display_lut);
     if (c->h_fc) cudaFreeHost(c->h_fc);
     if (c->h_out16) cudaFreeHost(c->h_out16);
     if (c->fc_event) cudaEventDestroy(c->fc_event);
@@ -825,6 +832,46 @@ int gs_set_gps_budget(gs_ctx* c, uint32_t max_work_items) {
     c->gps_max_work_items = max_work_items;
     gs_reset_accumulation(c);
     return GS_OK;
+}
+
+int gs_set_display_lut(gs_ctx* c, const uint16_t* lut, uint32_t lut_size, float log2_min, float log2_max) {
+    if (!c) return GS_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    // a queued gs_display may still read the old table
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cuda_fail(c, cudaGetLastError(), "stream sync");
+    dfree(c->display_lut);
+    c->lut_size = 0;
+    if (!lut) return GS_OK;
+    // src/gaussian_loader_gsanim.cpp:237,244
+    if (lut_size < 2 || lut_size > 256) return fail(c, GS_ERR_BAD_ARG, "display LUT size must be 2..256");
+    if (!(log2_min < log2_max)) return fail(c, GS_ERR_BAD_ARG, "display LUT needs log2_min < log2_max");
+    const size_t count = (size_t)lut_size * lut_size * lut_size * 3;
+    GS_CUDA(c, dalloc(&c->display_lut, count * sizeof(uint16_t)));
+    GS_CUDA(c, cudaMemcpy(c->display_lut, lut, count * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    c->lut_size = (int)lut_size;
+    c->lut_log2_min = log2_min;
+    c->lut_log2_max = log2_max;
+    return GS_OK;
+}
+
+int gs_display(gs_ctx* c, const uint16_t* rgba16f_in, float* rgba32f_out, int width, int height, float exposure_ev) {
+    if (!c || !rgba16f_in || !rgba32f_out || width <= 0 || height <= 0) return GS_ERR_BAD_ARG;
+    if (((uintptr_t)rgba16f_in & 7u) || ((uintptr_t)rgba32f_out & 15u))
+        return fail(c, GS_ERR_BAD_ARG, "gs_display buffers must be 8-byte (input) and 16-byte (output) aligned");
+    cudaSetDevice(c->device);
+    gs::DisplayParams p{};
+    p.in_rgba16f = rgba16f_in;
+    p.out_rgba32f = reinterpret_cast<float4*>(rgba32f_out);
+    p.width = width;
+    p.height = height;
+    p.lut = c->lut_size ? c->display_lut : nullptr;
+    p.lut_size = c->lut_size;
+    p.log2_min = c->lut_log2_min;
+    p.log2_max = c->lut_log2_max;
+    p.exposure_ev = exposure_ev;
+    gs::launch_display(p, c->num_sms, c->stream);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GS_OK : cuda_fail(c, e, "display kernel launch");
 }
 
 int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {

@@ -162,6 +162,24 @@ class Renderer:
     def reset_stochastic_accumulation(self) -> None:
         L.check(L.lib().gs_reset_accumulation(self._ctx), "gs_reset_accumulation", self._ctx)
 
+    # -- display transform ----------------------------------------------------
+    def set_display_lut(self, lut, log2_min: float = 0.0, log2_max: float = 1.0) -> None:
+        """gsanim 0.3 display LUT: (n, n, n, 3) uint16 indexed [z, y, x, rgb]; None removes it."""
+        if lut is None:
+            L.check(L.lib().gs_set_display_lut(self._ctx, None, 0, 0.0, 0.0), "gs_set_display_lut", self._ctx)
+            return
+        lut = np.ascontiguousarray(lut, dtype=np.uint16)
+        n = lut.shape[0]
+        if lut.shape != (n, n, n, 3):
+            raise ValueError("lut must be (n, n, n, 3) uint16")
+        L.check(L.lib().gs_set_display_lut(self._ctx, lut.ctypes.data, n, float(log2_min), float(log2_max)),
+                "gs_set_display_lut", self._ctx)
+
+    def display(self, in_ptr: int, out_ptr: int, width: int, height: int, exposure_ev: float = 0.0) -> None:
+        """Display pass of a gs_render frame (device addresses; stream-ordered)."""
+        L.check(L.lib().gs_display(self._ctx, C.c_void_p(in_ptr), C.c_void_p(out_ptr), int(width), int(height),
+                                   float(exposure_ev)), "gs_display", self._ctx)
+
     # -- frames ---------------------------------------------------------------
     def draw_frame(self, cam, out_ptr: int | None = None) -> np.ndarray | None:
         """Render one frame.  With out_ptr (device address of W*H*4 halves) the

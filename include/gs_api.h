@@ -172,6 +172,23 @@ int gs_render(gs_ctx* ctx, const gs_camera* cam, void* rgba16f_out);
  * device->host image copy, and waits for them. */
 int gs_render_host(gs_ctx* ctx, const gs_camera* cam, uint16_t* rgba16f_out_host);
 
+/* gsanim 0.3 display LUT: the scene's display_lut, lut_size, log2_min and
+ * log2_max (src/gsanim.h:33-35), uploaded by the renderer at
+ * src/renderer.cpp:870-881.  `lut` holds lut_size^3 x RGB uint16 values (x
+ * fastest, then y, then z), lut_size 2..256, log2_min < log2_max
+ * (src/gaussian_loader_gsanim.cpp:237,244).  Copies; waits for queued work on
+ * the context's stream.  lut = NULL removes it. */
+int gs_set_display_lut(gs_ctx* ctx, const uint16_t* lut, uint32_t lut_size, float log2_min, float log2_max);
+
+/* renderer_display_appearance (src/renderer.cpp:2120-2137): the display pass
+ * of a linear frame, shaders/accum.glsl:201-240 with the LUT, else the blit
+ * (:181-192).  rgba16f_in: a gs_render frame in device memory (width*height*4
+ * halves, 8-byte aligned); rgba32f_out: device memory for width*height*4
+ * floats (16-byte aligned); both top row first.  exposure_ev is the
+ * renderer's exposure_ev (src/renderer.h:168).  Stream-ordered. */
+int gs_display(gs_ctx* ctx, const uint16_t* rgba16f_in, float* rgba32f_out, int width, int height,
+               float exposure_ev);
+
 /* Statistics of the last frame (synchronises). */
 int gs_read_stats(gs_ctx* ctx, gs_stats* out);
 

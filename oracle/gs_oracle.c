@@ -849,3 +849,63 @@ float oc_halton(uint32_t index, uint32_t base) {              /* src/renderer.cp
     }
     return r;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Display transform (shaders/accum.glsl:201-240; blit :181-192).            */
+/* ------------------------------------------------------------------------ */
+float oc_half_to_float(uint16_t h) {
+    uint32_t sign = (uint32_t)(h >> 15) << 31, e = (h >> 10) & 31u, m = h & 1023u;
+    if (e == 31u) return fbits(sign | 0x7f800000u | (m << 13));
+    if (e == 0u) {
+        if (m == 0u) return fbits(sign);
+        float v = (float)m * 5.9604644775390625e-08f;   /* m * 2^-24, exact */
+        return sign ? -v : v;
+    }
+    return fbits(sign | ((e + 112u) << 23) | (m << 13));
+}
+
+static float oc_exp2f_det(float x) { return oc_expf(x * 0.6931471805599453f); }
+static float oc_log2f_det(float x) { return oc_logf(x) * 1.4426950216293335f; }
+
+static float lut_entry(const uint16_t* lut, int n, int x, int y, int z, int c) {
+    int i = ((z * n + y) * n + x) * 3 + c;                    /* shaders/accum.glsl:216-224 */
+    return (float)lut[i] / 65535.0f;
+}
+
+void oc_display(const uint16_t* in_half, int width, int height, const uint16_t* lut, int lut_size,
+                float log2_min, float log2_max, float exposure_ev, float* out_rgba) {
+    size_t npix = (size_t)width * (size_t)height;
+    float gain = oc_exp2f_det(exposure_ev);
+    float lo_clamp = oc_exp2f_det(log2_min);
+    float range = log2_max - log2_min;
+    float top = (float)(lut_size - 1);
+    for (size_t i = 0; i < npix; ++i) {
+        float px[4];
+        for (int c = 0; c < 4; ++c) px[c] = oc_half_to_float(in_half[i * 4 + c]);
+        float* o = out_rgba + i * 4;
+        if (!lut) { for (int c = 0; c < 4; ++c) o[c] = px[c]; continue; }
+        int lo[3], hi[3];
+        float f[3];
+        for (int c = 0; c < 3; ++c) {                          /* :226-232 */
+            float rad = px[c] * gain;
+            float s = g_clamp((oc_log2f_det(g_max(rad, lo_clamp)) - log2_min) / range, 0.0f, 1.0f);
+            if (s != s) s = 0.0f;                              /* NaN input: first lattice entry */
+            float p = s * top;
+            float fl = floorf(p);
+            lo[c] = (int)fl;
+            hi[c] = lo[c] + 1 < lut_size - 1 ? lo[c] + 1 : lut_size - 1;
+            f[c] = p - fl;
+        }
+        for (int c = 0; c < 3; ++c) {                          /* :233-238 */
+            int n = lut_size;
+            float a = g_mix(g_mix(lut_entry(lut, n, lo[0], lo[1], lo[2], c), lut_entry(lut, n, hi[0], lo[1], lo[2], c), f[0]),
+                            g_mix(lut_entry(lut, n, lo[0], hi[1], lo[2], c), lut_entry(lut, n, hi[0], hi[1], lo[2], c), f[0]),
+                            f[1]);
+            float b = g_mix(g_mix(lut_entry(lut, n, lo[0], lo[1], hi[2], c), lut_entry(lut, n, hi[0], lo[1], hi[2], c), f[0]),
+                            g_mix(lut_entry(lut, n, lo[0], hi[1], hi[2], c), lut_entry(lut, n, hi[0], hi[1], hi[2], c), f[0]),
+                            f[1]);
+            o[c] = g_mix(a, b, f[2]);
+        }
+        o[3] = 1.0f;
+    }
+}

@@ -121,6 +121,17 @@ void oc_taa(const float* cur_color, const float* cur_depth, const float* hist_co
             const float* prev_focal_clip, const float* proj_z, float history_valid,
             float view_changed, float* out_color, float* out_xyz);
 
+/* Display transform of a linear RGBA16F frame (shaders/accum.glsl:201-240,
+ * src/renderer.cpp:2120-2137): in_half = width*height*4 IEEE half bit
+ * patterns, lut = lut_size^3 x RGB uint16 (x fastest), or NULL for the plain
+ * blit (shaders/accum.glsl:181-192).  out_rgba: width*height*4 floats.
+ * exp2/log2 are oc_expf/oc_logf scaled by ln 2. */
+void oc_display(const uint16_t* in_half, int width, int height, const uint16_t* lut, int lut_size,
+                float log2_min, float log2_max, float exposure_ev, float* out_rgba);
+
+/* IEEE half bit pattern -> float (exact). */
+float oc_half_to_float(uint16_t h);
+
 /* Halton radical inverse (src/renderer.cpp:246-255). */
 float oc_halton(uint32_t index, uint32_t base);
 

@@ -18,6 +18,7 @@ SENTINEL = 0xFFFFFFFF
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_u16p = np.ctypeslib.ndpointer(np.uint16, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 
 
@@ -103,6 +104,11 @@ def lib():
                              _f32p, _f32p, C.c_float, C.c_float, _f32p, _f32p]
         L.oc_halton.restype = C.c_float
         L.oc_halton.argtypes = [C.c_uint32, C.c_uint32]
+        L.oc_display.restype = None
+        L.oc_display.argtypes = [_u16p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_float,
+                                 _f32p]
+        L.oc_half_to_float.restype = C.c_float
+        L.oc_half_to_float.argtypes = [C.c_uint16]
         _lib = L
     return _lib
 
@@ -212,6 +218,22 @@ def gps_frame(ids: np.ndarray, projected: np.ndarray, width: int, height: int, s
                        int(supersample), int(max_work_items), float(clip_z_01), int(bool(linear_color)),
                        float(frame_seed), float(bg), out.reshape(-1), depth.reshape(-1), stats)
     return out, depth, int(stats[0]), int(stats[1])
+
+
+def display(img_half: np.ndarray, lut, log2_min: float, log2_max: float, exposure_ev: float) -> np.ndarray:
+    """Display transform (shaders/accum.glsl:201-240, or the blit when lut is None) of an
+    (H, W, 4) float16 frame; lut is (n, n, n, 3) uint16 indexed [z, y, x, rgb].  -> (H, W, 4) float32."""
+    img = np.ascontiguousarray(img_half, np.float16)
+    h, w = img.shape[:2]
+    out = np.empty((h, w, 4), np.float32)
+    if lut is None:
+        lp, n = None, 0
+    else:
+        lut = np.ascontiguousarray(lut, np.uint16)
+        lp, n = lut.ctypes.data, lut.shape[0]
+    lib().oc_display(img.view(np.uint16).reshape(-1), w, h, lp, n, float(log2_min), float(log2_max),
+                     float(exposure_ev), out.reshape(-1))
+    return out
 
 
 def accum(sample: np.ndarray, history: np.ndarray, n: float):
