@@ -12,9 +12,10 @@
 // walks.
 //
 // The CTA tile's entries are written by a load-balanced expansion (entry e
-// finds its splat by binary search over the CTA's offsets), so the stores are
-// coalesced however many tiles a splat covers; the tile ids' digit
-// histograms for the tile sort are accumulated on the way.
+// finds its splat through a chunked owner map: marks at each splat's first
+// entry, then a block prefix maximum), so the stores are coalesced however
+// many tiles a splat covers; the tile ids' digit histograms for the tile sort
+// are accumulated on the way.
 //
 // Tile selection is conservative: the covered rectangle is intersected with
 // the bounding box of the ellipse where the Gaussian's alpha reaches 1/255

@@ -216,6 +216,14 @@ constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1u;
 typedef unsigned long long u64;
 
+// Programmatic dependent launch: a kernel launched with launch_pdl() may be
+// scheduled while its predecessor in the stream still runs, and must wait
+// here before touching anything the predecessor writes; a kernel triggers
+// early scheduling of its dependent once all of its CTAs have called
+// pdl_trigger() (or exited).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Status words carry their whole message (flag + value); the data a tile
 // writes is read only by later kernels, so publishing needs no release
 // ordering, and a relaxed GPU-scope store avoids a memory barrier per tile.

@@ -167,6 +167,25 @@ struct RasterParams {
     FrameCounters* fc;
 };
 
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while its predecessor in the stream finishes, and calls pdl_wait() before
+// it reads or writes anything the predecessor touches.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Launchers (each returns the number of kernels it launched).
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s);

@@ -133,6 +133,8 @@ __device__ PassIO plan_passes(const SortParams& p, int npasses, int pass, uint32
 }
 
 __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p, int pass, int npasses) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ uint32_t s_keys[kSortTile];
     __shared__ uint32_t s_vals[kSortTile];
     __shared__ uint32_t warp_hist[kSortWarps][kRadix];
@@ -261,6 +263,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
 }
 
 __global__ void sort_copy_kernel(SortParams p) {
+    pdl_wait();
+    pdl_trigger();
     const SortPlan* pl = p.plan;
     if (!pl->copy_needed) return;
     const uint32_t n = pl->count;
@@ -291,14 +295,19 @@ int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s) {
     uint32_t pass_grid = num_sms * (uint32_t)g_pass_blocks_per_sm;
     if (pass_grid > tiles_cap) pass_grid = tiles_cap > 0 ? tiles_cap : 1;
     for (int ps = 0; ps < npasses; ++ps) {
-        sort_pass_kernel<<<pass_grid, kSortThreads, 0, s>>>(p, ps, npasses);
+        // Passes after the first overlap their launch with the previous pass's
+        // tail (programmatic dependent launch).  Across stage boundaries
+        // (cull -> sort, bin -> tile sort) it measured slower, so the first
+        // pass is an ordinary launch.
+        if (ps == 0) sort_pass_kernel<<<pass_grid, kSortThreads, 0, s>>>(p, ps, npasses);
+        else launch_pdl(sort_pass_kernel, dim3(pass_grid), dim3(kSortThreads), 0, s, p, ps, npasses);
         ++launches;
     }
     if (p.land_in_buf0) {
         uint32_t g = (p.count_cap + 1023) / 1024;
         if (g > num_sms * 4) g = num_sms * 4;
         if (g == 0) g = 1;
-        sort_copy_kernel<<<g, 256, 0, s>>>(p);
+        launch_pdl(sort_copy_kernel, dim3(g), dim3(256), 0, s, p);
         ++launches;
     }
     return launches;
