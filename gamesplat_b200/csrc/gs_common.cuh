@@ -283,13 +283,15 @@ __device__ __forceinline__ uint32_t lookback_vec(const u64* status, size_t strid
 // Warp-cooperative look-back: all 32 lanes read a window of 32 predecessors
 // at once, the nearest inclusive word is found by ballot and the aggregates
 // after it are summed with a warp reduction.  Every lane returns the same
-// exclusive prefix.  Bounded like lookback_vec().
+// exclusive prefix, and every lane sees *timed_out if any lane's wait ran
+// out.  Bounded like lookback_vec().
 __device__ __forceinline__ uint32_t lookback_warp(const u64* status, uint32_t tile, uint32_t epoch,
-                                                  bool* timed_out) {
+                                                  bool* timed_out, uint32_t spin_limit = kSpinLimit) {
     const int lane = threadIdx.x & 31;
     uint32_t excl = 0;
     long long end = (long long)tile;  // window = [end - 32, end)
     uint32_t spins = 0;
+    bool ran_out = false;   // this lane's wait gave up (made warp-uniform at the end)
     while (end > 0) {
         const long long j = end - 32 + lane;
         uint32_t flag = kFlagInc, val = 0;   // before tile 0: an inclusive zero
@@ -299,7 +301,7 @@ __device__ __forceinline__ uint32_t lookback_warp(const u64* status, uint32_t ti
                 flag = (uint32_t)w & ~kValMask;
                 val = (uint32_t)w & kValMask;
                 if ((uint32_t)(w >> 32) == epoch && flag != 0u) break;
-                if (++spins > kSpinLimit) { *timed_out = true; flag = kFlagInc; val = 0; break; }
+                if (++spins > spin_limit) { ran_out = true; flag = kFlagInc; val = 0; break; }
                 if (spins > 64) __nanosleep(32);
             }
         }
@@ -312,6 +314,7 @@ __device__ __forceinline__ uint32_t lookback_warp(const u64* status, uint32_t ti
         excl += __reduce_add_sync(0xffffffffu, val);
         end -= 32;
     }
+    if (__any_sync(0xffffffffu, ran_out)) *timed_out = true;
     return excl;
 }
 

@@ -874,6 +874,29 @@ int gs_display(gs_ctx* c, const uint16_t* rgba16f_in, float* rgba32f_out, int wi
     return e == cudaSuccess ? GS_OK : cuda_fail(c, e, "display kernel launch");
 }
 
+int gs_debug_wait_probe(gs_ctx* c, int which, uint32_t spin_limit) {
+    if (!c || which < 0 || which > 1 || spin_limit == 0) return GS_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    // private words: the frame's counters and status arrays stay untouched
+    void* mem = nullptr;
+    const size_t status_bytes = 64 * sizeof(unsigned long long);
+    GS_CUDA(c, cudaMalloc(&mem, status_bytes + sizeof(FrameCounters)));
+    auto* status = static_cast<unsigned long long*>(mem);
+    auto* fc = reinterpret_cast<FrameCounters*>(static_cast<char*>(mem) + status_bytes);
+    cudaError_t e = cudaMemsetAsync(mem, 0, status_bytes + sizeof(FrameCounters), c->stream);
+    if (e == cudaSuccess) {
+        gs::launch_wait_probe(status, fc, /*epoch*/ 1u, which, spin_limit, c->stream);
+        e = cudaGetLastError();
+    }
+    FrameCounters h{};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, fc, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(mem);
+    if (e != cudaSuccess) return cuda_fail(c, e, "wait probe");
+    if (h.error_flags) return fail(c, GS_ERR_DEVICE_TIMEOUT, "a device-side wait ran out (probe)");
+    return GS_OK;
+}
+
 int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
     if (!c || !cam || !out) return GS_ERR_BAD_ARG;
     if (!c->n) return fail(c, GS_ERR_NO_SCENE, "no scene uploaded");

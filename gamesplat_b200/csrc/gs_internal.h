@@ -195,6 +195,9 @@ int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint3
 int launch_raster_alpha(const RasterParams& p, cudaStream_t s);
 int launch_raster_stochastic(const RasterParams& p, cudaStream_t s);
 
+int launch_wait_probe(const unsigned long long* status, FrameCounters* fc, uint32_t epoch, int which, uint32_t limit,
+                      cudaStream_t s);
+
 size_t sort_status_words(uint32_t count_cap);   // look-back words per pass
 int sort_passes(int begin_bit, int end_bit);
 }  // namespace gs

@@ -40,8 +40,8 @@ __device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t phase) {
 
 // Wait for completion of phase `phase` with a bounded number of polls.
 // Returns false if the limit ran out (the caller records an error flag).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
-    for (uint32_t i = 0; i < (1u << 22); ++i) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t limit = 1u << 22) {
+    for (uint32_t i = 0; i < limit; ++i) {
         if (mbar_test_wait(bar, phase)) return true;
         if (i > 16) __nanosleep(20);
     }

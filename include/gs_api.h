@@ -189,6 +189,14 @@ int gs_set_display_lut(gs_ctx* ctx, const uint16_t* lut, uint32_t lut_size, floa
 int gs_display(gs_ctx* ctx, const uint16_t* rgba16f_in, float* rgba32f_out, int width, int height,
                float exposure_ev);
 
+/* Diagnostics, no counterpart in the reference (its GL path has no device
+ * waits): runs one of the library's bounded device waits against a word that
+ * nothing publishes (which = 0: decoupled look-back; 1: mbarrier / TMA
+ * completion) with at most spin_limit polls, on private memory, and returns
+ * what a frame would: GS_ERR_DEVICE_TIMEOUT once the wait runs out.  The
+ * context stays usable.  Synchronises; allocates a few hundred bytes. */
+int gs_debug_wait_probe(gs_ctx* ctx, int which, uint32_t spin_limit);
+
 /* Statistics of the last frame (synchronises). */
 int gs_read_stats(gs_ctx* ctx, gs_stats* out);
 
