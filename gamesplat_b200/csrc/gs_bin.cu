@@ -39,19 +39,35 @@ __device__ __forceinline__ BinItem bin_one(const BinParams& p, uint32_t s, uint3
     const float4 co = P[0], cr = P[1], cd = P[2];
     PixelRect q;
     const float cutoff = alpha_cutoff(co.w);
-    bool ok = quad_rect(cr.x, cr.y, cr.z, cr.w, cd.w, p.jitter_x, p.jitter_y, vp_w, vp_h, ysign, p.width, p.height,
-                        &q);
+    bool ok;
+    if (p.envelope) {
+        // every quad of a jitter in [-0.5, 0.5]^2 lies inside the quad of
+        // radius + 0.5 without jitter; a pixel more on each side absorbs the
+        // snapping of the two rectangles' edges
+        ok = quad_rect(cr.x, cr.y, add(cr.z, 0.5f), add(cr.w, 0.5f), cd.w, 0.0f, 0.0f, vp_w, vp_h, ysign, p.width,
+                       p.height, &q);
+        if (ok) {
+            q.i0 = max(q.i0 - 1, 0);
+            q.j0 = max(q.j0 - 1, 0);
+            q.i1 = min(q.i1 + 1, p.width);
+            q.j1 = min(q.j1 + 1, p.height);
+        }
+    } else {
+        ok = quad_rect(cr.x, cr.y, cr.z, cr.w, cd.w, p.jitter_x, p.jitter_y, vp_w, vp_h, ysign, p.width, p.height, &q);
+    }
     ok = ok && cutoff <= 0.0f;
     if (!ok) return it;
     const float ccx = add(cr.x, p.jitter_x), ccy = add(cr.y, p.jitter_y);
     PixelRect rc = q;
-    // Bounding box of {d : conic(d) <= -2 cutoff}, widened by a pixel.
+    // Bounding box of {d : conic(d) <= -2 cutoff}, widened by a pixel (and by
+    // the jitter's half pixel in envelope mode).
     const float cx = cd.x, cy = cd.y, cz = cd.z;
     const float k = -2.0f * cutoff;
     const float dt = cx * cz - cy * cy;
+    const float margin = p.envelope ? 1.5f : 1.0f;
     if (dt > 0.0f) {
-        float hx = sqrtf(k * cz / dt) * 1.001f + 1.0f;
-        float hy = sqrtf(k * cx / dt) * 1.001f + 1.0f;
+        float hx = sqrtf(k * cz / dt) * 1.001f + margin;
+        float hy = sqrtf(k * cx / dt) * 1.001f + margin;
         float fi0 = ceilf(ccx - hx - 0.5f), fi1 = floorf(ccx + hx - 0.5f);
         float fj0 = ceilf(ccy - hy - 0.5f), fj1 = floorf(ccy + hy - 0.5f);
         rc.i0 = max(rc.i0, (int)fmaxf(fi0, -1.0f));
@@ -87,6 +103,13 @@ __device__ __forceinline__ BinItem bin_one(const BinParams& p, uint32_t s, uint3
     rec.splat_id = id;
     rec.hash_z = add((float)id, p.frame_seed);
     rec.opacity = co.w;
+    if (p.envelope) {   // the rasterizer derives each sample's quad from these
+        rec.cx = cr.x;
+        rec.cy = cr.y;
+        rec.log2_opacity = cr.z;
+        rec.rect_x = __float_as_uint(cd.w);
+        rec.rect_y = __float_as_uint(cr.w);
+    }
     float4* dst = reinterpret_cast<float4*>(p.records + s);
     const float4* src = reinterpret_cast<const float4*>(&rec);
     dst[0] = src[0];

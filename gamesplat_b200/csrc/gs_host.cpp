@@ -371,19 +371,9 @@ void run_depth_sort(gs_ctx* c) {
 }
 
 // Binning, tile sort and tile ranges for one raster pass.
-void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
+void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = false) {
     {
         StageScope sc(c, ST_BIN);
-        if (reset_ranges) {
-            // A second pass in the same frame: clear ranges, counters and the tile-sort plan.
-            cudaMemsetAsync(c->tile_ranges, 0, (size_t)c->tiles_cap * sizeof(uint2), c->stream);
-            cudaMemsetAsync(c->tile_plan, 0, sizeof(SortPlan), c->stream);
-            cudaMemsetAsync(c->tile_hist, 0, 4 * 256 * 4, c->stream);
-            // bin_ticket, tile_entries, tile_overflow are adjacent in FrameCounters.
-            cudaMemsetAsync(&c->fc->bin_ticket, 0, 3 * sizeof(uint32_t), c->stream);
-            ++c->epoch;
-            if (c->epoch == 0) ++c->epoch;
-        }
         gs::BinParams p{};
         p.depth_plan = c->depth_plan;
         p.projected = c->projected;
@@ -405,6 +395,7 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool reset_ranges) {
         p.status = c->bin_status;
         p.epoch = c->epoch;
         p.fc = c->fc;
+        p.envelope = envelope ? 1 : 0;
         sc.add(gs::launch_bin(p, c->n, c->num_sms, c->stream));
 
     }
@@ -455,7 +446,7 @@ float background(const gs_ctx* c) { return c->knobs.black_background ? 0.0f : 0.
 int render_alpha(gs_ctx* c, uint16_t* out) {
     run_cull(c);
     run_depth_sort(c);
-    run_binning(c, 0.0f, 0.0f, 0.0f, false);
+    run_binning(c, 0.0f, 0.0f, 0.0f);
     StageScope sc(c, ST_RASTER);
     gs::RasterParams r = raster_params(c, background(c));
     r.out_rgba16f = out;
@@ -503,6 +494,9 @@ int render_stochastic(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
 
     run_cull(c);
     run_depth_sort(c);
+    // One binning for every sample of the frame: tiles for any jitter, the
+    // rasterizer derives each sample's quad coverage.
+    run_binning(c, 0.0f, 0.0f, 0.0f, /*envelope*/ true);
     uint32_t write_index = c->accum_write_index & 1u;
     bool display_accum = false;
     for (uint32_t i = 0; i < render_samples; ++i) {
@@ -513,10 +507,15 @@ int render_stochastic(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
             jx = halton(jitter_index, 2u) - 0.5f;
             jy = halton(jitter_index, 3u) - 0.5f;
         }
-        run_binning(c, jx, jy, (float)c->frame_seed, i > 0);
         {
             StageScope sc(c, ST_RASTER);
             gs::RasterParams r = raster_params(c, bg);
+            r.jitter_x = jx;
+            r.jitter_y = jy;
+            r.frame_seed = (float)c->frame_seed;
+            r.vp_w = c->cam.viewport[0];
+            r.vp_h = c->cam.viewport[1];
+            r.clip_y_sign = c->cam.clip_y_sign;
             r.out_rgba32f = c->st.sample;
             r.out_depth = c->st.depth;
             r.rgba8 = c->knobs.linear_color ? 0 : 1;

@@ -83,6 +83,10 @@ constexpr int kTileH = 16;
 // exactly when -kSMin <= s <= s_max, with s_max = -2 cutoff, or the smallest
 // subnormal when cutoff == 0 (multiplying by -0.5 is exact except for
 // subnormal s, and those cases are what the two bounds absorb).
+//
+// Stochastic envelope records (BinParams::envelope) reuse three slots:
+// log2_opacity holds radius_x, rect_x holds the bits of ndc_z and rect_y the
+// bits of radius_y; cx, cy are un-jittered and hash_z is unused.
 struct __align__(16) RasterRecord {
     float cx, cy, conic_x, conic_2y;     // centre (+jitter), conic.x, 2*conic.y
     float conic_z, log2_opacity, s_max, r;
@@ -151,6 +155,11 @@ struct BinParams {
     unsigned long long* status;      // per-CTA-tile look-back words (epoch-tagged)
     uint32_t epoch;
     FrameCounters* fc;
+    // 1: stochastic envelope mode.  Tiles are chosen for every sub-pixel
+    // jitter in [-0.5, 0.5]^2 at once and the records keep the un-jittered
+    // quad (centre, radii, ndc_z), so one binning serves all samples of a
+    // frame; the rasterizer derives each sample's coverage.
+    int envelope;
 };
 
 struct RasterParams {
@@ -160,6 +169,10 @@ struct RasterParams {
     const uint2* tile_ranges;        // [start, end) per tile
     int width, height, tiles_x, tiles_y;
     float bg;
+    // stochastic mode (envelope records): the sample's jitter and seed, and
+    // the viewport of the quad computation
+    float jitter_x, jitter_y, frame_seed;
+    float vp_w, vp_h, clip_y_sign;
     uint16_t* out_rgba16f;           // width*height*4 halves, top row first
     float4* out_rgba32f;             // optional float copy (stochastic sample), top row first
     float* out_depth;                // optional window depth (stochastic), top row first

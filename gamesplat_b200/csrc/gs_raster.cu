@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ uint32_t s_bits[kBatch];
     __shared__ uint8_t s_mask[kBatch];
+    __shared__ float4 s_cen[kMode == 1 ? kBatch : 1];   // stochastic: jittered centre and hash z of the sample
 
     const uint32_t tile = blockIdx.x;
     const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
@@ -218,7 +219,26 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         for (uint32_t i = threadIdx.x; i < cnt; i += kRasterThreads) {
             const RasterRecord* R = recs + i;
             const uint2 rr = reinterpret_cast<const uint2*>(R)[5];
-            const uint32_t bits = rect_bits(rr.x, rr.y, x0, y0);
+            uint32_t bits;
+            float cen_x, cen_y;
+            if (kMode == 1) {
+                // envelope record: this sample's quad (same computation as
+                // the per-sample binning of the oracle) and jittered centre
+                PixelRect q;
+                const bool qok = quad_rect(R->cx, R->cy, R->log2_opacity, __uint_as_float(rr.y), __uint_as_float(rr.x),
+                                           p.jitter_x, p.jitter_y, p.vp_w, p.vp_h, p.clip_y_sign, p.width, p.height,
+                                           &q);
+                bits = qok ? rect_bits((uint32_t)q.i0 | ((uint32_t)q.i1 << 16), (uint32_t)q.j0 | ((uint32_t)q.j1 << 16),
+                                       x0, y0)
+                           : 0u;
+                cen_x = add(R->cx, p.jitter_x);
+                cen_y = add(R->cy, p.jitter_y);
+                s_cen[i] = make_float4(cen_x, cen_y, add((float)R->splat_id, p.frame_seed), 0.0f);
+            } else {
+                bits = rect_bits(rr.x, rr.y, x0, y0);
+                cen_x = R->cx;
+                cen_y = R->cy;
+            }
             s_bits[i] = bits;
             const uint32_t c = (uint32_t)((bits & 0x00FFu) != 0u) | ((uint32_t)((bits & 0xFF00u) != 0u) << 1);
             const uint32_t r = (uint32_t)((bits & 0x00FF0000u) != 0u) | ((uint32_t)((bits & 0xFF000000u) != 0u) << 1);
@@ -232,8 +252,8 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
                 for (uint32_t todo_w = blocks; todo_w; todo_w &= todo_w - 1u) {
                     const int w = __ffs(todo_w) - 1;
                     const uint32_t cb = (bits >> (8 * (w & 1))) & 0xFFu, rb = (bits >> (16 + 8 * (w >> 1))) & 0xFFu;
-                    const float bx = (float)(x0 + 8 * (w & 1)) + 0.5f - q0.x;
-                    const float by = (float)(y0 + 8 * (w >> 1)) + 0.5f - q0.y;
+                    const float bx = (float)(x0 + 8 * (w & 1)) + 0.5f - cen_x;
+                    const float by = (float)(y0 + 8 * (w >> 1)) + 0.5f - cen_y;
                     const float m = min_q_box(A, B, C, bx + (float)(__ffs(cb) - 1), bx + (float)(31 - __clz(cb)),
                                               by + (float)(__ffs(rb) - 1), by + (float)(31 - __clz(rb)));
                     if (m > thr) blocks &= ~(1u << w);
@@ -250,9 +270,16 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
             while (todo) {
                 const uint32_t j = c + (uint32_t)(__ffs(todo) - 1);
                 todo &= todo - 1u;
-                const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
+                float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
                 const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
                 const uint32_t bits = s_bits[j];
+                float hz = 0.0f;
+                if (kMode == 1) {
+                    const float4 cz = s_cen[j];
+                    q0.x = cz.x;
+                    q0.y = cz.y;
+                    hz = cz.z;
+                }
                 // splat_power()'s sum for both pixels with the shared first term
                 const float dx = sub(fcx, q0.x);
                 const float t0 = mul(mul(q0.z, dx), dx);
@@ -283,7 +310,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
                     const bool b0 = z24 < S0.best_d24 || (z24 == S0.best_d24 && id < S0.best_id);
                     const bool b1 = z24 < S1.best_d24 || (z24 == S1.best_d24 && id < S1.best_id);
                     const float2 q2 = reinterpret_cast<const float2*>(recs + j)[4];
-                    const float hz = __uint_as_float(q3.z), op = __uint_as_float(q3.w);
+                    const float op = __uint_as_float(q3.w);
                     if (live0 && !sdone0 && b0) stoch_step(S0, sq.x, op, fcx, fcy0, hz, z24, id, q1.w, q2.x, q2.y);
                     if (live1 && !sdone1 && b1) stoch_step(S1, sq.y, op, fcx, fcy1, hz, z24, id, q1.w, q2.x, q2.y);
                 }
