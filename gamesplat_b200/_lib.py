@@ -40,7 +40,7 @@ EXPORTS = (
     "gs_read_stats", "gs_debug_read", "gs_profile_enable", "gs_stage_times", "gs_stage_names", "gs_status_str",
     "gs_last_error", "gs_camera_uniforms", "gs_load_ply", "gs_pack_raw", "gs_sort_pairs_scratch_bytes",
     "gs_sort_pairs", "gs_sort_pairs_noalloc", "gs_upload_anim", "gs_set_anim_state", "gs_set_display_lut",
-    "gs_display", "gs_debug_wait_probe",
+    "gs_display", "gs_debug_wait_probe", "gs_pack_raw_device",
 )
 
 
@@ -149,6 +149,7 @@ def lib() -> C.CDLL:
         "gs_set_display_lut": (i32, [vp, vp, u32, C.c_float, C.c_float]),
         "gs_display": (i32, [vp, vp, vp, i32, i32, C.c_float]),
         "gs_debug_wait_probe": (i32, [vp, i32, u32]),
+        "gs_pack_raw_device": (i32, [vp, u64, vp, vp]),
         "gs_upload_anim": (i32, [vp, vp, u32, vp]),
         "gs_set_anim_state": (i32, [vp, i32, i32, f32]),
     }

@@ -235,6 +235,17 @@ int64_t gs_load_ply(const char* path, float* rows, uint64_t capacity);
  * opacity, scale_0..2, rot_0..3 (the 3DGS property order). */
 int gs_pack_raw(const float* raw, uint64_t count, float* rows);
 
+/* gs_pack_raw on the device (the loader transforms of
+ * src/gaussian_loader_ply.cpp:148-203 and pack_gpu_gaussians,
+ * src/gaussian.cpp:53-73): raw_dev and rows_dev are device memory (rows
+ * 16-byte aligned), stream-ordered on `stream` (a cudaStream_t, NULL = the
+ * default stream).  exp is correctly rounded here, while the reference's
+ * loader calls expf: where expf is not correctly rounded (about 0.008 % of
+ * float arguments) a scale can differ by one ulp and an opacity by up to two
+ * (through 1 / (1 + exp(-x))); every other field is identical.  Feed the
+ * rows to gs_upload_rows_device. */
+int gs_pack_raw_device(const float* raw_dev, uint64_t count, float* rows_dev, void* stream);
+
 /* ---- stage-level entry points (device pointers, stream-ordered) ---------- */
 
 /* Scratch bytes gs_sort_pairs needs for n pairs. */
