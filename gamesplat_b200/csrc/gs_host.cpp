@@ -103,6 +103,7 @@ struct gs_ctx {
     uint16_t* out16 = nullptr;     // internal RGBA16F (gs_render_host)
     uint16_t* h_out16 = nullptr;   // pinned
     size_t h_out16_bytes = 0;
+    cudaEvent_t chunk_events[8] = {};   // gs_render_host: readback chunks of a pageable destination
     gs::StochasticTargets st{};
     gs::GpsTargets gps{};
     uint32_t gps_max_work_items = 16u * 1024u * 1024u;
@@ -700,6 +701,8 @@ void gs_destroy(gs_ctx* c) {
     dfree(c->display_lut);
     if (c->h_fc) cudaFreeHost(c->h_fc);
     if (c->h_out16) cudaFreeHost(c->h_out16);
+    for (auto e : c->chunk_events)
+        if (e) cudaEventDestroy(e);
     if (c->fc_event) cudaEventDestroy(c->fc_event);
     for (auto& p : c->pending) {
         cudaEventDestroy(p.a);
@@ -924,7 +927,12 @@ int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
     int rc = ensure_targets(c, w, h);
     if (rc) return rc;
     const size_t bytes = (size_t)w * h * 8;
-    if (c->h_out16_bytes < bytes) {
+    // A page-locked destination is written by the copy engine directly;
+    // a pageable one goes through the context's pinned staging buffer.
+    cudaPointerAttributes pa{};
+    const bool pinned_out = cudaPointerGetAttributes(&pa, host_out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();   // a pageable pointer may leave an error to clear on older drivers
+    if (!pinned_out && c->h_out16_bytes < bytes) {
         if (c->h_out16) cudaFreeHost(c->h_out16);
         c->h_out16 = nullptr;
         c->h_out16_bytes = 0;
@@ -938,10 +946,37 @@ int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
         const bool pvalid = c->prev_cam_valid, tvalid = c->taa_prev_valid;
         rc = gs_render(c, cam, c->out16);
         if (rc) return rc;
-        GS_CUDA(c, cudaMemcpyAsync(c->h_out16, c->out16, bytes, cudaMemcpyDeviceToHost, c->stream));
-        GS_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (pinned_out) {
+            GS_CUDA(c, cudaMemcpyAsync(host_out, c->out16, bytes, cudaMemcpyDeviceToHost, c->stream));
+        } else {
+            // eight chunks, each with an event, so the host copies chunk i out of
+            // the staging buffer while the copy engine brings in chunk i + 1
+            for (int k = 0; k < 8; ++k) {
+                if (!c->chunk_events[k])
+                    GS_CUDA(c, cudaEventCreateWithFlags(&c->chunk_events[k], cudaEventDisableTiming));
+                const size_t b0 = bytes * k / 8, b1 = bytes * (k + 1) / 8;
+                GS_CUDA(c, cudaMemcpyAsync(reinterpret_cast<char*>(c->h_out16) + b0,
+                                           reinterpret_cast<const char*>(c->out16) + b0, b1 - b0,
+                                           cudaMemcpyDeviceToHost, c->stream));
+                GS_CUDA(c, cudaEventRecord(c->chunk_events[k], c->stream));
+            }
+        }
+        GS_CUDA(c, cudaEventSynchronize(c->fc_event));   // the frame's counters (recorded before the image copy)
         c->fc_pending = false;
-        if (!c->h_fc->tile_overflow) break;
+        if (!c->h_fc->tile_overflow) {
+            if (!pinned_out) {
+                for (int k = 0; k < 8; ++k) {
+                    const size_t b0 = bytes * k / 8, b1 = bytes * (k + 1) / 8;
+                    GS_CUDA(c, cudaEventSynchronize(c->chunk_events[k]));
+                    std::memcpy(reinterpret_cast<char*>(host_out) + b0, reinterpret_cast<const char*>(c->h_out16) + b0,
+                                b1 - b0);
+                }
+            } else {
+                GS_CUDA(c, cudaStreamSynchronize(c->stream));
+            }
+            break;
+        }
+        GS_CUDA(c, cudaStreamSynchronize(c->stream));
         uint64_t need = (uint64_t)c->h_fc->tile_entries + c->h_fc->tile_overflow;
         rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(need + need / 4 + 1024, 0x3FFFFFFFull));
         if (rc) return rc;
@@ -952,7 +987,12 @@ int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
         c->prev_cam_valid = pvalid;
         c->taa_prev_valid = tvalid;
     }
-    std::memcpy(host_out, c->h_out16, bytes);
+    if (c->h_fc->tile_overflow && !pinned_out) {
+        // still overflowing after the retries: hand back the last frame as is
+        // (gs_stats reports the overflow)
+        GS_CUDA(c, cudaStreamSynchronize(c->stream));
+        std::memcpy(host_out, c->h_out16, bytes);
+    }
     if (c->h_fc->error_flags & ~(uint32_t)gs::kErrTileOverflow)
         return fail(c, GS_ERR_DEVICE_TIMEOUT, "a device-side wait ran out");
     return GS_OK;
