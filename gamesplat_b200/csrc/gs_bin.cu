@@ -119,20 +119,22 @@ __device__ __forceinline__ BinItem bin_one(const BinParams& p, uint32_t s, uint3
     return it;
 }
 
+// Per-item entry information for the expansion kernel (item q = CTA tile *
+// kBinTile + position in the tile): global offset of its first entry, tile
+// rectangle origin tx0 | ty0 << 16, and width in tiles (0 when it has no
+// entries).
+
 __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
     __shared__ uint32_t scan_tmp[33];
     __shared__ uint32_t s_tile, s_excl, s_total;
     __shared__ uint32_t s_off[kBinTile];    // exclusive entry offset of each splat in the CTA tile
     __shared__ uint32_t s_org[kBinTile];    // tx0 | ty0 << 16 of its tile rectangle
-    __shared__ uint16_t s_w[kBinTile];      // width of its tile rectangle (tiles)
-    __shared__ uint32_t s_hist[3][256];     // tile-id digit histograms for the tile sort
-    __shared__ __align__(16) int32_t s_own[kBinChunk];   // owning splat of each entry of the current chunk
+    __shared__ uint16_t s_w[kBinTile];      // its width in tiles (0: no entries)
     const uint32_t n_vis = p.fc->visible_count;
     const uint32_t num_tiles = (n_vis + kBinTile - 1) / kBinTile;
     const uint32_t* __restrict__ sorted_ids = p.depth_plan->vfinal;
     const float vp_w = p.vp_w, vp_h = p.vp_h, ysign = p.clip_y_sign;
     const int t = threadIdx.x;
-    for (int i = t; i < 3 * 256; i += kBinThreads) (&s_hist[0][0])[i] = 0u;
 
     for (;;) {
         if (t == 0) s_tile = atomicAdd(&p.fc->bin_ticket, 1u);
@@ -140,8 +142,7 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
         const uint32_t tile = s_tile;
         if (tile >= num_tiles) break;
         // CTA tile b holds sorted positions top - 1, top - 2, ..., down to
-        // top - kBinTile (nearest splats first: their large footprints make
-        // the heavy tiles, which are then taken first instead of last).
+        // top - kBinTile (nearest splats first).
         const uint32_t top = n_vis - tile * kBinTile;
         const uint32_t cnt = min((uint32_t)kBinTile, top);
         // Splats striped over threads (coalesced id loads and record writes).
@@ -158,8 +159,8 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
                                                    : BinItem{0u, 0, -1, 0, -1};
             const int slot = i * kBinThreads + t;
             s_off[slot] = it.count;
-            s_org[slot] = (uint32_t)it.tx0 | ((uint32_t)it.ty0 << 16);
-            s_w[slot] = (uint16_t)(it.tx1 - it.tx0 + 1);
+            s_org[slot] = it.count ? (uint32_t)it.tx0 | ((uint32_t)it.ty0 << 16) : 0u;
+            s_w[slot] = it.count ? (uint16_t)(it.tx1 - it.tx0 + 1) : (uint16_t)0;
         }
         __syncthreads();
         // Exclusive scan of the counts in splat order (blocked: 4 per thread).
@@ -171,10 +172,8 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
         }
         uint32_t total;
         uint32_t run = block_excl_scan(sum, scan_tmp, &total);
-        uint32_t off[kBinItems];
 #pragma unroll
         for (int k = 0; k < kBinItems; ++k) {
-            off[k] = run;
             s_off[t * kBinItems + k] = run;
             run += c[k];
         }
@@ -206,55 +205,88 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
             }
         }
         __syncthreads();
-        // Load-balanced expansion in chunks of kBinChunk entries: each
-        // non-empty splat marks its first entry with its index, and a
-        // block-wide prefix maximum turns the marks into the owning splat of
-        // every entry (the owner of the chunk's first entries carries over
-        // from the previous chunk).
         const uint32_t excl = s_excl, cta_total = s_total;
-        int32_t carry = -1;
-        for (uint32_t e0 = 0; e0 < cta_total; e0 += kBinChunk) {
-            for (int i = t; i < kBinChunk; i += kBinThreads) s_own[i] = -1;
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < kBinItems; ++k)
-                if (c[k] != 0u && off[k] - e0 < (uint32_t)kBinChunk) s_own[off[k] - e0] = t * kBinItems + k;
-            __syncthreads();
-            static_assert(kBinChunk == 8 * kBinThreads, "eight entries per thread in the prefix maximum");
-            int4* own4 = reinterpret_cast<int4*>(s_own) + 2 * t;
-            int4 a = own4[0], bq = own4[1];
-            a.y = max(a.y, a.x);
-            a.z = max(a.z, a.y);
-            a.w = max(a.w, a.z);
-            bq.x = max(bq.x, a.w);
-            bq.y = max(bq.y, bq.x);
-            bq.z = max(bq.z, bq.y);
-            bq.w = max(bq.w, bq.z);
-            const int32_t pre = max(block_excl_max(bq.w, reinterpret_cast<int32_t*>(scan_tmp)), carry);
-            own4[0] = make_int4(max(a.x, pre), max(a.y, pre), max(a.z, pre), max(a.w, pre));
-            own4[1] = make_int4(max(bq.x, pre), max(bq.y, pre), max(bq.z, pre), max(bq.w, pre));
-            __syncthreads();
-            const uint32_t n_here = min((uint32_t)kBinChunk, cta_total - e0);
-            for (uint32_t i = t; i < n_here; i += kBinThreads) {
-                const uint32_t e = e0 + i;
-                const int lo = s_own[i];
-                if (lo < 0) continue;   // unreachable: entry 0's owner always marks slot 0
-                const uint32_t k = e - s_off[lo];
-                const uint32_t w = s_w[lo], org = s_org[lo];
-                const uint32_t ty = (org >> 16) + k / w, tx = (org & 0xFFFFu) + k % w;
-                const uint32_t tid = ty * (uint32_t)p.tiles_x + tx;
-                const uint32_t o = excl + e;
-                if (o < p.entry_cap) {
-                    p.entry_keys[o] = tid;
-                    p.entry_vals[o] = top - 1u - (uint32_t)lo;
-                    atomicAdd(&s_hist[0][tid & 255u], 1u);
-                    atomicAdd(&s_hist[1][(tid >> 8) & 255u], 1u);
-                    atomicAdd(&s_hist[2][(tid >> 16) & 255u], 1u);
+        // Per-item information for the expansion kernel (coalesced).
+        for (int j = t; j < (int)cnt; j += kBinThreads)
+            p.item_info[(size_t)tile * kBinTile + j] = make_uint4(excl + s_off[j], s_org[j], s_w[j], 0u);
+        // Owner of every expansion chunk that starts inside this CTA tile: the
+        // last item whose first entry is at or before the chunk start.
+        if (cta_total) {
+            const uint32_t c0 = (excl + kBinChunk - 1) / kBinChunk, c1 = (excl + cta_total - 1) / kBinChunk;
+            for (uint32_t ch = c0 + t; ch <= c1; ch += kBinThreads) {
+                if (ch >= p.chunk_cap) break;
+                const uint32_t rel = ch * kBinChunk - excl;
+                int lo = 0, hi = (int)cnt - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_off[mid] <= rel) lo = mid;
+                    else hi = mid - 1;
                 }
+                p.chunk_first[ch] = tile * kBinTile + (uint32_t)lo;
             }
-            carry = s_own[kBinChunk - 1];
-            __syncthreads();
         }
+        __syncthreads();
+    }
+}
+
+// Load-balanced expansion of the (tile id, sorted position) entries: chunk c
+// covers entries [c * kBinChunk, (c + 1) * kBinChunk); its items run from
+// chunk_first[c] to chunk_first[c + 1].  Each non-empty item marks its first
+// entry with its index and a block-wide prefix maximum gives every entry its
+// owner (the chunk's first entries belong to chunk_first[c]).  Entries are
+// written in the order the binning defined, so the result is the same
+// whichever CTA expands a chunk; the tile ids' digit histograms for the tile
+// sort are accumulated here.
+__global__ void __launch_bounds__(kBinThreads) expand_kernel(BinParams p) {
+    __shared__ uint32_t scan_tmp[33];
+    __shared__ uint32_t s_hist[3][256];
+    __shared__ __align__(16) int32_t s_own[kBinChunk];
+    const int t = threadIdx.x;
+    for (int i = t; i < 3 * 256; i += kBinThreads) (&s_hist[0][0])[i] = 0u;
+    const uint32_t n_vis = p.fc->visible_count;
+    const uint32_t entries = min(p.fc->tile_entries, p.entry_cap);
+    const uint32_t nchunks = (entries + kBinChunk - 1) / kBinChunk;
+    __syncthreads();
+    for (uint32_t ch = blockIdx.x; ch < nchunks && ch < p.chunk_cap; ch += gridDim.x) {
+        const uint32_t e0 = ch * kBinChunk, e1 = min(e0 + kBinChunk, entries);
+        const uint32_t qa = p.chunk_first[ch];
+        const uint32_t qb = (ch + 1 < nchunks && ch + 1 < p.chunk_cap) ? p.chunk_first[ch + 1] : n_vis - 1u;
+        for (int i = t; i < kBinChunk; i += kBinThreads) s_own[i] = -1;
+        __syncthreads();
+        for (uint32_t q = qa + 1u + (uint32_t)t; q <= qb && q < n_vis; q += kBinThreads) {
+            const uint4 inf = p.item_info[q];
+            if (inf.z && inf.x >= e0 && inf.x < e1) s_own[inf.x - e0] = (int32_t)(q - qa);
+        }
+        __syncthreads();
+        static_assert(kBinChunk == 8 * kBinThreads, "eight entries per thread in the prefix maximum");
+        int4* own4 = reinterpret_cast<int4*>(s_own) + 2 * t;
+        int4 a = own4[0], bq = own4[1];
+        a.x = max(a.x, 0);   // entries before the first mark belong to item qa
+        a.y = max(a.y, a.x);
+        a.z = max(a.z, a.y);
+        a.w = max(a.w, a.z);
+        bq.x = max(bq.x, a.w);
+        bq.y = max(bq.y, bq.x);
+        bq.z = max(bq.z, bq.y);
+        bq.w = max(bq.w, bq.z);
+        const int32_t pre = max(block_excl_max(bq.w, reinterpret_cast<int32_t*>(scan_tmp)), 0);
+        own4[0] = make_int4(max(a.x, pre), max(a.y, pre), max(a.z, pre), max(a.w, pre));
+        own4[1] = make_int4(max(bq.x, pre), max(bq.y, pre), max(bq.z, pre), max(bq.w, pre));
+        __syncthreads();
+        for (uint32_t i = t; i < e1 - e0; i += kBinThreads) {
+            const uint32_t q = qa + (uint32_t)s_own[i];
+            const uint4 inf = p.item_info[q];
+            const uint32_t k = e0 + i - inf.x;
+            const uint32_t w = max(inf.z, 1u);
+            const uint32_t ty = (inf.y >> 16) + k / w, tx = (inf.y & 0xFFFFu) + k % w;
+            const uint32_t tid = ty * (uint32_t)p.tiles_x + tx;
+            p.entry_keys[e0 + i] = tid;
+            p.entry_vals[e0 + i] = n_vis - 1u - q;
+            atomicAdd(&s_hist[0][tid & 255u], 1u);
+            atomicAdd(&s_hist[1][(tid >> 8) & 255u], 1u);
+            atomicAdd(&s_hist[2][(tid >> 16) & 255u], 1u);
+        }
+        __syncthreads();
     }
     __syncthreads();
     for (int i = t; i < 3 * 256; i += kBinThreads) {
@@ -277,11 +309,12 @@ __global__ void tile_ranges_kernel(const SortPlan* plan, const FrameCounters* fc
 
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s) {
     uint32_t tiles = (n_cap + kBinTile - 1) / kBinTile;
-    uint32_t grid = num_sms * 4;
+    uint32_t grid = num_sms * (1024 / kBinThreads);
     if (grid > tiles) grid = tiles;
     if (grid == 0) grid = 1;
     bin_kernel<<<grid, kBinThreads, 0, s>>>(p);
-    return 1;
+    expand_kernel<<<num_sms * (1024 / kBinThreads), kBinThreads, 0, s>>>(p);
+    return 2;
 }
 
 int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,

@@ -61,6 +61,9 @@ struct gs_ctx {
     uint32_t* keys[2] = {nullptr, nullptr};
     uint32_t* ids[2] = {nullptr, nullptr};
     RasterRecord* records = nullptr;
+    uint4* item_info = nullptr;          // binning -> expansion, one per visible splat
+    uint32_t* chunk_first = nullptr;     // binning -> expansion, one per entry chunk
+    uint32_t chunk_cap = 0;
     unsigned long long* cull_status = nullptr;
     unsigned long long* sort_status = nullptr;
     unsigned long long* bin_status = nullptr;
@@ -168,10 +171,13 @@ void release_scene(gs_ctx* c) {
         dfree(c->evals[k]);
     }
     dfree(c->records);
+    dfree(c->item_info);
     dfree(c->cull_status);
     dfree(c->sort_status);
     dfree(c->bin_status);
     dfree(c->tsort_status);
+    dfree(c->chunk_first);
+    c->chunk_cap = 0;
     gs::release_gps_scene(c->gps);
     dfree(c->anim_deltas);
     dfree(c->anim_scales);
@@ -239,11 +245,16 @@ int ensure_entries(gs_ctx* c, uint32_t cap) {
         dfree(c->evals[k]);
     }
     dfree(c->tsort_status);
+    dfree(c->chunk_first);
     c->entry_cap = 0;
+    c->chunk_cap = 0;
     for (int k = 0; k < 2; ++k) {
         GS_CUDA(c, dalloc(&c->ekeys[k], (size_t)cap * 4));
         GS_CUDA(c, dalloc(&c->evals[k], (size_t)cap * 4));
     }
+    const uint32_t chunks = cap / (uint32_t)gs::kBinChunk + 2u;
+    GS_CUDA(c, dalloc(&c->chunk_first, (size_t)chunks * 4));
+    c->chunk_cap = chunks;
     c->tsort_status_stride = gs::sort_status_words(cap);
     GS_CUDA(c, dalloc(&c->tsort_status, c->tsort_status_stride * 4 * sizeof(unsigned long long)));
     GS_CUDA(c, cudaMemsetAsync(c->tsort_status, 0, c->tsort_status_stride * 4 * sizeof(unsigned long long), c->stream));
@@ -392,6 +403,9 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = fals
         p.entry_keys = c->ekeys[1];
         p.entry_vals = c->evals[1];
         p.entry_cap = c->entry_cap;
+        p.item_info = c->item_info;
+        p.chunk_first = c->chunk_first;
+        p.chunk_cap = c->chunk_cap;
         p.tile_hist = c->tile_hist;
         p.status = c->bin_status;
         p.epoch = c->epoch;
@@ -764,6 +778,7 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
         GS_CUDA(c, dalloc(&c->ids[k], (size_t)n * 4));
     }
     GS_CUDA(c, dalloc(&c->records, (size_t)n * sizeof(RasterRecord)));
+    GS_CUDA(c, dalloc(&c->item_info, (size_t)n * sizeof(uint4)));
     const size_t cull_tiles = ((size_t)n + gs::kCullTile - 1) / gs::kCullTile;
     GS_CUDA(c, dalloc(&c->cull_status, cull_tiles * sizeof(unsigned long long)));
     c->sort_status_stride = gs::sort_status_words(n);

@@ -68,10 +68,10 @@ constexpr int kCullRounds = 4;
 constexpr int kCullTile = 32 * kCullRounds;
 
 // Binning configuration: 4 sorted splats per thread, 1024 per CTA tile.
-constexpr int kBinThreads = 256;
-constexpr int kBinItems = 4;
+constexpr int kBinThreads = 128;
+constexpr int kBinItems = 8;
 constexpr int kBinTile = kBinThreads * kBinItems;
-constexpr int kBinChunk = 2048;                 // entries expanded per round
+constexpr int kBinChunk = 8 * kBinThreads;     // entries expanded per round
 constexpr int kTileW = 16;
 constexpr int kTileH = 16;
 
@@ -151,6 +151,9 @@ struct BinParams {
     uint32_t* entry_keys;            // tile id per entry
     uint32_t* entry_vals;            // sorted position per entry
     uint32_t entry_cap;
+    uint4* item_info;                // per binned item: first entry, tx0 | ty0 << 16, width in tiles (0: none)
+    uint32_t* chunk_first;           // per expansion chunk: the item owning its first entry
+    uint32_t chunk_cap;              // chunk_first capacity (entry_cap / kBinChunk + 2)
     uint32_t* tile_hist;             // 3 x 256 digit histograms of the tile ids (zeroed per pass)
     unsigned long long* status;      // per-CTA-tile look-back words (epoch-tagged)
     uint32_t epoch;
