@@ -295,15 +295,34 @@ __global__ void __launch_bounds__(kBinThreads) expand_kernel(BinParams p) {
     }
 }
 
+// [start, end) of every tile's run in the tile-sorted entries: a thread
+// takes 8 consecutive keys (two 16-byte loads) and the keys either side.
 __global__ void tile_ranges_kernel(const SortPlan* plan, const FrameCounters* fc, uint2* ranges,
                                    uint32_t num_tiles) {
     const uint32_t E = fc->tile_entries;
     const uint32_t* keys = plan->kfinal;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        const uint32_t k = keys[e];
-        if (k >= num_tiles) continue;  // only after a failed (timed-out) sort
-        if (e == 0 || keys[e - 1] != k) ranges[k].x = e;
-        if (e == E - 1 || keys[e + 1] != k) ranges[k].y = e + 1;
+    const uint32_t groups = (E + 7) / 8;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += gridDim.x * blockDim.x) {
+        const uint32_t e0 = g * 8;
+        uint32_t k[10];   // k[0] = key e0 - 1, k[1..8] = keys e0..e0+7, k[9] = key e0 + 8
+        k[0] = e0 > 0 ? keys[e0 - 1] : 0xFFFFFFFFu;
+        if (e0 + 8 <= E) {
+            const uint4 a = reinterpret_cast<const uint4*>(keys + e0)[0];
+            const uint4 b = reinterpret_cast<const uint4*>(keys + e0)[1];
+            k[1] = a.x; k[2] = a.y; k[3] = a.z; k[4] = a.w;
+            k[5] = b.x; k[6] = b.y; k[7] = b.z; k[8] = b.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) k[1 + j] = e0 + j < E ? keys[e0 + j] : 0xFFFFFFFFu;
+        }
+        k[9] = e0 + 8 < E ? keys[e0 + 8] : 0xFFFFFFFFu;
+#pragma unroll
+        for (int j = 1; j <= 8; ++j) {
+            const uint32_t e = e0 + (uint32_t)(j - 1);
+            if (e >= E || k[j] >= num_tiles) continue;   // >= num_tiles only after a failed (timed-out) sort
+            if (e == 0 || k[j - 1] != k[j]) ranges[k[j]].x = e;
+            if (e == E - 1 || k[j + 1] != k[j]) ranges[k[j]].y = e + 1;
+        }
     }
 }
 
@@ -319,7 +338,7 @@ int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_
 
 int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
                        uint32_t num_tiles, uint32_t num_sms, cudaStream_t s) {
-    uint32_t grid = (entry_cap + 255) / 256;
+    uint32_t grid = (entry_cap / 8 + 255) / 256;
     if (grid > num_sms * 8) grid = num_sms * 8;
     if (grid == 0) grid = 1;
     tile_ranges_kernel<<<grid, 256, 0, s>>>(tile_plan, fc, ranges, num_tiles);
