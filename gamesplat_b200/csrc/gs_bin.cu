@@ -326,6 +326,40 @@ __global__ void tile_ranges_kernel(const SortPlan* plan, const FrameCounters* fc
     }
 }
 
+// Rasterization order: tiles by descending entry count (classes of powers
+// of two), so the heaviest tiles start in the first wave instead of
+// stretching the last one.  One CTA; the order within a class is immaterial
+// (each tile's CTA writes only its own pixels).
+__global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* __restrict__ ranges, uint32_t num_tiles,
+                                                          uint32_t* __restrict__ order) {
+    __shared__ uint32_t s_cnt[33], s_start[33];
+    const int t = threadIdx.x;
+    if (t < 33) s_cnt[t] = 0u;
+    __syncthreads();
+    auto cls = [&](uint32_t tl) -> uint32_t {
+        const uint2 r = ranges[tl];
+        const uint32_t w = r.y > r.x ? r.y - r.x : 0u;
+        return w ? (uint32_t)__clz(w) : 32u;   // 0 for the heaviest class, 32 for empty tiles
+    };
+    for (uint32_t tl = t; tl < num_tiles; tl += blockDim.x) atomicAdd(&s_cnt[cls(tl)], 1u);
+    __syncthreads();
+    if (t == 0) {
+        uint32_t run = 0;
+        for (int k = 0; k < 33; ++k) {
+            s_start[k] = run;
+            run += s_cnt[k];
+        }
+    }
+    __syncthreads();
+    for (uint32_t tl = t; tl < num_tiles; tl += blockDim.x) order[atomicAdd(&s_start[cls(tl)], 1u)] = tl;
+}
+
+int launch_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order, cudaStream_t s) {
+    if (num_tiles == 0) return 0;
+    tile_order_kernel<<<1, 1024, 0, s>>>(ranges, num_tiles, order);
+    return 1;
+}
+
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s) {
     uint32_t tiles = (n_cap + kBinTile - 1) / kBinTile;
     uint32_t grid = num_sms * (1024 / kBinThreads);

@@ -85,6 +85,7 @@ struct gs_ctx {
     uint32_t* depth_hist = nullptr;
     uint32_t* tile_hist = nullptr;
     uint2* tile_ranges = nullptr;
+    uint32_t* tile_order = nullptr;      // raster CTA -> tile (heaviest first)
     uint32_t tiles_cap = 0;
 
     // gsanim appearance deltas (renderer animation buffer, src/renderer.cpp:824-841)
@@ -191,6 +192,7 @@ void release_scene(gs_ctx* c) {
 void release_targets(gs_ctx* c) {
     dfree(c->out16);
     dfree(c->ctrl);
+    dfree(c->tile_order);
     c->fc = nullptr;
     gs::release_stochastic_targets(c->st);
     gs::release_gps_targets(c->gps);
@@ -292,6 +294,7 @@ int ensure_targets(gs_ctx* c, int w, int h) {
     c->tile_hist = reinterpret_cast<uint32_t*>(base + o_th);
     c->tile_ranges = reinterpret_cast<uint2*>(base + o_tr);
     GS_CUDA(c, cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream));
+    GS_CUDA(c, dalloc(&c->tile_order, (size_t)c->tiles_cap * sizeof(uint32_t)));
     GS_CUDA(c, dalloc(&c->out16, (size_t)w * h * 8));
     c->width = w;
     c->height = h;
@@ -438,6 +441,7 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = fals
         sc.add(gs::launch_sort(p, c->num_sms, c->stream));
         sc.add(gs::launch_tile_ranges(c->tile_plan, c->fc, c->entry_cap, c->tile_ranges, c->tiles_cap, c->num_sms,
                                        c->stream));
+        sc.add(gs::launch_tile_order(c->tile_ranges, c->tiles_cap, c->tile_order, c->stream));
     }
 }
 
@@ -447,6 +451,7 @@ gs::RasterParams raster_params(gs_ctx* c, float bg) {
     r.record_cap = c->n;
     r.tile_plan = c->tile_plan;
     r.tile_ranges = c->tile_ranges;
+    r.tile_order = c->tile_order;
     r.width = c->width;
     r.height = c->height;
     r.tiles_x = c->tiles_x;

@@ -170,6 +170,7 @@ struct RasterParams {
     uint32_t record_cap;             // records allocated (bounds every record index)
     const SortPlan* tile_plan;       // tile-sorted entry values at tile_plan->vfinal
     const uint2* tile_ranges;        // [start, end) per tile
+    const uint32_t* tile_order;      // tiles by descending work (CTA b rasterizes tile_order[b])
     int width, height, tiles_x, tiles_y;
     float bg;
     // stochastic mode (envelope records): the sample's jitter and seed, and
@@ -208,6 +209,7 @@ int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s);
 int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
                        uint32_t num_tiles, uint32_t num_sms, cudaStream_t s);
+int launch_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order, cudaStream_t s);
 int launch_raster_alpha(const RasterParams& p, cudaStream_t s);
 int launch_raster_stochastic(const RasterParams& p, cudaStream_t s);
 

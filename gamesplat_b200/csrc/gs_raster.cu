@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     __shared__ uint8_t s_mask[kBatch];
     __shared__ float4 s_cen[kMode == 1 ? kBatch : 1];   // stochastic: jittered centre and hash z of the sample
 
-    const uint32_t tile = blockIdx.x;
+    const uint32_t tile = p.tile_order[blockIdx.x];
     const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int x0 = tx * kTileW, y0 = ty * kTileH;
