@@ -326,26 +326,29 @@ __global__ void tile_ranges_kernel(const SortPlan* plan, const FrameCounters* fc
     }
 }
 
-// Rasterization order: tiles by descending entry count (classes of powers
-// of two), so the heaviest tiles start in the first wave instead of
+// Rasterization order: tiles by descending entry count (quarter-octave
+// classes), so the heaviest tiles start in the first wave instead of
 // stretching the last one.  One CTA; the order within a class is immaterial
 // (each tile's CTA writes only its own pixels).
 __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* __restrict__ ranges, uint32_t num_tiles,
                                                           uint32_t* __restrict__ order) {
-    __shared__ uint32_t s_cnt[33], s_start[33];
+    __shared__ uint32_t s_cnt[129], s_start[129];
     const int t = threadIdx.x;
-    if (t < 33) s_cnt[t] = 0u;
+    if (t < 129) s_cnt[t] = 0u;
     __syncthreads();
-    auto cls = [&](uint32_t tl) -> uint32_t {
+    auto cls = [&](uint32_t tl) -> uint32_t {   // quarter-octave classes, heaviest first
         const uint2 r = ranges[tl];
         const uint32_t w = r.y > r.x ? r.y - r.x : 0u;
-        return w ? (uint32_t)__clz(w) : 32u;   // 0 for the heaviest class, 32 for empty tiles
+        if (!w) return 128u;
+        const uint32_t lz = (uint32_t)__clz(w);
+        const uint32_t frac = lz >= 30 ? 0u : (w << (lz + 1)) >> 30;   // two bits after the leading one
+        return lz * 4u + (3u - frac);
     };
     for (uint32_t tl = t; tl < num_tiles; tl += blockDim.x) atomicAdd(&s_cnt[cls(tl)], 1u);
     __syncthreads();
     if (t == 0) {
         uint32_t run = 0;
-        for (int k = 0; k < 33; ++k) {
+        for (int k = 0; k < 129; ++k) {
             s_start[k] = run;
             run += s_cnt[k];
         }

@@ -15,7 +15,8 @@
 // completion on an mbarrier), double buffered so the next batch lands while
 // the current one is composited.  When a batch lands, one thread per record turns its pixel
 // rectangle into tile-relative column and row bit masks, so a pixel's
-// coverage test is one AND and one compare.
+// coverage test is one AND and one compare (in alpha mode the mask is also
+// written into the staged record next to g, b: one 16-byte load per splat).
 //
 // The two pixels of a thread share a column; their arithmetic runs as packed
 // f32x2 operations (add/mul/fma .rn on float pairs, each element rounded like
@@ -240,6 +241,11 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
                 cen_y = R->cy;
             }
             s_bits[i] = bits;
+            if (kMode == 0) {
+                // coverage bits next to g, b: one 16-byte load per splat in the loop
+                const_cast<RasterRecord*>(R)->rect_x = bits;
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            }
             const uint32_t c = (uint32_t)((bits & 0x00FFu) != 0u) | ((uint32_t)((bits & 0xFF00u) != 0u) << 1);
             const uint32_t r = (uint32_t)((bits & 0x00FF0000u) != 0u) | ((uint32_t)((bits & 0xFF000000u) != 0u) << 1);
             // block w = (w & 1, w >> 1): bit w set iff its column and row halves are covered
@@ -267,6 +273,45 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         for (uint32_t c = 0; c < cnt && !warp_done; c += 32) {
             const bool mine = c + lane < cnt && ((s_mask[c + lane] >> warp) & 1u);
             uint32_t todo = __ballot_sync(0xffffffffu, mine);
+            if (kMode == 0) {
+                // one splat of the warp's list into both pixels' state
+                auto alpha_one = [&](uint32_t j) {
+                    const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
+                    const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
+                    const uint4 q2u = reinterpret_cast<const uint4*>(recs + j)[2];
+                    const uint32_t bits = q2u.z;
+                    const float dx = sub(fcx, q0.x);
+                    const float t0 = mul(mul(q0.z, dx), dx);
+                    const float m = mul(q0.w, dx);
+                    const float2 dy = __fadd2_rn(fcy, f2(-q0.y));
+                    const float2 sq = __fadd2_rn(__fadd2_rn(f2(t0), __fmul2_rn(f2(m), dy)),
+                                                 __fmul2_rn(__fmul2_rn(f2(q1.x), dy), dy));
+                    const bool live0 = (bits & need0) == need0 && sq.x >= -__int_as_float(1) && sq.x <= q1.z;
+                    const bool live1 = (bits & need1) == need1 && sq.y >= -__int_as_float(1) && sq.y <= q1.z;
+                    const float2 q2 = make_float2(__uint_as_float(q2u.x), __uint_as_float(q2u.y));
+                    const float2 arg = __ffma2_rn(sq, f2(kNegHalfLog2e), f2(q1.y));
+                    const float a0 = live0 ? fminf(ex2_approx(arg.x), 0.99f) : 0.0f;
+                    const float a1 = live1 ? fminf(ex2_approx(arg.y), 0.99f) : 0.0f;
+                    const float2 w = __fmul2_rn(make_float2(a0, a1), T);
+                    C0 = __ffma2_rn(w, f2(q1.w), C0);
+                    C1 = __ffma2_rn(w, f2(q2.x), C1);
+                    C2 = __ffma2_rn(w, f2(q2.y), C2);
+                    T = __ffma2_rn(w, f2(-1.0f), T);
+                };
+                // two splats per trip: one loop test and one warp vote per pair
+                while (todo) {
+                    const uint32_t j = c + (uint32_t)(__ffs(todo) - 1);
+                    todo &= todo - 1u;
+                    alpha_one(j);
+                    if (todo) {
+                        const uint32_t j2 = c + (uint32_t)(__ffs(todo) - 1);
+                        todo &= todo - 1u;
+                        alpha_one(j2);
+                    }
+                    if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
+                }
+                continue;
+            }
             while (todo) {
                 const uint32_t j = c + (uint32_t)(__ffs(todo) - 1);
                 todo &= todo - 1u;
