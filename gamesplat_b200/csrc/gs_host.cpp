@@ -964,9 +964,18 @@ int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
         const uint32_t seed = c->frame_seed, samples = c->sample_count, widx = c->accum_write_index;
         const gs_camera pcam = c->prev_cam;
         const bool pvalid = c->prev_cam_valid, tvalid = c->taa_prev_valid;
-        rc = gs_render(c, cam, c->out16);
+        // Alpha frames into page-locked memory: the rasterizer writes the
+        // pixels straight into the host buffer (mapped, over PCIe), so the
+        // transfer overlaps the raster instead of following it.
+        void* mapped = nullptr;
+        const bool direct = pinned_out && c->knobs.render_mode == GS_MODE_ALPHA &&
+                            cudaHostGetDevicePointer(&mapped, host_out, 0) == cudaSuccess && mapped;
+        cudaGetLastError();
+        rc = gs_render(c, cam, direct ? mapped : static_cast<void*>(c->out16));
         if (rc) return rc;
-        if (pinned_out) {
+        if (direct) {
+            // written by the frame's kernels
+        } else if (pinned_out) {
             GS_CUDA(c, cudaMemcpyAsync(host_out, c->out16, bytes, cudaMemcpyDeviceToHost, c->stream));
         } else {
             // eight chunks, each with an event, so the host copies chunk i out of

@@ -1,7 +1,8 @@
 """gs_render_host readback paths give the same image as gs_render: a
-page-locked destination (copied into directly) and a pageable destination
-(chunked copy through pinned staging, overlapped with the host copy), at
-sizes that are not multiples of the tile size."""
+page-locked destination (alpha mode: the rasterizer writes the pixels into
+it through its mapped device address; other modes: one copy into it) and a
+pageable destination (chunked copy through pinned staging, overlapped with
+the host copy), at sizes that are not multiples of the tile size."""
 from __future__ import annotations
 
 import ctypes as C
