@@ -11,11 +11,14 @@
 // leaves each tile's list in front-to-back order, the order the rasterizer
 // walks.
 //
-// The CTA tile's entries are written by a load-balanced expansion (entry e
-// finds its splat through a chunked owner map: marks at each splat's first
-// entry, then a block prefix maximum), so the stores are coalesced however
-// many tiles a splat covers; the tile ids' digit histograms for the tile sort
-// are accumulated on the way.
+// Two kernels: bin_kernel does (a) and (b), counts each splat's entries and
+// finds the entry offsets; expand_kernel writes the entries, one chunk of the
+// global entry range per CTA round (entry e finds its splat through an owner
+// map: marks at each splat's first entry, then a block prefix maximum), so
+// the work is balanced however many tiles one splat covers and the stores are
+// coalesced; the tile ids' digit histograms for the tile sort are accumulated
+// on the way.  Two more small kernels follow the tile sort: the [start, end)
+// range of each tile, and the rasterization order (heaviest tiles first).
 //
 // Tile selection is conservative: the covered rectangle is intersected with
 // the bounding box of the ellipse where the Gaussian's alpha reaches 1/255

@@ -21,6 +21,9 @@
 // The two pixels of a thread share a column; their arithmetic runs as packed
 // f32x2 operations (add/mul/fma .rn on float pairs, each element rounded like
 // the scalar operation), which halves the issue slots of the per-pixel math.
+// In alpha mode a warp takes its splats two per loop trip (one loop test and
+// one "all pixels done" vote per pair).  CTA b rasterizes tile
+// tile_order[b]: the heaviest tiles first, so they do not form the last wave.
 //
 // Alpha mode: premultiplied "over" in FP32, front to back:
 //   C += T * alpha * rgb,  T -= T * alpha,  output (C + T*bg, 1 - T),
