@@ -81,6 +81,19 @@ def test_alpha_odd_sizes(w, h):
     assert gate["ok"], gate
 
 
+def test_alpha_4k_more_tiles_than_13_bits():
+    """3840x2160: 32 400 tiles (15-bit tile ids: the tile sort's second pass
+    has 7 bits), tile order over all of them."""
+    w, h = 3840, 2160
+    rows = small_rows(60_000, seed=9)
+    cam = small_cam(w, h)
+    ref_img, _ = oracle_alpha(rows, cam, w, h)
+    with make_renderer(rows) as r:
+        img = r.draw_frame(cam)
+    gate = image_gate(img, ref_img)
+    assert gate["ok"], gate
+
+
 def test_alpha_sh_degrees_and_grey_background():
     rows = small_rows(30_000, seed=9)
     cam = small_cam(320, 240)
