@@ -98,17 +98,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def profiled_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu capture of the
-    benchmark workload (profiles/traffic_room3m_1080p.txt), or None."""
+def profiled_traffic(*kernels: str):
+    """DRAM bytes per launch of the named kernels together (one launch each)
+    from the committed ncu capture of the benchmark workload
+    (profiles/traffic_room3m_1080p.txt), or None if one is missing."""
     p = ROOT / "profiles" / "traffic_room3m_1080p.txt"
     if not p.exists():
         return None
+    found = {}
     for line in p.read_text().splitlines():
         parts = line.split()
-        if len(parts) == 2 and parts[0] == kernel:
-            return int(parts[1])
-    return None
+        if len(parts) == 2 and parts[0] in kernels:
+            found[parts[0]] = int(parts[1])
+    if len(found) != len(kernels):
+        return None
+    return sum(found.values())
 
 
 def orbit_cameras(width=WIDTH, height=HEIGHT):
@@ -361,15 +365,17 @@ def run_ours(args):
         "cull": 16.0 * n + 272.0 * n_vis + 8.0 * n,
         "sort": 68.0 * n_vis,
     }
-    # The roofline kernel is the HBM-bound cull; the raster (the dominant
-    # stage) is issue-bound and reported separately in fragments/s.
+    # The roofline kernel is the HBM-bound cull (its two launches, visibility
+    # and projection, timed together as the cull stage); the raster (the
+    # dominant stage) is issue-bound and reported separately in fragments/s.
     roof_stage = "cull"
     achieved = alg[roof_stage] / (per_frame[roof_stage] / 1000.0) / 1e9
-    traffic = profiled_traffic("cull_kernel") if n == 3_000_000 else None
-    roofline = {"bound": "hbm", "kernel": "cull_kernel", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": alg[roof_stage],
-                "traffic_source": "profiles/cull_kernel_room3m_1080p.md" if traffic else None}
+    traffic = profiled_traffic("cull_visible_kernel", "cull_project_kernel") if n == 3_000_000 else None
+    roofline = {"bound": "hbm", "kernel": "cull_visible_kernel + cull_project_kernel<16>", "achieved": achieved,
+                "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": alg[roof_stage],
+                "traffic_source": "profiles/cull_visible_kernel_room3m_1080p.md + "
+                                  "profiles/cull_project_kernel_room3m_1080p.md" if traffic else None}
     raster = {"kernel": "raster_kernel<0>", "ms_per_frame": per_frame.get("raster"),
               "share_of_frame": per_frame.get("raster", 0.0) / (ms_max / args.steps),
               "bound": "instruction issue (ALU pipe)", "quad_fragments_per_frame": frags,

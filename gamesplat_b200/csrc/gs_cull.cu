@@ -1,22 +1,20 @@
-// Cull / project / SH kernel: shaders/cull.glsl:166-424 (+ cull_reset,
+// Cull / project / SH kernels: shaders/cull.glsl:166-424 (+ cull_reset,
 // :456-473, folded in) for the B200.
 //
-// Memory plan (HBM-bound, 256-byte GpuGaussian rows):
-//   * each lane reads the first 16 bytes (position, opacity) of its row and
-//     runs the near/frustum test;
-//   * the warp then fetches only the visible rows' remaining 16-byte chunks
-//     with coalesced 128-bit loads (consecutive lanes -> consecutive chunks)
-//     into a padded shared-memory stage (272-byte row stride: conflict-free
-//     128-bit shared loads);
-//   * culled rows cost one 32-byte sector, visible rows 256 bytes (fewer for
-//     sh_degree < 3);
-//   * visible (key, id) pairs are compacted in index order with a
-//     decoupled look-back over CTA tiles, so the depth sort runs on N_vis
+// Memory plan (HBM-bound, 256-byte GpuGaussian rows), two kernels:
+//   * cull_visible_kernel reads the first 16 bytes (position, opacity) of
+//     every row, runs the near/frustum test, computes the depth keys and
+//     compacts the visible (key, id) pairs in index order with a decoupled
+//     look-back over 128-row warp tiles, so the depth sort runs on N_vis
 //     pairs instead of N (the culled tail of the reference's all-N sort is
-//     all-equal (0xFFFFFFFF, 0xFFFFFFFF) pairs, so the result is identical).
+//     all-equal (0xFFFFFFFF, 0xFFFFFFFF) pairs, so the result is identical);
+//   * cull_project_kernel walks the compacted ids in groups of 32 and stages
+//     each visible row whole into a padded shared-memory row (272-byte
+//     stride: conflict-free 128-bit shared loads) with one TMA bulk copy,
+//     then projects it; culled rows cost one 32-byte sector, visible rows
+//     256 bytes (fewer for sh_degree < 3).
 // Arithmetic follows the GLSL operand order with unfused intrinsics so the
 // keys, cull mask and projected records match the CPU oracle bit for bit.
-#include <algorithm>
 
 #include "gs_common.cuh"
 #include "gs_internal.h"
@@ -27,7 +25,7 @@ namespace gs {
 static_assert(kCullRounds == 4, "the round loop selects per-round values among four scalars");
 constexpr int kStageStride = 17;  // float4 per staged row (16 + 1 pad)
 constexpr int kCullWarps = kCullThreads / 32;
-constexpr size_t kCullSmem = (size_t)kCullWarps * 2 * 32 * kStageStride * sizeof(float4);  // double-buffered
+constexpr size_t kCullSmem = (size_t)kCullWarps * 32 * kStageStride * sizeof(float4);  // one stage per warp
 
 struct CamRegs {
     float V[16];
@@ -205,20 +203,25 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
     out[3] = make_float4(a, mul(b, cam.ysign), c, det);
 }
 
-// Stage the visible rows of one 32-row round: lane l copies the first
-// kChunks 16-byte chunks of row wbase + l (if visible) to stage row l with
-// one TMA bulk copy; completion is counted on `bar`.
+// Stage one group of 32 compacted visible rows: lane l copies the first
+// kChunks 16-byte chunks of row ids[first + l] (if first + l < count) to
+// stage row l with one TMA bulk copy; completion is counted on `bar`.
+// Returns the lane's row id, or kSentinel past the end.
 template <int kChunks>
-__device__ __forceinline__ void stage_round(const float4* rows, uint32_t wbase, uint32_t mask, float4* stage,
-                                            uint64_t* bar, int lane, uint64_t policy) {
+__device__ __forceinline__ uint32_t stage_group(const float4* rows, const uint32_t* ids, uint32_t first,
+                                                uint32_t count, float4* stage, uint64_t* bar, int lane,
+                                                uint64_t policy) {
+    const uint32_t idx = first + (uint32_t)lane;
+    const uint32_t id = idx < count ? ids[idx] : kSentinel;
+    const uint32_t mask = __ballot_sync(0xffffffffu, id != kSentinel);
     if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)__popc(mask) * (uint32_t)(kChunks * 16));
     __syncwarp();
     // order this lane's earlier generic accesses to its stage row (reads, and
     // the in-place gsanim deltas) before the async-proxy refill
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if ((mask >> lane) & 1u)
-        bulk_g2s_hint(stage + lane * kStageStride, rows + (size_t)(wbase + lane) * 16, (uint32_t)(kChunks * 16), bar,
-                      policy);
+    if (id != kSentinel)
+        bulk_g2s_hint(stage + lane * kStageStride, rows + (size_t)id * 16, (uint32_t)(kChunks * 16), bar, policy);
+    return id;
 }
 
 // gsanim int8 appearance deltas applied in place to a staged row
@@ -250,190 +253,62 @@ __device__ void animate_row(const CullParams& p, uint32_t row, float4* staged, f
     staged[3] = c3;
 }
 
-// Every warp is independent: it takes 128-Gaussian warp tiles in ticket
-// order, tests visibility from the rows' first 16 bytes, stages round r+1's
-// visible rows (TMA bulk copies) while it projects round r, and places its
-// visible (key, id) pairs with a warp-level decoupled look-back.  The round
-// loop is not unrolled (one copy of the projection code: the SH degree 3 body
-// is large), so per-round values are picked out of small register arrays.
-template <int kChunks>  // 16-byte chunks of a row the SH degree needs: 4, 7, 10 or 16
-__global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
-    extern __shared__ float4 smem4[];
-    __shared__ __align__(8) uint64_t s_bar[kCullWarps][2];
-    __shared__ uint32_t s_hist[4][256];   // digit histograms of the emitted keys (for the depth sort)
+// Pass 1 (visibility and compaction): every warp takes 128-Gaussian warp
+// tiles in ticket order, tests visibility from the rows' first 16 bytes
+// (shaders/cull.glsl:209-220), computes the depth keys (:230-232), and places
+// its visible (key, id) pairs in index order with a warp-level decoupled
+// look-back; the 4 x 256 key-digit histograms of the depth sort are
+// accumulated in shared memory.
+__global__ void __launch_bounds__(kCullThreads) cull_visible_kernel(CullParams p) {
+    __shared__ uint32_t s_hist[4][256];
     for (int i = threadIdx.x; i < 4 * 256; i += kCullThreads) (&s_hist[0][0])[i] = 0u;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) {
-        mbar_init(&s_bar[warp][0], 1);
-        mbar_init(&s_bar[warp][1], 1);
-        mbar_fence_init();
-    }
     __syncthreads();
-    float4* const stage0 = smem4 + (size_t)warp * 2 * 32 * kStageStride;   // stage b at stage0 + b * 32 rows
-    uint32_t phase = 0;   // bit b: parity of the next completion of bar[b]
-    const uint32_t num_tiles = (p.n + kCullTile - 1) / kCullTile;
-    CamRegs cam;
-    load_cam(p.cam, cam);
+    const int lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
-    const bool animated = p.anim_deltas != nullptr &&
-                          (p.anim_state_a != 0 || (p.anim_weight > 0.0f && p.anim_state_b != 0));
-    bool stage_failed = false;
-    const uint64_t stream_policy = l2_policy_evict_first();
-
-    auto take_ticket = [&]() -> uint32_t {
-        uint32_t t = 0;
-        if (lane == 0) t = atomicAdd(&p.fc->cull_ticket, 1u);
-        return __shfl_sync(0xffffffffu, t, 0);
-    };
-    // First 16 bytes (position, opacity) of the tile's 4 x 32 rows.
-    auto load_heads = [&](uint32_t t, float4* c0) {
+    const uint32_t num_tiles = (p.n + kCullTile - 1) / kCullTile;
+    const float* V = p.cam.view;
+    const float P0 = p.cam.proj[0], P5 = p.cam.proj[5], ortho = p.cam.orthographic;
+    for (;;) {
+        uint32_t tile = 0;
+        if (lane == 0) tile = atomicAdd(&p.fc->cull_ticket, 1u);
+        tile = __shfl_sync(0xffffffffu, tile, 0);
+        if (tile >= num_tiles) break;
+        const uint32_t base = tile * kCullTile;
+        float4 c0[kCullRounds];
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) {
-            const uint32_t g = t * kCullTile + r * 32 + lane;
-            // default L2 policy: the row's bulk copy re-reads this sector soon
+            const uint32_t g = base + r * 32 + lane;
             c0[r] = g < p.n ? __ldg(p.rows + (size_t)g * 16) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-    };
-    // Visibility masks of a tile (shaders/cull.glsl:209-232), then stage its
-    // round 0 into buffer 0 and publish its visible count as an aggregate.
-    auto begin_tile = [&](uint32_t t, const float4* c0, uint32_t& m0, uint32_t& m1, uint32_t& m2,
-                          uint32_t& m3) -> uint32_t {
-        uint32_t total = 0;
+        uint32_t mask[kCullRounds], key[kCullRounds], total = 0;
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) {
-            const uint32_t g = t * kCullTile + r * 32 + lane;
+            const uint32_t g = base + r * 32 + lane;
             // p_view = view * vec4(position, 1.0)
-            const float vx = add(add(add(mul(cam.V[0], c0[r].x), mul(cam.V[4], c0[r].y)), mul(cam.V[8], c0[r].z)), cam.V[12]);
-            const float vy = add(add(add(mul(cam.V[1], c0[r].x), mul(cam.V[5], c0[r].y)), mul(cam.V[9], c0[r].z)), cam.V[13]);
-            const float vz = add(add(add(mul(cam.V[2], c0[r].x), mul(cam.V[6], c0[r].y)), mul(cam.V[10], c0[r].z)), cam.V[14]);
+            const float vx = add(add(add(mul(V[0], c0[r].x), mul(V[4], c0[r].y)), mul(V[8], c0[r].z)), V[12]);
+            const float vy = add(add(add(mul(V[1], c0[r].x), mul(V[5], c0[r].y)), mul(V[9], c0[r].z)), V[13]);
+            const float vz = add(add(add(mul(V[2], c0[r].x), mul(V[6], c0[r].y)), mul(V[10], c0[r].z)), V[14]);
             bool visible = g < p.n && (vz <= -0.2f);
             if (visible) {
                 float inv_z = dv(-1.0f, vz);
-                float ndc_x = add(mul(mul(mul(cam.P0, vx), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P0, vx), cam.ortho));
-                float ndc_y = add(mul(mul(mul(cam.P5, vy), inv_z), sub(1.0f, cam.ortho)), mul(mul(cam.P5, vy), cam.ortho));
+                float ndc_x = add(mul(mul(mul(P0, vx), inv_z), sub(1.0f, ortho)), mul(mul(P0, vx), ortho));
+                float ndc_y = add(mul(mul(mul(P5, vy), inv_z), sub(1.0f, ortho)), mul(mul(P5, vy), ortho));
                 visible = fabsf(ndc_x) <= 1.3f && fabsf(ndc_y) <= 1.3f;
             }
-            const uint32_t m = __ballot_sync(0xffffffffu, visible);
-            if (r == 0) m0 = m;
-            if (r == 1) m1 = m;
-            if (r == 2) m2 = m;
-            if (r == 3) m3 = m;
-            total += __popc(m);
-        }
-        stage_round<kChunks>(p.rows, t * kCullTile, m0, stage0, &s_bar[warp][0], lane, stream_policy);
-        if (lane == 0) st_relaxed64(p.status + t, status_word(p.epoch, t == 0 ? kFlagInc : kFlagAgg, total));
-        return total;
-    };
-
-    // Tiles are software-pipelined: the next tile's ticket and row heads are
-    // fetched while this tile projects, and its visibility, round-0 staging
-    // and aggregate publish happen during this tile's last round.
-    float4 heads[kCullRounds];
-    uint32_t mask0 = 0u, mask1 = 0u, mask2 = 0u, mask3 = 0u;
-    uint32_t tile = take_ticket();
-    uint32_t total = 0;
-    if (tile < num_tiles) {
-        load_heads(tile, heads);
-        total = begin_tile(tile, heads, mask0, mask1, mask2, mask3);
-    }
-    while (tile < num_tiles) {
-        const uint32_t base = tile * kCullTile;
-        // next tile's ticket: requested now, read in round 1 (its latency is
-        // hidden behind round 0), its row heads loaded then for round 3
-        uint32_t ticket_raw = 0u;
-        if (lane == 0) ticket_raw = atomicAdd(&p.fc->cull_ticket, 1u);
-        uint32_t ntile = num_tiles;
-        uint32_t nmask0 = 0u, nmask1 = 0u, nmask2 = 0u, nmask3 = 0u;
-        uint32_t ntotal = 0;
-
-        uint32_t key0 = 0u, key1 = 0u, key2 = 0u, key3 = 0u;
-        uint32_t d0 = 0, d2 = 0, d3 = 0, d4 = 0, d6 = 0, d7 = 0, m1 = 0, m5 = 0;
-#pragma unroll 1
-        for (int r = 0; r < kCullRounds; ++r) {
-            // scalar selects (no dynamically indexed arrays, which would live
-            // in local memory)
-            const uint32_t mr = r == 0 ? mask0 : r == 1 ? mask1 : r == 2 ? mask2 : mask3;
-            const uint32_t mnext = r == 0 ? mask1 : r == 1 ? mask2 : mask3;
-            const int b = r & 1;
-            if (r == 1) {
-                ntile = __shfl_sync(0xffffffffu, ticket_raw, 0);
-                if (ntile < num_tiles) load_heads(ntile, heads);
-            }
-            if (r + 1 < kCullRounds)
-                stage_round<kChunks>(p.rows, base + (r + 1) * 32, mnext, stage0 + (b ^ 1) * 32 * kStageStride,
-                                     &s_bar[warp][b ^ 1], lane, stream_policy);
-            else if (ntile < num_tiles)   // buffer 0 is free: round 2 is done
-                ntotal = begin_tile(ntile, heads, nmask0, nmask1, nmask2, nmask3);
-            if (!mbar_wait_bounded(&s_bar[warp][b], (phase >> b) & 1u)) stage_failed = true;
-            phase ^= 1u << b;
-            float4* const cur = stage0 + b * 32 * kStageStride;
-            const uint32_t g = base + r * 32 + lane;
-            const bool visible = (mr >> lane) & 1u;
-            uint32_t key = 0u;
-            if (visible) {
-                float4 rec[4];
-                float qa, gp;
-                float4* row = cur + lane * kStageStride;
-                const float4 c0 = row[0];
-                const float vx = add(add(add(mul(cam.V[0], c0.x), mul(cam.V[4], c0.y)), mul(cam.V[8], c0.z)), cam.V[12]);
-                const float vy = add(add(add(mul(cam.V[1], c0.x), mul(cam.V[5], c0.y)), mul(cam.V[9], c0.z)), cam.V[13]);
-                const float vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
-                if (animated) {
-                    float4 c3 = row[3];
-                    animate_row(p, g, row, c3);
-                }
-                project_visible(row, c0, vx, vy, vz, cam, p.sh_degree, p.sh_lod_distance, rec, &qa, &gp);
-                float4* dst = p.projected + (size_t)g * 4;
-                dst[0] = rec[0];
-                dst[1] = rec[1];
-                dst[2] = rec[2];
-                dst[3] = rec[3];
-                key = 0xFFFFFFFFu - __float_as_uint(g_max(-vz, 0.0f));
-                if (p.collect_stats) {
-                    // shaders/cull.glsl:296-318
-                    const uint32_t qpx = g_f2u_sat(g_min(g_max(0.0f, qa), 4294967295.0f));
-                    const uint32_t gpx = g_f2u_sat(g_min(ceilf(gp), 4294967295.0f));
-                    d0 += (uint32_t)(qpx + 1023u) >> 10u;
-                    m1 = max(m1, qpx);
-                    d2 += qpx > 1024u;
-                    d3 += qpx > 16384u;
-                    d4 += (uint32_t)(gpx + 1023u) >> 10u;
-                    m5 = max(m5, gpx);
-                    d6 += gpx > 1024u;
-                    d7 += gpx > 16384u;
-                }
-            } else if (g < p.n && p.write_invisible) {
+            key[r] = 0xFFFFFFFFu - __float_as_uint(g_max(-vz, 0.0f));
+            mask[r] = __ballot_sync(0xffffffffu, visible);
+            total += __popc(mask[r]);
+            if (!visible && g < p.n && p.write_invisible) {   // shaders/cull.glsl:222-228
                 float4* dst = p.projected + (size_t)g * 4;
                 dst[0] = make_float4(0.f, 0.f, 0.f, 0.f);
                 dst[1] = make_float4(0.f, 0.f, 0.f, 0.f);
                 dst[2] = make_float4(1.f, 0.f, 1.f, 1.f);
                 dst[3] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            key0 = r == 0 ? key : key0;
-            key1 = r == 1 ? key : key1;
-            key2 = r == 2 ? key : key2;
-            key3 = r == 3 ? key : key3;
-            // every lane is done reading stage[b] before round r + 2 refills it
-            __syncwarp();
         }
-        if (p.collect_stats) {
-            const uint32_t s0 = __reduce_add_sync(0xffffffffu, d0), s2 = __reduce_add_sync(0xffffffffu, d2);
-            const uint32_t s3 = __reduce_add_sync(0xffffffffu, d3), s4 = __reduce_add_sync(0xffffffffu, d4);
-            const uint32_t s6 = __reduce_add_sync(0xffffffffu, d6), s7 = __reduce_add_sync(0xffffffffu, d7);
-            const uint32_t x1 = __reduce_max_sync(0xffffffffu, m1), x5 = __reduce_max_sync(0xffffffffu, m5);
-            if (lane == 0) {
-                if (s0) atomicAdd(&p.fc->diag[0], s0);
-                if (x1) atomicMax(&p.fc->diag[1], x1);
-                if (s2) atomicAdd(&p.fc->diag[2], s2);
-                if (s3) atomicAdd(&p.fc->diag[3], s3);
-                if (s4) atomicAdd(&p.fc->diag[4], s4);
-                if (x5) atomicMax(&p.fc->diag[5], x5);
-                if (s6) atomicAdd(&p.fc->diag[6], s6);
-                if (s7) atomicAdd(&p.fc->diag[7], s7);
-            }
-        }
-        // Warp-level ordered compaction (decoupled look-back over warp tiles).
         uint32_t excl = 0;
+        if (lane == 0)
+            st_relaxed64(p.status + tile, status_word(p.epoch, tile == 0 ? kFlagInc : kFlagAgg, total));
         if (tile > 0) {
             bool to = false;
             excl = lookback_warp(p.status, tile, p.epoch, &to);
@@ -446,25 +321,16 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
         uint32_t before = 0;
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) {
-            const uint32_t mr = r == 0 ? mask0 : r == 1 ? mask1 : r == 2 ? mask2 : mask3;
-            if ((mr >> lane) & 1u) {
-                const uint32_t o = excl + before + __popc(mr & lt);
-                const uint32_t kr = r == 0 ? key0 : r == 1 ? key1 : r == 2 ? key2 : key3;
-                p.keys_out[o] = kr;
+            if ((mask[r] >> lane) & 1u) {
+                const uint32_t o = excl + before + __popc(mask[r] & lt);
+                p.keys_out[o] = key[r];
                 p.ids_out[o] = base + r * 32 + lane;
 #pragma unroll
-                for (int ps = 0; ps < 4; ++ps) atomicAdd(&s_hist[ps][(kr >> (8 * ps)) & 255u], 1u);
+                for (int ps = 0; ps < 4; ++ps) atomicAdd(&s_hist[ps][(key[r] >> (8 * ps)) & 255u], 1u);
             }
-            before += __popc(mr);
+            before += __popc(mask[r]);
         }
-        tile = ntile;
-        total = ntotal;
-        mask0 = nmask0;
-        mask1 = nmask1;
-        mask2 = nmask2;
-        mask3 = nmask3;
     }
-    if (stage_failed) atomicOr(&p.fc->error_flags, kErrCullStage);
     __syncthreads();
     for (int i = threadIdx.x; i < 4 * 256; i += kCullThreads) {
         const uint32_t c = (&s_hist[0][0])[i];
@@ -472,28 +338,121 @@ __global__ void __launch_bounds__(kCullThreads, 3) cull_kernel(CullParams p) {
     }
 }
 
+// Pass 2 (projection): warps take groups of 32 compacted visible rows
+// (statically: group = warp + k * warps), stage a group's rows into their
+// shared-memory rows (TMA bulk copies), project them and write the projected
+// records (shaders/cull.glsl:234-423).  Every lane holds a visible row, so no
+// projection issue slot is spent on culled rows.  One stage per warp lets 6
+// CTAs (24 warps) share an SM; the other warps' math hides a warp's staging
+// wait (measured faster than two stages per warp at 3 CTAs per SM).
+template <int kChunks>  // 16-byte chunks of a row the SH degree needs: 4, 7, 10 or 16
+__global__ void __launch_bounds__(kCullThreads, 6) cull_project_kernel(CullParams p) {
+    extern __shared__ float4 smem4[];
+    __shared__ __align__(8) uint64_t s_bar[kCullWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        mbar_init(&s_bar[warp], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    float4* const stage0 = smem4 + (size_t)warp * 32 * kStageStride;
+    const uint32_t n_vis = p.fc->visible_count;
+    const uint32_t groups = (n_vis + 31) / 32;
+    const uint32_t wg = blockIdx.x * kCullWarps + warp, nw = gridDim.x * kCullWarps;
+    CamRegs cam;
+    load_cam(p.cam, cam);
+    const bool animated = p.anim_deltas != nullptr &&
+                          (p.anim_state_a != 0 || (p.anim_weight > 0.0f && p.anim_state_b != 0));
+    const uint64_t stream_policy = l2_policy_evict_first();
+    bool stage_failed = false;
+    uint32_t phase = 0;   // parity of the next completion of the warp's barrier
+    uint32_t d0 = 0, d2 = 0, d3 = 0, d4 = 0, d6 = 0, d7 = 0, m1 = 0, m5 = 0;
+    for (uint32_t g = wg; g < groups; g += nw) {
+        const uint32_t id = stage_group<kChunks>(p.rows, p.ids_out, g * 32u, n_vis, stage0, &s_bar[warp], lane,
+                                                 stream_policy);
+        if (!mbar_wait_bounded(&s_bar[warp], phase)) stage_failed = true;
+        phase ^= 1u;
+        if (id != kSentinel) {
+            float4* row = stage0 + lane * kStageStride;
+            const float4 c0 = row[0];
+            const float vx = add(add(add(mul(cam.V[0], c0.x), mul(cam.V[4], c0.y)), mul(cam.V[8], c0.z)), cam.V[12]);
+            const float vy = add(add(add(mul(cam.V[1], c0.x), mul(cam.V[5], c0.y)), mul(cam.V[9], c0.z)), cam.V[13]);
+            const float vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
+            if (animated) {
+                float4 c3 = row[3];
+                animate_row(p, id, row, c3);
+            }
+            float4 rec[4];
+            float qa, gp;
+            project_visible(row, c0, vx, vy, vz, cam, p.sh_degree, p.sh_lod_distance, rec, &qa, &gp);
+            float4* dst = p.projected + (size_t)id * 4;
+            dst[0] = rec[0];
+            dst[1] = rec[1];
+            dst[2] = rec[2];
+            dst[3] = rec[3];
+            if (p.collect_stats) {
+                // shaders/cull.glsl:296-318
+                const uint32_t qpx = g_f2u_sat(g_min(g_max(0.0f, qa), 4294967295.0f));
+                const uint32_t gpx = g_f2u_sat(g_min(ceilf(gp), 4294967295.0f));
+                d0 += (uint32_t)(qpx + 1023u) >> 10u;
+                m1 = max(m1, qpx);
+                d2 += qpx > 1024u;
+                d3 += qpx > 16384u;
+                d4 += (uint32_t)(gpx + 1023u) >> 10u;
+                m5 = max(m5, gpx);
+                d6 += gpx > 1024u;
+                d7 += gpx > 16384u;
+            }
+        }
+        // every lane is done with the stage before the next group refills it
+        __syncwarp();
+    }
+    if (stage_failed) atomicOr(&p.fc->error_flags, kErrCullStage);
+    if (p.collect_stats) {
+        const uint32_t s0 = __reduce_add_sync(0xffffffffu, d0), s2 = __reduce_add_sync(0xffffffffu, d2);
+        const uint32_t s3 = __reduce_add_sync(0xffffffffu, d3), s4 = __reduce_add_sync(0xffffffffu, d4);
+        const uint32_t s6 = __reduce_add_sync(0xffffffffu, d6), s7 = __reduce_add_sync(0xffffffffu, d7);
+        const uint32_t x1 = __reduce_max_sync(0xffffffffu, m1), x5 = __reduce_max_sync(0xffffffffu, m5);
+        if (lane == 0) {
+            if (s0) atomicAdd(&p.fc->diag[0], s0);
+            if (x1) atomicMax(&p.fc->diag[1], x1);
+            if (s2) atomicAdd(&p.fc->diag[2], s2);
+            if (s3) atomicAdd(&p.fc->diag[3], s3);
+            if (s4) atomicAdd(&p.fc->diag[4], s4);
+            if (x5) atomicMax(&p.fc->diag[5], x5);
+            if (s6) atomicAdd(&p.fc->diag[6], s6);
+            if (s7) atomicAdd(&p.fc->diag[7], s7);
+        }
+    }
+}
+
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(cull_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
-        cudaFuncSetAttribute(cull_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
-        cudaFuncSetAttribute(cull_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
-        cudaFuncSetAttribute(cull_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_project_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_project_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_project_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_project_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         attr_set = true;
     }
     int deg = p.sh_degree < 0 ? 0 : (p.sh_degree > 3 ? 3 : p.sh_degree);
     if (p.anim_deltas) deg = 3;   // the delta pass touches every SH slot of the staged row
-    uint32_t tiles = (p.n + kCullTile - 1) / kCullTile;
-    uint32_t warps = num_sms * 3 * kCullWarps;
-    uint32_t grid = (std::min(warps, tiles) + kCullWarps - 1) / kCullWarps;
-    if (grid == 0) return 0;
+    const uint32_t tiles = (p.n + kCullTile - 1) / kCullTile;
+    if (tiles == 0) return 0;
+    uint32_t vgrid = (tiles + kCullWarps - 1) / kCullWarps;
+    if (vgrid > num_sms * 16) vgrid = num_sms * 16;
+    cull_visible_kernel<<<vgrid, kCullThreads, 0, s>>>(p);
+    // projection: persistent, as many CTAs as fit (6 per SM) for the largest possible visible count
+    const uint32_t groups_cap = (p.n + 31) / 32;
+    uint32_t pgrid = num_sms * 6;
+    if (pgrid * kCullWarps > groups_cap) pgrid = (groups_cap + kCullWarps - 1) / kCullWarps;
     switch (deg) {
-        case 0: cull_kernel<4><<<grid, kCullThreads, kCullSmem, s>>>(p); break;
-        case 1: cull_kernel<7><<<grid, kCullThreads, kCullSmem, s>>>(p); break;
-        case 2: cull_kernel<10><<<grid, kCullThreads, kCullSmem, s>>>(p); break;
-        default: cull_kernel<16><<<grid, kCullThreads, kCullSmem, s>>>(p); break;
+        case 0: cull_project_kernel<4><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
+        case 1: cull_project_kernel<7><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
+        case 2: cull_project_kernel<10><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
+        default: cull_project_kernel<16><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
     }
-    return 1;
+    return 2;
 }
 
 }  // namespace gs
