@@ -3,7 +3,10 @@
 //
 // Memory plan (HBM-bound, 256-byte GpuGaussian rows), two kernels:
 //   * cull_visible_kernel reads the first 16 bytes (position, opacity) of
-//     every row, runs the near/frustum test, computes the depth keys and
+//     every row from the heads array (a contiguous copy of them written once
+//     per upload by gather_heads_kernel: reading them out of the rows would
+//     fetch at least one 32-byte sector, in practice 128 bytes, per 16 bytes
+//     used), runs the near/frustum test, computes the depth keys and
 //     compacts the visible (key, id) pairs in index order with a decoupled
 //     look-back over 128-row warp tiles, so the depth sort runs on N_vis
 //     pairs instead of N (the culled tail of the reference's all-N sort is
@@ -253,6 +256,21 @@ __device__ void animate_row(const CullParams& p, uint32_t row, float4* staged, f
     staged[3] = c3;
 }
 
+// Copies the first 16 bytes of every row into the contiguous heads array
+// (run once per upload; the rows are written nowhere else).
+__global__ void gather_heads_kernel(const float4* __restrict__ rows, float4* __restrict__ heads, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        heads[i] = __ldg(rows + (size_t)i * 16);
+}
+
+int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t num_sms, cudaStream_t s) {
+    if (n == 0) return 0;
+    uint32_t grid = (n + 255) / 256;
+    if (grid > num_sms * 8) grid = num_sms * 8;
+    gather_heads_kernel<<<grid, 256, 0, s>>>(rows, heads, n);
+    return 1;
+}
+
 // Pass 1 (visibility and compaction): every warp takes 128-Gaussian warp
 // tiles in ticket order, tests visibility from the rows' first 16 bytes
 // (shaders/cull.glsl:209-220), computes the depth keys (:230-232), and places
@@ -278,7 +296,7 @@ __global__ void __launch_bounds__(kCullThreads) cull_visible_kernel(CullParams p
 #pragma unroll
         for (int r = 0; r < kCullRounds; ++r) {
             const uint32_t g = base + r * 32 + lane;
-            c0[r] = g < p.n ? __ldg(p.rows + (size_t)g * 16) : make_float4(0.f, 0.f, 0.f, 0.f);
+            c0[r] = g < p.n ? __ldg(p.heads + g) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         uint32_t mask[kCullRounds], key[kCullRounds], total = 0;
 #pragma unroll

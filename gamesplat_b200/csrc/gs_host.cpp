@@ -57,6 +57,7 @@ struct gs_ctx {
     // scene
     uint32_t n = 0;
     float4* rows = nullptr;
+    float4* heads = nullptr;             // first 16 bytes of every row, contiguous (cull visibility pass)
     float4* projected = nullptr;
     uint32_t* keys[2] = {nullptr, nullptr};
     uint32_t* ids[2] = {nullptr, nullptr};
@@ -164,6 +165,7 @@ void dfree(T*& p) {
 
 void release_scene(gs_ctx* c) {
     dfree(c->rows);
+    dfree(c->heads);
     dfree(c->projected);
     for (int k = 0; k < 2; ++k) {
         dfree(c->keys[k]);
@@ -338,6 +340,7 @@ void run_cull(gs_ctx* c) {
     StageScope sc(c, ST_CULL);
     gs::CullParams p{};
     p.rows = c->rows;
+    p.heads = c->heads;
     p.n = c->n;
     p.cam = c->cam;
     p.sh_degree = std::max(0, std::min(3, c->knobs.sh_degree));
@@ -777,6 +780,7 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
     release_scene(c);
     const uint32_t n = (uint32_t)count;
     GS_CUDA(c, dalloc(&c->rows, (size_t)n * 256));
+    GS_CUDA(c, dalloc(&c->heads, (size_t)n * 16));
     GS_CUDA(c, dalloc(&c->projected, (size_t)n * 64));
     for (int k = 0; k < 2; ++k) {
         GS_CUDA(c, dalloc(&c->keys[k], (size_t)n * 4));
@@ -795,6 +799,8 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
     GS_CUDA(c, cudaMemsetAsync(c->bin_status, 0, bin_tiles * 8, c->stream));
     GS_CUDA(c, cudaMemsetAsync(c->projected, 0, (size_t)n * 64, c->stream));
     GS_CUDA(c, cudaMemcpyAsync(c->rows, rows, (size_t)n * 256, kind, c->stream));
+    gs::launch_gather_heads(c->rows, c->heads, n, c->num_sms, c->stream);
+    GS_CUDA(c, cudaGetLastError());
     c->n = n;
     int rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(std::max<uint64_t>(8ull * n, 1u << 20), 0x3FFFFFFFull));
     if (rc) return rc;

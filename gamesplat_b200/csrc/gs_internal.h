@@ -102,6 +102,7 @@ static_assert(sizeof(RasterRecord) == 64, "RasterRecord must be 64 bytes");
 
 struct CullParams {
     const float4* rows;          // N x 16 float4 (GpuGaussian)
+    const float4* heads;         // N float4: the first 16 bytes of every row (position, opacity), kept beside the rows
     uint32_t n;
     gs_camera cam;               // the frame's CameraUniforms, by value (constant-bank operands)
     int sh_degree;
@@ -205,6 +206,7 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, s
 
 // Launchers (each returns the number of kernels it launched).
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s);
+int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t num_sms, cudaStream_t s);
 int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s);
 int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
