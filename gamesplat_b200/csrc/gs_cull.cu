@@ -8,7 +8,7 @@
 //     fetch at least one 32-byte sector, in practice 128 bytes, per 16 bytes
 //     used), runs the near/frustum test, computes the depth keys and
 //     compacts the visible (key, id) pairs in index order with a decoupled
-//     look-back over 128-row warp tiles, so the depth sort runs on N_vis
+//     look-back over 2048-row CTA tiles, so the depth sort runs on N_vis
 //     pairs instead of N (the culled tail of the reference's all-N sort is
 //     all-equal (0xFFFFFFFF, 0xFFFFFFFF) pairs, so the result is identical);
 //   * cull_project_kernel walks the compacted ids in groups of 32 and stages
@@ -25,7 +25,6 @@
 
 namespace gs {
 
-static_assert(kCullRounds == 4, "the round loop selects per-round values among four scalars");
 constexpr int kStageStride = 17;  // float4 per staged row (16 + 1 pad)
 constexpr int kCullWarps = kCullThreads / 32;
 constexpr size_t kCullSmem = (size_t)kCullWarps * 32 * kStageStride * sizeof(float4);  // one stage per warp
@@ -271,62 +270,82 @@ int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t 
     return 1;
 }
 
-// Pass 1 (visibility and compaction): every warp takes 128-Gaussian warp
-// tiles in ticket order, tests visibility from the rows' first 16 bytes
-// (shaders/cull.glsl:209-220), computes the depth keys (:230-232), and places
-// its visible (key, id) pairs in index order with a warp-level decoupled
-// look-back; the 4 x 256 key-digit histograms of the depth sort are
-// accumulated in shared memory.
-__global__ void __launch_bounds__(kCullThreads) cull_visible_kernel(CullParams p) {
+// Pass 1 (visibility and compaction): each CTA takes one 2048-row tile by
+// ticket (tickets follow CTA start order, so every tile a look-back waits on
+// belongs to a CTA that is already running), loads 8 heads per thread
+// (coalesced, all in flight at once), tests visibility
+// (shaders/cull.glsl:209-220), computes the depth keys (:230-232) and places
+// the tile's visible (key, id) pairs in index order: a block scan of the
+// per-(row group, warp) counts, then one warp-level decoupled look-back per
+// tile.  The 4 x 256 key-digit histograms of the depth sort are accumulated in
+// shared memory; the top digit (sign and high exponent bits, a handful of
+// values in a scene) is aggregated per warp first, since 32 lanes adding to
+// one shared word would serialize.
+__global__ void __launch_bounds__(kCullVisThreads) cull_visible_kernel(CullParams p) {
+    constexpr int kWarps = kCullVisThreads / 32;
+    static_assert(kCullVisItems * kWarps == 64, "the count scan gives each lane two (row group, warp) counts");
     __shared__ uint32_t s_hist[4][256];
-    for (int i = threadIdx.x; i < 4 * 256; i += kCullThreads) (&s_hist[0][0])[i] = 0u;
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
+    __shared__ uint32_t s_cnt[kCullVisItems * kWarps];   // (row group, warp) order = index order
+    __shared__ uint32_t s_tile, s_excl;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t lt = (1u << lane) - 1u;
-    const uint32_t num_tiles = (p.n + kCullTile - 1) / kCullTile;
+    for (int i = t; i < 4 * 256; i += kCullVisThreads) (&s_hist[0][0])[i] = 0u;
+    if (t == 0) s_tile = atomicAdd(&p.fc->cull_ticket, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t num_tiles = (p.n + kCullVisTile - 1) / kCullVisTile;
+    if (tile >= num_tiles) return;   // uniform over the CTA
+    const uint32_t base = tile * kCullVisTile;
     const float* V = p.cam.view;
     const float P0 = p.cam.proj[0], P5 = p.cam.proj[5], ortho = p.cam.orthographic;
-    for (;;) {
-        uint32_t tile = 0;
-        if (lane == 0) tile = atomicAdd(&p.fc->cull_ticket, 1u);
-        tile = __shfl_sync(0xffffffffu, tile, 0);
-        if (tile >= num_tiles) break;
-        const uint32_t base = tile * kCullTile;
-        float4 c0[kCullRounds];
+    float4 c0[kCullVisItems];
 #pragma unroll
-        for (int r = 0; r < kCullRounds; ++r) {
-            const uint32_t g = base + r * 32 + lane;
-            c0[r] = g < p.n ? __ldg(p.heads + g) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        uint32_t mask[kCullRounds], key[kCullRounds], total = 0;
+    for (int k = 0; k < kCullVisItems; ++k) {
+        const uint32_t g = base + k * kCullVisThreads + t;
+        c0[k] = g < p.n ? __ldg(p.heads + g) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    uint32_t mask[kCullVisItems], key[kCullVisItems];
 #pragma unroll
-        for (int r = 0; r < kCullRounds; ++r) {
-            const uint32_t g = base + r * 32 + lane;
-            // p_view = view * vec4(position, 1.0)
-            const float vx = add(add(add(mul(V[0], c0[r].x), mul(V[4], c0[r].y)), mul(V[8], c0[r].z)), V[12]);
-            const float vy = add(add(add(mul(V[1], c0[r].x), mul(V[5], c0[r].y)), mul(V[9], c0[r].z)), V[13]);
-            const float vz = add(add(add(mul(V[2], c0[r].x), mul(V[6], c0[r].y)), mul(V[10], c0[r].z)), V[14]);
-            bool visible = g < p.n && (vz <= -0.2f);
-            if (visible) {
-                float inv_z = dv(-1.0f, vz);
-                float ndc_x = add(mul(mul(mul(P0, vx), inv_z), sub(1.0f, ortho)), mul(mul(P0, vx), ortho));
-                float ndc_y = add(mul(mul(mul(P5, vy), inv_z), sub(1.0f, ortho)), mul(mul(P5, vy), ortho));
-                visible = fabsf(ndc_x) <= 1.3f && fabsf(ndc_y) <= 1.3f;
-            }
-            key[r] = 0xFFFFFFFFu - __float_as_uint(g_max(-vz, 0.0f));
-            mask[r] = __ballot_sync(0xffffffffu, visible);
-            total += __popc(mask[r]);
-            if (!visible && g < p.n && p.write_invisible) {   // shaders/cull.glsl:222-228
-                float4* dst = p.projected + (size_t)g * 4;
-                dst[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-                dst[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-                dst[2] = make_float4(1.f, 0.f, 1.f, 1.f);
-                dst[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+    for (int k = 0; k < kCullVisItems; ++k) {
+        const uint32_t g = base + k * kCullVisThreads + t;
+        // p_view = view * vec4(position, 1.0)
+        const float vx = add(add(add(mul(V[0], c0[k].x), mul(V[4], c0[k].y)), mul(V[8], c0[k].z)), V[12]);
+        const float vy = add(add(add(mul(V[1], c0[k].x), mul(V[5], c0[k].y)), mul(V[9], c0[k].z)), V[13]);
+        const float vz = add(add(add(mul(V[2], c0[k].x), mul(V[6], c0[k].y)), mul(V[10], c0[k].z)), V[14]);
+        bool visible = g < p.n && (vz <= -0.2f);
+        if (visible) {
+            float inv_z = dv(-1.0f, vz);
+            float ndc_x = add(mul(mul(mul(P0, vx), inv_z), sub(1.0f, ortho)), mul(mul(P0, vx), ortho));
+            float ndc_y = add(mul(mul(mul(P5, vy), inv_z), sub(1.0f, ortho)), mul(mul(P5, vy), ortho));
+            visible = fabsf(ndc_x) <= 1.3f && fabsf(ndc_y) <= 1.3f;
         }
-        uint32_t excl = 0;
+        key[k] = 0xFFFFFFFFu - __float_as_uint(g_max(-vz, 0.0f));
+        mask[k] = __ballot_sync(0xffffffffu, visible);
+        if (lane == 0) s_cnt[k * kWarps + warp] = (uint32_t)__popc(mask[k]);
+        if (!visible && g < p.n && p.write_invisible) {   // shaders/cull.glsl:222-228
+            float4* dst = p.projected + (size_t)g * 4;
+            dst[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+            dst[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            dst[2] = make_float4(1.f, 0.f, 1.f, 1.f);
+            dst[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // exclusive scan of the 64 counts in index order, two per lane
+        const uint32_t a = s_cnt[2 * lane], b = s_cnt[2 * lane + 1];
+        uint32_t incl = a + b;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        s_cnt[2 * lane] = incl - a - b;
+        s_cnt[2 * lane + 1] = incl - b;
         if (lane == 0)
             st_relaxed64(p.status + tile, status_word(p.epoch, tile == 0 ? kFlagInc : kFlagAgg, total));
+        uint32_t excl = 0;
         if (tile > 0) {
             bool to = false;
             excl = lookback_warp(p.status, tile, p.epoch, &to);
@@ -335,22 +354,32 @@ __global__ void __launch_bounds__(kCullThreads) cull_visible_kernel(CullParams p
                 st_relaxed64(p.status + tile, status_word(p.epoch, kFlagInc, excl + total));
             }
         }
-        if (lane == 0 && tile == num_tiles - 1) p.fc->visible_count = excl + total;
-        uint32_t before = 0;
-#pragma unroll
-        for (int r = 0; r < kCullRounds; ++r) {
-            if ((mask[r] >> lane) & 1u) {
-                const uint32_t o = excl + before + __popc(mask[r] & lt);
-                p.keys_out[o] = key[r];
-                p.ids_out[o] = base + r * 32 + lane;
-#pragma unroll
-                for (int ps = 0; ps < 4; ++ps) atomicAdd(&s_hist[ps][(key[r] >> (8 * ps)) & 255u], 1u);
-            }
-            before += __popc(mask[r]);
+        if (lane == 0) {
+            s_excl = excl;
+            if (tile == num_tiles - 1) p.fc->visible_count = excl + total;
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < 4 * 256; i += kCullThreads) {
+    const uint32_t excl = s_excl;
+#pragma unroll
+    for (int k = 0; k < kCullVisItems; ++k) {
+        const bool v = (mask[k] >> lane) & 1u;
+        const uint32_t kk = key[k];
+        if (v) {
+            const uint32_t o = excl + s_cnt[k * kWarps + warp] + (uint32_t)__popc(mask[k] & lt);
+            p.keys_out[o] = kk;
+            p.ids_out[o] = base + k * kCullVisThreads + t;
+            atomicAdd(&s_hist[0][kk & 255u], 1u);
+            atomicAdd(&s_hist[1][(kk >> 8) & 255u], 1u);
+            atomicAdd(&s_hist[2][(kk >> 16) & 255u], 1u);
+        }
+        // invisible lanes match among themselves (256 is no digit) and add nothing
+        const uint32_t d3 = v ? (kk >> 24) : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d3);
+        if (v && lane == __ffs(peers) - 1) atomicAdd(&s_hist[3][d3], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    for (int i = t; i < 4 * 256; i += kCullVisThreads) {
         const uint32_t c = (&s_hist[0][0])[i];
         if (c) atomicAdd(p.key_hist + i, c);
     }
@@ -455,11 +484,9 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
     }
     int deg = p.sh_degree < 0 ? 0 : (p.sh_degree > 3 ? 3 : p.sh_degree);
     if (p.anim_deltas) deg = 3;   // the delta pass touches every SH slot of the staged row
-    const uint32_t tiles = (p.n + kCullTile - 1) / kCullTile;
+    const uint32_t tiles = (p.n + kCullVisTile - 1) / kCullVisTile;
     if (tiles == 0) return 0;
-    uint32_t vgrid = (tiles + kCullWarps - 1) / kCullWarps;
-    if (vgrid > num_sms * 16) vgrid = num_sms * 16;
-    cull_visible_kernel<<<vgrid, kCullThreads, 0, s>>>(p);
+    cull_visible_kernel<<<tiles, kCullVisThreads, 0, s>>>(p);   // one CTA per tile
     // projection: persistent, as many CTAs as fit (6 per SM) for the largest possible visible count
     const uint32_t groups_cap = (p.n + 31) / 32;
     uint32_t pgrid = num_sms * 6;

@@ -788,7 +788,7 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
     }
     GS_CUDA(c, dalloc(&c->records, (size_t)n * sizeof(RasterRecord)));
     GS_CUDA(c, dalloc(&c->item_info, (size_t)n * sizeof(uint4)));
-    const size_t cull_tiles = ((size_t)n + gs::kCullTile - 1) / gs::kCullTile;
+    const size_t cull_tiles = ((size_t)n + gs::kCullVisTile - 1) / gs::kCullVisTile;
     GS_CUDA(c, dalloc(&c->cull_status, cull_tiles * sizeof(unsigned long long)));
     c->sort_status_stride = gs::sort_status_words(n);
     GS_CUDA(c, dalloc(&c->sort_status, c->sort_status_stride * 4 * sizeof(unsigned long long)));

@@ -61,11 +61,13 @@ constexpr int kSortLookback = 8;                       // look-back words read p
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 
-// Cull configuration: 128-thread CTAs; each warp works alone on 128-Gaussian
-// warp tiles (4 rounds of 32), which are the units of the look-back.
+// Cull configuration.  Visibility pass: 256-thread CTAs, 8 rows per thread;
+// its 2048-row CTA tiles are the units of the look-back.  Projection pass:
+// 128-thread CTAs, each warp stages and projects 32 visible rows at a time.
+constexpr int kCullVisThreads = 256;
+constexpr int kCullVisItems = 8;
+constexpr int kCullVisTile = kCullVisThreads * kCullVisItems;
 constexpr int kCullThreads = 128;
-constexpr int kCullRounds = 4;
-constexpr int kCullTile = 32 * kCullRounds;
 
 // Binning configuration: 4 sorted splats per thread, 1024 per CTA tile.
 constexpr int kBinThreads = 128;
