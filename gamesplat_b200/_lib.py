@@ -19,6 +19,7 @@ GS_ERR_NO_SCENE = -5
 GS_ERR_BUDGET_REFUSED = -6
 GS_ERR_NO_DEVICE = -7
 GS_ERR_TOO_LARGE = -8
+GS_ERR_FORMAT = -9
 
 GS_MODE_ALPHA = 0
 GS_MODE_STOCHASTIC = 1
@@ -40,7 +41,9 @@ EXPORTS = (
     "gs_read_stats", "gs_debug_read", "gs_profile_enable", "gs_stage_times", "gs_stage_names", "gs_status_str",
     "gs_last_error", "gs_camera_uniforms", "gs_load_ply", "gs_pack_raw", "gs_sort_pairs_scratch_bytes",
     "gs_sort_pairs", "gs_sort_pairs_noalloc", "gs_upload_anim", "gs_set_anim_state", "gs_set_display_lut",
-    "gs_display", "gs_debug_wait_probe", "gs_pack_raw_device",
+    "gs_display", "gs_debug_wait_probe", "gs_pack_raw_device", "gs_gsanim_load", "gs_gsanim_free",
+    "gs_gsanim_get_info", "gs_gsanim_rows", "gs_gsanim_deltas", "gs_gsanim_layer_data", "gs_gsanim_display_lut",
+    "gs_gsanim_layer_name", "gs_gsanim_sample", "gs_gsanim_layer_weights",
 )
 
 
@@ -93,6 +96,23 @@ class GsStats(C.Structure):
         ("error_flags", C.c_uint32),
         ("kernel_launches", C.c_uint32),
         ("reserved", C.c_uint32 * 5),
+    ]
+
+
+class GsGsanimInfo(C.Structure):
+    """gs_gsanim_info (include/gs_api.h)."""
+
+    _fields_ = [
+        ("version", C.c_uint32),
+        ("gaussian_count", C.c_uint32),
+        ("state_count", C.c_uint32),
+        ("layer_count", C.c_uint32),
+        ("key_count", C.c_uint32),
+        ("lut_size", C.c_uint32),
+        ("linear", C.c_int32),
+        ("log2_min", C.c_float),
+        ("log2_max", C.c_float),
+        ("duration_seconds", C.c_double),
     ]
 
 
@@ -152,6 +172,17 @@ def lib() -> C.CDLL:
         "gs_pack_raw_device": (i32, [vp, u64, vp, vp]),
         "gs_upload_anim": (i32, [vp, vp, u32, vp]),
         "gs_set_anim_state": (i32, [vp, i32, i32, f32]),
+        "gs_gsanim_load": (i32, [C.c_char_p, C.POINTER(vp)]),
+        "gs_gsanim_free": (None, [vp]),
+        "gs_gsanim_get_info": (i32, [vp, C.POINTER(GsGsanimInfo)]),
+        "gs_gsanim_rows": (i32, [vp, vp]),
+        "gs_gsanim_deltas": (i32, [vp, vp, vp]),
+        "gs_gsanim_layer_data": (i32, [vp, vp]),
+        "gs_gsanim_display_lut": (i32, [vp, vp]),
+        "gs_gsanim_layer_name": (C.c_int64, [vp, u32, vp, u64]),
+        "gs_gsanim_sample": (i32, [vp, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_float)]),
+        "gs_gsanim_layer_weights": (i32, [vp, C.c_double, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -2,7 +2,8 @@
 
 Every source under gamesplat_b200/csrc is compiled with
   -gencode arch=compute_100a,code=sm_100a -lineinfo -O3
-and linked with the static CUDA runtime into gamesplat_b200/libgs_cuda.so.
+and linked with the static CUDA runtime (and the system zlib, for the gsanim
+archive reader) into gamesplat_b200/libgs_cuda.so.
 Host C++ is compiled with -ffp-contract=off so host-side float results
 (camera uniforms, PLY transforms) match the reference's host code.
 """
@@ -64,7 +65,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(compile_one, sources()))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [cc, *ARCH, "-shared", "-cudart", "static", *[str(o) for o in objs], "-o", str(tmp)]
+    cmd = [cc, *ARCH, "-shared", "-cudart", "static", *[str(o) for o in objs], "-lz", "-o", str(tmp)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -1,0 +1,880 @@
+// gsanim assets on the host: the archive reader, manifest validation, base
+// PLY decode and playback sampling of src/gaussian_loader_gsanim.cpp
+// (gaussian_load_gsanim :386-495, gsanim_sample :497-509,
+// gsanim_layer_weights :511-531).  The result feeds the device path:
+// gs_gsanim_rows -> gs_upload_rows, gs_gsanim_deltas -> gs_upload_anim,
+// gs_gsanim_sample -> gs_set_anim_state, gs_gsanim_display_lut ->
+// gs_set_display_lut.
+//
+// An asset is accepted exactly when the reference loader accepts it:
+//   * a ZIP archive of at most 512 MiB with exactly four entries, stored or
+//     deflated, unencrypted, none a directory, each name one of the six
+//     payload names and none repeated, every payload's CRC-32 verified;
+//   * manifest.json: at most 1 MiB of strict JSON (UTF-8 checked, escapes
+//     checked, nesting depth at most 32), then the version-specific fields;
+//   * base.ply: the 62-float little-endian layout, comment lines allowed
+//     between header lines, every value finite, decoded scales finite with
+//     finite squares, quaternion norms above 1e-8; every decoded appearance
+//     state finite (0.1 / 0.2), no appearance in the base (0.3);
+//   * scales.bin: 48 finite positive floats; deltas.bin: (states - 1) x N x 48
+//     int8 without -128 (0.1 / 0.2); layers.bin: layers x N x 48 finite
+//     halves; display_lut.bin: size^3 RGB uint16 (0.3).
+// The archive reader is written here over zlib's raw inflate, with the
+// reference archive reader's acceptance rules (data in front of the archive,
+// the stored-size test, empty entries); archives with ZIP64 records are
+// rejected (a 512 MiB archive of four entries never needs them).
+#include <zlib.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gs_api.h"
+
+struct gs_gsanim {
+    struct Key {
+        double time_seconds = 0;
+        uint32_t state = 0;
+        bool linear = false;              // outgoing interval (0.2)
+        bool has_interpolation = false;
+    };
+    struct LayerKey {
+        double time_seconds = 0;
+        std::array<float, 3> weight{};
+        bool linear = false;
+    };
+    struct Layer {
+        std::string name;
+        std::vector<LayerKey> keys;
+    };
+    uint32_t version = 0;                 // 1, 2, 3 for "0.1", "0.2", "0.3"
+    uint32_t gaussian_count = 0;
+    uint32_t state_count = 0;
+    double duration = 0;
+    bool linear = false;
+    std::vector<Key> keys;
+    std::vector<Layer> layers;
+    std::vector<uint16_t> layer_data;     // IEEE half bits, layer / row / coefficient
+    std::vector<uint16_t> display_lut;    // RGB uint16 UNORM, red fastest
+    uint32_t lut_size = 0;
+    float log2_min = 0, log2_max = 0;
+    std::vector<int8_t> deltas;           // state-major, original row order, 48 per row
+    float scales[48] = {};
+    std::vector<float> rows;              // GpuGaussian rows, 64 floats each
+};
+
+namespace {
+
+constexpr size_t kMaxText = 1024 * 1024;              // manifest, PLY header
+constexpr size_t kMaxPayload = 256u * 1024 * 1024;    // deltas / layer coefficients
+constexpr uint32_t kMaxGaussians = 1000000;
+constexpr long kMaxArchive = 512l * 1024 * 1024;
+
+uint16_t le16(const uint8_t* p) { return (uint16_t)(p[0] | p[1] << 8); }
+uint32_t le32(const uint8_t* p) { return (uint32_t)p[0] | (uint32_t)p[1] << 8 | (uint32_t)p[2] << 16 | (uint32_t)p[3] << 24; }
+float lef32(const uint8_t* p) {
+    const uint32_t b = le32(p);
+    float v;
+    std::memcpy(&v, &b, 4);
+    return v;
+}
+
+// ---- ZIP archive ------------------------------------------------------------
+
+struct ZipEntry {
+    std::string name;                     // raw bytes (may hold NUL)
+    uint16_t flags = 0, method = 0;
+    uint32_t crc = 0, csize = 0, usize = 0, local = 0, external_attr = 0;
+};
+
+struct Zip {
+    std::vector<uint8_t> bytes;
+    std::vector<ZipEntry> entries;
+    size_t base = 0;    // bytes before the archive proper (data in front of it)
+    size_t size = 0;    // archive size from `base`
+
+    // Bytes [ofs, ofs + count) of the archive (relative to `base`), or
+    // nullptr when the file ends first.
+    const uint8_t* at(uint64_t ofs, uint64_t count) const {
+        const uint64_t abs = (uint64_t)base + ofs;
+        if (abs > bytes.size() || count > bytes.size() - abs) return nullptr;
+        return bytes.data() + abs;
+    }
+
+    // The end-of-central-directory record: the last signature with a whole
+    // record after it, searched backwards in 4 KiB windows (overlapping by 3
+    // bytes) until a window starts 64 KiB + 22 bytes or more before the end.
+    bool locate_end(size_t& eocd) const {
+        const size_t n = bytes.size();
+        if (n < 22) return false;
+        size_t cur = n > 4096 ? n - 4096 : 0;
+        for (;;) {
+            const size_t m = std::min<size_t>(4096, n - cur);
+            for (long i = (long)m - 4; i >= 0; --i) {
+                if (le32(&bytes[cur + (size_t)i]) == 0x06054b50u && n - (cur + (size_t)i) >= 22) {
+                    eocd = cur + (size_t)i;
+                    return true;
+                }
+            }
+            if (cur == 0 || n - cur >= 65535u + 22u) return false;
+            cur = cur > 4093 ? cur - 4093 : 0;
+        }
+    }
+
+    // Central directory.  Offsets in the archive are relative to its start,
+    // which is where the directory's own offset and size say it is: data in
+    // front of the archive (the gap between the directory's end and the end
+    // record) shifts every offset.
+    bool open() {
+        size_t eocd;
+        if (!locate_end(eocd)) return false;
+        const uint8_t* e = &bytes[eocd];
+        if (eocd >= 20 + 56 && le32(&bytes[eocd - 20]) == 0x07064b50u) return false;   // ZIP64
+        const uint32_t disk = le16(e + 4), cd_disk = le16(e + 6), on_disk = le16(e + 8), total = le16(e + 10);
+        const uint32_t cd_size = le32(e + 12), cd_off = le32(e + 16);
+        if (total != on_disk) return false;
+        if ((disk | cd_disk) != 0 && (disk != 1 || cd_disk != 1)) return false;
+        if ((uint64_t)cd_size < (uint64_t)total * 46) return false;
+        if ((uint64_t)cd_off + cd_size > bytes.size() || eocd < (uint64_t)cd_off + cd_size) return false;
+        base = eocd - ((size_t)cd_off + cd_size);
+        size = bytes.size() - base;
+        if (!total) return true;
+        const uint8_t* cd = at(cd_off, cd_size);
+        if (!cd) return false;
+        size_t left = cd_size;
+        for (uint32_t i = 0; i < total; ++i) {
+            if (left < 46 || le32(cd) != 0x02014b50u) return false;
+            ZipEntry z;
+            z.flags = le16(cd + 8);
+            z.method = le16(cd + 10);
+            z.crc = le32(cd + 16);
+            z.csize = le32(cd + 20);
+            z.usize = le32(cd + 24);
+            const uint32_t name_len = le16(cd + 28), extra_len = le16(cd + 30), comment_len = le16(cd + 32);
+            const uint32_t start_disk = le16(cd + 34);
+            z.external_attr = le32(cd + 38);
+            z.local = le32(cd + 42);
+            if (z.csize == 0xFFFFFFFFu || z.usize == 0xFFFFFFFFu || z.local == 0xFFFFFFFFu) return false;  // ZIP64
+            // A stored entry must keep its size, unless the 32-bit word at the
+            // method field (method and modification time together) is nonzero;
+            // a nonempty entry must have compressed bytes.
+            if ((le32(cd + 10) == 0 && z.usize != z.csize) || (z.usize && !z.csize)) return false;
+            if (start_disk == 0xFFFF || (start_disk != disk && start_disk != 1)) return false;
+            if ((uint64_t)z.local + 30 + z.csize > size) return false;
+            if (z.flags & 0x2000u) return false;   // masked local headers
+            const size_t header = 46 + (size_t)name_len + extra_len + comment_len;
+            if (header > left) return false;
+            z.name.assign((const char*)cd + 46, name_len);
+            entries.push_back(std::move(z));
+            cd += header;
+            left -= header;
+        }
+        return true;
+    }
+
+    static bool is_directory(const ZipEntry& z) {
+        return (!z.name.empty() && z.name.back() == '/') || (z.external_attr & 0x10u);
+    }
+    static bool usable(const ZipEntry& z) {
+        // not encrypted (traditional or strong), not patch data, stored or deflated
+        return !(z.flags & (0x1u | 0x40u | 0x20u)) && (z.method == 0 || z.method == 8);
+    }
+
+    // Payload of entry z into out (z.usize bytes), CRC-32 checked.  An entry
+    // without compressed bytes is empty and not checked.  A stored entry
+    // reads its uncompressed size.
+    bool extract(const ZipEntry& z, std::vector<uint8_t>& out) const {
+        out.assign(z.usize, 0);
+        if (!z.csize) return true;
+        const uint8_t* local = at(z.local, 30);
+        if (!local || le32(local) != 0x04034b50u) return false;
+        const uint64_t data = (uint64_t)z.local + 30 + le16(local + 26) + le16(local + 28);
+        if (data + z.csize > size) return false;
+        if (z.method == 0) {
+            const uint8_t* src = at(data, z.usize);
+            if (!src) return false;
+            if (z.usize) std::memcpy(out.data(), src, z.usize);
+        } else {
+            const uint8_t* src = at(data, z.csize);
+            if (!src) return false;
+            z_stream st{};
+            if (inflateInit2(&st, -15) != Z_OK) return false;
+            st.next_in = const_cast<Bytef*>(src);
+            st.avail_in = z.csize;
+            st.next_out = out.data();
+            st.avail_out = z.usize;
+            const int rc = inflate(&st, Z_FINISH);
+            const bool done = rc == Z_STREAM_END && st.total_out == z.usize;
+            inflateEnd(&st);
+            if (!done) return false;
+        }
+        const uLong crc = crc32(crc32(0L, Z_NULL, 0), out.data(), (uInt)out.size());
+        return (uint32_t)crc == z.crc;
+    }
+};
+
+// ---- JSON -------------------------------------------------------------------
+
+// Strict syntax check and tree of one JSON text.  Strings keep their raw
+// bytes between the quotes (escapes undecoded), numbers their text.
+struct Json {
+    enum Type { kNull, kBool, kNum, kStr, kArr, kObj };
+    struct Node {
+        Type type;
+        const char* b;
+        const char* e;
+        std::vector<int> kids;   // arrays: elements; objects: key, value, key, value, ...
+    };
+    std::vector<Node> nodes;
+    const unsigned char* p = nullptr;
+    const unsigned char* end = nullptr;
+
+    void space() {
+        while (p != end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n')) ++p;
+    }
+    bool take(char c) {
+        space();
+        if (p == end || *p != (unsigned char)c) return false;
+        ++p;
+        return true;
+    }
+    int add(Type t, const unsigned char* b, const unsigned char* e) {
+        nodes.push_back(Node{t, (const char*)b, (const char*)e, {}});
+        return (int)nodes.size() - 1;
+    }
+    static bool is_hex(unsigned char c) {
+        return (c >= '0' && c <= '9') || (c >= 'a' && c <= 'f') || (c >= 'A' && c <= 'F');
+    }
+    // A string: UTF-8 and escapes checked.
+    int string() {
+        if (!take('"')) return -1;
+        const unsigned char* b = p;
+        while (p != end) {
+            unsigned c = *p++;
+            if (c == '"') return add(kStr, b, p - 1);
+            if (c < 32) return -1;
+            if (c == '\\') {
+                if (p == end) return -1;
+                c = *p++;
+                if (c == 'u') {
+                    for (int i = 0; i < 4; ++i) {
+                        if (p == end || !is_hex(*p)) return -1;
+                        ++p;
+                    }
+                } else if (c != 0 && !std::strchr("\"\\/bfnrt", (int)c)) {
+                    // (a NUL after the backslash passes the reference's
+                    // strchr test, which finds the terminator)
+                    return -1;
+                }
+            } else if (c >= 128) {
+                if (c < 0xc2 || c > 0xf4) return -1;
+                const unsigned count = c >= 0xf0 ? 3 : c >= 0xe0 ? 2 : 1;
+                unsigned value = c & (count == 3 ? 7u : count == 2 ? 15u : 31u);
+                for (unsigned i = 0; i < count; ++i) {
+                    if (p == end || (*p & 0xc0) != 0x80) return -1;
+                    value = (value << 6) | (*p++ & 63u);
+                }
+                const unsigned least = count == 3 ? 65536u : count == 2 ? 2048u : 128u;
+                if (value < least || value > 0x10ffff || (value >= 0xd800 && value <= 0xdfff)) return -1;
+            }
+        }
+        return -1;
+    }
+    int value(int depth = 0) {
+        space();
+        if (p == end || depth > 32) return -1;
+        if (*p == '"') return string();
+        if (*p == '{' || *p == '[') {
+            const bool object = *p++ == '{';
+            const int me = add(object ? kObj : kArr, p - 1, p);
+            const char close = object ? '}' : ']';
+            if (take(close)) return me;
+            do {
+                if (object) {
+                    const int k = string();
+                    if (k < 0 || !take(':')) return -1;
+                    nodes[me].kids.push_back(k);
+                }
+                const int v = value(depth + 1);
+                if (v < 0) return -1;
+                nodes[me].kids.push_back(v);
+                if (take(close)) return me;
+            } while (take(','));
+            return -1;
+        }
+        static const char* words[] = {"true", "false", "null"};
+        for (int w = 0; w < 3; ++w) {
+            const size_t n = std::strlen(words[w]);
+            if ((size_t)(end - p) >= n && !std::memcmp(p, words[w], n)) {
+                p += n;
+                return add(w == 2 ? kNull : kBool, p - n, p);
+            }
+        }
+        const unsigned char* b = p;
+        if (*p == '-') ++p;
+        if (p == end) return -1;
+        if (*p == '0') {
+            ++p;
+        } else {
+            if (*p < '1' || *p > '9') return -1;
+            while (p != end && *p >= '0' && *p <= '9') ++p;
+        }
+        if (p != end && *p == '.') {
+            ++p;
+            const unsigned char* s = p;
+            while (p != end && *p >= '0' && *p <= '9') ++p;
+            if (p == s) return -1;
+        }
+        if (p != end && (*p == 'e' || *p == 'E')) {
+            ++p;
+            if (p != end && (*p == '-' || *p == '+')) ++p;
+            const unsigned char* s = p;
+            while (p != end && *p >= '0' && *p <= '9') ++p;
+            if (p == s) return -1;
+        }
+        return add(kNum, b, p);
+    }
+    // The whole text must be one value (whitespace around it allowed).
+    int parse(const std::vector<uint8_t>& text) {
+        p = text.data();
+        end = text.data() + text.size();
+        const int root = value();
+        if (root < 0) return -1;
+        space();
+        return p == end ? root : -1;
+    }
+
+    const Node& at(int i) const { return nodes[(size_t)i]; }
+
+    // A finite number written in at most 64 characters.
+    bool number(int i, double& out) const {
+        const Node& v = at(i);
+        if (v.type != kNum || v.e - v.b > 64) return false;
+        const std::string text(v.b, v.e);
+        char* stop = nullptr;
+        out = std::strtod(text.c_str(), &stop);
+        return stop == text.c_str() + text.size() && std::isfinite(out);
+    }
+    // A number in [0, max] written with digits only (an optional minus sign).
+    bool integer(int i, uint32_t& out, uint32_t max) const {
+        double n;
+        if (!number(i, n) || n < 0 || n > max) return false;
+        const Node& v = at(i);
+        for (const char* q = v.b + (*v.b == '-' ? 1 : 0); q != v.e; ++q)
+            if (*q < '0' || *q > '9') return false;
+        out = (uint32_t)n;
+        return true;
+    }
+    static unsigned hex4(const char* q) {
+        unsigned n = 0;
+        for (int k = 0; k < 4; ++k) {
+            const unsigned c = (unsigned char)q[k];
+            n = n * 16 + (c <= '9' ? c - '0' : (c | 32) - 'a' + 10);
+        }
+        return n;
+    }
+    // A string equal to the ASCII text `want`, \uXXXX escapes allowed (no
+    // other escape).
+    bool identifier(int i, const char* want) const {
+        const Node& v = at(i);
+        if (v.type != kStr) return false;
+        for (const char* q = v.b; q != v.e; ++q) {
+            unsigned c = (unsigned char)*q;
+            if (c == '\\') {
+                if (++q == v.e || *q != 'u' || v.e - q < 5) return false;
+                c = hex4(q + 1);
+                q += 4;
+            }
+            if (!*want || c != (unsigned char)*want++) return false;
+        }
+        return *want == 0;
+    }
+    // The decoded bytes (UTF-8) of a string; unpaired surrogates fail.
+    bool decoded(int i, std::string& out) const {
+        const Node& v = at(i);
+        if (v.type != kStr) return false;
+        for (const char* q = v.b; q != v.e;) {
+            unsigned c = (unsigned char)*q++;
+            if (c != '\\') {
+                out += (char)c;
+                continue;
+            }
+            c = (unsigned char)*q++;
+            if (c != 'u') {
+                static const char from[] = "\"\\/bfnrt";
+                static const char to[] = "\"\\/\b\f\n\r\t";
+                out += c == 0 ? '\0' : to[std::strchr(from, (int)c) - from];
+                continue;
+            }
+            c = hex4(q);
+            q += 4;
+            if (c >= 0xd800 && c <= 0xdbff) {
+                if (v.e - q < 6 || q[0] != '\\' || q[1] != 'u') return false;
+                const unsigned low = hex4(q + 2);
+                q += 6;
+                if (low < 0xdc00 || low > 0xdfff) return false;
+                c = 0x10000 + ((c - 0xd800) << 10) + (low - 0xdc00);
+            } else if (c >= 0xdc00 && c <= 0xdfff) {
+                return false;
+            }
+            if (c < 128) {
+                out += (char)c;
+            } else if (c < 2048) {
+                out += (char)(0xc0 | (c >> 6));
+                out += (char)(0x80 | (c & 63));
+            } else if (c < 65536) {
+                out += (char)(0xe0 | (c >> 12));
+                out += (char)(0x80 | ((c >> 6) & 63));
+                out += (char)(0x80 | (c & 63));
+            } else {
+                out += (char)(0xf0 | (c >> 18));
+                out += (char)(0x80 | ((c >> 12) & 63));
+                out += (char)(0x80 | ((c >> 6) & 63));
+                out += (char)(0x80 | (c & 63));
+            }
+        }
+        return true;
+    }
+    bool mode(int i, bool& linear) const {
+        linear = identifier(i, "linear");
+        return linear || identifier(i, "step");
+    }
+};
+
+// ---- manifest ---------------------------------------------------------------
+
+bool parse_layers(const Json& j, int arr, gs_gsanim& a) {
+    if (j.at(arr).type != Json::kArr) return false;
+    for (int li : j.at(arr).kids) {
+        if (j.at(li).type != Json::kObj || a.layers.size() >= 256) return false;
+        gs_gsanim::Layer layer;
+        unsigned fields = 0;
+        const auto& lk = j.at(li).kids;
+        for (size_t m = 0; m + 1 < lk.size(); m += 2) {
+            const int k = lk[m], v = lk[m + 1];
+            if (j.identifier(k, "name")) {
+                if ((fields & 1) || !j.decoded(v, layer.name) || layer.name.empty()) return false;
+                fields |= 1;
+            } else if (j.identifier(k, "keys")) {
+                if ((fields & 2) || j.at(v).type != Json::kArr) return false;
+                fields |= 2;
+                for (int ki : j.at(v).kids) {
+                    if (j.at(ki).type != Json::kObj || layer.keys.size() >= 65536) return false;
+                    gs_gsanim::LayerKey key;
+                    unsigned seen = 0;
+                    const auto& kk = j.at(ki).kids;
+                    for (size_t q = 0; q + 1 < kk.size(); q += 2) {
+                        const int name = kk[q], val = kk[q + 1];
+                        const unsigned bit = j.identifier(name, "time_seconds") ? 1u
+                                             : j.identifier(name, "weight")     ? 2u
+                                             : j.identifier(name, "interpolation") ? 4u : 0u;
+                        if (!bit) continue;
+                        if (seen & bit) return false;
+                        seen |= bit;
+                        if (bit == 1 && !j.number(val, key.time_seconds)) return false;
+                        if (bit == 4 && !j.mode(val, key.linear)) return false;
+                        if (bit == 2) {
+                            if (j.at(val).type != Json::kArr) return false;
+                            unsigned c = 0;
+                            for (int comp : j.at(val).kids) {
+                                double n;
+                                if (c == 3 || !j.number(comp, n) || n < 0 || !std::isfinite((float)n)) return false;
+                                key.weight[c++] = (float)n;
+                            }
+                            if (c != 3) return false;
+                        }
+                    }
+                    if (seen != 7) return false;
+                    layer.keys.push_back(key);
+                }
+            }
+        }
+        if (fields != 3 || layer.keys.empty()) return false;
+        for (const auto& prev : a.layers)
+            if (prev.name == layer.name) return false;
+        a.layers.push_back(std::move(layer));
+    }
+    return !a.layers.empty();
+}
+
+bool parse_display(const Json& j, int obj, gs_gsanim& a) {
+    if (j.at(obj).type != Json::kObj) return false;
+    static const char* names[] = {"type", "encoding", "layout", "size", "log2_min", "log2_max"};
+    static const char* values[] = {"lut3d_log2", "uint16_unorm_rgb", "r_fastest"};
+    unsigned seen = 0;
+    const auto& kids = j.at(obj).kids;
+    for (size_t m = 0; m + 1 < kids.size(); m += 2) {
+        const int k = kids[m], v = kids[m + 1];
+        int field = -1;
+        for (int i = 0; i < 6; ++i)
+            if (j.identifier(k, names[i])) field = i;
+        if (field < 0) continue;
+        if (seen & (1u << field)) return false;
+        seen |= 1u << field;
+        if (field < 3 && !j.identifier(v, values[field])) return false;
+        if (field == 3 && (!j.integer(v, a.lut_size, 256) || a.lut_size < 2)) return false;
+        if (field >= 4) {
+            double n;
+            if (!j.number(v, n) || !std::isfinite((float)n)) return false;
+            (field == 4 ? a.log2_min : a.log2_max) = (float)n;
+        }
+    }
+    return seen == 63 && a.log2_min < a.log2_max;
+}
+
+bool parse_manifest(const std::vector<uint8_t>& text, gs_gsanim& a) {
+    Json j;
+    const int root = j.parse(text);
+    if (root < 0 || j.at(root).type != Json::kObj) return false;
+    const auto& kids = j.at(root).kids;
+    // the version first, wherever it stands: it decides which fields count
+    bool version_seen = false;
+    for (size_t m = 0; m + 1 < kids.size(); m += 2) {
+        if (!j.identifier(kids[m], "version")) continue;
+        if (version_seen) return false;
+        version_seen = true;
+        const int v = kids[m + 1];
+        a.version = j.identifier(v, "0.1") ? 1 : j.identifier(v, "0.2") ? 2 : j.identifier(v, "0.3") ? 3 : 0;
+    }
+    if (!version_seen || !a.version) return false;
+    static const char* names[] = {"format", "version", "gaussian_count", "state_count", "sh_degree",
+                                  "coordinate_system", "color_encoding", "duration_seconds", "interpolation",
+                                  "keys", "layers", "display_transform"};
+    bool linear_color = false;
+    unsigned seen = 0;
+    for (size_t m = 0; m + 1 < kids.size(); m += 2) {
+        const int k = kids[m], v = kids[m + 1];
+        int field = -1;
+        for (int i = 0; i < 12; ++i)
+            if (j.identifier(k, names[i])) field = i;
+        if (field < 0) continue;
+        if (a.version != 3 && field >= 10) continue;
+        if (a.version == 3 && (field == 3 || field == 8 || field == 9)) continue;
+        if (seen & (1u << field)) return false;
+        seen |= 1u << field;
+        uint32_t degree;
+        switch (field) {
+            case 0: if (!j.identifier(v, "gsanim")) return false; break;
+            case 1: break;
+            case 2: if (!j.integer(v, a.gaussian_count, kMaxGaussians) || !a.gaussian_count) return false; break;
+            case 3: if (!j.integer(v, a.state_count, 256) || a.state_count < 2) return false; break;
+            case 4: if (!j.integer(v, degree, 3) || degree != 3) return false; break;
+            case 5: if (!j.identifier(v, "blender_world_z_up_meters")) return false; break;
+            case 6:
+                linear_color = j.identifier(v, "scene_linear_rec709");
+                if (!linear_color && !j.identifier(v, "display_referred_agx_baked")) return false;
+                break;
+            case 7: if (!j.number(v, a.duration) || a.duration <= 0) return false; break;
+            case 8:
+                if (!j.mode(v, a.linear)) return false;
+                break;
+            case 9: {
+                if (j.at(v).type != Json::kArr) return false;
+                for (int ki : j.at(v).kids) {
+                    if (j.at(ki).type != Json::kObj || a.keys.size() >= 65536) return false;
+                    gs_gsanim::Key key;
+                    unsigned fields = 0;
+                    const auto& kk = j.at(ki).kids;
+                    for (size_t q = 0; q + 1 < kk.size(); q += 2) {
+                        const int name = kk[q], val = kk[q + 1];
+                        if (j.identifier(name, "time_seconds")) {
+                            if ((fields & 1) || !j.number(val, key.time_seconds)) return false;
+                            fields |= 1;
+                        } else if (j.identifier(name, "state")) {
+                            if ((fields & 2) || !j.integer(val, key.state, 255)) return false;
+                            fields |= 2;
+                        } else if (a.version == 2 && j.identifier(name, "interpolation")) {
+                            if (key.has_interpolation) return false;
+                            key.has_interpolation = true;
+                            if (!j.mode(val, key.linear)) return false;
+                        }
+                    }
+                    if (fields != 3) return false;
+                    a.keys.push_back(key);
+                }
+                break;
+            }
+            case 10: if (!parse_layers(j, v, a)) return false; break;
+            case 11: if (!parse_display(j, v, a)) return false; break;
+        }
+    }
+    const unsigned required = a.version == 3 ? 0xcf7u : 0x3ffu;
+    if ((seen & required) != required || linear_color != (a.version == 3)) return false;
+    if (a.version == 3) {
+        for (const auto& layer : a.layers) {
+            if (layer.keys.front().time_seconds != 0) return false;
+            double previous = -1;
+            for (const auto& key : layer.keys) {
+                if (key.time_seconds <= previous || key.time_seconds >= a.duration) return false;
+                previous = key.time_seconds;
+            }
+        }
+        return true;
+    }
+    if (a.keys.empty() || a.keys.front().time_seconds != 0) return false;
+    double previous = -1;
+    for (const auto& key : a.keys) {
+        if (a.version == 2 && !key.has_interpolation) return false;
+        if (key.state >= a.state_count || key.time_seconds <= previous || key.time_seconds >= a.duration) return false;
+        previous = key.time_seconds;
+    }
+    return true;
+}
+
+// ---- base.ply -----------------------------------------------------------------
+
+// Header check; on success `offset` is the first body byte.
+bool ply_header(const std::vector<uint8_t>& bytes, uint32_t count, size_t& offset) {
+    offset = 0;
+    std::string text;
+    auto line = [&]() {
+        const size_t start = offset;
+        while (offset < bytes.size() && offset < kMaxText && bytes[offset] != '\n') ++offset;
+        if (offset == bytes.size() || offset == kMaxText) return false;
+        text.assign((const char*)bytes.data() + start, offset - start);
+        ++offset;
+        return text.find('\r') == std::string::npos;
+    };
+    if (!line() || text != "ply" || !line() || text != "format binary_little_endian 1.0") return false;
+    std::vector<std::string> expected{"element vertex " + std::to_string(count)};
+    for (const char* n : {"x", "y", "z", "nx", "ny", "nz"}) expected.push_back(std::string("property float ") + n);
+    for (int i = 0; i < 3; ++i) expected.push_back("property float f_dc_" + std::to_string(i));
+    for (int i = 0; i < 45; ++i) expected.push_back("property float f_rest_" + std::to_string(i));
+    expected.push_back("property float opacity");
+    for (int i = 0; i < 3; ++i) expected.push_back("property float scale_" + std::to_string(i));
+    for (int i = 0; i < 4; ++i) expected.push_back("property float rot_" + std::to_string(i));
+    expected.push_back("end_header");
+    for (const std::string& want : expected) {
+        do {
+            if (!line()) return false;
+        } while (text == "comment" || text.compare(0, 8, "comment ") == 0);
+        if (text != want) return false;
+    }
+    return bytes.size() - offset == (size_t)count * 248;
+}
+
+int load(const char* path, gs_gsanim* a) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return GS_ERR_FORMAT;
+    long length = -1;
+    if (!std::fseek(f, 0, SEEK_END)) length = std::ftell(f);
+    if (length < 0 || length > kMaxArchive || std::fseek(f, 0, SEEK_SET)) {
+        std::fclose(f);
+        return GS_ERR_FORMAT;
+    }
+    Zip zip;
+    zip.bytes.resize((size_t)length);
+    const bool read_ok = std::fread(zip.bytes.data(), 1, zip.bytes.size(), f) == zip.bytes.size();
+    std::fclose(f);
+    if (!read_ok || !zip.open() || zip.entries.size() != 4) return GS_ERR_FORMAT;
+
+    static const char* names[] = {"manifest.json", "base.ply", "scales.bin", "deltas.bin", "layers.bin",
+                                  "display_lut.bin"};
+    const ZipEntry* stats[6] = {};
+    unsigned seen = 0;
+    for (const ZipEntry& z : zip.entries) {
+        if (Zip::is_directory(z) || !Zip::usable(z)) return GS_ERR_FORMAT;
+        int which = -1;
+        for (int i = 0; i < 6; ++i)
+            if (z.name == names[i]) which = i;
+        if (which < 0 || (seen & (1u << which))) return GS_ERR_FORMAT;
+        seen |= 1u << which;
+        stats[which] = &z;
+    }
+    if (!stats[0] || !stats[0]->usize || stats[0]->usize > kMaxText) return GS_ERR_FORMAT;
+    std::vector<uint8_t> bytes;
+    if (!zip.extract(*stats[0], bytes) || !parse_manifest(bytes, *a)) return GS_ERR_FORMAT;
+    if (seen != (a->version == 3 ? 51u : 15u)) return GS_ERR_FORMAT;
+    const uint64_t n = a->gaussian_count;
+    const uint64_t body = n * 248;
+    if (stats[1]->usize <= body || stats[1]->usize > body + kMaxText) return GS_ERR_FORMAT;
+    if (a->version == 3) {
+        const uint64_t layer_bytes = (uint64_t)a->layers.size() * n * 96;
+        const uint64_t lut_bytes = (uint64_t)a->lut_size * a->lut_size * a->lut_size * 6;
+        if (layer_bytes > kMaxPayload || stats[4]->usize != layer_bytes || stats[5]->usize != lut_bytes)
+            return GS_ERR_FORMAT;
+        for (int entry : {4, 5}) {
+            if (!zip.extract(*stats[entry], bytes)) return GS_ERR_FORMAT;
+            auto& out = entry == 4 ? a->layer_data : a->display_lut;
+            out.resize(bytes.size() / 2);
+            for (size_t i = 0; i < out.size(); ++i) {
+                out[i] = le16(&bytes[i * 2]);
+                if (entry == 4 && (out[i] & 0x7c00) == 0x7c00) return GS_ERR_FORMAT;   // inf / NaN half
+            }
+        }
+    } else {
+        const uint64_t delta_bytes = (uint64_t)(a->state_count - 1) * n * 48;
+        if (delta_bytes > kMaxPayload || stats[3]->usize != delta_bytes || stats[2]->usize != 192)
+            return GS_ERR_FORMAT;
+        if (!zip.extract(*stats[2], bytes)) return GS_ERR_FORMAT;
+        for (int k = 0; k < 48; ++k) {
+            a->scales[k] = lef32(&bytes[k * 4]);
+            if (!std::isfinite(a->scales[k]) || a->scales[k] <= 0) return GS_ERR_FORMAT;
+        }
+        if (!zip.extract(*stats[3], bytes)) return GS_ERR_FORMAT;
+        a->deltas.assign(bytes.begin(), bytes.end());
+        for (int8_t q : a->deltas)
+            if (q == -128) return GS_ERR_FORMAT;
+    }
+    if (!zip.extract(*stats[1], bytes)) return GS_ERR_FORMAT;
+    size_t offset;
+    if (!ply_header(bytes, a->gaussian_count, offset)) return GS_ERR_FORMAT;
+    // Decode and validate every row (the reference's Gaussian checks), then
+    // pack: raw order x y z, f_dc, f_rest, opacity, scale, rot (gs_pack_raw).
+    std::vector<float> raw((size_t)n * 59);
+    for (uint64_t i = 0; i < n; ++i) {
+        float v[62];
+        for (int k = 0; k < 62; ++k) {
+            v[k] = lef32(&bytes[offset + (size_t)i * 248 + (size_t)k * 4]);
+            if (!std::isfinite(v[k])) return GS_ERR_FORMAT;
+            if (a->version == 3 && k >= 6 && k < 54 && v[k] != 0) return GS_ERR_FORMAT;
+        }
+        for (int k = 0; k < 3; ++k) {
+            const float s = std::exp(v[55 + k]);
+            if (!std::isfinite(s) || s <= 0 || !std::isfinite(s * s)) return GS_ERR_FORMAT;
+        }
+        const float norm = std::sqrt(v[58] * v[58] + v[59] * v[59] + v[60] * v[60] + v[61] * v[61]);
+        if (!std::isfinite(norm) || norm <= 1e-8f) return GS_ERR_FORMAT;
+        // every appearance state must decode to finite coefficients
+        for (uint32_t s = 1; a->version != 3 && s < a->state_count; ++s) {
+            for (int k = 0; k < 48; ++k) {
+                const float delta = (float)a->deltas[((size_t)(s - 1) * n + i) * 48 + (size_t)k] * a->scales[k];
+                if (!std::isfinite(delta) || !std::isfinite(v[6 + k] + delta)) return GS_ERR_FORMAT;
+            }
+        }
+        float* r = &raw[(size_t)i * 59];
+        r[0] = v[0];
+        r[1] = v[1];
+        r[2] = v[2];
+        std::memcpy(r + 3, v + 6, 56 * sizeof(float));   // f_dc, f_rest, opacity, scale, rot
+    }
+    a->rows.resize((size_t)n * 64);
+    return gs_pack_raw(raw.data(), n, a->rows.data());
+}
+
+// Playback position in [0, duration) (negative times wrap).
+double wrap(double seconds, double duration) {
+    double u = std::fmod(seconds, duration);
+    if (u < 0) u += duration;
+    if (u >= duration) u = 0;
+    return u;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gs_gsanim_load(const char* path, gs_gsanim** out) {
+    if (!out) return GS_ERR_BAD_ARG;
+    *out = nullptr;
+    if (!path) return GS_ERR_BAD_ARG;
+    try {
+        gs_gsanim* a = new gs_gsanim;
+        const int rc = load(path, a);
+        if (rc != GS_OK) {
+            delete a;
+            return rc;
+        }
+        *out = a;
+        return GS_OK;
+    } catch (const std::bad_alloc&) {
+        return GS_ERR_OOM;
+    }
+}
+
+void gs_gsanim_free(gs_gsanim* a) { delete a; }
+
+int gs_gsanim_get_info(const gs_gsanim* a, gs_gsanim_info* out) {
+    if (!a || !out) return GS_ERR_BAD_ARG;
+    std::memset(out, 0, sizeof(*out));
+    out->version = a->version;
+    out->gaussian_count = a->gaussian_count;
+    out->state_count = a->version == 3 ? 0 : a->state_count;
+    out->layer_count = (uint32_t)a->layers.size();
+    out->key_count = (uint32_t)a->keys.size();
+    out->lut_size = a->lut_size;
+    out->linear = a->linear ? 1 : 0;
+    out->log2_min = a->log2_min;
+    out->log2_max = a->log2_max;
+    out->duration_seconds = a->duration;
+    return GS_OK;
+}
+
+int gs_gsanim_rows(const gs_gsanim* a, float* rows) {
+    if (!a || !rows) return GS_ERR_BAD_ARG;
+    std::memcpy(rows, a->rows.data(), a->rows.size() * sizeof(float));
+    return GS_OK;
+}
+
+int gs_gsanim_deltas(const gs_gsanim* a, int8_t* deltas, float* scales) {
+    if (!a) return GS_ERR_BAD_ARG;
+    if (deltas && !a->deltas.empty()) std::memcpy(deltas, a->deltas.data(), a->deltas.size());
+    if (scales) std::memcpy(scales, a->scales, sizeof(a->scales));
+    return GS_OK;
+}
+
+int gs_gsanim_layer_data(const gs_gsanim* a, uint16_t* halves) {
+    if (!a || !halves) return GS_ERR_BAD_ARG;
+    if (!a->layer_data.empty()) std::memcpy(halves, a->layer_data.data(), a->layer_data.size() * 2);
+    return GS_OK;
+}
+
+int gs_gsanim_display_lut(const gs_gsanim* a, uint16_t* rgb) {
+    if (!a || !rgb) return GS_ERR_BAD_ARG;
+    if (!a->display_lut.empty()) std::memcpy(rgb, a->display_lut.data(), a->display_lut.size() * 2);
+    return GS_OK;
+}
+
+int64_t gs_gsanim_layer_name(const gs_gsanim* a, uint32_t layer, char* buf, uint64_t capacity) {
+    if (!a || layer >= a->layers.size() || (!buf && capacity)) return GS_ERR_BAD_ARG;
+    const std::string& n = a->layers[layer].name;
+    if (capacity) std::memcpy(buf, n.data(), n.size() < capacity ? n.size() : (size_t)capacity);
+    return (int64_t)n.size();
+}
+
+int gs_gsanim_sample(const gs_gsanim* a, double seconds, int32_t* state_a, int32_t* state_b, float* weight) {
+    if (!a || !state_a || !state_b || !weight) return GS_ERR_BAD_ARG;
+    *state_a = *state_b = 0;
+    *weight = 0.0f;
+    if (!std::isfinite(seconds) || !std::isfinite(a->duration) || a->duration <= 0 || a->keys.empty())
+        return GS_OK;
+    const double u = wrap(seconds, a->duration);
+    const auto next = std::upper_bound(a->keys.begin(), a->keys.end(), u,
+                                       [](double t, const gs_gsanim::Key& k) { return t < k.time_seconds; });
+    const size_t i = next == a->keys.begin() ? 0 : (size_t)(next - a->keys.begin() - 1);
+    const int state = (int)a->keys[i].state;
+    *state_a = *state_b = state;
+    if (!(a->version == 2 ? a->keys[i].linear : a->linear) || a->keys.size() == 1) return GS_OK;
+    const size_t jn = (i + 1) % a->keys.size();
+    const double end = jn ? a->keys[jn].time_seconds : a->duration;
+    *state_b = (int)a->keys[jn].state;
+    *weight = (float)((u - a->keys[i].time_seconds) / (end - a->keys[i].time_seconds));
+    return GS_OK;
+}
+
+int gs_gsanim_layer_weights(const gs_gsanim* a, double seconds, float* weights) {
+    if (!a || (!weights && !a->layers.empty())) return GS_ERR_BAD_ARG;
+    if (a->version != 3 || !std::isfinite(seconds) || !std::isfinite(a->duration) || a->duration <= 0) return 0;
+    const double u = wrap(seconds, a->duration);
+    for (size_t l = 0; l < a->layers.size(); ++l) {
+        const auto& keys = a->layers[l].keys;
+        if (keys.empty()) return 0;
+        const auto next = std::upper_bound(keys.begin(), keys.end(), u,
+                                           [](double t, const gs_gsanim::LayerKey& k) { return t < k.time_seconds; });
+        const size_t i = next == keys.begin() ? 0 : (size_t)(next - keys.begin() - 1);
+        const size_t jn = (i + 1) % keys.size();
+        const double end = jn ? keys[jn].time_seconds : a->duration;
+        const double w = keys[i].linear && keys.size() > 1 ? (u - keys[i].time_seconds) / (end - keys[i].time_seconds) : 0;
+        for (int c = 0; c < 3; ++c) weights[l * 3 + c] = (float)((1 - w) * keys[i].weight[c] + w * keys[jn].weight[c]);
+    }
+    return (int)a->layers.size();
+}
+
+}  // extern "C"

@@ -669,6 +669,7 @@ const char* gs_status_str(int s) {
         case GS_ERR_BUDGET_REFUSED: return "GPS budget resize refused";
         case GS_ERR_NO_DEVICE: return "no CUDA device";
         case GS_ERR_TOO_LARGE: return "size beyond limit";
+        case GS_ERR_FORMAT: return "not a valid asset";
         default: return "unknown status";
     }
 }

@@ -43,7 +43,8 @@ typedef enum gs_status {
     GS_ERR_NO_SCENE = -5,         /* render before upload */
     GS_ERR_BUDGET_REFUSED = -6,   /* GPS budget resize refused; the old budget is kept */
     GS_ERR_NO_DEVICE = -7,        /* no usable CUDA device */
-    GS_ERR_TOO_LARGE = -8         /* size beyond a documented limit */
+    GS_ERR_TOO_LARGE = -8,        /* size beyond a documented limit */
+    GS_ERR_FORMAT = -9            /* file missing, unreadable or not a valid asset */
 } gs_status;
 
 /* src/renderer.h:58-64 SplatRenderMode */
@@ -245,6 +246,63 @@ int gs_pack_raw(const float* raw, uint64_t count, float* rows);
  * (through 1 / (1 + exp(-x))); every other field is identical.  Feed the
  * rows to gs_upload_rows_device. */
 int gs_pack_raw_device(const float* raw_dev, uint64_t count, float* rows_dev, void* stream);
+
+/* ---- gsanim assets (host, no GPU) ---------------------------------------- */
+
+typedef struct gs_gsanim gs_gsanim;
+
+typedef struct gs_gsanim_info {
+    uint32_t version;          /* 1, 2, 3: manifest version "0.1", "0.2", "0.3" */
+    uint32_t gaussian_count;
+    uint32_t state_count;      /* appearance states incl. the base state 0 (0.1 / 0.2; 0 for 0.3) */
+    uint32_t layer_count;      /* appearance layers (0.3) */
+    uint32_t key_count;        /* state keys (0.1 / 0.2) */
+    uint32_t lut_size;         /* display LUT edge (0.3) */
+    int32_t linear;            /* manifest interpolation "linear" (0.1 / 0.2) */
+    float log2_min, log2_max;  /* display LUT domain (0.3) */
+    double duration_seconds;
+} gs_gsanim_info;
+
+/* gaussian_load_gsanim (src/gaussian_loader_gsanim.cpp:386-495): read and
+ * validate a .gsanim archive (manifest.json, base.ply and scales.bin +
+ * deltas.bin, or layers.bin + display_lut.bin).  Accepts exactly what the
+ * reference loader accepts; GS_ERR_FORMAT otherwise (*out = NULL).  The
+ * handle owns the decoded asset until gs_gsanim_free. */
+int gs_gsanim_load(const char* path, gs_gsanim** out);
+void gs_gsanim_free(gs_gsanim* asset);
+int gs_gsanim_get_info(const gs_gsanim* asset, gs_gsanim_info* out);
+
+/* The base Gaussians as GpuGaussian rows, gaussian_count x 64 floats (the
+ * loader's Gaussian decode + pack_gpu_gaussians, src/gaussian.cpp:53-73):
+ * the input of gs_upload_rows. */
+int gs_gsanim_rows(const gs_gsanim* asset, float* rows);
+
+/* GSAnim::deltas ((state_count - 1) x gaussian_count x 48 int8) and
+ * GSAnim::scales (48 floats), src/gsanim.h:47-49: the inputs of
+ * gs_upload_anim.  Either pointer may be NULL. */
+int gs_gsanim_deltas(const gs_gsanim* asset, int8_t* deltas, float* scales);
+
+/* GSAnim::layer_data (layer_count x gaussian_count x 48 IEEE half bits) and
+ * GSAnim::display_lut (lut_size^3 x 3 uint16, red fastest), src/gsanim.h:38-41;
+ * the LUT is the input of gs_set_display_lut. */
+int gs_gsanim_layer_data(const gs_gsanim* asset, uint16_t* halves);
+int gs_gsanim_display_lut(const gs_gsanim* asset, uint16_t* rgb);
+
+/* Layer `layer`'s decoded UTF-8 name (GSAnimLayer::name; may hold NUL bytes):
+ * copies min(length, capacity) bytes and returns the length. */
+int64_t gs_gsanim_layer_name(const gs_gsanim* asset, uint32_t layer, char* buf, uint64_t capacity);
+
+/* gsanim_sample (src/gaussian_loader_gsanim.cpp:497-509): the appearance
+ * states and blend weight at `seconds` (wrapped into [0, duration)); state 0
+ * for both and weight 0 for non-finite times or 0.3 assets.  The input of
+ * gs_set_anim_state. */
+int gs_gsanim_sample(const gs_gsanim* asset, double seconds, int32_t* state_a, int32_t* state_b, float* weight);
+
+/* gsanim_layer_weights (src/gaussian_loader_gsanim.cpp:511-531): the RGB
+ * weight of each layer at `seconds` into weights[layer_count * 3]; returns
+ * the number of layers weighted, 0 (the reference's empty result) for 0.1 /
+ * 0.2 assets and non-finite times. */
+int gs_gsanim_layer_weights(const gs_gsanim* asset, double seconds, float* weights);
 
 /* ---- stage-level entry points (device pointers, stream-ordered) ---------- */
 

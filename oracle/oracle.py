@@ -132,8 +132,73 @@ def ref():
         R.ref_camera_matrices.restype = None
         R.ref_camera_matrices.argtypes = [_f32p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                           C.c_int, C.c_float, C.c_float, C.c_float, _f32p, _f32p]
+        vp = C.c_void_p
+        R.ref_gsanim_open.restype = vp
+        R.ref_gsanim_open.argtypes = [C.c_char_p]
+        R.ref_gsanim_close.restype = None
+        R.ref_gsanim_close.argtypes = [vp]
+        R.ref_gsanim_info.restype = None
+        R.ref_gsanim_info.argtypes = [vp, _u32p, _f32p, C.POINTER(C.c_double)]
+        for name in ("ref_gsanim_rows", "ref_gsanim_layer_data", "ref_gsanim_display_lut"):
+            getattr(R, name).restype = None
+            getattr(R, name).argtypes = [vp, vp]
+        R.ref_gsanim_deltas.restype = None
+        R.ref_gsanim_deltas.argtypes = [vp, vp, vp]
+        R.ref_gsanim_layer_name.restype = C.c_uint32
+        R.ref_gsanim_layer_name.argtypes = [vp, C.c_uint32, C.c_char_p, C.c_uint32]
+        R.ref_gsanim_sample.restype = None
+        R.ref_gsanim_sample.argtypes = [vp, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_float)]
+        R.ref_gsanim_layer_weights.restype = C.c_uint32
+        R.ref_gsanim_layer_weights.argtypes = [vp, C.c_double, vp]
         _ref = R
     return _ref
+
+
+def ref_gsanim(path, times=()):
+    """The reference loader's view of a gsanim archive (gaussian_load_gsanim,
+    src/gaussian_loader_gsanim.cpp:386-495), or None when it rejects the file:
+    a dict of the decoded arrays, plus gsanim_sample and gsanim_layer_weights
+    at each of `times`."""
+    R = ref()
+    h = R.ref_gsanim_open(str(path).encode())
+    if not h:
+        return None
+    try:
+        ints = np.zeros(7, np.uint32)
+        floats = np.zeros(2, np.float32)
+        dur = C.c_double()
+        R.ref_gsanim_info(h, ints, floats, C.byref(dur))
+        version, n, states, layers, keys, lut, linear = (int(v) for v in ints)
+        rows = np.zeros((n, 64), np.float32)
+        R.ref_gsanim_rows(h, rows.ctypes.data)
+        deltas = np.zeros((max(states - 1, 0), n, 48), np.int8)
+        scales = np.zeros(48, np.float32)
+        R.ref_gsanim_deltas(h, deltas.ctypes.data, scales.ctypes.data)
+        layer_data = np.zeros((layers, n, 48), np.uint16)
+        R.ref_gsanim_layer_data(h, layer_data.ctypes.data)
+        display_lut = np.zeros((lut ** 3, 3), np.uint16)
+        R.ref_gsanim_display_lut(h, display_lut.ctypes.data)
+        names = []
+        for i in range(layers):
+            length = R.ref_gsanim_layer_name(h, i, None, 0)
+            buf = C.create_string_buffer(max(int(length), 1))
+            R.ref_gsanim_layer_name(h, i, buf, length)
+            names.append(buf.raw[:length])
+        samples, weights = [], []
+        for t in times:
+            a, b, w = C.c_int32(), C.c_int32(), C.c_float()
+            R.ref_gsanim_sample(h, float(t), C.byref(a), C.byref(b), C.byref(w))
+            samples.append((a.value, b.value, w.value))
+            out = np.zeros((max(layers, 1), 3), np.float32)
+            k = R.ref_gsanim_layer_weights(h, float(t), out.ctypes.data)
+            weights.append(out[:k])
+        return dict(version=version, gaussian_count=n, state_count=states, layer_count=layers, key_count=keys,
+                    lut_size=lut, linear=bool(linear), log2_min=float(floats[0]), log2_max=float(floats[1]),
+                    duration=dur.value, rows=rows, deltas=deltas, scales=scales, layer_data=layer_data,
+                    display_lut=display_lut, layer_names=names, samples=samples, layer_weights=weights)
+    finally:
+        R.ref_gsanim_close(h)
 
 
 # --------------------------------------------------------------------------

@@ -6,18 +6,21 @@
 //                                                src/gaussian.cpp:53-73)
 //   - cull_gaussians + sort_gaussians           (src/gaussian.cpp:77-181)
 //   - camera_get_view_matrix / camera_get_proj_matrix (src/camera.cpp:137-245)
+//   - gaussian_load_gsanim, gsanim_sample, gsanim_layer_weights
+//                                               (src/gaussian_loader_gsanim.cpp:386-531)
 // Never linked into the product.
 #include <SDL3/SDL.h>
 #include <cstdint>
 #include <cstring>
 #include <cstdlib>
+#define SJ_IMPL
+#include "sj.h"
 #include "gaussian.h"
+#include "gsanim.h"
 #include "camera.h"
 
-// The reference's load_gaussian_scene dispatches to loaders we do not build.
+// The reference's load_gaussian_scene dispatches to a loader we do not build.
 bool gaussian_load_sog(const char*, GaussianScene*) { return false; }
-bool gaussian_load_gsanim(const char*, GaussianScene*) { return false; }
-struct GSAnim;
 
 extern "C" {
 
@@ -69,6 +72,85 @@ void ref_camera_matrices(const float pos[3], float yaw, float pitch, float fov_y
     cam.z_up = z_up != 0; cam.ortho_size = ortho_size; cam.ortho_blend = ortho_blend;
     camera_get_view_matrix(&cam, view16);
     camera_get_proj_matrix(&cam, aspect, proj16);
+}
+
+// ---- gsanim archives --------------------------------------------------------
+// A loaded scene behind an opaque handle (NULL when the reference loader
+// rejects the file).
+void* ref_gsanim_open(const char* path) {
+    GaussianScene* scene = new GaussianScene;
+    memset(scene, 0, sizeof(*scene));
+    if (!gaussian_load_gsanim(path, scene)) {
+        delete scene;
+        return nullptr;
+    }
+    return scene;
+}
+
+void ref_gsanim_close(void* h) {
+    GaussianScene* scene = (GaussianScene*)h;
+    if (!scene) return;
+    free_scene(scene);
+    delete scene;
+}
+
+// ints: version, gaussian_count, state_count, layer_count, key_count, lut_size, linear
+// floats: log2_min, log2_max; duration: seconds
+void ref_gsanim_info(void* h, uint32_t* ints, float* floats, double* duration) {
+    const GSAnim& a = *((GaussianScene*)h)->animation;
+    ints[0] = (uint32_t)a.version;
+    ints[1] = a.gaussian_count;
+    ints[2] = a.state_count;
+    ints[3] = (uint32_t)a.layers.size();
+    ints[4] = (uint32_t)a.keys.size();
+    ints[5] = a.lut_size;
+    ints[6] = a.linear ? 1u : 0u;
+    floats[0] = a.log2_min;
+    floats[1] = a.log2_max;
+    *duration = a.duration;
+}
+
+void ref_gsanim_rows(void* h, float* rows) {
+    const GaussianScene* scene = (const GaussianScene*)h;
+    pack_gpu_gaussians(scene, 0, scene->gaussian_count, (GpuGaussian*)rows);
+}
+
+void ref_gsanim_deltas(void* h, int8_t* deltas, float* scales) {
+    const GSAnim& a = *((GaussianScene*)h)->animation;
+    if (!a.deltas.empty()) memcpy(deltas, a.deltas.data(), a.deltas.size());
+    memcpy(scales, a.scales, sizeof(a.scales));
+}
+
+void ref_gsanim_layer_data(void* h, uint16_t* out) {
+    const GSAnim& a = *((GaussianScene*)h)->animation;
+    if (!a.layer_data.empty()) memcpy(out, a.layer_data.data(), a.layer_data.size() * 2);
+}
+
+void ref_gsanim_display_lut(void* h, uint16_t* out) {
+    const GSAnim& a = *((GaussianScene*)h)->animation;
+    if (!a.display_lut.empty()) memcpy(out, a.display_lut.data(), a.display_lut.size() * 2);
+}
+
+// Byte length of layer i's name; copies min(length, cap) bytes.
+uint32_t ref_gsanim_layer_name(void* h, uint32_t i, char* buf, uint32_t cap) {
+    const GSAnim& a = *((GaussianScene*)h)->animation;
+    const std::string& n = a.layers[i].name;
+    memcpy(buf, n.data(), n.size() < cap ? n.size() : cap);
+    return (uint32_t)n.size();
+}
+
+void ref_gsanim_sample(void* h, double seconds, int32_t* state_a, int32_t* state_b, float* weight) {
+    const GSAnimSample s = gsanim_sample(*((GaussianScene*)h)->animation, seconds);
+    *state_a = s.state_a;
+    *state_b = s.state_b;
+    *weight = s.weight;
+}
+
+// Number of layers weighted (0 = the reference's empty result).
+uint32_t ref_gsanim_layer_weights(void* h, double seconds, float* out) {
+    const auto w = gsanim_layer_weights(*((GaussianScene*)h)->animation, seconds);
+    for (size_t i = 0; i < w.size(); ++i) memcpy(out + 3 * i, w[i].data(), 12);
+    return (uint32_t)w.size();
 }
 
 }  // extern "C"
