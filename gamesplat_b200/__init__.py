@@ -15,7 +15,9 @@ from .renderer import (  # noqa: F401
     camera_to_array,
     camera_uniforms,
     load_ply,
+    load_sog,
     pack_raw,
     sort_pairs,
     sort_pairs_scratch_bytes,
+    webp_decode,
 )

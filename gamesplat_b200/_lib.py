@@ -43,7 +43,8 @@ EXPORTS = (
     "gs_sort_pairs", "gs_sort_pairs_noalloc", "gs_upload_anim", "gs_set_anim_state", "gs_set_display_lut",
     "gs_display", "gs_debug_wait_probe", "gs_pack_raw_device", "gs_gsanim_load", "gs_gsanim_free",
     "gs_gsanim_get_info", "gs_gsanim_rows", "gs_gsanim_deltas", "gs_gsanim_layer_data", "gs_gsanim_display_lut",
-    "gs_gsanim_layer_name", "gs_gsanim_sample", "gs_gsanim_layer_weights",
+    "gs_gsanim_layer_name", "gs_gsanim_sample", "gs_gsanim_layer_weights", "gs_webp_decode_rgba",
+    "gs_load_sog",
 )
 
 
@@ -183,6 +184,8 @@ def lib() -> C.CDLL:
         "gs_gsanim_sample": (i32, [vp, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                    C.POINTER(C.c_float)]),
         "gs_gsanim_layer_weights": (i32, [vp, C.c_double, vp]),
+        "gs_webp_decode_rgba": (i32, [C.c_char_p, u64, C.POINTER(C.c_int32), C.POINTER(C.c_int32), vp, u64]),
+        "gs_load_sog": (C.c_int64, [C.c_char_p, vp, u64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -19,12 +19,9 @@
 //   * scales.bin: 48 finite positive floats; deltas.bin: (states - 1) x N x 48
 //     int8 without -128 (0.1 / 0.2); layers.bin: layers x N x 48 finite
 //     halves; display_lut.bin: size^3 RGB uint16 (0.3).
-// The archive reader is written here over zlib's raw inflate, with the
-// reference archive reader's acceptance rules (data in front of the archive,
-// the stored-size test, empty entries); archives with ZIP64 records are
-// rejected (a 512 MiB archive of four entries never needs them).
-#include <zlib.h>
-
+// The archive reader (gs_zip.h) follows the reference archive reader's
+// acceptance rules; archives with ZIP64 records are rejected (a 512 MiB
+// archive of four entries never needs them).
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -37,6 +34,8 @@
 #include <vector>
 
 #include "../../include/gs_api.h"
+#include "gs_json.h"
+#include "gs_zip.h"
 
 struct gs_gsanim {
     struct Key {
@@ -72,6 +71,10 @@ struct gs_gsanim {
 
 namespace {
 
+using gs::Json;
+using gs::Zip;
+using gs::ZipEntry;
+
 constexpr size_t kMaxText = 1024 * 1024;              // manifest, PLY header
 constexpr size_t kMaxPayload = 256u * 1024 * 1024;    // deltas / layer coefficients
 constexpr uint32_t kMaxGaussians = 1000000;
@@ -85,368 +88,6 @@ float lef32(const uint8_t* p) {
     std::memcpy(&v, &b, 4);
     return v;
 }
-
-// ---- ZIP archive ------------------------------------------------------------
-
-struct ZipEntry {
-    std::string name;                     // raw bytes (may hold NUL)
-    uint16_t flags = 0, method = 0;
-    uint32_t crc = 0, csize = 0, usize = 0, local = 0, external_attr = 0;
-};
-
-struct Zip {
-    std::vector<uint8_t> bytes;
-    std::vector<ZipEntry> entries;
-    size_t base = 0;    // bytes before the archive proper (data in front of it)
-    size_t size = 0;    // archive size from `base`
-
-    // Bytes [ofs, ofs + count) of the archive (relative to `base`), or
-    // nullptr when the file ends first.
-    const uint8_t* at(uint64_t ofs, uint64_t count) const {
-        const uint64_t abs = (uint64_t)base + ofs;
-        if (abs > bytes.size() || count > bytes.size() - abs) return nullptr;
-        return bytes.data() + abs;
-    }
-
-    // The end-of-central-directory record: the last signature with a whole
-    // record after it, searched backwards in 4 KiB windows (overlapping by 3
-    // bytes) until a window starts 64 KiB + 22 bytes or more before the end.
-    bool locate_end(size_t& eocd) const {
-        const size_t n = bytes.size();
-        if (n < 22) return false;
-        size_t cur = n > 4096 ? n - 4096 : 0;
-        for (;;) {
-            const size_t m = std::min<size_t>(4096, n - cur);
-            for (long i = (long)m - 4; i >= 0; --i) {
-                if (le32(&bytes[cur + (size_t)i]) == 0x06054b50u && n - (cur + (size_t)i) >= 22) {
-                    eocd = cur + (size_t)i;
-                    return true;
-                }
-            }
-            if (cur == 0 || n - cur >= 65535u + 22u) return false;
-            cur = cur > 4093 ? cur - 4093 : 0;
-        }
-    }
-
-    // Central directory.  Offsets in the archive are relative to its start,
-    // which is where the directory's own offset and size say it is: data in
-    // front of the archive (the gap between the directory's end and the end
-    // record) shifts every offset.
-    bool open() {
-        size_t eocd;
-        if (!locate_end(eocd)) return false;
-        const uint8_t* e = &bytes[eocd];
-        if (eocd >= 20 + 56 && le32(&bytes[eocd - 20]) == 0x07064b50u) return false;   // ZIP64
-        const uint32_t disk = le16(e + 4), cd_disk = le16(e + 6), on_disk = le16(e + 8), total = le16(e + 10);
-        const uint32_t cd_size = le32(e + 12), cd_off = le32(e + 16);
-        if (total != on_disk) return false;
-        if ((disk | cd_disk) != 0 && (disk != 1 || cd_disk != 1)) return false;
-        if ((uint64_t)cd_size < (uint64_t)total * 46) return false;
-        if ((uint64_t)cd_off + cd_size > bytes.size() || eocd < (uint64_t)cd_off + cd_size) return false;
-        base = eocd - ((size_t)cd_off + cd_size);
-        size = bytes.size() - base;
-        if (!total) return true;
-        const uint8_t* cd = at(cd_off, cd_size);
-        if (!cd) return false;
-        size_t left = cd_size;
-        for (uint32_t i = 0; i < total; ++i) {
-            if (left < 46 || le32(cd) != 0x02014b50u) return false;
-            ZipEntry z;
-            z.flags = le16(cd + 8);
-            z.method = le16(cd + 10);
-            z.crc = le32(cd + 16);
-            z.csize = le32(cd + 20);
-            z.usize = le32(cd + 24);
-            const uint32_t name_len = le16(cd + 28), extra_len = le16(cd + 30), comment_len = le16(cd + 32);
-            const uint32_t start_disk = le16(cd + 34);
-            z.external_attr = le32(cd + 38);
-            z.local = le32(cd + 42);
-            if (z.csize == 0xFFFFFFFFu || z.usize == 0xFFFFFFFFu || z.local == 0xFFFFFFFFu) return false;  // ZIP64
-            // A stored entry must keep its size, unless the 32-bit word at the
-            // method field (method and modification time together) is nonzero;
-            // a nonempty entry must have compressed bytes.
-            if ((le32(cd + 10) == 0 && z.usize != z.csize) || (z.usize && !z.csize)) return false;
-            if (start_disk == 0xFFFF || (start_disk != disk && start_disk != 1)) return false;
-            if ((uint64_t)z.local + 30 + z.csize > size) return false;
-            if (z.flags & 0x2000u) return false;   // masked local headers
-            const size_t header = 46 + (size_t)name_len + extra_len + comment_len;
-            if (header > left) return false;
-            z.name.assign((const char*)cd + 46, name_len);
-            entries.push_back(std::move(z));
-            cd += header;
-            left -= header;
-        }
-        return true;
-    }
-
-    static bool is_directory(const ZipEntry& z) {
-        return (!z.name.empty() && z.name.back() == '/') || (z.external_attr & 0x10u);
-    }
-    static bool usable(const ZipEntry& z) {
-        // not encrypted (traditional or strong), not patch data, stored or deflated
-        return !(z.flags & (0x1u | 0x40u | 0x20u)) && (z.method == 0 || z.method == 8);
-    }
-
-    // Payload of entry z into out (z.usize bytes), CRC-32 checked.  An entry
-    // without compressed bytes is empty and not checked.  A stored entry
-    // reads its uncompressed size.
-    bool extract(const ZipEntry& z, std::vector<uint8_t>& out) const {
-        out.assign(z.usize, 0);
-        if (!z.csize) return true;
-        const uint8_t* local = at(z.local, 30);
-        if (!local || le32(local) != 0x04034b50u) return false;
-        const uint64_t data = (uint64_t)z.local + 30 + le16(local + 26) + le16(local + 28);
-        if (data + z.csize > size) return false;
-        if (z.method == 0) {
-            const uint8_t* src = at(data, z.usize);
-            if (!src) return false;
-            if (z.usize) std::memcpy(out.data(), src, z.usize);
-        } else {
-            const uint8_t* src = at(data, z.csize);
-            if (!src) return false;
-            z_stream st{};
-            if (inflateInit2(&st, -15) != Z_OK) return false;
-            st.next_in = const_cast<Bytef*>(src);
-            st.avail_in = z.csize;
-            st.next_out = out.data();
-            st.avail_out = z.usize;
-            const int rc = inflate(&st, Z_FINISH);
-            const bool done = rc == Z_STREAM_END && st.total_out == z.usize;
-            inflateEnd(&st);
-            if (!done) return false;
-        }
-        const uLong crc = crc32(crc32(0L, Z_NULL, 0), out.data(), (uInt)out.size());
-        return (uint32_t)crc == z.crc;
-    }
-};
-
-// ---- JSON -------------------------------------------------------------------
-
-// Strict syntax check and tree of one JSON text.  Strings keep their raw
-// bytes between the quotes (escapes undecoded), numbers their text.
-struct Json {
-    enum Type { kNull, kBool, kNum, kStr, kArr, kObj };
-    struct Node {
-        Type type;
-        const char* b;
-        const char* e;
-        std::vector<int> kids;   // arrays: elements; objects: key, value, key, value, ...
-    };
-    std::vector<Node> nodes;
-    const unsigned char* p = nullptr;
-    const unsigned char* end = nullptr;
-
-    void space() {
-        while (p != end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n')) ++p;
-    }
-    bool take(char c) {
-        space();
-        if (p == end || *p != (unsigned char)c) return false;
-        ++p;
-        return true;
-    }
-    int add(Type t, const unsigned char* b, const unsigned char* e) {
-        nodes.push_back(Node{t, (const char*)b, (const char*)e, {}});
-        return (int)nodes.size() - 1;
-    }
-    static bool is_hex(unsigned char c) {
-        return (c >= '0' && c <= '9') || (c >= 'a' && c <= 'f') || (c >= 'A' && c <= 'F');
-    }
-    // A string: UTF-8 and escapes checked.
-    int string() {
-        if (!take('"')) return -1;
-        const unsigned char* b = p;
-        while (p != end) {
-            unsigned c = *p++;
-            if (c == '"') return add(kStr, b, p - 1);
-            if (c < 32) return -1;
-            if (c == '\\') {
-                if (p == end) return -1;
-                c = *p++;
-                if (c == 'u') {
-                    for (int i = 0; i < 4; ++i) {
-                        if (p == end || !is_hex(*p)) return -1;
-                        ++p;
-                    }
-                } else if (c != 0 && !std::strchr("\"\\/bfnrt", (int)c)) {
-                    // (a NUL after the backslash passes the reference's
-                    // strchr test, which finds the terminator)
-                    return -1;
-                }
-            } else if (c >= 128) {
-                if (c < 0xc2 || c > 0xf4) return -1;
-                const unsigned count = c >= 0xf0 ? 3 : c >= 0xe0 ? 2 : 1;
-                unsigned value = c & (count == 3 ? 7u : count == 2 ? 15u : 31u);
-                for (unsigned i = 0; i < count; ++i) {
-                    if (p == end || (*p & 0xc0) != 0x80) return -1;
-                    value = (value << 6) | (*p++ & 63u);
-                }
-                const unsigned least = count == 3 ? 65536u : count == 2 ? 2048u : 128u;
-                if (value < least || value > 0x10ffff || (value >= 0xd800 && value <= 0xdfff)) return -1;
-            }
-        }
-        return -1;
-    }
-    int value(int depth = 0) {
-        space();
-        if (p == end || depth > 32) return -1;
-        if (*p == '"') return string();
-        if (*p == '{' || *p == '[') {
-            const bool object = *p++ == '{';
-            const int me = add(object ? kObj : kArr, p - 1, p);
-            const char close = object ? '}' : ']';
-            if (take(close)) return me;
-            do {
-                if (object) {
-                    const int k = string();
-                    if (k < 0 || !take(':')) return -1;
-                    nodes[me].kids.push_back(k);
-                }
-                const int v = value(depth + 1);
-                if (v < 0) return -1;
-                nodes[me].kids.push_back(v);
-                if (take(close)) return me;
-            } while (take(','));
-            return -1;
-        }
-        static const char* words[] = {"true", "false", "null"};
-        for (int w = 0; w < 3; ++w) {
-            const size_t n = std::strlen(words[w]);
-            if ((size_t)(end - p) >= n && !std::memcmp(p, words[w], n)) {
-                p += n;
-                return add(w == 2 ? kNull : kBool, p - n, p);
-            }
-        }
-        const unsigned char* b = p;
-        if (*p == '-') ++p;
-        if (p == end) return -1;
-        if (*p == '0') {
-            ++p;
-        } else {
-            if (*p < '1' || *p > '9') return -1;
-            while (p != end && *p >= '0' && *p <= '9') ++p;
-        }
-        if (p != end && *p == '.') {
-            ++p;
-            const unsigned char* s = p;
-            while (p != end && *p >= '0' && *p <= '9') ++p;
-            if (p == s) return -1;
-        }
-        if (p != end && (*p == 'e' || *p == 'E')) {
-            ++p;
-            if (p != end && (*p == '-' || *p == '+')) ++p;
-            const unsigned char* s = p;
-            while (p != end && *p >= '0' && *p <= '9') ++p;
-            if (p == s) return -1;
-        }
-        return add(kNum, b, p);
-    }
-    // The whole text must be one value (whitespace around it allowed).
-    int parse(const std::vector<uint8_t>& text) {
-        p = text.data();
-        end = text.data() + text.size();
-        const int root = value();
-        if (root < 0) return -1;
-        space();
-        return p == end ? root : -1;
-    }
-
-    const Node& at(int i) const { return nodes[(size_t)i]; }
-
-    // A finite number written in at most 64 characters.
-    bool number(int i, double& out) const {
-        const Node& v = at(i);
-        if (v.type != kNum || v.e - v.b > 64) return false;
-        const std::string text(v.b, v.e);
-        char* stop = nullptr;
-        out = std::strtod(text.c_str(), &stop);
-        return stop == text.c_str() + text.size() && std::isfinite(out);
-    }
-    // A number in [0, max] written with digits only (an optional minus sign).
-    bool integer(int i, uint32_t& out, uint32_t max) const {
-        double n;
-        if (!number(i, n) || n < 0 || n > max) return false;
-        const Node& v = at(i);
-        for (const char* q = v.b + (*v.b == '-' ? 1 : 0); q != v.e; ++q)
-            if (*q < '0' || *q > '9') return false;
-        out = (uint32_t)n;
-        return true;
-    }
-    static unsigned hex4(const char* q) {
-        unsigned n = 0;
-        for (int k = 0; k < 4; ++k) {
-            const unsigned c = (unsigned char)q[k];
-            n = n * 16 + (c <= '9' ? c - '0' : (c | 32) - 'a' + 10);
-        }
-        return n;
-    }
-    // A string equal to the ASCII text `want`, \uXXXX escapes allowed (no
-    // other escape).
-    bool identifier(int i, const char* want) const {
-        const Node& v = at(i);
-        if (v.type != kStr) return false;
-        for (const char* q = v.b; q != v.e; ++q) {
-            unsigned c = (unsigned char)*q;
-            if (c == '\\') {
-                if (++q == v.e || *q != 'u' || v.e - q < 5) return false;
-                c = hex4(q + 1);
-                q += 4;
-            }
-            if (!*want || c != (unsigned char)*want++) return false;
-        }
-        return *want == 0;
-    }
-    // The decoded bytes (UTF-8) of a string; unpaired surrogates fail.
-    bool decoded(int i, std::string& out) const {
-        const Node& v = at(i);
-        if (v.type != kStr) return false;
-        for (const char* q = v.b; q != v.e;) {
-            unsigned c = (unsigned char)*q++;
-            if (c != '\\') {
-                out += (char)c;
-                continue;
-            }
-            c = (unsigned char)*q++;
-            if (c != 'u') {
-                static const char from[] = "\"\\/bfnrt";
-                static const char to[] = "\"\\/\b\f\n\r\t";
-                out += c == 0 ? '\0' : to[std::strchr(from, (int)c) - from];
-                continue;
-            }
-            c = hex4(q);
-            q += 4;
-            if (c >= 0xd800 && c <= 0xdbff) {
-                if (v.e - q < 6 || q[0] != '\\' || q[1] != 'u') return false;
-                const unsigned low = hex4(q + 2);
-                q += 6;
-                if (low < 0xdc00 || low > 0xdfff) return false;
-                c = 0x10000 + ((c - 0xd800) << 10) + (low - 0xdc00);
-            } else if (c >= 0xdc00 && c <= 0xdfff) {
-                return false;
-            }
-            if (c < 128) {
-                out += (char)c;
-            } else if (c < 2048) {
-                out += (char)(0xc0 | (c >> 6));
-                out += (char)(0x80 | (c & 63));
-            } else if (c < 65536) {
-                out += (char)(0xe0 | (c >> 12));
-                out += (char)(0x80 | ((c >> 6) & 63));
-                out += (char)(0x80 | (c & 63));
-            } else {
-                out += (char)(0xf0 | (c >> 18));
-                out += (char)(0x80 | ((c >> 12) & 63));
-                out += (char)(0x80 | ((c >> 6) & 63));
-                out += (char)(0x80 | (c & 63));
-            }
-        }
-        return true;
-    }
-    bool mode(int i, bool& linear) const {
-        linear = identifier(i, "linear");
-        return linear || identifier(i, "step");
-    }
-};
 
 // ---- manifest ---------------------------------------------------------------
 

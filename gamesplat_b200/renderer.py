@@ -67,6 +67,28 @@ def load_ply(path: str) -> np.ndarray:
     return rows
 
 
+def load_sog(path: str) -> np.ndarray:
+    """GpuGaussian rows (N x 64 float32) of a SOG archive, reference loader decode."""
+    n = L.lib().gs_load_sog(str(path).encode(), None, 0)
+    if n < 0:
+        raise L.GsError(int(n), "gs_load_sog", str(path))
+    rows = np.empty((n, 64), np.float32)
+    got = L.lib().gs_load_sog(str(path).encode(), rows.ctypes.data, n)
+    if got != n:
+        raise L.GsError(int(got) if got < 0 else L.GS_ERR_BAD_ARG, "gs_load_sog", str(path))
+    return rows
+
+
+def webp_decode(data: bytes) -> np.ndarray:
+    """H x W x 4 uint8 RGBA pixels of a lossless WebP image (the SOG image format)."""
+    w, h = C.c_int32(), C.c_int32()
+    L.check(L.lib().gs_webp_decode_rgba(data, len(data), C.byref(w), C.byref(h), None, 0), "gs_webp_decode_rgba")
+    out = np.empty((h.value, w.value, 4), np.uint8)
+    L.check(L.lib().gs_webp_decode_rgba(data, len(data), C.byref(w), C.byref(h), out.ctypes.data, out.size),
+            "gs_webp_decode_rgba")
+    return out
+
+
 def pack_raw(raw: np.ndarray) -> np.ndarray:
     """Raw 3DGS attributes (N x 59: xyz, f_dc, f_rest, opacity, scale, rot) -> GpuGaussian rows."""
     raw = np.ascontiguousarray(raw, dtype=np.float32)

@@ -247,6 +247,24 @@ int gs_pack_raw(const float* raw, uint64_t count, float* rows);
  * rows to gs_upload_rows_device. */
 int gs_pack_raw_device(const float* raw_dev, uint64_t count, float* rows_dev, void* stream);
 
+/* Load a SOG archive (version 2: meta.json and lossless WebP images) into
+ * GpuGaussian rows with the reference loader's decode (gaussian_load_sog,
+ * src/gaussian_loader_sog.cpp:126-551, and pack_gpu_gaussians,
+ * src/gaussian.cpp:53-73).  With rows == NULL returns the Gaussian count;
+ * otherwise fills min(count, capacity) rows.  GS_ERR_FORMAT (< 0) for files
+ * the reference loader rejects, and for lossy WebP images and meta texts
+ * that are not valid JSON, which it may accept. */
+int64_t gs_load_sog(const char* path, float* rows, uint64_t capacity);
+
+/* Decode a lossless WebP image (RIFF container or raw VP8L bitstream), the
+ * image format of SOG archives, to RGBA8 rows top first: the WebPGetInfo +
+ * WebPDecodeRGBA pair of the SOG loader (src/gaussian_loader_sog.cpp:98-124)
+ * for lossless images.  Writes the size, and the pixels when `capacity` holds
+ * width * height * 4 bytes.  GS_ERR_FORMAT for invalid, lossy or animated
+ * images. */
+int gs_webp_decode_rgba(const uint8_t* data, uint64_t size, int32_t* width, int32_t* height, uint8_t* rgba,
+                        uint64_t capacity);
+
 /* ---- gsanim assets (host, no GPU) ---------------------------------------- */
 
 typedef struct gs_gsanim gs_gsanim;

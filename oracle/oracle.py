@@ -151,8 +151,35 @@ def ref():
                                         C.POINTER(C.c_float)]
         R.ref_gsanim_layer_weights.restype = C.c_uint32
         R.ref_gsanim_layer_weights.argtypes = [vp, C.c_double, vp]
+        R.ref_sog_rows.restype = C.c_uint32
+        R.ref_sog_rows.argtypes = [C.c_char_p, vp, C.c_uint32]
+        R.ref_webp_decode.restype = C.c_int
+        R.ref_webp_decode.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, C.c_size_t]
         _ref = R
     return _ref
+
+
+def ref_sog_rows(path):
+    """GpuGaussian rows of a SOG archive through the reference loader
+    (gaussian_load_sog + pack_gpu_gaussians), or None when it rejects the file."""
+    R = ref()
+    n = R.ref_sog_rows(str(path).encode(), None, 0)
+    if n == 0:
+        return None
+    rows = np.zeros((n, 64), np.float32)
+    R.ref_sog_rows(str(path).encode(), rows.ctypes.data, n)
+    return rows
+
+
+def ref_webp_decode(data: bytes):
+    """H x W x 4 RGBA8 through WebPGetInfo + WebPDecodeRGBA, or None."""
+    R = ref()
+    w, h = C.c_int(), C.c_int()
+    if not R.ref_webp_decode(data, len(data), C.byref(w), C.byref(h), None, 0):
+        return None
+    out = np.zeros((h.value, w.value, 4), np.uint8)
+    R.ref_webp_decode(data, len(data), C.byref(w), C.byref(h), out.ctypes.data, out.size)
+    return out
 
 
 def ref_gsanim(path, times=()):

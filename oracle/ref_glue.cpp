@@ -8,6 +8,8 @@
 //   - camera_get_view_matrix / camera_get_proj_matrix (src/camera.cpp:137-245)
 //   - gaussian_load_gsanim, gsanim_sample, gsanim_layer_weights
 //                                               (src/gaussian_loader_gsanim.cpp:386-531)
+//   - gaussian_load_sog + pack_gpu_gaussians    (src/gaussian_loader_sog.cpp:126-551)
+//   - WebPGetInfo + WebPDecodeRGBA (the vendored libwebp decoder the SOG loader calls)
 // Never linked into the product.
 #include <SDL3/SDL.h>
 #include <cstdint>
@@ -19,8 +21,8 @@
 #include "gsanim.h"
 #include "camera.h"
 
-// The reference's load_gaussian_scene dispatches to a loader we do not build.
-bool gaussian_load_sog(const char*, GaussianScene*) { return false; }
+#include "gaussian_loader.h"
+#include "webp/decode.h"
 
 extern "C" {
 
@@ -151,6 +153,35 @@ uint32_t ref_gsanim_layer_weights(void* h, double seconds, float* out) {
     const auto w = gsanim_layer_weights(*((GaussianScene*)h)->animation, seconds);
     for (size_t i = 0; i < w.size(); ++i) memcpy(out + 3 * i, w[i].data(), 12);
     return (uint32_t)w.size();
+}
+
+// ---- SOG archives and their WebP images ----------------------------------------
+// Gaussian count of a .sog archive (0 when the reference loader rejects it);
+// with rows != NULL and count <= capacity, also its pack_gpu_gaussians rows.
+uint32_t ref_sog_rows(const char* path, float* rows, uint32_t capacity) {
+    GaussianScene scene;
+    memset(&scene, 0, sizeof(scene));
+    if (!gaussian_load_sog(path, &scene)) return 0;
+    const uint32_t n = scene.gaussian_count;
+    if (rows && n <= capacity) pack_gpu_gaussians(&scene, 0, n, (GpuGaussian*)rows);
+    free_scene(&scene);
+    return n;
+}
+
+// The SOG loader's image decode (load_sog_image, src/gaussian_loader_sog.cpp:98-124):
+// 1 and the image size when WebPGetInfo and WebPDecodeRGBA both succeed; the
+// RGBA8 pixels go to rgba when it holds w * h * 4 bytes (capacity).
+int ref_webp_decode(const uint8_t* data, size_t size, int* w, int* h, uint8_t* rgba, size_t capacity) {
+    *w = *h = 0;
+    int iw = 0, ih = 0;
+    if (!WebPGetInfo(data, size, &iw, &ih) || iw <= 0 || ih <= 0) return 0;
+    uint8_t* px = WebPDecodeRGBA(data, size, &iw, &ih);
+    if (!px) return 0;
+    *w = iw;
+    *h = ih;
+    if (rgba && (size_t)iw * (size_t)ih * 4 <= capacity) memcpy(rgba, px, (size_t)iw * (size_t)ih * 4);
+    WebPFree(px);
+    return 1;
 }
 
 }  // extern "C"
