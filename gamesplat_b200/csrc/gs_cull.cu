@@ -19,6 +19,8 @@
 // Arithmetic follows the GLSL operand order with unfused intrinsics so the
 // keys, cull mask and projected records match the CPU oracle bit for bit.
 
+#include <cuda_fp16.h>
+
 #include "gs_common.cuh"
 #include "gs_internal.h"
 #include "gs_tma.cuh"
@@ -81,6 +83,41 @@ __device__ __forceinline__ void sh_acc(float* res, float w, float a, float b, fl
 
 // Full projection of one visible Gaussian (shaders/cull.glsl:234-423).
 // row: staged chunks 1..15 of the row in shared memory; c0 = chunk 0.
+// SH colour before the bias (shaders/cull.glsl:355-408): DC at row[3].xyz,
+// SH(k) = floats 16 + 3k .. 18 + 3k (chunks 4..15).
+__device__ __forceinline__ void sh_eval(const float4* row, float x, float y, float z, int eff, float* res) {
+    const float4 c3 = row[3];
+    res[0] = mul(SH_C0, c3.x);
+    res[1] = mul(SH_C0, c3.y);
+    res[2] = mul(SH_C0, c3.z);
+    if (eff >= 1) {
+        float4 q4 = row[4], q5 = row[5], q6 = row[6];
+        sh_acc(res, mul(-SH_C1, y), q4.x, q4.y, q4.z);
+        sh_acc(res, mul(SH_C1, z), q4.w, q5.x, q5.y);
+        sh_acc(res, mul(-SH_C1, x), q5.z, q5.w, q6.x);
+        if (eff >= 2) {
+            float4 q7 = row[7], q8 = row[8], q9 = row[9];
+            float xx = mul(x, x), yy = mul(y, y), zz = mul(z, z);
+            float xy = mul(x, y), yz = mul(y, z), xz = mul(z, x);
+            sh_acc(res, mul(SH_C2_0, xy), q6.y, q6.z, q6.w);
+            sh_acc(res, mul(SH_C2_1, yz), q7.x, q7.y, q7.z);
+            sh_acc(res, mul(SH_C2_2, sub(sub(mul(2.0f, zz), xx), yy)), q7.w, q8.x, q8.y);
+            sh_acc(res, mul(SH_C2_3, xz), q8.z, q8.w, q9.x);
+            sh_acc(res, mul(SH_C2_4, sub(xx, yy)), q9.y, q9.z, q9.w);
+            if (eff >= 3) {
+                float4 qa = row[10], qb = row[11], qc = row[12], qd = row[13], qe = row[14], qf = row[15];
+                sh_acc(res, mul(mul(SH_C3_0, y), sub(mul(3.0f, xx), yy)), qa.x, qa.y, qa.z);
+                sh_acc(res, mul(mul(SH_C3_1, xy), z), qa.w, qb.x, qb.y);
+                sh_acc(res, mul(mul(SH_C3_2, y), sub(sub(mul(4.0f, zz), xx), yy)), qb.z, qb.w, qc.x);
+                sh_acc(res, mul(mul(SH_C3_3, z), sub(sub(mul(2.0f, zz), mul(3.0f, xx)), mul(3.0f, yy))), qc.y, qc.z, qc.w);
+                sh_acc(res, mul(mul(SH_C3_4, x), sub(sub(mul(4.0f, zz), xx), yy)), qd.x, qd.y, qd.z);
+                sh_acc(res, mul(mul(SH_C3_5, z), sub(xx, yy)), qd.w, qe.x, qe.y);
+                sh_acc(res, mul(mul(SH_C3_6, x), sub(xx, mul(3.0f, yy))), qe.z, qe.w, qf.x);
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ void project_visible(const float4* row, float4 c0, float vx, float vy, float vz,
                                                 const CamRegs& cam, int sh_degree, float sh_lod, float4* out,
                                                 float* quad_area, float* gps_points) {
@@ -168,34 +205,8 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
 
     int eff = sh_degree;
     if (sh_lod > 0.0f && (-vz) > sh_lod) eff = 0;
-    float res[3] = {mul(SH_C0, c3.x), mul(SH_C0, c3.y), mul(SH_C0, c3.z)};
-    if (eff >= 1) {
-        // SH(k) = floats 16 + 3k .. 18 + 3k  (chunks 4..15)
-        float4 q4 = row[4], q5 = row[5], q6 = row[6];
-        sh_acc(res, mul(-SH_C1, y), q4.x, q4.y, q4.z);
-        sh_acc(res, mul(SH_C1, z), q4.w, q5.x, q5.y);
-        sh_acc(res, mul(-SH_C1, x), q5.z, q5.w, q6.x);
-        if (eff >= 2) {
-            float4 q7 = row[7], q8 = row[8], q9 = row[9];
-            float xx = mul(x, x), yy = mul(y, y), zz = mul(z, z);
-            float xy = mul(x, y), yz = mul(y, z), xz = mul(z, x);
-            sh_acc(res, mul(SH_C2_0, xy), q6.y, q6.z, q6.w);
-            sh_acc(res, mul(SH_C2_1, yz), q7.x, q7.y, q7.z);
-            sh_acc(res, mul(SH_C2_2, sub(sub(mul(2.0f, zz), xx), yy)), q7.w, q8.x, q8.y);
-            sh_acc(res, mul(SH_C2_3, xz), q8.z, q8.w, q9.x);
-            sh_acc(res, mul(SH_C2_4, sub(xx, yy)), q9.y, q9.z, q9.w);
-            if (eff >= 3) {
-                float4 qa = row[10], qb = row[11], qc = row[12], qd = row[13], qe = row[14], qf = row[15];
-                sh_acc(res, mul(mul(SH_C3_0, y), sub(mul(3.0f, xx), yy)), qa.x, qa.y, qa.z);
-                sh_acc(res, mul(mul(SH_C3_1, xy), z), qa.w, qb.x, qb.y);
-                sh_acc(res, mul(mul(SH_C3_2, y), sub(sub(mul(4.0f, zz), xx), yy)), qb.z, qb.w, qc.x);
-                sh_acc(res, mul(mul(SH_C3_3, z), sub(sub(mul(2.0f, zz), mul(3.0f, xx)), mul(3.0f, yy))), qc.y, qc.z, qc.w);
-                sh_acc(res, mul(mul(SH_C3_4, x), sub(sub(mul(4.0f, zz), xx), yy)), qd.x, qd.y, qd.z);
-                sh_acc(res, mul(mul(SH_C3_5, z), sub(xx, yy)), qd.w, qe.x, qe.y);
-                sh_acc(res, mul(mul(SH_C3_6, x), sub(xx, mul(3.0f, yy))), qe.z, qe.w, qf.x);
-            }
-        }
-    }
+    float res[3];
+    sh_eval(row, x, y, z, eff, res);
 #pragma unroll
     for (int k = 0; k < 3; ++k) res[k] = g_max(add(res[k], 0.5f), 0.0f);
 
@@ -473,6 +484,43 @@ __global__ void __launch_bounds__(kCullThreads, 6) cull_project_kernel(CullParam
     }
 }
 
+// Pass 3, gsanim 0.3 assets only (shaders/cull.glsl:141-148, 354-416): the
+// colour of every compacted visible row is the sum over the layers of
+// max(SH colour, 0) * the layer's RGB weight, without the +0.5 bias, where
+// layer l's 48 half coefficients replace the row's DC (slots 12..14) and SH
+// (slot 16 + 3k + c holds j = 3 + 15c + k).  The view direction, the SH
+// degree and its distance LOD are those of the projection pass, computed
+// with the same operations; the record's other fields stay as projected.
+__global__ void __launch_bounds__(256) cull_layers_kernel(CullParams p) {
+    const uint32_t n_vis = p.fc->visible_count;
+    CamRegs cam;
+    load_cam(p.cam, cam);
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n_vis; v += gridDim.x * blockDim.x) {
+        const uint32_t id = p.ids_out[v];
+        const float4 c0 = __ldg(p.heads + id);
+        const float vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
+        const float ddx = sub(c0.x, cam.camw[0]), ddy = sub(c0.y, cam.camw[1]), ddz = sub(c0.z, cam.camw[2]);
+        const float len = __fsqrt_rn(add(add(mul(ddx, ddx), mul(ddy, ddy)), mul(ddz, ddz)));
+        const float x = dv(ddx, len), y = dv(ddy, len), z = dv(ddz, len);
+        int eff = p.sh_degree;
+        if (p.sh_lod_distance > 0.0f && (-vz) > p.sh_lod_distance) eff = 0;
+        float4 row[16];
+        float* f = reinterpret_cast<float*>(row);
+        float col[3] = {0.0f, 0.0f, 0.0f};
+        for (int l = 0; l < p.layer_count; ++l) {
+            const unsigned short* h =
+                reinterpret_cast<const unsigned short*>(p.layer_halves) + ((size_t)l * p.n + id) * 48u;
+            for (int j = 0; j < 3; ++j) f[12 + j] = __half2float(__ushort_as_half(__ldg(h + j)));
+            for (int slot = 16; slot < 61; ++slot)
+                f[slot] = __half2float(__ushort_as_half(__ldg(h + 3 + ((slot - 16) % 3) * 15 + (slot - 16) / 3)));
+            float r3[3];
+            sh_eval(row, x, y, z, eff, r3);
+            for (int k = 0; k < 3; ++k) col[k] = add(col[k], mul(g_max(r3[k], 0.0f), __ldg(p.layer_weights + l * 3 + k)));
+        }
+        p.projected[(size_t)id * 4] = make_float4(col[0], col[1], col[2], c0.w);
+    }
+}
+
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
     static bool attr_set = false;
     if (!attr_set) {
@@ -496,6 +544,12 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
         case 1: cull_project_kernel<7><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
         case 2: cull_project_kernel<10><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
         default: cull_project_kernel<16><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
+    }
+    if (p.layer_count > 0) {
+        uint32_t lgrid = (p.n + 255) / 256;
+        if (lgrid > num_sms * 8) lgrid = num_sms * 8;
+        cull_layers_kernel<<<lgrid, 256, 0, s>>>(p);
+        return 3;
     }
     return 2;
 }

@@ -95,6 +95,12 @@ struct gs_ctx {
     uint32_t anim_states = 0;     // delta states (state 0 = the uploaded rows)
     int anim_a = 0, anim_b = 0;
     float anim_w = 0.0f;
+    // gsanim 0.3 appearance layers (renderer animation buffer of version 3 assets)
+    uint16_t* layer_halves = nullptr;
+    uint32_t layers_uploaded = 0;
+    float* layer_weights = nullptr;      // 256 x 3 floats (device)
+    uint32_t layer_count = 0;            // layers weighted in the next frames (0: layer path off)
+    std::vector<float> layer_weights_host;
 
     // camera
     gs_camera cam{};                 // the frame's camera (kernels take it by value)
@@ -187,6 +193,11 @@ void release_scene(gs_ctx* c) {
     c->anim_states = 0;
     c->anim_a = c->anim_b = 0;
     c->anim_w = 0.0f;
+    dfree(c->layer_halves);
+    dfree(c->layer_weights);
+    c->layers_uploaded = 0;
+    c->layer_count = 0;
+    c->layer_weights_host.clear();
     c->n = 0;
     c->entry_cap = 0;
 }
@@ -359,6 +370,11 @@ void run_cull(gs_ctx* c) {
         p.anim_state_a = c->anim_a;
         p.anim_state_b = c->anim_b;
         p.anim_weight = c->anim_w;
+    }
+    if (c->layer_count) {
+        p.layer_halves = c->layer_halves;
+        p.layer_weights = c->layer_weights;
+        p.layer_count = (int)c->layer_count;
     }
     p.fc = c->fc;
     sc.add(gs::launch_cull(p, c->num_sms, c->stream));
@@ -850,6 +866,44 @@ int gs_set_anim_state(gs_ctx* c, int state_a, int state_b, float weight) {
     c->anim_a = state_a;
     c->anim_b = state_b;
     c->anim_w = weight;
+    return GS_OK;
+}
+
+int gs_upload_layers(gs_ctx* c, const uint16_t* halves, uint32_t layer_count) {
+    if (!c || (layer_count && !halves)) return GS_ERR_BAD_ARG;
+    if (!c->n) return fail(c, GS_ERR_NO_SCENE, "upload the Gaussians before their layers");
+    if (layer_count > 256) return fail(c, GS_ERR_TOO_LARGE, "more than 256 layers");
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    dfree(c->layer_halves);
+    c->layers_uploaded = 0;
+    c->layer_count = 0;
+    c->layer_weights_host.clear();
+    gs_reset_accumulation(c);
+    if (layer_count == 0) return GS_OK;
+    const size_t bytes = (size_t)layer_count * c->n * 48u * sizeof(uint16_t);
+    GS_CUDA(c, dalloc(&c->layer_halves, bytes));
+    if (!c->layer_weights) GS_CUDA(c, dalloc(&c->layer_weights, 256 * 3 * sizeof(float)));
+    GS_CUDA(c, cudaMemcpyAsync(c->layer_halves, halves, bytes, cudaMemcpyHostToDevice, c->stream));
+    GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->layers_uploaded = layer_count;
+    return GS_OK;
+}
+
+int gs_set_layer_weights(gs_ctx* c, const float* weights, uint32_t count) {
+    if (!c || (count && !weights)) return GS_ERR_BAD_ARG;
+    if (count > c->layers_uploaded) return fail(c, GS_ERR_BAD_ARG, "more layer weights than uploaded layers");
+    std::vector<float> w(weights, weights + (size_t)count * 3);
+    // src/renderer.cpp:2153-2155: a new playback position of a layered asset resets accumulation
+    if (w != c->layer_weights_host) gs_reset_accumulation(c);
+    c->layer_weights_host = w;
+    c->layer_count = count;
+    if (count) {
+        cudaSetDevice(c->device);
+        // from pageable memory: the source is copied before the call returns
+        GS_CUDA(c, cudaMemcpyAsync(c->layer_weights, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                   c->stream));
+    }
     return GS_OK;
 }
 

@@ -122,6 +122,10 @@ struct CullParams {
     const float* anim_scales;    // 48 (device)
     int anim_state_a, anim_state_b;
     float anim_weight;
+    // gsanim 0.3 appearance layers (shaders/cull.glsl:141-148, 354-416); layer_count 0 = none
+    const uint16_t* layer_halves;   // [(l * n + row) * 48 + j] IEEE half bits
+    const float* layer_weights;     // [l * 3 + c] (device)
+    int layer_count;
     FrameCounters* fc;
 };
 

@@ -174,6 +174,20 @@ class Renderer:
         L.check(L.lib().gs_set_anim_state(self._ctx, int(state_a), int(state_b), float(weight)),
                 "gs_set_anim_state", self._ctx)
 
+    def upload_layers(self, halves: np.ndarray) -> None:
+        """gsanim 0.3 appearance layers: (layers, N, 48) uint16 IEEE half bits; 0 layers removes them."""
+        halves = np.ascontiguousarray(halves, dtype=np.uint16)
+        if halves.ndim != 3 or halves.shape[2] != 48:
+            raise ValueError("halves must be (layers, N, 48) uint16")
+        L.check(L.lib().gs_upload_layers(self._ctx, halves.ctypes.data, halves.shape[0]), "gs_upload_layers",
+                self._ctx)
+
+    def set_layer_weights(self, weights: np.ndarray) -> None:
+        """RGB weight per layer for the next frames ((count, 3) float32); an empty array turns layers off."""
+        weights = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1, 3)
+        L.check(L.lib().gs_set_layer_weights(self._ctx, weights.ctypes.data, weights.shape[0]),
+                "gs_set_layer_weights", self._ctx)
+
     def set_gps_work_budget(self, max_work_items: int) -> bool:
         st = L.lib().gs_set_gps_budget(self._ctx, int(max_work_items))
         if st == L.GS_ERR_BUDGET_REFUSED:

@@ -155,6 +155,22 @@ int gs_upload_anim(gs_ctx* ctx, const int8_t* deltas, uint32_t num_states, const
  * (1 - weight) * state_a + weight * state_b.  A change resets accumulation. */
 int gs_set_anim_state(gs_ctx* ctx, int state_a, int state_b, float weight);
 
+/* gsanim 0.3 appearance layers: the renderer's animation buffer for version 3
+ * assets (src/renderer.cpp:840-864, GSAnim::layer_data), layer_count x N x 48
+ * IEEE half bits, [(layer * N + row) * 48 + j] with j = DC 0..2, then
+ * 3 + channel * 15 + k.  Upload after gs_upload_rows (at most 256 layers);
+ * layer_count = 0 removes them.  Copies; the caller keeps ownership. */
+int gs_upload_layers(gs_ctx* ctx, const uint16_t* halves, uint32_t layer_count);
+
+/* The layer weights of the next frames: gsanim_layer_weights at the playback
+ * time (src/renderer.cpp:1829-1835), weights[count * 3] RGB per layer, count
+ * at most the uploaded layers (1 for the renderer's first_layer_only).  With
+ * count > 0 the cull colours each splat as the sum over the layers of
+ * max(SH colour of the layer's coefficients, 0) * weight, without the +0.5
+ * bias (shaders/cull.glsl:141-148, 354-416); count = 0 turns the layer path
+ * off.  Changed weights reset accumulation. */
+int gs_set_layer_weights(gs_ctx* ctx, const float* weights, uint32_t count);
+
 /* renderer_set_gps_work_budget (src/renderer.h:252): replace only the GPS work
  * buffer; on failure the old budget and buffer are kept
  * (src/renderer.cpp:1076-1123). */

@@ -178,9 +178,60 @@ static void anim_row(const oc_anim* a, uint32_t row, const float* in, float* out
     }
 }
 
+/* gsanim 0.3 appearance layers (shaders/cull.glsl:141-148, 354-416): layer
+ * l's 48 half coefficients of a row replace its DC and SH slots; each layer's
+ * colour is evaluated without the +0.5 bias, clamped at 0, weighted per
+ * channel and summed. */
+typedef struct oc_layers {
+    const uint16_t* halves;  /* [(l * n + row) * 48 + j], j = DC 0..2, then 3 + c*15 + k */
+    uint32_t n;
+    int count;
+    const float* weights;    /* [l * 3 + c] */
+} oc_layers;
+
+static void layer_row(const oc_layers* L, int l, uint32_t row, const float* in, float* out) {
+    for (int k = 0; k < 64; ++k) out[k] = in[k];
+    const uint16_t* h = L->halves + ((size_t)l * L->n + row) * 48u;
+    for (int j = 0; j < 3; ++j) out[12 + j] = oc_half_to_float(h[j]);
+    for (int slot = 16; slot < 61; ++slot)
+        out[slot] = oc_half_to_float(h[3 + ((slot - 16) % 3) * 15 + (slot - 16) / 3]);
+}
+
+/* SH colour before the bias (shaders/cull.glsl:355-408): DC at r[12..14],
+ * SH(k) at r[16 + 3k .. 18 + 3k]. */
+static void sh_eval(const float* r, float x, float y, float z, int eff_degree, float* res) {
+    res[0] = SH_C0 * r[12];
+    res[1] = SH_C0 * r[13];
+    res[2] = SH_C0 * r[14];
+    const float* sh = r + 16;  /* SH(k) = sh + 3k */
+    if (eff_degree >= 1) {
+        sh_add(res, -SH_C1 * y, sh + 0);
+        sh_add(res, SH_C1 * z, sh + 3);
+        sh_add(res, -SH_C1 * x, sh + 6);
+        if (eff_degree >= 2) {
+            float xx = x * x, yy = y * y, zz = z * z;
+            float xy = x * y, yz = y * z, xz = z * x;
+            sh_add(res, SH_C2_0 * xy, sh + 9);
+            sh_add(res, SH_C2_1 * yz, sh + 12);
+            sh_add(res, SH_C2_2 * ((2.0f * zz - xx) - yy), sh + 15);
+            sh_add(res, SH_C2_3 * xz, sh + 18);
+            sh_add(res, SH_C2_4 * (xx - yy), sh + 21);
+            if (eff_degree >= 3) {
+                sh_add(res, (SH_C3_0 * y) * (3.0f * xx - yy), sh + 24);
+                sh_add(res, (SH_C3_1 * xy) * z, sh + 27);
+                sh_add(res, (SH_C3_2 * y) * ((4.0f * zz - xx) - yy), sh + 30);
+                sh_add(res, (SH_C3_3 * z) * ((2.0f * zz - 3.0f * xx) - 3.0f * yy), sh + 33);
+                sh_add(res, (SH_C3_4 * x) * ((4.0f * zz - xx) - yy), sh + 36);
+                sh_add(res, (SH_C3_5 * z) * (xx - yy), sh + 39);
+                sh_add(res, (SH_C3_6 * x) * (xx - 3.0f * yy), sh + 42);
+            }
+        }
+    }
+}
+
 static void cull_one(const float* r, uint32_t idx, const oc_camera* cam, int sh_degree,
-                     float sh_lod_distance, int collect_stats, uint32_t* ids, uint32_t* keys,
-                     float* out, uint32_t* visible_count, uint32_t* diag) {
+                     float sh_lod_distance, int collect_stats, const oc_layers* layers, uint32_t* ids,
+                     uint32_t* keys, float* out, uint32_t* visible_count, uint32_t* diag) {
     const float* V = cam->view;
     const float* P = cam->proj;
     float px = r[0], py = r[1], pz = r[2], opacity = r[3];
@@ -303,34 +354,18 @@ static void cull_one(const float* r, uint32_t idx, const oc_camera* cam, int sh_
     if (sh_lod_distance > 0.0f && (-vz) > sh_lod_distance) eff_degree = 0;
 
     float res[3];                                                /* :353-417 */
-    res[0] = SH_C0 * r[12];
-    res[1] = SH_C0 * r[13];
-    res[2] = SH_C0 * r[14];
-    const float* sh = r + 16;  /* SH(k) = sh + 3k */
-    if (eff_degree >= 1) {
-        sh_add(res, -SH_C1 * y, sh + 0);
-        sh_add(res, SH_C1 * z, sh + 3);
-        sh_add(res, -SH_C1 * x, sh + 6);
-        if (eff_degree >= 2) {
-            float xx = x * x, yy = y * y, zz = z * z;
-            float xy = x * y, yz = y * z, xz = z * x;
-            sh_add(res, SH_C2_0 * xy, sh + 9);
-            sh_add(res, SH_C2_1 * yz, sh + 12);
-            sh_add(res, SH_C2_2 * ((2.0f * zz - xx) - yy), sh + 15);
-            sh_add(res, SH_C2_3 * xz, sh + 18);
-            sh_add(res, SH_C2_4 * (xx - yy), sh + 21);
-            if (eff_degree >= 3) {
-                sh_add(res, (SH_C3_0 * y) * (3.0f * xx - yy), sh + 24);
-                sh_add(res, (SH_C3_1 * xy) * z, sh + 27);
-                sh_add(res, (SH_C3_2 * y) * ((4.0f * zz - xx) - yy), sh + 30);
-                sh_add(res, (SH_C3_3 * z) * ((2.0f * zz - 3.0f * xx) - 3.0f * yy), sh + 33);
-                sh_add(res, (SH_C3_4 * x) * ((4.0f * zz - xx) - yy), sh + 36);
-                sh_add(res, (SH_C3_5 * z) * (xx - yy), sh + 39);
-                sh_add(res, (SH_C3_6 * x) * (xx - 3.0f * yy), sh + 42);
-            }
+    if (layers && layers->count > 0) {
+        float tmp[64], r3[3];
+        res[0] = res[1] = res[2] = 0.0f;
+        for (int l = 0; l < layers->count; ++l) {
+            layer_row(layers, l, idx, r, tmp);
+            sh_eval(tmp, x, y, z, eff_degree, r3);
+            for (int k = 0; k < 3; ++k) res[k] = res[k] + g_max(r3[k], 0.0f) * layers->weights[l * 3 + k];
         }
+    } else {
+        sh_eval(r, x, y, z, eff_degree, res);
+        for (int k = 0; k < 3; ++k) res[k] = g_max(res[k] + 0.5f, 0.0f);
     }
-    for (int k = 0; k < 3; ++k) res[k] = g_max(res[k] + 0.5f, 0.0f);
 
     out[0] = res[0]; out[1] = res[1]; out[2] = res[2]; out[3] = opacity;   /* :420-423 */
     out[4] = cx; out[5] = rcy; out[6] = radius_x; out[7] = radius_y;
@@ -354,9 +389,22 @@ void oc_cull_anim(const float* rows, uint32_t n, const oc_camera* cam, int sh_de
             anim_row(&a, i, row, tmp);
             row = tmp;
         }
-        cull_one(row, i, cam, sh_degree, sh_lod_distance, collect_stats, ids, keys,
+        cull_one(row, i, cam, sh_degree, sh_lod_distance, collect_stats, NULL, ids, keys,
                  projected + (size_t)i * 16, visible_count, diag);
     }
+}
+
+void oc_cull_layers(const float* rows, uint32_t n, const oc_camera* cam, int sh_degree,
+                    float sh_lod_distance, int collect_stats, const uint16_t* halves, int layer_count,
+                    const float* weights, uint32_t* ids, uint32_t* keys, float* projected,
+                    uint32_t* visible_count, uint32_t* diag) {
+    *visible_count = 0;
+    for (int k = 0; k < 8; ++k) diag[k] = 0;
+    for (uint32_t i = 0; i < n; ++i) { ids[i] = OC_SENTINEL; keys[i] = OC_SENTINEL; }
+    oc_layers L = {halves, n, layer_count, weights};
+    for (uint32_t i = 0; i < n; ++i)
+        cull_one(rows + (size_t)i * 64, i, cam, sh_degree, sh_lod_distance, collect_stats, &L, ids, keys,
+                 projected + (size_t)i * 16, visible_count, diag);
 }
 
 void oc_cull(const float* rows, uint32_t n, const oc_camera* cam, int sh_degree,

@@ -67,6 +67,15 @@ void oc_cull_anim(const float* rows, uint32_t n, const oc_camera* cam, int sh_de
                   int state_a, int state_b, float weight, uint32_t* ids, uint32_t* keys,
                   float* projected, uint32_t* visible_count, uint32_t* diag);
 
+/* oc_cull with gsanim 0.3 appearance layers (shaders/cull.glsl:141-148,
+ * 354-416): halves[(l*n + row)*48 + j] replace the DC and SH coefficients of
+ * layer l; the colour is the sum over layers of max(SH colour, 0) * weights[l*3 + c]
+ * (no +0.5 bias).  layer_count 0 is oc_cull. */
+void oc_cull_layers(const float* rows, uint32_t n, const oc_camera* cam, int sh_degree,
+                    float sh_lod_distance, int collect_stats, const uint16_t* halves, int layer_count,
+                    const float* weights, uint32_t* ids, uint32_t* keys, float* projected,
+                    uint32_t* visible_count, uint32_t* diag);
+
 /* Stable ascending LSD radix sort (8-bit digits, 4 passes) of (key, id) pairs,
  * the order shaders/sort.glsl:26-163 produces. */
 void oc_sort_pairs(const uint32_t* keys_in, const uint32_t* ids_in, uint32_t n,

@@ -107,6 +107,9 @@ def lib():
         L.oc_display.restype = None
         L.oc_display.argtypes = [_u16p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_float,
                                  _f32p]
+        L.oc_cull_layers.restype = None
+        L.oc_cull_layers.argtypes = [_f32p, C.c_uint32, C.POINTER(OcCamera), C.c_int, C.c_float, C.c_int, C.c_void_p,
+                                     C.c_int, C.c_void_p, _u32p, _u32p, _f32p, C.POINTER(C.c_uint32), _u32p]
         L.oc_half_to_float.restype = C.c_float
         L.oc_half_to_float.argtypes = [C.c_uint16]
         _lib = L
@@ -243,6 +246,25 @@ def cull(rows: np.ndarray, cam: np.ndarray, sh_degree: int = 3, sh_lod_distance:
     cs = camera_struct(cam)
     lib().oc_cull(rows.reshape(-1), n, C.byref(cs), int(sh_degree), float(sh_lod_distance),
                   int(bool(collect_stats)), ids, keys, proj.reshape(-1), C.byref(vc), diag)
+    return ids, keys, proj, int(vc.value), diag
+
+
+def cull_layers(rows: np.ndarray, cam: np.ndarray, halves: np.ndarray, weights: np.ndarray, sh_degree: int = 3,
+                sh_lod_distance: float = 0.0):
+    """oc_cull with gsanim 0.3 layers (halves: (layers, N, 48) uint16 half bits, weights: (layers, 3) float32)."""
+    rows = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1, 64)
+    n = rows.shape[0]
+    halves = np.ascontiguousarray(halves, dtype=np.uint16)
+    weights = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1, 3)
+    ids = np.empty(n, np.uint32)
+    keys = np.empty(n, np.uint32)
+    proj = np.empty((n, 16), np.float32)
+    vc = C.c_uint32(0)
+    diag = np.zeros(8, np.uint32)
+    cs = camera_struct(cam)
+    lib().oc_cull_layers(rows.reshape(-1), n, C.byref(cs), int(sh_degree), float(sh_lod_distance), 1,
+                         halves.ctypes.data, int(weights.shape[0]), weights.ctypes.data, ids, keys,
+                         proj.reshape(-1), C.byref(vc), diag)
     return ids, keys, proj, int(vc.value), diag
 
 
