@@ -38,8 +38,8 @@ def test_struct_layouts_match_header():
 
 def test_status_strings():
     lib = L.lib()
-    for s in range(-8, 1):
-        assert lib.gs_status_str(s)
+    for s in range(-9, 1):
+        assert lib.gs_status_str(s) != b"unknown status"
     assert lib.gs_status_str(-99) == b"unknown status"
 
 
@@ -81,3 +81,71 @@ def test_malformed_ply_rejected(tmp_path):
                   b"property float z\nend_header\n" + np.zeros(3, np.float32).tobytes())
     rows = np.empty((4, 64), np.float32)
     assert L.lib().gs_load_ply(str(p).encode(), rows.ctypes.data, 4) == L.GS_ERR_BAD_ARG   # short read
+
+
+C_CONSUMER = r"""
+#include <stdio.h>
+#include <stdlib.h>
+#include "gs_api.h"
+
+int main(int argc, char** argv) {
+    gs_gsanim* a = NULL;
+    if (gs_gsanim_load(argv[1], &a) != GS_OK) return 10;
+    gs_gsanim_info info;
+    if (gs_gsanim_get_info(a, &info) != GS_OK) return 11;
+    float* rows = (float*)malloc((size_t)info.gaussian_count * 64 * sizeof(float));
+    if (gs_gsanim_rows(a, rows) != GS_OK) return 12;
+    int32_t sa, sb;
+    float w;
+    gs_gsanim_sample(a, 2.75, &sa, &sb, &w);
+    printf("%u %u %u %d %d %.9g %.9g %zu\n", info.version, info.gaussian_count, info.state_count, sa, sb,
+           (double)w, (double)rows[4], sizeof(gs_gsanim_info));
+    gs_gsanim_free(a);
+    int64_t n = gs_load_sog(argv[2], NULL, 0);
+    if (n <= 0) return 13;
+    float* srows = (float*)malloc((size_t)n * 64 * sizeof(float));
+    if (gs_load_sog(argv[2], srows, (uint64_t)n) != n) return 14;
+    printf("%lld %.9g\n", (long long)n, (double)srows[8]);
+    printf("%d\n", gs_gsanim_load("/nonexistent.gsanim", &a));
+    free(rows);
+    free(srows);
+    return 0;
+}
+"""
+
+
+def test_c_consumer_of_the_header(tmp_path):
+    """The header is plain C: a C99 program includes it, links the library
+    and reads a gsanim and a SOG archive through the host entry points."""
+    import shutil
+    import subprocess
+
+    from tests import gsanim_fixture as F
+    from tests import sog_fixture as S
+
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    m, b, s, d = F.v01_asset(n=4, states=3, seed=30, interpolation="linear")
+    ga = F.pack(tmp_path / "a.gsanim", F.entries_v01(m, b, s, d))
+    meta, imgs = S.sog_asset(5, seed=31)
+    so = S.pack(tmp_path / "a.sog", S.entries(meta, imgs))
+    src = tmp_path / "consumer.c"
+    src.write_text(C_CONSUMER)
+    exe = tmp_path / "consumer"
+    lib_dir = L.LIB_PATH.parent
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", str(HEADER.parent), str(src), "-o", str(exe),
+                    "-L", str(lib_dir), "-lgs_cuda", f"-Wl,-rpath,{lib_dir}"], check=True)
+    out = subprocess.run([str(exe), str(ga), str(so)], capture_output=True, text=True, check=True).stdout.split("\n")
+    from gamesplat_b200 import load_gsanim, load_sog
+
+    a = load_gsanim(ga)
+    version, n, states, sa, sb, w, scale0, info_size = out[0].split()
+    assert (int(version), int(n), int(states)) == (1, 4, 3)
+    assert (int(sa), int(sb), np.float32(w)) == tuple(a.sample(2.75)[:2]) + (np.float32(a.sample(2.75)[2]),)
+    assert np.float32(scale0) == a.rows[0, 4]
+    assert int(info_size) == C.sizeof(L.GsGsanimInfo)
+    n_sog, q0 = out[1].split()
+    rows = load_sog(so)
+    assert int(n_sog) == rows.shape[0] and np.float32(q0) == rows[0, 8]
+    assert int(out[2]) == L.GS_ERR_FORMAT
+    a.close()
