@@ -44,7 +44,7 @@ EXPORTS = (
     "gs_display", "gs_debug_wait_probe", "gs_pack_raw_device", "gs_gsanim_load", "gs_gsanim_free",
     "gs_gsanim_get_info", "gs_gsanim_rows", "gs_gsanim_deltas", "gs_gsanim_layer_data", "gs_gsanim_display_lut",
     "gs_gsanim_layer_name", "gs_gsanim_sample", "gs_gsanim_layer_weights", "gs_webp_decode_rgba",
-    "gs_load_sog", "gs_upload_layers", "gs_set_layer_weights",
+    "gs_load_sog", "gs_upload_layers", "gs_set_layer_weights", "gs_debug_fail_alloc",
 )
 
 
@@ -188,6 +188,7 @@ def lib() -> C.CDLL:
         "gs_load_sog": (C.c_int64, [C.c_char_p, vp, u64]),
         "gs_upload_layers": (i32, [vp, vp, u32]),
         "gs_set_layer_weights": (i32, [vp, vp, u32]),
+        "gs_debug_fail_alloc": (i32, [C.c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -155,12 +155,12 @@ int ensure_stochastic_targets(StochasticTargets& t, int w, int h, cudaStream_t s
     if (t.width == w && t.height == h && t.sample) return 0;
     release_stochastic_targets(t);
     const size_t npix = (size_t)w * h;
-    if (cudaMalloc(&t.sample, npix * 16) != cudaSuccess) return GS_ERR_OOM;
-    if (cudaMalloc(&t.depth, npix * 4) != cudaSuccess) return GS_ERR_OOM;
+    if (gs::device_malloc(reinterpret_cast<void**>(&t.sample), npix * 16) != cudaSuccess) return GS_ERR_OOM;
+    if (gs::device_malloc(reinterpret_cast<void**>(&t.depth), npix * 4) != cudaSuccess) return GS_ERR_OOM;
     for (int k = 0; k < 2; ++k) {
-        if (cudaMalloc(&t.accum[k], npix * 16) != cudaSuccess) return GS_ERR_OOM;
-        if (cudaMalloc(&t.xyz[k], npix * 16) != cudaSuccess) return GS_ERR_OOM;
-        if (cudaMalloc(&t.frame_avg[k], npix * 16) != cudaSuccess) return GS_ERR_OOM;
+        if (gs::device_malloc(reinterpret_cast<void**>(&t.accum[k]), npix * 16) != cudaSuccess) return GS_ERR_OOM;
+        if (gs::device_malloc(reinterpret_cast<void**>(&t.xyz[k]), npix * 16) != cudaSuccess) return GS_ERR_OOM;
+        if (gs::device_malloc(reinterpret_cast<void**>(&t.frame_avg[k]), npix * 16) != cudaSuccess) return GS_ERR_OOM;
         cudaMemsetAsync(t.accum[k], 0, npix * 16, s);
         cudaMemsetAsync(t.xyz[k], 0, npix * 16, s);
         cudaMemsetAsync(t.frame_avg[k], 0, npix * 16, s);

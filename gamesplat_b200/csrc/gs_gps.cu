@@ -183,7 +183,7 @@ int ensure_gps_targets(GpsTargets& g, int width, int height, uint32_t ss, uint32
         g.width = g.height = 0;
         g.ss = 0;
         size_t count = (size_t)width * ss * height * ss;
-        if (cudaMalloc(&g.packed, count * 8) != cudaSuccess) return GS_ERR_OOM;
+        if (gs::device_malloc(reinterpret_cast<void**>(&g.packed), count * 8) != cudaSuccess) return GS_ERR_OOM;
         g.width = width;
         g.height = height;
         g.ss = ss;
@@ -192,7 +192,7 @@ int ensure_gps_targets(GpsTargets& g, int width, int height, uint32_t ss, uint32
         cudaFree(g.prepared);
         g.prepared = nullptr;
         g.prepared_cap = 0;
-        if (cudaMalloc(&g.prepared, (size_t)(n ? n : 1) * 48) != cudaSuccess) return GS_ERR_OOM;
+        if (gs::device_malloc(reinterpret_cast<void**>(&g.prepared), (size_t)(n ? n : 1) * 48) != cudaSuccess) return GS_ERR_OOM;
         g.prepared_cap = n;
     }
     if (!g.work || g.work_cap != max_work_items) {
@@ -209,7 +209,7 @@ int resize_gps_work(GpsTargets& g, uint32_t max_work_items, cudaStream_t s) {
     if (max_work_items == 0) return GS_ERR_BAD_ARG;
     if (g.work && g.work_cap == max_work_items) return 0;
     uint2* nw = nullptr;
-    if (cudaMalloc(&nw, (size_t)max_work_items * sizeof(uint2)) != cudaSuccess) {
+    if (gs::device_malloc(reinterpret_cast<void**>(&nw), (size_t)max_work_items * sizeof(uint2)) != cudaSuccess) {
         cudaGetLastError();
         return GS_ERR_OOM;
     }

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <atomic>
 #include <vector>
 
 #include "gs_internal.h"
@@ -160,7 +161,12 @@ template <class T>
 cudaError_t dalloc(T** p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
-    return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+    return gs::device_malloc(reinterpret_cast<void**>(p), bytes);
+}
+
+// Tile-entry capacity of a scene of n Gaussians before any frame overflowed it.
+uint32_t default_entry_cap(uint32_t n) {
+    return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(8ull * n, 1u << 20), 0x3FFFFFFFull);
 }
 
 template <class T>
@@ -669,10 +675,35 @@ int render_gps(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
 
 }  // namespace
 
+namespace {
+std::atomic<int64_t> g_fail_alloc_countdown{-1};   // allocations to let pass before one fails; -1: off
+}  // namespace
+
+namespace gs {
+cudaError_t device_malloc(void** p, size_t bytes) {
+    *p = nullptr;
+    int64_t left = g_fail_alloc_countdown.load();
+    while (left >= 0 && !g_fail_alloc_countdown.compare_exchange_weak(left, left - 1)) {
+    }
+    if (left == 0) return cudaErrorMemoryAllocation;   // injected failure (once)
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();   // reported through the return value only
+        *p = nullptr;
+    }
+    return e;
+}
+}  // namespace gs
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
+
+int gs_debug_fail_alloc(int64_t after) {
+    g_fail_alloc_countdown.store(after < 0 ? -1 : after);
+    return GS_OK;
+}
 
 const char* gs_status_str(int s) {
     switch (s) {
@@ -818,9 +849,9 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
     GS_CUDA(c, cudaMemcpyAsync(c->rows, rows, (size_t)n * 256, kind, c->stream));
     gs::launch_gather_heads(c->rows, c->heads, n, c->num_sms, c->stream);
     GS_CUDA(c, cudaGetLastError());
+    int rc = ensure_entries(c, default_entry_cap(n));
+    if (rc) return rc;   // the scene stays unloaded: every buffer must exist before n is set
     c->n = n;
-    int rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(std::max<uint64_t>(8ull * n, 1u << 20), 0x3FFFFFFFull));
-    if (rc) return rc;
     GS_CUDA(c, cudaStreamSynchronize(c->stream));
     gs_reset_accumulation(c);
     return GS_OK;
@@ -846,11 +877,17 @@ int gs_upload_anim(gs_ctx* c, const int8_t* deltas, uint32_t num_states, const f
     c->anim_w = 0.0f;
     if (num_states == 0) return GS_OK;
     const size_t bytes = (size_t)num_states * c->n * 48u;
-    GS_CUDA(c, dalloc(&c->anim_deltas, bytes));
-    GS_CUDA(c, dalloc(&c->anim_scales, 48 * sizeof(float)));
-    GS_CUDA(c, cudaMemcpyAsync(c->anim_deltas, deltas, bytes, cudaMemcpyHostToDevice, c->stream));
-    GS_CUDA(c, cudaMemcpyAsync(c->anim_scales, scales, 48 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-    GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaError_t e = dalloc(&c->anim_deltas, bytes);
+    if (e == cudaSuccess) e = dalloc(&c->anim_scales, 48 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->anim_deltas, deltas, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->anim_scales, scales, 48 * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {   // all or nothing: no half-uploaded animation stays behind
+        dfree(c->anim_deltas);
+        dfree(c->anim_scales);
+        return cuda_fail(c, e, "animation upload");
+    }
     c->anim_states = num_states;
     gs_reset_accumulation(c);
     return GS_OK;
@@ -882,10 +919,14 @@ int gs_upload_layers(gs_ctx* c, const uint16_t* halves, uint32_t layer_count) {
     gs_reset_accumulation(c);
     if (layer_count == 0) return GS_OK;
     const size_t bytes = (size_t)layer_count * c->n * 48u * sizeof(uint16_t);
-    GS_CUDA(c, dalloc(&c->layer_halves, bytes));
-    if (!c->layer_weights) GS_CUDA(c, dalloc(&c->layer_weights, 256 * 3 * sizeof(float)));
-    GS_CUDA(c, cudaMemcpyAsync(c->layer_halves, halves, bytes, cudaMemcpyHostToDevice, c->stream));
-    GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaError_t e = dalloc(&c->layer_halves, bytes);
+    if (e == cudaSuccess && !c->layer_weights) e = dalloc(&c->layer_weights, 256 * 3 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->layer_halves, halves, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {   // all or nothing
+        dfree(c->layer_halves);
+        return cuda_fail(c, e, "layer upload");
+    }
     c->layers_uploaded = layer_count;
     return GS_OK;
 }
@@ -963,7 +1004,7 @@ int gs_debug_wait_probe(gs_ctx* c, int which, uint32_t spin_limit) {
     // private words: the frame's counters and status arrays stay untouched
     void* mem = nullptr;
     const size_t status_bytes = 64 * sizeof(unsigned long long);
-    GS_CUDA(c, cudaMalloc(&mem, status_bytes + sizeof(FrameCounters)));
+    GS_CUDA(c, gs::device_malloc(&mem, status_bytes + sizeof(FrameCounters)));
     auto* status = static_cast<unsigned long long*>(mem);
     auto* fc = reinterpret_cast<FrameCounters*>(static_cast<char*>(mem) + status_bytes);
     cudaError_t e = cudaMemsetAsync(mem, 0, status_bytes + sizeof(FrameCounters), c->stream);
@@ -989,6 +1030,10 @@ int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
     if (rc) return rc;
     rc = check_previous_frame(c);
     if (rc) return rc;
+    if (!c->entry_cap) {   // a failed growth freed the entry buffers: no frame runs without them
+        rc = ensure_entries(c, default_entry_cap(c->n));
+        if (rc) return rc;
+    }
     begin_frame(c, cam);
     uint16_t* o = static_cast<uint16_t*>(out);
     switch (c->knobs.render_mode) {

@@ -210,6 +210,11 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, s
     return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+// Every device allocation of the library goes through here: cudaMalloc, with
+// a failed call's error cleared (it is reported through the return value),
+// and the allocation-failure injection of gs_debug_fail_alloc.
+cudaError_t device_malloc(void** p, size_t bytes);
+
 // Launchers (each returns the number of kernels it launched).
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t num_sms, cudaStream_t s);

@@ -263,6 +263,16 @@ int gs_pack_raw(const float* raw, uint64_t count, float* rows);
  * rows to gs_upload_rows_device. */
 int gs_pack_raw_device(const float* raw_dev, uint64_t count, float* rows_dev, void* stream);
 
+/* Allocation-failure injection (no counterpart in the reference, whose
+ * renderer refuses oversized scenes before allocating, src/renderer.cpp:717-763):
+ * the device allocation after `after` more successful ones fails once with
+ * GS_ERR_OOM, as a full GPU would make it fail; after < 0 turns it off.
+ * Process-wide.  Every entry point that allocates leaves its context usable
+ * after such a failure: a failed upload leaves no scene (GS_ERR_NO_SCENE
+ * until the next successful one), a failed frame allocation fails that frame
+ * only, and nothing half-uploaded stays behind. */
+int gs_debug_fail_alloc(int64_t after);
+
 /* Load a SOG archive (version 2: meta.json and lossless WebP images) into
  * GpuGaussian rows with the reference loader's decode (gaussian_load_sog,
  * src/gaussian_loader_sog.cpp:126-551, and pack_gpu_gaussians,
