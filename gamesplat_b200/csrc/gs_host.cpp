@@ -13,6 +13,7 @@
 // on one stream without host synchronisation; element counts that depend on
 // the camera (visible splats, tile entries, GPS work) stay on the device.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -230,12 +231,18 @@ cudaEvent_t take_event(gs_ctx* c) {
     return e;
 }
 
+// NVTX range names of the stages (the reference's profiler zones,
+// src/renderer.cpp:1890-1937,1984-2088): visible to nsys / ncu --nvtx.
+const char* const kStageRanges[ST_COUNT] = {"gs cull/project", "gs depth sort", "gs bin", "gs tile sort",
+                                            "gs raster", "gs accumulate", "gs gps splat"};
+
 struct StageScope {
     gs_ctx* c;
     int stage;
     cudaEvent_t a = nullptr;
     uint32_t launches = 0;
     StageScope(gs_ctx* ctx, int s) : c(ctx), stage(s) {
+        nvtxRangePushA(kStageRanges[s]);
         if (c->profiling) {
             a = take_event(c);
             cudaEventRecord(a, c->stream);
@@ -249,6 +256,7 @@ struct StageScope {
             cudaEventRecord(b, c->stream);
             c->pending.push_back({a, b, stage, launches});
         }
+        nvtxRangePop();
     }
 };
 
@@ -1034,6 +1042,7 @@ int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
         rc = ensure_entries(c, default_entry_cap(c->n));
         if (rc) return rc;
     }
+    nvtxRangePushA("gs_render");
     begin_frame(c, cam);
     uint16_t* o = static_cast<uint16_t*>(out);
     switch (c->knobs.render_mode) {
@@ -1042,6 +1051,7 @@ int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
         default: rc = render_gps(c, cam, o); break;
     }
     end_frame(c);
+    nvtxRangePop();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     return rc;

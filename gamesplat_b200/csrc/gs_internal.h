@@ -69,7 +69,8 @@ constexpr int kCullVisItems = 8;
 constexpr int kCullVisTile = kCullVisThreads * kCullVisItems;
 constexpr int kCullThreads = 128;
 
-// Binning configuration: 4 sorted splats per thread, 1024 per CTA tile.
+// Binning configuration: 8 sorted splats per thread, 1024 per CTA tile; the
+// expansion takes the global entry range in chunks of 1024 entries.
 constexpr int kBinThreads = 128;
 constexpr int kBinItems = 8;
 constexpr int kBinTile = kBinThreads * kBinItems;
