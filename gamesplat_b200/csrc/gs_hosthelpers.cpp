@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -211,7 +212,8 @@ extern "C" int gs_pack_raw(const float* raw, uint64_t count, float* rows) {
     return GS_OK;
 }
 
-extern "C" int64_t gs_load_ply(const char* path, float* rows, uint64_t capacity) {
+namespace {
+int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
     if (!path) return GS_ERR_BAD_ARG;
     FILE* f = std::fopen(path, "rb");
     if (!f) return GS_ERR_BAD_ARG;
@@ -266,4 +268,13 @@ extern "C" int64_t gs_load_ply(const char* path, float* rows, uint64_t capacity)
     }
     std::fclose(f);
     return (int64_t)vertex_count;
+}
+}  // namespace
+
+extern "C" int64_t gs_load_ply(const char* path, float* rows, uint64_t capacity) {
+    try {
+        return load_ply(path, rows, capacity);
+    } catch (const std::bad_alloc&) {   // a header declaring more properties than memory holds
+        return GS_ERR_OOM;
+    }
 }

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <new>
 
 namespace gs {
 namespace {
@@ -237,7 +238,10 @@ bool read_image(Bits& br, uint32_t xsize, uint32_t ysize, bool main, std::vector
             return false;
     }
     const uint64_t total = (uint64_t)xsize * ysize;
-    out.assign((size_t)total, 0u);
+    // grown pixel by pixel within reserved space: a stream that ends early
+    // never touches the pages of the size its header declared
+    out.clear();
+    out.reserve((size_t)total);
     std::vector<uint32_t> cache((size_t)cache_size, 0u);
     uint64_t cached = 0;   // pixels inserted into the cache so far
     auto insert_upto = [&](uint64_t end) {
@@ -254,17 +258,21 @@ bool read_image(Bits& br, uint32_t xsize, uint32_t ysize, bool main, std::vector
         const int code = g.green.read(br);
         if (code < 256) {
             const uint32_t r = (uint32_t)g.red.read(br), b = (uint32_t)g.blue.read(br), a = (uint32_t)g.alpha.read(br);
-            out[(size_t)pos++] = a << 24 | r << 16 | (uint32_t)code << 8 | b;
+            out.push_back(a << 24 | r << 16 | (uint32_t)code << 8 | b);
+            ++pos;
         } else if (code < 256 + 24) {
             const uint32_t length = copy_value(br, code - 256);
             const int dsym = g.dist.read(br);
             const uint32_t dist = plane_distance(xsize, copy_value(br, dsym));
             if (br.overrun() || dist > pos || length > total - pos) return false;
-            for (uint32_t k = 0; k < length; ++k, ++pos) out[(size_t)pos] = out[(size_t)(pos - dist)];
+            for (uint32_t k = 0; k < length; ++k, ++pos) {
+                const uint32_t v = out[(size_t)(pos - dist)];
+                out.push_back(v);
+            }
         } else {
             if (!cache_bits) return false;
             insert_upto(pos);
-            out[(size_t)pos] = cache[(size_t)(code - 280)];
+            out.push_back(cache[(size_t)(code - 280)]);
             ++pos;
         }
         if (cache_bits) insert_upto(pos);
@@ -482,7 +490,14 @@ extern "C" int gs_webp_decode_rgba(const uint8_t* data, uint64_t size, int32_t* 
     if (!data || !width || !height) return GS_ERR_BAD_ARG;
     std::vector<uint8_t> px;
     int w = 0, h = 0;
-    if (!gs::webp_decode_rgba(data, (size_t)size, &w, &h, &px)) {
+    bool ok = false;
+    try {
+        ok = gs::webp_decode_rgba(data, (size_t)size, &w, &h, &px);
+    } catch (const std::bad_alloc&) {
+        *width = *height = 0;
+        return GS_ERR_OOM;
+    }
+    if (!ok) {
         *width = *height = 0;
         return GS_ERR_FORMAT;
     }

@@ -348,3 +348,34 @@ def test_webp_mutations_agree():
                 del blob[pos]
         decoded += same_webp(bytes(blob))
     assert 0 < decoded < 1500
+
+
+def test_webp_declared_size_beyond_the_data():
+    """A 16384 x 16384 lossless stream whose pixels need one bit each but
+    ends after 16 bytes of them: both decoders reject it, and this one does
+    so without committing memory for the declared size."""
+    import resource
+
+    bits = []
+
+    def put(value, n):
+        bits.extend((value >> i) & 1 for i in range(n))
+
+    put(0x2F, 8)
+    put(16383, 14)
+    put(16383, 14)
+    put(0, 1)
+    put(0, 3)
+    put(0, 1)      # no transform
+    put(0, 1)      # no color cache
+    put(0, 1)      # no meta prefix codes
+    put(1, 1); put(1, 1); put(1, 1); put(0, 8); put(1, 8)     # green: symbols 0 and 1, one bit each
+    for _ in range(4):                                         # red, blue, alpha, distance: one symbol
+        put(1, 1); put(0, 1); put(0, 1); put(0, 1)
+    put(0x5A5A5A5A5A5A5A5A5A5A5A5A5A5A5A5A, 128)            # 128 pixels of data, then the stream ends
+    data = bytes(sum(b << i for i, b in enumerate(bits[k:k + 8])) for k in range(0, len(bits), 8))
+    before = resource.getrusage(resource.RUSAGE_SELF).ru_maxrss
+    assert decode_ours(data) is None
+    grown_kb = resource.getrusage(resource.RUSAGE_SELF).ru_maxrss - before
+    assert grown_kb < 64 * 1024, grown_kb          # far below the 1 GiB the header declares
+    assert O.ref_webp_decode(data) is None
