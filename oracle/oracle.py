@@ -154,12 +154,25 @@ def ref():
                                         C.POINTER(C.c_float)]
         R.ref_gsanim_layer_weights.restype = C.c_uint32
         R.ref_gsanim_layer_weights.argtypes = [vp, C.c_double, vp]
+        R.ref_time_cull_sort_rows.restype = C.c_double
+        R.ref_time_cull_sort_rows.argtypes = [_f32p, C.c_uint32, _f32p, _f32p, C.c_float, C.POINTER(C.c_uint32)]
         R.ref_sog_rows.restype = C.c_uint32
         R.ref_sog_rows.argtypes = [C.c_char_p, vp, C.c_uint32]
         R.ref_webp_decode.restype = C.c_int
         R.ref_webp_decode.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, C.c_size_t]
         _ref = R
     return _ref
+
+
+def ref_cull_sort_seconds(rows: np.ndarray, cam: np.ndarray):
+    """(seconds, visible count) of the reference's single-threaded CPU
+    cull_gaussians + sort_gaussians (src/gaussian.cpp:77-181) on `rows`."""
+    rows = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1, 64)
+    cam = np.asarray(cam, dtype=np.float32).reshape(-1)
+    vis = C.c_uint32(0)
+    sec = ref().ref_time_cull_sort_rows(rows.reshape(-1), rows.shape[0], np.ascontiguousarray(cam[0:16]),
+                                        np.ascontiguousarray(cam[16:32]), float(cam[34]), C.byref(vis))
+    return float(sec), int(vis.value)
 
 
 def ref_sog_rows(path):

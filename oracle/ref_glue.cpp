@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <cstring>
 #include <cstdlib>
+#include <ctime>
 #define SJ_IMPL
 #include "sj.h"
 #include "gaussian.h"
@@ -61,6 +62,50 @@ uint32_t ref_cull_sort_ply(const char* path, const float* view, const float* pro
     memcpy(sorted, scene.sorted_indices, vc * sizeof(uint32_t));
     free_scene(&scene);
     return vc;
+}
+
+// Seconds of the reference's single-threaded CPU cull_gaussians +
+// sort_gaussians (src/gaussian.cpp:77-181) on a scene given as GpuGaussian
+// rows (unpacked field by field into the reference's Gaussian structs first,
+// outside the timed region); the visible count in *visible.
+double ref_time_cull_sort_rows(const float* rows, uint32_t n, const float* view, const float* proj,
+                               float ortho_blend, uint32_t* visible) {
+    GaussianScene scene;
+    memset(&scene, 0, sizeof(scene));
+    scene.gaussian_count = n;
+    scene.gaussians = (Gaussian*)calloc(n, sizeof(Gaussian));
+    scene.visible_indices = (uint32_t*)malloc((size_t)n * 4);
+    scene.visible_depths = (float*)malloc((size_t)n * 4);
+    scene.sorted_indices = (uint32_t*)malloc((size_t)n * 4);
+    scene.scratch_indices = (uint32_t*)malloc((size_t)n * 4);
+    scene.scratch_keys = (uint32_t*)malloc((size_t)n * 4);
+    scene.scratch_keys2 = (uint32_t*)malloc((size_t)n * 4);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float* d = rows + (size_t)i * 64;
+        Gaussian& g = scene.gaussians[i];
+        memcpy(g.position, d, 12);
+        g.opacity = d[3];
+        memcpy(g.scale, d + 4, 12);
+        memcpy(g.rotation, d + 8, 16);
+        memcpy(g.color, d + 12, 12);
+        memcpy(g.sh_rest, d + 16, 45 * 4);
+    }
+    timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    cull_gaussians(&scene, view, proj, ortho_blend);
+    SortContext ctx;
+    ctx.depths = scene.visible_depths;
+    ctx.input_indices = scene.visible_indices;
+    ctx.count = scene.visible_count;
+    ctx.sorted_indices = scene.sorted_indices;
+    ctx.scratch_indices = scene.scratch_indices;
+    ctx.scratch_keys = scene.scratch_keys;
+    ctx.scratch_keys2 = scene.scratch_keys2;
+    sort_gaussians(&ctx);
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    *visible = scene.visible_count;
+    free_scene(&scene);
+    return (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
 }
 
 void ref_camera_matrices(const float pos[3], float yaw, float pitch, float fov_y, float near_plane,
