@@ -142,7 +142,8 @@ def dist_setup(n_gpus):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        # ranks do the same work between collectives: a short timeout turns a lost rank into an error
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
