@@ -21,6 +21,8 @@
 
 #include <cuda_fp16.h>
 
+#include <atomic>
+
 #include "gs_common.cuh"
 #include "gs_internal.h"
 #include "gs_tma.cuh"
@@ -522,13 +524,18 @@ __global__ void __launch_bounds__(256) cull_layers_kernel(CullParams p) {
 }
 
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
-    static bool attr_set = false;
-    if (!attr_set) {
+    // the shared-memory limit is a per-device function attribute: raise it
+    // once on every device this process launches on
+    static std::atomic<uint64_t> attr_devices{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = dev >= 0 && dev < 64 ? 1ull << dev : 0ull;
+    if (!bit || !(attr_devices.load() & bit)) {
         cudaFuncSetAttribute(cull_project_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         cudaFuncSetAttribute(cull_project_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         cudaFuncSetAttribute(cull_project_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         cudaFuncSetAttribute(cull_project_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
-        attr_set = true;
+        attr_devices.fetch_or(bit);
     }
     int deg = p.sh_degree < 0 ? 0 : (p.sh_degree > 3 ? 3 : p.sh_degree);
     if (p.anim_deltas) deg = 3;   // the delta pass touches every SH slot of the staged row
