@@ -217,18 +217,26 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
     if (!path) return GS_ERR_BAD_ARG;
     FILE* f = std::fopen(path, "rb");
     if (!f) return GS_ERR_BAD_ARG;
+    // Header rules of src/gaussian_loader_ply.cpp:27-75: lines read 511
+    // bytes at a time; any "format" line without binary_little_endian fails
+    // (no format line is accepted); the vertex count is atoi's, as 32 bits;
+    // every vertex property advances the stride, and the first 128 keep
+    // their names for lookup.
     char line[512];
-    uint64_t vertex_count = 0;
-    bool in_vertex = false, header_done = false, binary_le = false;
+    uint32_t vertex_count = 0;
+    bool in_vertex = false, header_done = false;
     int stride = 0;
     std::vector<std::pair<std::string, int>> props;  // name, byte offset
     while (std::fgets(line, sizeof(line), f)) {
         size_t len = std::strlen(line);
         while (len > 0 && (line[len - 1] == '\n' || line[len - 1] == '\r')) line[--len] = 0;
         if (!std::strcmp(line, "end_header")) { header_done = true; break; }
-        if (!std::strncmp(line, "format ", 7)) binary_le = std::strstr(line, "binary_little_endian") != nullptr;
+        if (!std::strncmp(line, "format ", 7) && !std::strstr(line, "binary_little_endian")) {
+            std::fclose(f);
+            return GS_ERR_BAD_ARG;
+        }
         if (!std::strncmp(line, "element vertex ", 15)) {
-            vertex_count = std::strtoull(line + 15, nullptr, 10);
+            vertex_count = (uint32_t)std::atoi(line + 15);
             in_vertex = true;
             continue;
         }
@@ -236,12 +244,12 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
         if (in_vertex && !std::strncmp(line, "property ", 9)) {
             char type[32], name[64];
             if (std::sscanf(line, "property %31s %63s", type, name) == 2) {
-                props.emplace_back(name, stride);
+                if (props.size() < 128) props.emplace_back(name, stride);
                 stride += type_size(type);
             }
         }
     }
-    if (!header_done || !binary_le || vertex_count == 0 || vertex_count > 0xFFFFFFFFull) {
+    if (!header_done || vertex_count == 0) {
         std::fclose(f);
         return GS_ERR_BAD_ARG;
     }
@@ -253,10 +261,30 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
             if (p.first == nm) { off[a] = p.second; break; }
     }
     if (off[A_X] < 0 || off[A_Y] < 0 || off[A_Z] < 0) { std::fclose(f); return GS_ERR_BAD_ARG; }
+    // scale_0, rot_0 and f_dc_0 each stand for their whole group: a file
+    // that names the first without the others has no defined decode (the
+    // reference reads a byte before the row for the missing ones), so it is
+    // rejected.
+    for (int first : {A_S0, A_R0, A_DC0}) {
+        const int last = first == A_R0 ? first + 3 : first + 2;
+        for (int a = first + 1; a <= last && off[first] >= 0; ++a)
+            if (off[a] < 0) { std::fclose(f); return GS_ERR_BAD_ARG; }
+    }
+    // the body must hold every vertex (the reference's loader fails on a short read)
+    const long body_at = std::ftell(f);
+    long body_end = -1;
+    if (body_at >= 0 && !std::fseek(f, 0, SEEK_END)) body_end = std::ftell(f);
+    if (body_end < body_at || std::fseek(f, body_at, SEEK_SET) ||
+        (uint64_t)(body_end - body_at) < (uint64_t)vertex_count * (uint64_t)stride) {
+        std::fclose(f);
+        return GS_ERR_BAD_ARG;
+    }
     if (!rows) { std::fclose(f); return (int64_t)vertex_count; }
     const uint64_t n = vertex_count < capacity ? vertex_count : capacity;
     const uint64_t batch = 4096;
-    std::vector<unsigned char> raw((size_t)batch * stride);
+    // every value is read as 4 bytes whatever its declared size: the padding
+    // keeps a narrower last property of the last row inside the buffer
+    std::vector<unsigned char> raw((size_t)batch * stride + 4, 0);
     for (uint64_t i = 0; i < n; i += batch) {
         uint64_t cnt = n - i < batch ? n - i : batch;
         if (std::fread(raw.data(), stride, cnt, f) != cnt) { std::fclose(f); return GS_ERR_BAD_ARG; }

@@ -242,9 +242,13 @@ int gs_camera_uniforms(const float position[3], float yaw, float pitch, float fo
                        int height, int webgpu, gs_camera* out);
 
 /* Load a binary little-endian 3DGS PLY into GpuGaussian rows with the
- * reference loader's transforms (src/gaussian_loader_ply.cpp:14-228 and
- * pack_gpu_gaussians, src/gaussian.cpp:53-73).  With rows == NULL returns the
- * vertex count; otherwise fills min(count, capacity) rows.  < 0 on error. */
+ * reference loader's header rules and transforms
+ * (src/gaussian_loader_ply.cpp:14-228 and pack_gpu_gaussians,
+ * src/gaussian.cpp:53-73).  With rows == NULL returns the vertex count (the
+ * body must hold that many vertices); otherwise fills min(count, capacity)
+ * rows.  < 0 on error.  A file naming scale_0, rot_0 or f_dc_0 without the
+ * rest of its group is rejected: the reference reads outside the row for the
+ * missing members, so it has no defined result to match. */
 int64_t gs_load_ply(const char* path, float* rows, uint64_t capacity);
 
 /* The same transforms on raw PLY-layout attributes already in memory:
