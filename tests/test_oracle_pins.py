@@ -162,3 +162,32 @@ def test_composite_fp16_rounding_gap_is_small():
     assert fa == fb > 0
     gap = np.abs(a.astype(np.float16).astype(np.float32) - b).max()
     assert gap < 0.05
+
+
+def test_camera_uniforms_random_sweep_match_reference_camera():
+    """gs_camera_uniforms against the reference's camera_get_view_matrix /
+    camera_get_proj_matrix (src/camera.cpp:137-245) over seeded random fly
+    cameras: positions, yaw and pitch over their whole range, field of view,
+    near and far planes, z-up, orthographic size and blend, odd aspect ratios."""
+    if not O.ref_available():
+        pytest.skip("reference CPU build (oracle/_ref) not present")
+    ref = O.ref()
+    rng = np.random.default_rng(123)
+    for k in range(500):
+        pos = rng.uniform(-50, 50, 3).astype(np.float32)
+        yaw, pitch = np.float32(rng.uniform(-7, 7)), np.float32(rng.uniform(-1.55, 1.55))
+        fov = np.float32(rng.uniform(0.2, 2.5))
+        near = np.float32(rng.uniform(0.01, 1.0))
+        far = np.float32(near * rng.uniform(10, 10000))
+        z_up = bool(rng.integers(0, 2))
+        ortho_size = np.float32(rng.uniform(0.1, 20))
+        blend = np.float32(rng.choice([0.0, 1.0, rng.uniform(0, 1)]))
+        w, h = int(rng.integers(1, 4096)), int(rng.integers(1, 4096))
+        cam = R.camera_uniforms(pos, yaw, pitch, w, h, fov_y=fov, near_plane=near, far_plane=far, z_up=z_up,
+                                 ortho_size=ortho_size, ortho_blend=blend)
+        view = np.zeros(16, np.float32)
+        proj = np.zeros(16, np.float32)
+        aspect = np.float32(np.float32(w) / np.float32(h))
+        ref.ref_camera_matrices(pos, yaw, pitch, fov, near, far, int(z_up), ortho_size, blend, aspect, view, proj)
+        assert np.array_equal(cam[:16].view(np.uint32), view.view(np.uint32)), k
+        assert np.array_equal(cam[16:32].view(np.uint32), proj.view(np.uint32)), k
