@@ -64,13 +64,11 @@ uint32_t ref_cull_sort_ply(const char* path, const float* view, const float* pro
     return vc;
 }
 
-// Seconds of the reference's single-threaded CPU cull_gaussians +
-// sort_gaussians (src/gaussian.cpp:77-181) on a scene given as GpuGaussian
-// rows (unpacked field by field into the reference's Gaussian structs first,
-// outside the timed region); the visible count in *visible.
-double ref_time_cull_sort_rows(const float* rows, uint32_t n, const float* view, const float* proj,
-                               float ortho_blend, uint32_t* visible) {
-    GaussianScene scene;
+}  // extern "C"
+
+// A reference scene holding GpuGaussian rows, unpacked field by field into
+// its Gaussian structs (the inverse of pack_gpu_gaussians).
+static void scene_from_rows(GaussianScene& scene, const float* rows, uint32_t n) {
     memset(&scene, 0, sizeof(scene));
     scene.gaussian_count = n;
     scene.gaussians = (Gaussian*)calloc(n, sizeof(Gaussian));
@@ -90,6 +88,32 @@ double ref_time_cull_sort_rows(const float* rows, uint32_t n, const float* view,
         memcpy(g.color, d + 12, 12);
         memcpy(g.sh_rest, d + 16, 45 * 4);
     }
+}
+
+extern "C" {
+
+// The reference's CPU cull_gaussians (src/gaussian.cpp:77-102) on GpuGaussian
+// rows: visible indices and their positive view depths; returns the count.
+uint32_t ref_cull_rows(const float* rows, uint32_t n, const float* view, const float* proj, float ortho_blend,
+                       uint32_t* visible, float* depths) {
+    GaussianScene scene;
+    scene_from_rows(scene, rows, n);
+    cull_gaussians(&scene, view, proj, ortho_blend);
+    const uint32_t vc = scene.visible_count;
+    memcpy(visible, scene.visible_indices, (size_t)vc * 4);
+    memcpy(depths, scene.visible_depths, (size_t)vc * 4);
+    free_scene(&scene);
+    return vc;
+}
+
+// Seconds of the reference's single-threaded CPU cull_gaussians +
+// sort_gaussians (src/gaussian.cpp:77-181) on a scene given as GpuGaussian
+// rows (unpacked into the reference's Gaussian structs first, outside the
+// timed region); the visible count in *visible.
+double ref_time_cull_sort_rows(const float* rows, uint32_t n, const float* view, const float* proj,
+                               float ortho_blend, uint32_t* visible) {
+    GaussianScene scene;
+    scene_from_rows(scene, rows, n);
     timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
     cull_gaussians(&scene, view, proj, ortho_blend);

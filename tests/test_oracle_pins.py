@@ -191,3 +191,42 @@ def test_camera_uniforms_random_sweep_match_reference_camera():
         ref.ref_camera_matrices(pos, yaw, pitch, fov, near, far, int(z_up), ortho_size, blend, aspect, view, proj)
         assert np.array_equal(cam[:16].view(np.uint32), view.view(np.uint32)), k
         assert np.array_equal(cam[16:32].view(np.uint32), proj.view(np.uint32)), k
+
+
+def test_oracle_cull_random_sweep_matches_reference_cull():
+    """Visible set and depth keys of the oracle cull against the reference's
+    cull_gaussians (src/gaussian.cpp:77-102) over seeded random scenes and
+    cameras, orthographic blends included; positions cluster around the near
+    plane and the frustum's 1.3 NDC margin so that the boundary cases occur."""
+    if not O.ref_available():
+        pytest.skip("reference CPU build (oracle/_ref) not present")
+    ref = O.ref()
+    rng = np.random.default_rng(321)
+    for k in range(40):
+        n = 4000
+        w, h = int(rng.integers(64, 2000)), int(rng.integers(64, 2000))
+        blend = float(rng.choice([0.0, 1.0, rng.uniform(0, 1)]))
+        cam = R.camera_uniforms(rng.uniform(-3, 3, 3), rng.uniform(-3, 3), rng.uniform(-1.4, 1.4), w, h,
+                                fov_y=float(rng.uniform(0.3, 2.0)), ortho_size=float(rng.uniform(0.5, 10)),
+                                ortho_blend=blend)
+        rows = np.zeros((n, 64), np.float32)
+        # points along view rays through the NDC margin and depths around the near plane
+        V = cam[:16].reshape(4, 4).T.astype(np.float64)         # column-major view matrix
+        ndc = rng.uniform(-1.5, 1.5, (n, 2))
+        depth = np.where(rng.random(n) < 0.3, rng.uniform(0.15, 0.25, n), rng.uniform(0.2, 40, n))
+        p_view = np.stack([ndc[:, 0] * depth, ndc[:, 1] * depth, -depth, np.ones(n)], 1)
+        world = (np.linalg.inv(V) @ p_view.T).T[:, :3]
+        rows[:, 0:3] = world.astype(np.float32)
+        rows[:, 3] = 0.5
+        rows[:, 4:7] = 0.01
+        rows[:, 8] = 1.0
+        ids, keys, _, vc, _ = O.cull(rows, cam)
+        vis = np.zeros(n, np.uint32)
+        dep = np.zeros(n, np.float32)
+        rc = ref.ref_cull_rows(rows.reshape(-1), n, np.ascontiguousarray(cam[:16]), np.ascontiguousarray(cam[16:32]),
+                               blend, vis, dep)
+        ours = np.nonzero(ids != O.SENTINEL)[0].astype(np.uint32)
+        assert rc == vc == ours.size, k
+        assert np.array_equal(vis[:rc], ours), k
+        ref_keys = (np.uint32(0xFFFFFFFF) - dep[:rc].view(np.uint32)).astype(np.uint32)
+        assert np.array_equal(keys[ours], ref_keys), k
