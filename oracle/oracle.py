@@ -156,6 +156,8 @@ def ref():
         R.ref_gsanim_layer_weights.argtypes = [vp, C.c_double, vp]
         R.ref_cull_rows.restype = C.c_uint32
         R.ref_cull_rows.argtypes = [_f32p, C.c_uint32, _f32p, _f32p, C.c_float, _u32p, _f32p]
+        R.ref_cull_sort_rows.restype = C.c_uint32
+        R.ref_cull_sort_rows.argtypes = [_f32p, C.c_uint32, _f32p, _f32p, C.c_float, _u32p]
         R.ref_time_cull_sort_rows.restype = C.c_double
         R.ref_time_cull_sort_rows.argtypes = [_f32p, C.c_uint32, _f32p, _f32p, C.c_float, C.POINTER(C.c_uint32)]
         R.ref_sog_rows.restype = C.c_uint32

@@ -106,6 +106,29 @@ uint32_t ref_cull_rows(const float* rows, uint32_t n, const float* view, const f
     return vc;
 }
 
+// The reference's CPU cull_gaussians + sort_gaussians (src/gaussian.cpp:77-181)
+// on GpuGaussian rows: its back-to-front order of the visible indices;
+// returns the visible count.
+uint32_t ref_cull_sort_rows(const float* rows, uint32_t n, const float* view, const float* proj, float ortho_blend,
+                            uint32_t* sorted) {
+    GaussianScene scene;
+    scene_from_rows(scene, rows, n);
+    cull_gaussians(&scene, view, proj, ortho_blend);
+    SortContext ctx;
+    ctx.depths = scene.visible_depths;
+    ctx.input_indices = scene.visible_indices;
+    ctx.count = scene.visible_count;
+    ctx.sorted_indices = scene.sorted_indices;
+    ctx.scratch_indices = scene.scratch_indices;
+    ctx.scratch_keys = scene.scratch_keys;
+    ctx.scratch_keys2 = scene.scratch_keys2;
+    sort_gaussians(&ctx);
+    const uint32_t vc = scene.visible_count;
+    memcpy(sorted, scene.sorted_indices, (size_t)vc * 4);
+    free_scene(&scene);
+    return vc;
+}
+
 // Seconds of the reference's single-threaded CPU cull_gaussians +
 // sort_gaussians (src/gaussian.cpp:77-181) on a scene given as GpuGaussian
 // rows (unpacked into the reference's Gaussian structs first, outside the

@@ -230,3 +230,37 @@ def test_oracle_cull_random_sweep_matches_reference_cull():
         assert np.array_equal(vis[:rc], ours), k
         ref_keys = (np.uint32(0xFFFFFFFF) - dep[:rc].view(np.uint32)).astype(np.uint32)
         assert np.array_equal(keys[ours], ref_keys), k
+
+
+def test_oracle_sort_random_sweep_matches_reference_sort_modulo_ties():
+    """The oracle's depth order against the reference's sort_gaussians
+    (src/gaussian.cpp:116-181) over seeded scenes in which most depths tie
+    exactly (points on a few planes facing the camera): the same order once
+    ties are broken the same way, the reference giving equal keys in
+    descending index and the shader sort in ascending index."""
+    if not O.ref_available():
+        pytest.skip("reference CPU build (oracle/_ref) not present")
+    ref = O.ref()
+    rng = np.random.default_rng(654)
+    for k in range(20):
+        n = 3000
+        cam = R.camera_uniforms([0.0, 0.0, 0.0], 0.0, 0.0, 640, 360)
+        V = cam[:16].reshape(4, 4).T.astype(np.float64)
+        levels = rng.uniform(1.0, 30.0, int(rng.integers(1, 12))).astype(np.float32)
+        depth = rng.choice(levels, n).astype(np.float64)
+        ndc = rng.uniform(-0.5, 0.5, (n, 2))
+        p_view = np.stack([ndc[:, 0] * depth, ndc[:, 1] * depth, -depth, np.ones(n)], 1)
+        rows = np.zeros((n, 64), np.float32)
+        rows[:, 0:3] = (np.linalg.inv(V) @ p_view.T).T[:, :3].astype(np.float32)
+        rows[:, 3], rows[:, 4:7], rows[:, 8] = 0.5, 0.01, 1.0
+        ids, keys, _, vc, _ = O.cull(rows, cam)
+        ks, si = O.sort_pairs(keys, ids)
+        srt = np.zeros(n, np.uint32)
+        rc = ref.ref_cull_sort_rows(rows.reshape(-1), n, np.ascontiguousarray(cam[:16]),
+                                    np.ascontiguousarray(cam[16:32]), 0.0, srt)
+        assert rc == vc, k
+        back_to_front = srt[:rc]
+        ref_keys = keys[back_to_front]
+        assert np.array_equal(np.sort(ref_keys), ks[:vc]), k
+        assert np.array_equal(back_to_front[np.lexsort((back_to_front, ref_keys))], si[:vc]), k
+        assert np.unique(ks[:vc]).size < vc // 10        # ties everywhere
