@@ -28,14 +28,17 @@ struct Bits {
     size_t n;
     uint64_t pos = 0;   // bits consumed
     Bits(const uint8_t* data, size_t size) : p(data), n(size) {}
+    // the next `count` (<= 32) bits: one 8-byte window (zeros past the end)
     uint32_t peek(int count) const {
-        uint32_t v = 0;
-        uint64_t at = pos;
-        for (int i = 0; i < count; ++i, ++at) {
-            const uint64_t byte = at >> 3;
-            if (byte < n) v |= (uint32_t)((p[byte] >> (at & 7)) & 1u) << i;
+        const uint64_t byte = pos >> 3;
+        uint64_t w = 0;
+        if (byte + 8 <= n) {
+            std::memcpy(&w, p + byte, 8);
+        } else if (byte < n) {
+            std::memcpy(&w, p + byte, (size_t)(n - byte));
         }
-        return v;
+        w >>= (pos & 7);
+        return count >= 32 ? (uint32_t)w : (uint32_t)(w & ((1ull << count) - 1));
     }
     uint32_t read(int count) {
         const uint32_t v = peek(count);
@@ -243,39 +246,39 @@ bool read_image(Bits& br, uint32_t xsize, uint32_t ysize, bool main, std::vector
     out.clear();
     out.reserve((size_t)total);
     std::vector<uint32_t> cache((size_t)cache_size, 0u);
-    uint64_t cached = 0;   // pixels inserted into the cache so far
-    auto insert_upto = [&](uint64_t end) {
-        for (; cached < end; ++cached) {
-            const uint32_t argb = out[(size_t)cached];
-            cache[(0x1e35a7bdu * argb) >> (32 - cache_bits)] = argb;
-        }
+    const int cache_shift = 32 - cache_bits;
+    // every decoded pixel enters the color cache, in order
+    auto emit = [&](uint32_t argb) {
+        out.push_back(argb);
+        if (cache_bits) cache[(0x1e35a7bdu * argb) >> cache_shift] = argb;
     };
     uint64_t pos = 0;
+    uint32_t x = 0, y = 0;
     while (pos < total) {
-        const uint32_t x = (uint32_t)(pos % xsize), y = (uint32_t)(pos / xsize);
         const Group& g = meta.empty() ? groups[0]
                                       : groups[meta[(size_t)((y >> prefix_bits) * groups_x + (x >> prefix_bits))]];
         const int code = g.green.read(br);
+        uint32_t advance = 1;
         if (code < 256) {
             const uint32_t r = (uint32_t)g.red.read(br), b = (uint32_t)g.blue.read(br), a = (uint32_t)g.alpha.read(br);
-            out.push_back(a << 24 | r << 16 | (uint32_t)code << 8 | b);
-            ++pos;
+            emit(a << 24 | r << 16 | (uint32_t)code << 8 | b);
         } else if (code < 256 + 24) {
             const uint32_t length = copy_value(br, code - 256);
             const int dsym = g.dist.read(br);
             const uint32_t dist = plane_distance(xsize, copy_value(br, dsym));
             if (br.overrun() || dist > pos || length > total - pos) return false;
-            for (uint32_t k = 0; k < length; ++k, ++pos) {
-                const uint32_t v = out[(size_t)(pos - dist)];
-                out.push_back(v);
-            }
+            for (uint32_t k = 0; k < length; ++k) emit(out[(size_t)(pos + k - dist)]);
+            advance = length;
         } else {
             if (!cache_bits) return false;
-            insert_upto(pos);
-            out.push_back(cache[(size_t)(code - 280)]);
-            ++pos;
+            emit(cache[(size_t)(code - 280)]);
         }
-        if (cache_bits) insert_upto(pos);
+        pos += advance;
+        x += advance;
+        if (x >= xsize) {
+            y += x / xsize;
+            x %= xsize;
+        }
         if (br.overrun()) return false;
     }
     return !br.overrun();
