@@ -15,6 +15,7 @@ from .renderer import (  # noqa: F401
     camera_to_array,
     camera_uniforms,
     load_ply,
+    load_scene,
     load_sog,
     pack_raw,
     sort_pairs,

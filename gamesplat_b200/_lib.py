@@ -45,6 +45,7 @@ EXPORTS = (
     "gs_gsanim_get_info", "gs_gsanim_rows", "gs_gsanim_deltas", "gs_gsanim_layer_data", "gs_gsanim_display_lut",
     "gs_gsanim_layer_name", "gs_gsanim_sample", "gs_gsanim_layer_weights", "gs_webp_decode_rgba",
     "gs_load_sog", "gs_upload_layers", "gs_set_layer_weights", "gs_debug_fail_alloc",
+    "gs_load_scene",
 )
 
 
@@ -189,6 +190,7 @@ def lib() -> C.CDLL:
         "gs_upload_layers": (i32, [vp, vp, u32]),
         "gs_set_layer_weights": (i32, [vp, vp, u32]),
         "gs_debug_fail_alloc": (i32, [C.c_int64]),
+        "gs_load_scene": (C.c_int64, [C.c_char_p, vp, u64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1,6 +1,7 @@
 // Host-side helpers of the C ABI that need no GPU: camera uniforms and PLY
 // ingestion into GpuGaussian rows.  Compiled with -ffp-contract=off so the
 // float results match the reference's own host code bit for bit.
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -305,4 +306,49 @@ extern "C" int64_t gs_load_ply(const char* path, float* rows, uint64_t capacity)
     } catch (const std::bad_alloc&) {   // a header declaring more properties than memory holds
         return GS_ERR_OOM;
     }
+}
+
+namespace {
+bool ends_with_ci(const char* s, const char* suffix) {
+    const size_t sl = std::strlen(s), tl = std::strlen(suffix);
+    if (tl > sl) return false;
+    s += sl - tl;
+    for (size_t i = 0; i < tl; ++i)
+        if (std::tolower((unsigned char)s[i]) != std::tolower((unsigned char)suffix[i])) return false;
+    return true;
+}
+}  // namespace
+
+extern "C" int64_t gs_load_scene(const char* path, float* rows, uint64_t capacity) {
+    if (!path) return GS_ERR_BAD_ARG;
+    // load_gaussian_scene (src/gaussian.cpp:27-40): the format by the file
+    // name's extension, case-insensitively
+    if (ends_with_ci(path, ".gsanim")) {
+        gs_gsanim* a = nullptr;
+        const int rc = gs_gsanim_load(path, &a);
+        if (rc != GS_OK) return rc;
+        gs_gsanim_info info;
+        gs_gsanim_get_info(a, &info);
+        int64_t n = (int64_t)info.gaussian_count;
+        if (rows) {
+            if (capacity >= info.gaussian_count) {
+                gs_gsanim_rows(a, rows);
+            } else {
+                std::vector<float> all;
+                try {
+                    all.resize((size_t)info.gaussian_count * 64);
+                } catch (const std::bad_alloc&) {
+                    gs_gsanim_free(a);
+                    return GS_ERR_OOM;
+                }
+                gs_gsanim_rows(a, all.data());
+                std::memcpy(rows, all.data(), (size_t)capacity * 64 * sizeof(float));
+            }
+        }
+        gs_gsanim_free(a);
+        return n;
+    }
+    if (ends_with_ci(path, ".ply")) return gs_load_ply(path, rows, capacity);
+    if (ends_with_ci(path, ".sog")) return gs_load_sog(path, rows, capacity);
+    return GS_ERR_FORMAT;
 }

@@ -67,6 +67,19 @@ def load_ply(path: str) -> np.ndarray:
     return rows
 
 
+def load_scene(path: str) -> np.ndarray:
+    """GpuGaussian rows (N x 64 float32) of a .ply, .sog or .gsanim file, chosen by extension
+    (load_gaussian_scene)."""
+    n = L.lib().gs_load_scene(str(path).encode(), None, 0)
+    if n < 0:
+        raise L.GsError(int(n), "gs_load_scene", str(path))
+    rows = np.empty((n, 64), np.float32)
+    got = L.lib().gs_load_scene(str(path).encode(), rows.ctypes.data, n)
+    if got != n:
+        raise L.GsError(int(got) if got < 0 else L.GS_ERR_BAD_ARG, "gs_load_scene", str(path))
+    return rows
+
+
 def load_sog(path: str) -> np.ndarray:
     """GpuGaussian rows (N x 64 float32) of a SOG archive, reference loader decode."""
     n = L.lib().gs_load_sog(str(path).encode(), None, 0)

@@ -277,6 +277,14 @@ int gs_pack_raw_device(const float* raw_dev, uint64_t count, float* rows_dev, vo
  * only, and nothing half-uploaded stays behind. */
 int gs_debug_fail_alloc(int64_t after);
 
+/* load_gaussian_scene (src/gaussian.cpp:27-40): a scene file by its
+ * extension, case-insensitively (.gsanim, .ply, .sog), as GpuGaussian rows
+ * (for .gsanim the base Gaussians; its animation through gs_gsanim_load).
+ * With rows == NULL returns the Gaussian count; otherwise fills
+ * min(count, capacity) rows.  < 0 on error; GS_ERR_FORMAT for other
+ * extensions. */
+int64_t gs_load_scene(const char* path, float* rows, uint64_t capacity);
+
 /* Load a SOG archive (version 2: meta.json and lossless WebP images) into
  * GpuGaussian rows with the reference loader's decode (gaussian_load_sog,
  * src/gaussian_loader_sog.cpp:126-551, and pack_gpu_gaussians,
