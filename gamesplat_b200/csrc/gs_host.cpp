@@ -1029,8 +1029,18 @@ int gs_debug_wait_probe(gs_ctx* c, int which, uint32_t spin_limit) {
     return GS_OK;
 }
 
+// The image rules are GL's: window y from the bottom, depth clipped to
+// [-1, 1] (src/main.cpp:1275-1281, the non-WGPU branch).  The WGPU branch
+// (clip_y_sign -1, clip_z_01 1) rasterises with a top-left fragment origin,
+// which no kernel here follows, so such a camera is refused instead of
+// drawn wrongly.
+static bool gl_clip_convention(const gs_camera* cam) {
+    return cam->clip_y_sign == 1.0f && cam->clip_z_01 == 0.0f;
+}
+
 int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
     if (!c || !cam || !out) return GS_ERR_BAD_ARG;
+    if (!gl_clip_convention(cam)) return fail(c, GS_ERR_BAD_ARG, "only the GL clip convention is drawn");
     if (!c->n) return fail(c, GS_ERR_NO_SCENE, "no scene uploaded");
     cudaSetDevice(c->device);
     int w = (int)(cam->viewport[0] + 0.5f), h = (int)(cam->viewport[1] + 0.5f);  // src/renderer.cpp:2193-2196
@@ -1059,6 +1069,7 @@ int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
 
 int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
     if (!c || !cam || !host_out) return GS_ERR_BAD_ARG;
+    if (!gl_clip_convention(cam)) return fail(c, GS_ERR_BAD_ARG, "only the GL clip convention is drawn");
     int w = (int)(cam->viewport[0] + 0.5f), h = (int)(cam->viewport[1] + 0.5f);
     int rc = ensure_targets(c, w, h);
     if (rc) return rc;

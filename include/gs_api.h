@@ -182,7 +182,11 @@ int gs_reset_accumulation(gs_ctx* ctx);
 /* renderer_draw_frame (src/renderer.h:265), splatting path only: cull,
  * (alpha) sort, then composite / stochastic / GPS according to the mode, into
  * caller-owned device memory `rgba16f_out` (width*height*4 halves, top row
- * first; width/height = round(cam->viewport)).  `cam` is host memory. */
+ * first; width/height = round(cam->viewport)).  `cam` is host memory.
+ * Only the GL clip convention (clip_y_sign 1, clip_z_01 0; the non-WGPU
+ * branch of src/main.cpp:1275-1281) is drawn: other cameras return
+ * GS_ERR_BAD_ARG, since the WGPU backend's top-left fragment origin is not
+ * what the kernels rasterise. */
 int gs_render(gs_ctx* ctx, const gs_camera* cam, void* rgba16f_out);
 
 /* gs_render into host memory: includes the host->device camera copy and the
@@ -236,7 +240,8 @@ const char* gs_last_error(const gs_ctx* ctx);
 /* CameraUniforms of the reference fly camera: camera_get_view_matrix /
  * camera_get_proj_matrix (src/camera.cpp:137-245) and the uniform setup of
  * src/main.cpp:1264-1281 (persp_focal = H/2/tan(fov/2), ortho_focal =
- * H/(2 ortho_size), GL clip conventions unless webgpu != 0). */
+ * H/(2 ortho_size), GL clip conventions unless webgpu != 0; gs_render
+ * draws the GL ones only). */
 int gs_camera_uniforms(const float position[3], float yaw, float pitch, float fov_y, float near_plane,
                        float far_plane, int z_up, float ortho_size, float ortho_blend, int width,
                        int height, int webgpu, gs_camera* out);
