@@ -1038,13 +1038,27 @@ static bool gl_clip_convention(const gs_camera* cam) {
     return cam->clip_y_sign == 1.0f && cam->clip_z_01 == 0.0f;
 }
 
+// Target size: the viewport rounded to whole pixels (src/renderer.cpp:2193-2196),
+// range-checked as a float first so that NaN or huge viewports never reach
+// the integer conversion.
+static int viewport_dims(gs_ctx* c, const gs_camera* cam, int* w, int* h) {
+    const float vw = cam->viewport[0] + 0.5f, vh = cam->viewport[1] + 0.5f;
+    if (!(vw >= 1.0f && vh >= 1.0f)) return fail(c, GS_ERR_BAD_ARG, "viewport must be positive");
+    if (vw >= 32768.0f || vh >= 32768.0f) return fail(c, GS_ERR_TOO_LARGE, "viewport beyond 32767 pixels");
+    *w = (int)vw;
+    *h = (int)vh;
+    return GS_OK;
+}
+
 int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
     if (!c || !cam || !out) return GS_ERR_BAD_ARG;
     if (!gl_clip_convention(cam)) return fail(c, GS_ERR_BAD_ARG, "only the GL clip convention is drawn");
     if (!c->n) return fail(c, GS_ERR_NO_SCENE, "no scene uploaded");
     cudaSetDevice(c->device);
-    int w = (int)(cam->viewport[0] + 0.5f), h = (int)(cam->viewport[1] + 0.5f);  // src/renderer.cpp:2193-2196
-    int rc = ensure_targets(c, w, h);
+    int w = 0, h = 0;
+    int rc = viewport_dims(c, cam, &w, &h);
+    if (rc) return rc;
+    rc = ensure_targets(c, w, h);
     if (rc) return rc;
     rc = check_previous_frame(c);
     if (rc) return rc;
@@ -1070,8 +1084,10 @@ int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
 int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
     if (!c || !cam || !host_out) return GS_ERR_BAD_ARG;
     if (!gl_clip_convention(cam)) return fail(c, GS_ERR_BAD_ARG, "only the GL clip convention is drawn");
-    int w = (int)(cam->viewport[0] + 0.5f), h = (int)(cam->viewport[1] + 0.5f);
-    int rc = ensure_targets(c, w, h);
+    int w = 0, h = 0;
+    int rc = viewport_dims(c, cam, &w, &h);
+    if (rc) return rc;
+    rc = ensure_targets(c, w, h);
     if (rc) return rc;
     const size_t bytes = (size_t)w * h * 8;
     // A page-locked destination is written by the copy engine directly;

@@ -4,6 +4,8 @@ depth-sort permutation bit-exact; RGBA16F image within max-abs 2^-9 per
 channel and PSNR >= 55 dB of the CPU oracle (FP32 composite, rounded once)."""
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -156,6 +158,17 @@ def test_errors_are_status_codes():
     with pytest.raises(L.GsError) as e:
         r.draw_frame(bad)
     assert e.value.status == L.GS_ERR_BAD_ARG
+    # viewports that are not finite or beyond 32767 pixels are refused before
+    # any target is sized (the output buffer is never touched)
+    buf = np.zeros(4, np.float16)
+    for v, status in ((float("nan"), L.GS_ERR_BAD_ARG), (-5.0, L.GS_ERR_BAD_ARG), (0.49, L.GS_ERR_BAD_ARG),
+                      (float("inf"), L.GS_ERR_TOO_LARGE), (1e10, L.GS_ERR_TOO_LARGE), (32767.6, L.GS_ERR_TOO_LARGE)):
+        for axis in (32, 33):
+            bad = cam.copy()
+            bad[axis] = v
+            cc = RR.camera_from_array(bad)
+            assert L.lib().gs_render_host(r._ctx, C.byref(cc), buf.ctypes.data) == status, (axis, v)
+    assert r.draw_frame(cam).shape == (64, 64, 4)
     assert r.set_gps_work_budget(0) is False
     assert r.set_gps_work_budget(1 << 16) is True
     r.destroy()
