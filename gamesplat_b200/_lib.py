@@ -45,7 +45,7 @@ EXPORTS = (
     "gs_gsanim_get_info", "gs_gsanim_rows", "gs_gsanim_deltas", "gs_gsanim_layer_data", "gs_gsanim_display_lut",
     "gs_gsanim_layer_name", "gs_gsanim_sample", "gs_gsanim_layer_weights", "gs_webp_decode_rgba",
     "gs_load_sog", "gs_upload_layers", "gs_set_layer_weights", "gs_debug_fail_alloc",
-    "gs_load_scene",
+    "gs_load_scene", "gs_scene_device_bytes",
 )
 
 
@@ -79,7 +79,8 @@ class GsKnobs(C.Structure):
         ("splat_diagnostics_enabled", C.c_int32),
         ("linear_color", C.c_int32),
         ("write_invisible_records", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("gpu_budget_mb", C.c_uint32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -191,6 +192,7 @@ def lib() -> C.CDLL:
         "gs_set_layer_weights": (i32, [vp, vp, u32]),
         "gs_debug_fail_alloc": (i32, [C.c_int64]),
         "gs_load_scene": (C.c_int64, [C.c_char_p, vp, u64]),
+        "gs_scene_device_bytes": (u64, [u64, C.c_uint32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -170,6 +170,26 @@ uint32_t default_entry_cap(uint32_t n) {
     return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(8ull * n, 1u << 20), 0x3FFFFFFFull);
 }
 
+// Device bytes of a scene of n Gaussians with a GPS budget of work_items:
+// what an upload allocates (rows, heads, projected records, sort pairs,
+// raster records, binning state, look-back words, tile entries at their
+// initial capacity) plus the GPS prepared records and work items.  The
+// counterpart of renderer_scene_buffer_bytes (src/renderer.cpp:705-709) for
+// this layout.  Frame targets (sized by the viewport) are not counted there
+// either.
+uint64_t scene_device_bytes(uint32_t n, uint32_t work_items) {
+    uint64_t b = (uint64_t)work_items * sizeof(uint2);
+    if (!n) return b;
+    b += (uint64_t)n * (256u + 16u + 64u + 16u + sizeof(RasterRecord) + sizeof(uint4) + 48u);
+    b += ((uint64_t)n + gs::kCullVisTile - 1) / gs::kCullVisTile * 8u;
+    b += (uint64_t)gs::sort_status_words(n) * 4u * 8u;
+    b += ((uint64_t)n + gs::kBinTile - 1) / gs::kBinTile * 8u;
+    const uint32_t cap = default_entry_cap(n);
+    b += (uint64_t)cap * 16u + ((uint64_t)cap / gs::kBinChunk + 2u) * 4u;
+    b += (uint64_t)gs::sort_status_words(cap) * 4u * 8u;
+    return b;
+}
+
 template <class T>
 void dfree(T*& p) {
     if (p) cudaFree(reinterpret_cast<void*>(p));
@@ -259,6 +279,38 @@ struct StageScope {
         nvtxRangePop();
     }
 };
+
+// renderer_gpu_buffer_limits (src/renderer.cpp:713-732), the NVIDIA branch:
+// new allocations stay within 4/5 of the device's free memory, and the
+// retained scene buffers within gpu_budget_mb when it is set.
+struct MemoryLimits {
+    uint64_t scene_cap;
+    uint64_t allocation_budget;
+};
+
+MemoryLimits memory_limits(const gs_ctx* c) {
+    MemoryLimits m{UINT64_MAX, UINT64_MAX};
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) m.allocation_budget = (uint64_t)free_b * 4u / 5u;
+    else cudaGetLastError();   // the allocations themselves will report the failure
+    if (c->knobs.gpu_budget_mb) m.scene_cap = (uint64_t)c->knobs.gpu_budget_mb << 20;
+    return m;
+}
+
+uint64_t anim_device_bytes(uint32_t n, uint32_t states) {
+    return states ? (uint64_t)states * n * 48u + 48u * sizeof(float) : 0u;
+}
+
+uint64_t layer_device_bytes(uint32_t n, uint32_t layers) {
+    return layers ? (uint64_t)layers * n * 48u * sizeof(uint16_t) + 256u * 3u * sizeof(float) : 0u;
+}
+
+std::string mib(uint64_t bytes) {
+    if (bytes == UINT64_MAX) return "unlimited";
+    char buf[32];
+    std::snprintf(buf, sizeof(buf), "%.1f MiB", (double)bytes / 1048576.0);
+    return buf;
+}
 
 int entry_bits(uint32_t tiles) {
     int bits = 1;
@@ -832,9 +884,16 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
     if (count == 0) return fail(c, GS_ERR_BAD_ARG, "empty scene");  // src/renderer.cpp:757
     if (count > (1ull << 30) - 1) return fail(c, GS_ERR_TOO_LARGE, "more than 2^30-1 Gaussians");
     cudaSetDevice(c->device);
+    const uint32_t n = (uint32_t)count;
+    {   // src/renderer.cpp:739-763: refuse before touching the resident scene
+        const MemoryLimits lim = memory_limits(c);
+        const uint64_t need = scene_device_bytes(n, std::max(c->gps_max_work_items, 1u));
+        const uint64_t budget = std::min(lim.scene_cap, lim.allocation_budget);
+        if (need > budget)
+            return fail(c, GS_ERR_TOO_LARGE, "scene needs " + mib(need) + " of device memory; budget " + mib(budget));
+    }
     cudaStreamSynchronize(c->stream);
     release_scene(c);
-    const uint32_t n = (uint32_t)count;
     GS_CUDA(c, dalloc(&c->rows, (size_t)n * 256));
     GS_CUDA(c, dalloc(&c->heads, (size_t)n * 16));
     GS_CUDA(c, dalloc(&c->projected, (size_t)n * 64));
@@ -877,6 +936,14 @@ int gs_upload_anim(gs_ctx* c, const int8_t* deltas, uint32_t num_states, const f
     if (!c || (num_states && (!deltas || !scales))) return GS_ERR_BAD_ARG;
     if (!c->n) return fail(c, GS_ERR_NO_SCENE, "upload the Gaussians before their animation");
     cudaSetDevice(c->device);
+    if (num_states) {   // the old animation stays when the new one is refused
+        const MemoryLimits lim = memory_limits(c);
+        const uint64_t add = anim_device_bytes(c->n, num_states);
+        const uint64_t kept = scene_device_bytes(c->n, std::max(c->gps_max_work_items, 1u)) +
+                              layer_device_bytes(c->n, c->layers_uploaded);
+        if (add > lim.allocation_budget || kept + add > lim.scene_cap)
+            return fail(c, GS_ERR_TOO_LARGE, "animation needs " + mib(add) + " of device memory beyond the budget");
+    }
     cudaStreamSynchronize(c->stream);
     dfree(c->anim_deltas);
     dfree(c->anim_scales);
@@ -919,6 +986,14 @@ int gs_upload_layers(gs_ctx* c, const uint16_t* halves, uint32_t layer_count) {
     if (!c->n) return fail(c, GS_ERR_NO_SCENE, "upload the Gaussians before their layers");
     if (layer_count > 256) return fail(c, GS_ERR_TOO_LARGE, "more than 256 layers");
     cudaSetDevice(c->device);
+    if (layer_count) {   // the old layers stay when the new ones are refused
+        const MemoryLimits lim = memory_limits(c);
+        const uint64_t add = layer_device_bytes(c->n, layer_count);
+        const uint64_t kept = scene_device_bytes(c->n, std::max(c->gps_max_work_items, 1u)) +
+                              anim_device_bytes(c->n, c->anim_states);
+        if (add > lim.allocation_budget || kept + add > lim.scene_cap)
+            return fail(c, GS_ERR_TOO_LARGE, "layers need " + mib(add) + " of device memory beyond the budget");
+    }
     cudaStreamSynchronize(c->stream);
     dfree(c->layer_halves);
     c->layers_uploaded = 0;
@@ -959,6 +1034,16 @@ int gs_set_layer_weights(gs_ctx* c, const float* weights, uint32_t count) {
 int gs_set_gps_budget(gs_ctx* c, uint32_t max_work_items) {
     if (!c) return GS_ERR_BAD_ARG;
     if (max_work_items == 0) return fail(c, GS_ERR_BUDGET_REFUSED, "GPS budget must be >= 1");
+    if (max_work_items == c->gps_max_work_items) return GS_OK;
+    {   // src/renderer.cpp:1080-1092: the replacement against free memory, the scene against the cap
+        cudaSetDevice(c->device);
+        const MemoryLimits lim = memory_limits(c);
+        const uint64_t add = (uint64_t)max_work_items * sizeof(uint2);
+        const uint64_t total = scene_device_bytes(c->n, max_work_items) + anim_device_bytes(c->n, c->anim_states) +
+                               layer_device_bytes(c->n, c->layers_uploaded);
+        if (add > lim.allocation_budget || total > lim.scene_cap)
+            return fail(c, GS_ERR_BUDGET_REFUSED, "GPS work buffer of " + mib(add) + " refused by the memory budget");
+    }
     int rc = gs::resize_gps_work(c->gps, max_work_items, c->stream);
     if (rc) return fail(c, GS_ERR_BUDGET_REFUSED, "GPS work buffer resize refused; old budget kept");
     c->gps_max_work_items = max_work_items;
@@ -1048,6 +1133,11 @@ static int viewport_dims(gs_ctx* c, const gs_camera* cam, int* w, int* h) {
     *w = (int)vw;
     *h = (int)vh;
     return GS_OK;
+}
+
+uint64_t gs_scene_device_bytes(uint64_t count, uint32_t gps_work_items) {
+    if (count == 0 || count > (1ull << 30) - 1) return 0;
+    return scene_device_bytes((uint32_t)count, std::max(gps_work_items, 1u));
 }
 
 int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {

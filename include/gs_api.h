@@ -85,7 +85,11 @@ typedef struct gs_knobs {
                                                  (gsanim 0.3 path); 0: RGBA8 sample target */
     int32_t write_invisible_records;          /* 1: also write the reference's record for culled
                                                  Gaussians (debug/parity); default 0 */
-    int32_t reserved[4];
+    uint32_t gpu_budget_mb;                   /* cap on the scene's device memory in MiB (Renderer
+                                                 gpu_budget_bytes = MiB << 20, src/renderer.h:175,
+                                                 src/main.cpp:352-359); 0: none beyond 4/5 of the
+                                                 free device memory; default 0 */
+    int32_t reserved[3];
 } gs_knobs;
 
 /* Per-frame statistics (the reference's SplatDiagnostics, src/renderer.h:28-38,
@@ -178,6 +182,17 @@ int gs_set_gps_budget(gs_ctx* ctx, uint32_t max_work_items);
 
 /* renderer_reset_stochastic_accumulation (src/renderer.h:261). */
 int gs_reset_accumulation(gs_ctx* ctx);
+
+/* Device bytes of a scene of `count` Gaussians with a GPS budget of
+ * `gps_work_items` (renderer_scene_buffer_bytes, src/renderer.cpp:705-709, for
+ * this library's layout): what gs_upload_rows allocates plus the GPS
+ * prepared records and work items; frame targets not included.  0 for a count
+ * outside 1..2^30-1.  Host only.  gs_upload_rows refuses a scene with
+ * GS_ERR_TOO_LARGE, before it touches the resident one, when this exceeds
+ * gpu_budget_mb or 4/5 of the device's free memory (src/renderer.cpp:739-763);
+ * gs_upload_anim and gs_upload_layers check their own bytes the same way, and
+ * gs_set_gps_budget its new work buffer (GS_ERR_BUDGET_REFUSED). */
+uint64_t gs_scene_device_bytes(uint64_t count, uint32_t gps_work_items);
 
 /* renderer_draw_frame (src/renderer.h:265), splatting path only: cull,
  * (alpha) sort, then composite / stochastic / GPS according to the mode, into
