@@ -45,7 +45,7 @@ EXPORTS = (
     "gs_gsanim_get_info", "gs_gsanim_rows", "gs_gsanim_deltas", "gs_gsanim_layer_data", "gs_gsanim_display_lut",
     "gs_gsanim_layer_name", "gs_gsanim_sample", "gs_gsanim_layer_weights", "gs_webp_decode_rgba",
     "gs_load_sog", "gs_upload_layers", "gs_set_layer_weights", "gs_debug_fail_alloc",
-    "gs_load_scene", "gs_scene_device_bytes",
+    "gs_load_scene", "gs_scene_device_bytes", "gs_upload_rows_range",
 )
 
 
@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
         "gs_set_mode": (i32, [vp, i32]),
         "gs_upload_rows": (i32, [vp, vp, u64]),
         "gs_upload_rows_device": (i32, [vp, vp, u64]),
+        "gs_upload_rows_range": (i32, [vp, vp, u64, u64]),
         "gs_set_gps_budget": (i32, [vp, u32]),
         "gs_reset_accumulation": (i32, [vp]),
         "gs_render": (i32, [vp, C.POINTER(GsCamera), vp]),

@@ -932,6 +932,21 @@ int gs_upload_rows_device(gs_ctx* c, const float* rows, uint64_t count) {
     return upload_common(c, rows, count, cudaMemcpyDeviceToDevice);
 }
 
+int gs_upload_rows_range(gs_ctx* c, const float* rows, uint64_t first, uint64_t count) {
+    if (!c || (!rows && count)) return GS_ERR_BAD_ARG;
+    if (!c->n) return fail(c, GS_ERR_NO_SCENE, "upload the scene before replacing rows of it");
+    if (first > c->n || count > c->n - first) return fail(c, GS_ERR_BAD_ARG, "row range beyond the scene");
+    if (!count) return GS_OK;
+    cudaSetDevice(c->device);
+    // stream-ordered after the frames already queued, which read the old rows
+    GS_CUDA(c, cudaMemcpyAsync(c->rows + first * 16, rows, count * 256, cudaMemcpyHostToDevice, c->stream));
+    gs::launch_gather_heads(c->rows + first * 16, c->heads + first, (uint32_t)count, c->num_sms, c->stream);
+    GS_CUDA(c, cudaGetLastError());
+    GS_CUDA(c, cudaStreamSynchronize(c->stream));   // the caller may reuse `rows` on return
+    gs_reset_accumulation(c);
+    return GS_OK;
+}
+
 int gs_upload_anim(gs_ctx* c, const int8_t* deltas, uint32_t num_states, const float* scales) {
     if (!c || (num_states && (!deltas || !scales))) return GS_ERR_BAD_ARG;
     if (!c->n) return fail(c, GS_ERR_NO_SCENE, "upload the Gaussians before their animation");

@@ -170,6 +170,14 @@ class Renderer:
             raise ValueError("rows must be N x 64 float32 GpuGaussian rows")
         L.check(L.lib().gs_upload_rows(self._ctx, rows.ctypes.data, rows.shape[0]), "gs_upload_rows", self._ctx)
 
+    def upload_rows_range(self, rows: np.ndarray, first: int) -> None:
+        """Replace rows [first, first + len(rows)) of the resident scene."""
+        rows = np.ascontiguousarray(rows, dtype=np.float32)
+        if rows.ndim != 2 or rows.shape[1] != 64:
+            raise ValueError("rows must be N x 64 float32 GpuGaussian rows")
+        L.check(L.lib().gs_upload_rows_range(self._ctx, rows.ctypes.data, int(first), rows.shape[0]),
+                "gs_upload_rows_range", self._ctx)
+
     def upload_gaussians_device(self, ptr: int, count: int) -> None:
         L.check(L.lib().gs_upload_rows_device(self._ctx, C.c_void_p(ptr), count), "gs_upload_rows_device",
                 self._ctx)

@@ -145,6 +145,15 @@ int gs_upload_rows(gs_ctx* ctx, const float* rows, uint64_t count);
 /* As gs_upload_rows, from device memory (stream-ordered copy). */
 int gs_upload_rows_device(gs_ctx* ctx, const float* rows_dev, uint64_t count);
 
+/* Replace rows [first, first + count) of the resident scene with `count`
+ * GpuGaussian rows from host memory (the per-chunk copy of
+ * renderer_upload_gaussians, src/renderer.cpp:896-919, applied to a range of
+ * a scene already uploaded): for hosts that edit or stream part of a scene
+ * without re-uploading all of it.  Queued after the frames already issued,
+ * returns once the copy is done, and resets accumulation.  GS_ERR_NO_SCENE
+ * without a scene, GS_ERR_BAD_ARG for a range beyond it. */
+int gs_upload_rows_range(gs_ctx* ctx, const float* rows, uint64_t first, uint64_t count);
+
 /* gsanim appearance states (the renderer's animation buffer,
  * src/renderer.cpp:824-841, decoded by shaders/cull.glsl:125-164):
  * `deltas` holds num_states x N x 48 int8 values (state-major, row, then
