@@ -325,6 +325,24 @@ def composite_alpha(sorted_ids: np.ndarray, projected: np.ndarray, width: int, h
     return out, int(frags)
 
 
+def sh_to_fp16(rows: np.ndarray) -> np.ndarray:
+    """The rows with their SH coefficients (DC at [12:15], the 45 others at
+    [16:61]) rounded to IEEE half and back: what a row layout that stores SH
+    in FP16 hands the cull, whose arithmetic stays FP32."""
+    r = np.array(rows, dtype=np.float32, copy=True).reshape(-1, 64)
+    r[:, 12:15] = r[:, 12:15].astype(np.float16).astype(np.float32)
+    r[:, 16:61] = r[:, 16:61].astype(np.float16).astype(np.float32)
+    return r
+
+
+def conic_to_fp16(projected: np.ndarray) -> np.ndarray:
+    """Projected records with the conic (record floats [8:11]) rounded to IEEE
+    half and back: FP16 conic storage between the cull and the compositor."""
+    p = np.array(projected, dtype=np.float32, copy=True).reshape(-1, 16)
+    p[:, 8:11] = p[:, 8:11].astype(np.float16).astype(np.float32)
+    return p
+
+
 def stochastic_sample(ids: np.ndarray, projected: np.ndarray, width: int, height: int, frame_seed: float,
                       cam: np.ndarray | None = None, bg: float = 0.0, jitter=(0.0, 0.0), rgba8: bool = True):
     vp_w, vp_h, ysign = _vp(cam, width, height)
