@@ -65,6 +65,31 @@ def test_null_arguments_rejected():
     assert lib.gs_sort_pairs(None, None, None, None, 0, 0, 32, None, 0, None) == L.GS_OK
 
 
+def test_every_context_entry_rejects_a_null_context():
+    """No entry point dereferences a null context or handle (CPU: none of
+    these reach the device)."""
+    lib = L.lib()
+    bad = L.GS_ERR_BAD_ARG
+    calls = {
+        "gs_render_host": (None, None, None), "gs_upload_rows_device": (None, None, 0),
+        "gs_upload_rows_range": (None, None, 0, 0), "gs_upload_anim": (None, None, 0, None),
+        "gs_set_anim_state": (None, 0, 0, 0.0), "gs_upload_layers": (None, None, 0),
+        "gs_set_layer_weights": (None, None, 0), "gs_get_knobs": (None, None), "gs_set_knobs": (None, None),
+        "gs_set_mode": (None, 0), "gs_reset_accumulation": (None,), "gs_set_display_lut": (None, None, 0, 0.0, 1.0),
+        "gs_display": (None, None, None, 1, 1, 0.0), "gs_read_stats": (None, None),
+        "gs_debug_read": (None, 0, None, 0), "gs_profile_enable": (None, 1),
+        "gs_stage_times": (None, None, None, 0, 0), "gs_debug_wait_probe": (None, 0, 1),
+        "gs_gsanim_load": (b"x.gsanim", None), "gs_gsanim_get_info": (None, None), "gs_gsanim_rows": (None, None),
+        "gs_gsanim_deltas": (None, None, None), "gs_gsanim_layer_data": (None, None),
+        "gs_gsanim_display_lut": (None, None), "gs_gsanim_layer_name": (None, 0, None, 0),
+        "gs_gsanim_sample": (None, 0.0, None, None, None), "gs_gsanim_layer_weights": (None, 0.0, None),
+    }
+    for name, args in calls.items():
+        assert getattr(lib, name)(*args) == bad, name
+    assert lib.gs_last_error(None) == b"null context"
+    lib.gs_gsanim_free(None)
+
+
 def test_sort_scratch_size_grows_with_n():
     lib = L.lib()
     a, b = lib.gs_sort_pairs_scratch_bytes(1000), lib.gs_sort_pairs_scratch_bytes(1_000_000)
