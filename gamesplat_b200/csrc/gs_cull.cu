@@ -124,7 +124,7 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
                                                 const CamRegs& cam, int sh_degree, float sh_lod, float4* out,
                                                 float* quad_area, float* gps_points) {
     const float t = cam.ortho;
-    float4 c1 = row[1], c2 = row[2], c3 = row[3];
+    float4 c1 = row[1], c2 = row[2];
     float sx = c1.x, sy = c1.y, sz = c1.z;
     float qw = c2.x, qx = c2.y, qy = c2.z, qz = c2.w;
 
