@@ -6,8 +6,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
+#include <memory>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gs_api.h"
@@ -216,7 +219,8 @@ extern "C" int gs_pack_raw(const float* raw, uint64_t count, float* rows) {
 namespace {
 int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
     if (!path) return GS_ERR_BAD_ARG;
-    FILE* f = std::fopen(path, "rb");
+    std::unique_ptr<FILE, int (*)(FILE*)> file(std::fopen(path, "rb"), &std::fclose);   // closed on every return
+    FILE* const f = file.get();
     if (!f) return GS_ERR_BAD_ARG;
     // Header rules of src/gaussian_loader_ply.cpp:27-75: lines read 511
     // bytes at a time; any "format" line without binary_little_endian fails
@@ -233,7 +237,6 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
         while (len > 0 && (line[len - 1] == '\n' || line[len - 1] == '\r')) line[--len] = 0;
         if (!std::strcmp(line, "end_header")) { header_done = true; break; }
         if (!std::strncmp(line, "format ", 7) && !std::strstr(line, "binary_little_endian")) {
-            std::fclose(f);
             return GS_ERR_BAD_ARG;
         }
         if (!std::strncmp(line, "element vertex ", 15)) {
@@ -251,7 +254,6 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
         }
     }
     if (!header_done || vertex_count == 0) {
-        std::fclose(f);
         return GS_ERR_BAD_ARG;
     }
     int off[A_COUNT];
@@ -261,7 +263,7 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
         for (auto& p : props)
             if (p.first == nm) { off[a] = p.second; break; }
     }
-    if (off[A_X] < 0 || off[A_Y] < 0 || off[A_Z] < 0) { std::fclose(f); return GS_ERR_BAD_ARG; }
+    if (off[A_X] < 0 || off[A_Y] < 0 || off[A_Z] < 0) { return GS_ERR_BAD_ARG; }
     // scale_0, rot_0 and f_dc_0 each stand for their whole group: a file
     // that names the first without the others has no defined decode (the
     // reference reads a byte before the row for the missing ones), so it is
@@ -269,7 +271,7 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
     for (int first : {A_S0, A_R0, A_DC0}) {
         const int last = first == A_R0 ? first + 3 : first + 2;
         for (int a = first + 1; a <= last && off[first] >= 0; ++a)
-            if (off[a] < 0) { std::fclose(f); return GS_ERR_BAD_ARG; }
+            if (off[a] < 0) { return GS_ERR_BAD_ARG; }
     }
     // the body must hold every vertex (the reference's loader fails on a short read)
     const long body_at = std::ftell(f);
@@ -277,26 +279,53 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
     if (body_at >= 0 && !std::fseek(f, 0, SEEK_END)) body_end = std::ftell(f);
     if (body_end < body_at || std::fseek(f, body_at, SEEK_SET) ||
         (uint64_t)(body_end - body_at) < (uint64_t)vertex_count * (uint64_t)stride) {
-        std::fclose(f);
         return GS_ERR_BAD_ARG;
     }
-    if (!rows) { std::fclose(f); return (int64_t)vertex_count; }
+    if (!rows) { return (int64_t)vertex_count; }
     const uint64_t n = vertex_count < capacity ? vertex_count : capacity;
-    const uint64_t batch = 4096;
-    // every value is read as 4 bytes whatever its declared size: the padding
-    // keeps a narrower last property of the last row inside the buffer
-    std::vector<unsigned char> raw((size_t)batch * stride + 4, 0);
-    for (uint64_t i = 0; i < n; i += batch) {
-        uint64_t cnt = n - i < batch ? n - i : batch;
-        if (std::fread(raw.data(), stride, cnt, f) != cnt) { std::fclose(f); return GS_ERR_BAD_ARG; }
-        for (uint64_t k = 0; k < cnt; ++k) {
-            const unsigned char* v = raw.data() + k * stride;
+    // Blocks of rows: while worker threads transform block b (rows are
+    // independent, so the result does not depend on the split), this thread
+    // reads block b + 1.  Every value is read as 4 bytes whatever its
+    // declared size: the padding keeps a narrower last property of the last
+    // row inside the buffer.
+    const uint64_t batch = 65536;
+    std::vector<unsigned char> raw[2];
+    raw[0].assign((size_t)batch * stride + 4, 0);
+    raw[1].assign((size_t)batch * stride + 4, 0);
+    auto transform = [&](const unsigned char* buf, uint64_t first, uint64_t lo, uint64_t hi) {
+        for (uint64_t k = lo; k < hi; ++k) {
+            const unsigned char* v = buf + k * stride;
             pack_row([&](int a) -> const void* { return off[a] >= 0 ? v + off[a] : nullptr; },
-                     rows + (i + k) * 64);
+                     rows + (first + k) * 64);
         }
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned workers = hw > 1 ? (hw - 1 < 15 ? hw - 1 : 15) : 0;
+    uint64_t cnt = n < batch ? n : batch;
+    bool ok = std::fread(raw[0].data(), stride, cnt, f) == cnt;
+    for (uint64_t i = 0, b = 0; ok && i < n; i += cnt, b ^= 1) {
+        cnt = n - i < batch ? n - i : batch;
+        const uint64_t next = n - (i + cnt) < batch ? n - (i + cnt) : batch;
+        const unsigned char* buf = raw[b].data();
+        const uint64_t per = workers ? (cnt + workers - 1) / workers : cnt;
+        std::vector<std::thread> pool;
+        uint64_t inline_from = 0;   // rows no worker took (all of them without workers)
+        if (workers && cnt >= 2048) {
+            try {
+                pool.reserve(workers);
+                for (unsigned w = 0; w < workers && inline_from < cnt; ++w) {
+                    const uint64_t lo = inline_from, hi = lo + per < cnt ? lo + per : cnt;
+                    pool.emplace_back(transform, buf, i, lo, hi);
+                    inline_from = hi;
+                }
+            } catch (const std::exception&) {   // no memory or no more threads: the rest runs here
+            }
+        }
+        if (next) ok = std::fread(raw[b ^ 1].data(), stride, next, f) == next;
+        transform(buf, i, inline_from, cnt);
+        for (auto& t : pool) t.join();
     }
-    std::fclose(f);
-    return (int64_t)vertex_count;
+    return ok ? (int64_t)vertex_count : GS_ERR_BAD_ARG;
 }
 }  // namespace
 
