@@ -17,7 +17,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <exception>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gs_api.h"
@@ -263,10 +265,41 @@ int load(const char* path, std::vector<float>& rows) {
         if (!ar.find(*f)) return GS_ERR_FORMAT;
     if (meta.has_shN && (!ar.find(meta.shN_files[0]) || !ar.find(meta.shN_files[1]))) return GS_ERR_FORMAT;
 
-    Image means_l, means_u, scales, quats, sh0;
-    if (!ar.image(meta.means_files[0], means_l) || !ar.image(meta.means_files[1], means_u) ||
-        !ar.image(meta.scales_file, scales) || !ar.image(meta.quats_file, quats) || !ar.image(meta.sh0_file, sh0))
-        return GS_ERR_FORMAT;
+    // The images decode independently, each on its own thread; their
+    // results are then checked in the order a serial decode would meet them,
+    // so the verdict (and an allocation failure) is the serial one.
+    enum { kMeansL, kMeansU, kScales, kQuats, kSh0, kCentroids, kLabels, kImages };
+    const std::string* files[kImages] = {&meta.means_files[0], &meta.means_files[1], &meta.scales_file,
+                                         &meta.quats_file, &meta.sh0_file, &meta.shN_files[0], &meta.shN_files[1]};
+    const int count = meta.has_shN ? kImages : kCentroids;
+    Image img[kImages];
+    int state[kImages] = {};   // 1 decoded, 0 invalid, -1 out of memory
+    auto decode = [&](int k) {
+        try {
+            state[k] = ar.image(*files[k], img[k]) ? 1 : 0;
+        } catch (const std::bad_alloc&) {
+            state[k] = -1;
+        }
+    };
+    {
+        std::vector<std::thread> pool;
+        int next = 0;
+        try {
+            pool.reserve((size_t)count);
+            for (; next < count; ++next) pool.emplace_back(decode, next);
+        } catch (const std::exception&) {   // no more threads: the rest decode here
+        }
+        for (int k = next; k < count; ++k) decode(k);
+        for (auto& t : pool) t.join();
+    }
+    auto usable = [&](int k) {
+        if (state[k] < 0) throw std::bad_alloc();
+        return state[k] == 1;
+    };
+    for (int k = kMeansL; k <= kSh0; ++k)
+        if (!usable(k)) return GS_ERR_FORMAT;
+    Image &means_l = img[kMeansL], &means_u = img[kMeansU], &scales = img[kScales], &quats = img[kQuats],
+          &sh0 = img[kSh0];
     const int w = means_l.w, h = means_l.h;
     for (const Image* im : {&means_u, &scales, &quats, &sh0})
         if (im->w != w || im->h != h) return GS_ERR_FORMAT;
@@ -303,8 +336,8 @@ int load(const char* path, std::vector<float>& rows) {
     }
     if (meta.has_shN) {
         const int coeffs = meta.shN_bands == 1 ? 3 : meta.shN_bands == 2 ? 8 : 15;
-        Image centroids, labels;
-        if (!ar.image(meta.shN_files[0], centroids) || !ar.image(meta.shN_files[1], labels)) return GS_ERR_FORMAT;
+        if (!usable(kCentroids) || !usable(kLabels)) return GS_ERR_FORMAT;
+        const Image &centroids = img[kCentroids], &labels = img[kLabels];
         if ((uint64_t)n > (uint64_t)labels.w * (uint64_t)labels.h) return GS_ERR_FORMAT;
         if (centroids.w < 64 * coeffs || centroids.h < (meta.shN_count + 63) / 64) return GS_ERR_FORMAT;
         for (uint32_t i = 0; i < n; ++i) {
