@@ -35,6 +35,7 @@
 
 #include "../../include/gs_api.h"
 #include "gs_json.h"
+#include "gs_parallel.h"
 #include "gs_zip.h"
 
 struct gs_gsanim {
@@ -369,33 +370,41 @@ int load(const char* path, gs_gsanim* a) {
     if (!ply_header(bytes, a->gaussian_count, offset)) return GS_ERR_FORMAT;
     // Decode and validate every row (the reference's Gaussian checks), then
     // pack: raw order x y z, f_dc, f_rest, opacity, scale, rot (gs_pack_raw).
+    // Rows are independent: they are checked on worker threads in slices, and
+    // the asset is rejected when any row fails, whichever slice finds it.
     std::vector<float> raw((size_t)n * 59);
-    for (uint64_t i = 0; i < n; ++i) {
-        float v[62];
-        for (int k = 0; k < 62; ++k) {
-            v[k] = lef32(&bytes[offset + (size_t)i * 248 + (size_t)k * 4]);
-            if (!std::isfinite(v[k])) return GS_ERR_FORMAT;
-            if (a->version == 3 && k >= 6 && k < 54 && v[k] != 0) return GS_ERR_FORMAT;
-        }
-        for (int k = 0; k < 3; ++k) {
-            const float s = std::exp(v[55 + k]);
-            if (!std::isfinite(s) || s <= 0 || !std::isfinite(s * s)) return GS_ERR_FORMAT;
-        }
-        const float norm = std::sqrt(v[58] * v[58] + v[59] * v[59] + v[60] * v[60] + v[61] * v[61]);
-        if (!std::isfinite(norm) || norm <= 1e-8f) return GS_ERR_FORMAT;
-        // every appearance state must decode to finite coefficients
-        for (uint32_t s = 1; a->version != 3 && s < a->state_count; ++s) {
-            for (int k = 0; k < 48; ++k) {
-                const float delta = (float)a->deltas[((size_t)(s - 1) * n + i) * 48 + (size_t)k] * a->scales[k];
-                if (!std::isfinite(delta) || !std::isfinite(v[6 + k] + delta)) return GS_ERR_FORMAT;
+    const gs_gsanim& asset = *a;
+    const bool rows_ok = gs::parallel_ranges(n, 4096, [&](uint64_t lo, uint64_t hi) {
+        for (uint64_t i = lo; i < hi; ++i) {
+            float v[62];
+            for (int k = 0; k < 62; ++k) {
+                v[k] = lef32(&bytes[offset + (size_t)i * 248 + (size_t)k * 4]);
+                if (!std::isfinite(v[k])) return false;
+                if (asset.version == 3 && k >= 6 && k < 54 && v[k] != 0) return false;
             }
+            for (int k = 0; k < 3; ++k) {
+                const float s = std::exp(v[55 + k]);
+                if (!std::isfinite(s) || s <= 0 || !std::isfinite(s * s)) return false;
+            }
+            const float norm = std::sqrt(v[58] * v[58] + v[59] * v[59] + v[60] * v[60] + v[61] * v[61]);
+            if (!std::isfinite(norm) || norm <= 1e-8f) return false;
+            // every appearance state must decode to finite coefficients
+            for (uint32_t s = 1; asset.version != 3 && s < asset.state_count; ++s) {
+                for (int k = 0; k < 48; ++k) {
+                    const float delta =
+                        (float)asset.deltas[((size_t)(s - 1) * n + i) * 48 + (size_t)k] * asset.scales[k];
+                    if (!std::isfinite(delta) || !std::isfinite(v[6 + k] + delta)) return false;
+                }
+            }
+            float* r = &raw[(size_t)i * 59];
+            r[0] = v[0];
+            r[1] = v[1];
+            r[2] = v[2];
+            std::memcpy(r + 3, v + 6, 56 * sizeof(float));   // f_dc, f_rest, opacity, scale, rot
         }
-        float* r = &raw[(size_t)i * 59];
-        r[0] = v[0];
-        r[1] = v[1];
-        r[2] = v[2];
-        std::memcpy(r + 3, v + 6, 56 * sizeof(float));   // f_dc, f_rest, opacity, scale, rot
-    }
+        return true;
+    });
+    if (!rows_ok) return GS_ERR_FORMAT;
     a->rows.resize((size_t)n * 64);
     return gs_pack_raw(raw.data(), n, a->rows.data());
 }
