@@ -14,8 +14,9 @@ replicas (each rank renders its own orbit frames; no collective on the data
 path), value = total frames / max time.  `e2e` re-times K frames through
 gs_render_host (camera host->device, image device->host each frame).
 The reference arm (--impl reference) times the CPU oracle port of the same
-frame on all host cores (the reference's own CPU code covers only cull +
-sort; its cull+sort timing is reported beside it).
+frame on all host cores, on rows and cameras built by the reference's own
+loader and camera code, without loading libgs_cuda.so (the reference's own
+CPU code covers only cull + sort; its cull+sort timing is reported beside it).
 """
 from __future__ import annotations
 
@@ -132,6 +133,38 @@ def make_rows(n=3_000_000):
     return rows
 
 
+def bench_config(n, world):
+    """The workload, identical in both arms."""
+    return {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT, "mode": "alpha",
+            "output": "RGBA16F", "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (768 MB of rows), no flush"}
+
+
+def _scene_module():
+    """gamesplat_b200/scene.py (numpy only) loaded by path, so that the
+    reference arm never imports the package that wraps libgs_cuda.so."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("_bench_scene", ROOT / "gamesplat_b200" / "scene.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_inputs(n=3_000_000):
+    """Rows and orbit cameras of the benchmark workload built by the
+    reference's own CPU code only (oracle/_ref, compiled from its sources):
+    the seeded scene goes through a PLY file into gaussian_load_ply +
+    pack_gpu_gaussians, and the cameras come from camera_get_view_matrix /
+    camera_get_proj_matrix with the frame setup of src/main.cpp:1264-1281."""
+    from oracle import oracle as O
+
+    sc = _scene_module()
+    rows = O.ref_rows_from_raw(sc.room_scene(1, n))
+    cams = [O.ref_camera_uniforms(*sc.orbit_pose(k, FRAMES), WIDTH, HEIGHT) for k in range(FRAMES)]
+    return rows, cams
+
+
 def dist_setup(n_gpus):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -177,15 +210,19 @@ def reference_cull_sort(rows, cam):
 
 
 def run_reference(args):
-    world, rank, local, pg = dist_setup(args.gpus)
+    """The reference arm: the same frames on the host cores.  The reference's
+    own renderer draws through GL (unavailable on this box), so each frame is
+    the CPU oracle's restatement of that path (cull + SH + sort + composite,
+    kind "port"), with rows and cameras built by the reference's own loader
+    and camera code; the reference's own CPU cull + sort is timed beside it.
+    Rank 0 alone runs; the other ranks exit without work."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     if rank != 0:
-        if pg:
-            pg.destroy_process_group()
         return
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    rows = make_rows()
-    cams = orbit_cameras()
+    rows, cams = reference_inputs(args.gaussians)
     for i in range(args.warmup):
         cpu_frame(rows, cams[i % FRAMES])
     t0 = time.perf_counter()
@@ -194,19 +231,134 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     fps = args.steps / dt
     line = {
-        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded room3m scene, orbit cameras)",
-        "config": {"workload": WORKLOAD, "gaussians": 3_000_000, "width": WIDTH, "height": HEIGHT,
-                   "l2": "inputs larger than L2 (768 MB of rows)"},
+        "data": "synthetic (seeded room3m scene: 3M SH3 Gaussians, 120-frame orbit cameras)",
+        "config": bench_config(rows.shape[0], world),
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} full frames of the orbit, oracle cull+SH+sort+composite, "
-                                   f"OpenMP on {cores} threads"},
+                                   f"OpenMP on {cores} threads; rows and cameras from the reference's own "
+                                   f"PLY loader and camera code"},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_cpu_cull_sort": reference_cull_sort(rows, cams[0]),
     }
     print(json.dumps(line), flush=True)
+
+
+DENOISER_WEIGHTS = ROOT / "gamesplat_b200" / "denoiser_room3m.f32"
+
+
+def _ssim_psnr(a, b):
+    """PSNR (RGBA) and mean SSIM (RGB, 11-tap Gaussian window, sigma 1.5) of
+    two H x W x 4 float tensors on the device."""
+    import torch
+    import torch.nn.functional as F
+
+    mse = float(((a - b) ** 2).mean())
+    psnr = float("inf") if mse == 0 else 10.0 * np.log10(1.0 / mse)
+    k = torch.exp(-torch.arange(-5, 6, device=a.device, dtype=torch.float32) ** 2 / 4.5)
+    k = (k / k.sum()).view(1, 1, 1, 11).repeat(3, 1, 1, 1)
+
+    def blur(t):
+        t = F.conv2d(t, k, padding=(0, 5), groups=3)
+        return F.conv2d(t, k.transpose(2, 3), padding=(5, 0), groups=3)
+
+    x = a[..., :3].permute(2, 0, 1).unsqueeze(0)
+    y = b[..., :3].permute(2, 0, 1).unsqueeze(0)
+    mx, my = blur(x), blur(y)
+    sxx, syy, sxy = blur(x * x) - mx * mx, blur(y * y) - my * my, blur(x * y) - mx * my
+    c1, c2 = 0.01 ** 2, 0.03 ** 2
+    s = ((2 * mx * my + c1) * (2 * sxy + c2)) / ((mx * mx + my * my + c1) * (sxx + syy + c2))
+    return psnr, float(s[..., 5:-5, 5:-5].mean())
+
+
+def denoised_mode(r, stream, out, frame, args, rank):
+    """The denoised stochastic mode on the benchmark scene: frame time over the
+    orbit (two stochastic samples per pixel, TAA history, the denoiser and
+    the sorted-alpha fallback of tiles over the 40 dB budget), and its quality
+    against the sorted-alpha frame on held-out random orbit cameras (each
+    after `history` frames approaching it along the orbit): PSNR and SSIM with
+    and without the fallback, and the fallback rate."""
+    import torch
+
+    from gamesplat_b200 import Denoiser
+    from gamesplat_b200.train_denoiser import ORBIT_FRAMES, orbit_camera
+
+    if not DENOISER_WEIGHTS.exists():
+        return {"unavailable": "no trained denoiser parameters (gamesplat_b200/denoiser_room3m.f32)"}
+    d = Denoiser(0, stream=stream.cuda_stream)
+    d.set_params(np.fromfile(DENOISER_WEIGHTS, dtype="<f4"))
+    r.set_denoiser(d)
+    r.set_denoise_budget(1e-4, True)
+    r.set(splat_render_mode="denoised", black_background=1)
+    r.reset_stochastic_accumulation()
+    nm = min(args.steps, 20) if args.denoise_frames is None else args.denoise_frames
+    for i in range(5):
+        r.draw_frame(frame(i), out_ptr=out.data_ptr())
+    stream.synchronize()
+    r.profile(True)
+    r.stage_times(reset=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fb = 0
+    for i in range(nm):
+        r.draw_frame(frame(args.warmup + i), out_ptr=out.data_ptr())
+    e1.record(stream)
+    stream.synchronize()
+    mms = e0.elapsed_time(e1) / nm
+    st_m = {k: round(v[0] / nm, 4) for k, v in r.stage_times(reset=True).items() if v[0] > 0}
+    r.profile(False)
+    entry = {"ms_per_frame": mms, "fps": 1000.0 / mms, "frames": nm, "stages_ms_per_frame": st_m,
+             "samples_per_pixel": 2, "tile_budget_db": 40.0, "denoiser": "5 x 3x3 conv, 32 ch, U-Net skip, bf16 "
+             "tensor cores (tcgen05), fp32 accumulation"}
+    # quality on held-out cameras
+    cams = args.denoise_eval_cameras
+    if cams > 0 and rank == 0:
+        rng = np.random.default_rng(5)          # training cameras use seed 4
+        angles = rng.uniform(0.0, 2.0 * np.pi, size=cams)
+        step = 2.0 * np.pi / ORBIT_FRAMES
+        W, H = WIDTH, HEIGHT
+        alpha_r = type(r)(0, stream=stream.cuda_stream)
+        alpha_r.set(splat_render_mode="alpha", black_background=1)
+        alpha_r.upload_gaussians(_bench_rows_cache[0])
+        ref = torch.empty(H, W, 4, dtype=torch.float16, device="cuda")
+        img_fb = torch.empty(H, W, 4, dtype=torch.float16, device="cuda")
+        img_nf = torch.empty(H, W, 4, dtype=torch.float16, device="cuda")
+        ps_fb, ss_fb, ps_nf, ss_nf, fbt = [], [], [], [], []
+        tiles = ((W + 15) // 16) * ((H + 15) // 16)
+        for a in angles:
+            for budget_fb, img in ((True, img_fb), (False, img_nf)):
+                r.set_denoise_budget(1e-4, budget_fb)
+                r.reset_stochastic_accumulation()
+                for k in range(args.denoise_history, -1, -1):
+                    r.draw_frame(orbit_camera(float(a) - k * step, W, H), out_ptr=img.data_ptr())
+                if budget_fb:
+                    fbt.append(r.stats().denoise_fallback_tiles / tiles)
+            alpha_r.draw_frame(orbit_camera(float(a), W, H), out_ptr=ref.data_ptr())
+            stream.synchronize()
+            p, s_ = _ssim_psnr(img_fb.float(), ref.float())
+            ps_fb.append(p)
+            ss_fb.append(s_)
+            p, s_ = _ssim_psnr(img_nf.float(), ref.float())
+            ps_nf.append(p)
+            ss_nf.append(s_)
+        alpha_r.destroy()
+        entry["quality"] = {
+            "cameras": cams, "history_frames": args.denoise_history, "seed": 5,
+            "psnr_db_mean": float(np.mean(ps_fb)), "psnr_db_min": float(np.min(ps_fb)),
+            "ssim_mean": float(np.mean(ss_fb)), "fallback_tile_rate": float(np.mean(fbt)),
+            "frames_at_or_above_40db": float(np.mean(np.asarray(ps_fb) >= 40.0)),
+            "denoiser_only_psnr_db_mean": float(np.mean(ps_nf)), "denoiser_only_ssim_mean": float(np.mean(ss_nf)),
+            "denoiser_only_frames_at_or_above_40db": float(np.mean(np.asarray(ps_nf) >= 40.0)),
+        }
+    r.set_denoiser(None)
+    d.close()
+    return entry
+
+
+_bench_rows_cache = []
 
 
 def run_ours(args):
@@ -217,6 +369,7 @@ def run_ours(args):
     from gamesplat_b200 import Renderer, replicas
 
     rows = make_rows(args.gaussians)
+    _bench_rows_cache.append(rows)
     n = rows.shape[0]
     cams = orbit_cameras()
     stream = torch.cuda.Stream()
@@ -355,6 +508,12 @@ def run_ours(args):
             modes[mode] = entry
         r.set(splat_render_mode="alpha", black_background=1)
 
+    if not args.no_modes:
+        den = denoised_mode(r, stream, out, frame, args, rank)
+        if den is not None:
+            modes["denoised"] = den
+        r.set(splat_render_mode="alpha", black_background=1)
+
     r.destroy()
     if pg:
         pg.destroy_process_group()
@@ -408,9 +567,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded room3m scene: 3M SH3 Gaussians, 120-frame orbit cameras)",
-        "config": {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT, "mode": "alpha",
-                   "output": "RGBA16F", "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (768 MB of rows), no flush"},
+        "config": bench_config(n, world),
         "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": 160,
                 "d2h_bytes_per_step": WIDTH * HEIGHT * 8, "host_buffer": "page-locked",
                 "pageable_value": e2e_pageable_fps},
@@ -439,6 +596,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-modes", action="store_true", help="skip the stochastic and GPS mode figures")
+    ap.add_argument("--denoise-eval-cameras", type=int, default=200,
+                    help="held-out cameras of the denoised mode's quality figures (0: skip)")
+    ap.add_argument("--denoise-history", type=int, default=16,
+                    help="frames along the orbit before each held-out camera (the TAA history)")
+    ap.add_argument("--denoise-frames", type=int, default=None, help="timed denoised frames (default min(steps, 20))")
     ap.add_argument("--gaussians", type=int, default=3_000_000,
                     help="scene size (the benchmark workload is 3M; smaller only for profiling captures)")
     args = ap.parse_args()

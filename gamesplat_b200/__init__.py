@@ -7,6 +7,7 @@ The CUDA library is required: importing works without it, but every render
 call raises if libgs_cuda.so is missing.  There is no CPU fallback.
 """
 from ._lib import GsError, LIB_PATH  # noqa: F401
+from .denoiser import Denoiser  # noqa: F401
 from .gsanim import GSAnim, load_gsanim  # noqa: F401
 from .renderer import (  # noqa: F401
     MODE_NAMES,

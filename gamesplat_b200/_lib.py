@@ -24,6 +24,7 @@ GS_ERR_FORMAT = -9
 GS_MODE_ALPHA = 0
 GS_MODE_STOCHASTIC = 1
 GS_MODE_GPS = 2
+GS_MODE_DENOISED = 3
 
 GS_DEBUG_IDS = 0
 GS_DEBUG_KEYS = 1
@@ -46,6 +47,11 @@ EXPORTS = (
     "gs_gsanim_layer_name", "gs_gsanim_sample", "gs_gsanim_layer_weights", "gs_webp_decode_rgba",
     "gs_load_sog", "gs_upload_layers", "gs_set_layer_weights", "gs_debug_fail_alloc",
     "gs_load_scene", "gs_scene_device_bytes", "gs_upload_rows_range",
+    "gs_denoiser_param_count", "gs_denoiser_create", "gs_denoiser_destroy", "gs_denoiser_init_params",
+    "gs_denoiser_set_params", "gs_denoiser_get_params", "gs_denoiser_get_grads", "gs_denoiser_forward",
+    "gs_denoiser_backward", "gs_denoiser_loss", "gs_denoiser_adam", "gs_denoiser_train_step", "gs_denoiser_status",
+    "gs_conv3x3_scratch_bytes", "gs_conv3x3_bf16", "gs_conv3x3_wgrad_bf16",
+    "gs_set_denoiser", "gs_set_denoise_budget", "gs_render_features",
 )
 
 
@@ -98,7 +104,8 @@ class GsStats(C.Structure):
         ("frame_seed", C.c_uint32),
         ("error_flags", C.c_uint32),
         ("kernel_launches", C.c_uint32),
-        ("reserved", C.c_uint32 * 5),
+        ("denoise_fallback_tiles", C.c_uint32),
+        ("reserved", C.c_uint32 * 4),
     ]
 
 
@@ -194,6 +201,25 @@ def lib() -> C.CDLL:
         "gs_debug_fail_alloc": (i32, [C.c_int64]),
         "gs_load_scene": (C.c_int64, [C.c_char_p, vp, u64]),
         "gs_scene_device_bytes": (u64, [u64, C.c_uint32]),
+        "gs_denoiser_param_count": (u64, []),
+        "gs_denoiser_create": (i32, [C.POINTER(vp), i32, vp]),
+        "gs_denoiser_destroy": (None, [vp]),
+        "gs_denoiser_init_params": (i32, [vp, u64]),
+        "gs_denoiser_set_params": (i32, [vp, vp, u64]),
+        "gs_denoiser_get_params": (i32, [vp, vp, u64]),
+        "gs_denoiser_get_grads": (i32, [vp, vp, u64]),
+        "gs_denoiser_forward": (i32, [vp, vp, i32, i32, i32, vp]),
+        "gs_denoiser_backward": (i32, [vp, vp, vp, i32, i32, i32]),
+        "gs_denoiser_loss": (i32, [vp, vp, vp, vp, i32, i32, i32, f32, f32, vp, vp]),
+        "gs_denoiser_adam": (i32, [vp, f32]),
+        "gs_denoiser_train_step": (i32, [vp, vp, vp, i32, i32, i32, f32, vp]),
+        "gs_denoiser_status": (i32, [vp]),
+        "gs_conv3x3_scratch_bytes": (C.c_size_t, [i32, i32]),
+        "gs_set_denoiser": (i32, [vp, vp]),
+        "gs_set_denoise_budget": (i32, [vp, f32, i32]),
+        "gs_render_features": (i32, [vp, C.POINTER(GsCamera), vp]),
+        "gs_conv3x3_bf16": (i32, [vp, vp, i32, i32, i32, i32, i32, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp]),
+        "gs_conv3x3_wgrad_bf16": (i32, [vp, vp, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -27,6 +27,8 @@
 #include "gs_internal.h"
 #include "gs_extra.h"
 #include "gs_display.h"
+#include "gs_denoise.h"
+#include "gs_denoiser.h"
 
 using gs::FrameCounters;
 using gs::RasterRecord;
@@ -34,8 +36,8 @@ using gs::SortPlan;
 
 namespace {
 
-enum Stage { ST_CULL = 0, ST_SORT, ST_BIN, ST_TILE_SORT, ST_RASTER, ST_ACCUM, ST_GPS, ST_COUNT };
-const char* kStageNames = "cull,sort,bin,tile_sort,raster,accum,gps";
+enum Stage { ST_CULL = 0, ST_SORT, ST_BIN, ST_TILE_SORT, ST_RASTER, ST_ACCUM, ST_GPS, ST_DENOISE, ST_COUNT };
+const char* kStageNames = "cull,sort,bin,tile_sort,raster,accum,gps,denoise";
 
 struct DevBuf {
     void* p = nullptr;
@@ -109,6 +111,11 @@ struct gs_ctx {
     FrameCounters* h_fc = nullptr;  // pinned readback
     cudaEvent_t fc_event = nullptr;
     bool fc_pending = false;
+    // the frame's counters read back right after binning, while the rest of
+    // the frame is still queued: gs_render checks the tile entries there
+    FrameCounters* h_bin_fc = nullptr;
+    cudaEvent_t bin_event = nullptr;
+    bool bin_recorded = false;
     uint32_t epoch = 0;
 
     // image targets
@@ -120,6 +127,16 @@ struct gs_ctx {
     gs::StochasticTargets st{};
     gs::GpsTargets gps{};
     uint32_t gps_max_work_items = 16u * 1024u * 1024u;
+
+    // denoised mode: the attached denoiser (not owned), its input features
+    // (W x H x 16 bf16), the tiles over the error budget and its knobs
+    gs_denoiser* denoiser = nullptr;
+    __nv_bfloat16* features = nullptr;
+    size_t features_pix = 0;
+    uint32_t* fallback_tiles = nullptr;   // tiles_cap entries
+    float* tile_error = nullptr;          // tiles_cap estimated MSE per tile
+    float denoise_budget = 1.0e-4f;       // tile MSE budget: 40 dB PSNR
+    int denoise_fallback = 1;
 
     // stochastic / accumulation state (src/renderer.h:230-246)
     uint32_t frame_seed = 0;
@@ -233,6 +250,10 @@ void release_targets(gs_ctx* c) {
     dfree(c->out16);
     dfree(c->ctrl);
     dfree(c->tile_order);
+    dfree(c->features);
+    dfree(c->fallback_tiles);
+    dfree(c->tile_error);
+    c->features_pix = 0;
     c->fc = nullptr;
     gs::release_stochastic_targets(c->st);
     gs::release_gps_targets(c->gps);
@@ -254,7 +275,7 @@ cudaEvent_t take_event(gs_ctx* c) {
 // NVTX range names of the stages (the reference's profiler zones,
 // src/renderer.cpp:1890-1937,1984-2088): visible to nsys / ncu --nvtx.
 const char* const kStageRanges[ST_COUNT] = {"gs cull/project", "gs depth sort", "gs bin", "gs tile sort",
-                                            "gs raster", "gs accumulate", "gs gps splat"};
+                                            "gs raster", "gs accumulate", "gs gps splat", "gs denoise"};
 
 struct StageScope {
     gs_ctx* c;
@@ -500,7 +521,10 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = fals
         p.fc = c->fc;
         p.envelope = envelope ? 1 : 0;
         sc.add(gs::launch_bin(p, c->n, c->num_sms, c->stream));
-
+        // the entry count is final once the expansion ran
+        cudaMemcpyAsync(c->h_bin_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
+        cudaEventRecord(c->bin_event, c->stream);
+        c->bin_recorded = true;
     }
     {
         StageScope sc(c, ST_TILE_SORT);
@@ -682,6 +706,119 @@ int render_stochastic(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
     return GS_OK;
 }
 
+// TAA uniforms of a frame (shaders/accum.glsl:65-76; src/renderer.cpp:2426-2485).
+gs::TaaUniforms taa_uniforms(const gs_camera* cam, const gs_camera& prev_cam, const float inv_view[16],
+                             bool has_history, bool cam_changed) {
+    gs::TaaUniforms u{};
+    std::memcpy(u.inv_view, inv_view, sizeof(u.inv_view));
+    std::memcpy(u.prev_view, has_history ? prev_cam.view : cam->view, sizeof(u.prev_view));
+    u.viewport_orthographic[0] = cam->viewport[0];
+    u.viewport_orthographic[1] = cam->viewport[1];
+    u.viewport_orthographic[2] = cam->orthographic;
+    u.viewport_orthographic[3] = has_history ? prev_cam.orthographic : cam->orthographic;
+    u.focal_clip[0] = cam->persp_focal;
+    u.focal_clip[1] = cam->ortho_focal;
+    u.focal_clip[2] = cam->clip_y_sign;
+    u.focal_clip[3] = cam->clip_z_01;
+    u.prev_focal_clip[0] = has_history ? prev_cam.persp_focal : cam->persp_focal;
+    u.prev_focal_clip[1] = has_history ? prev_cam.ortho_focal : cam->ortho_focal;
+    u.prev_focal_clip[2] = has_history ? prev_cam.clip_y_sign : cam->clip_y_sign;
+    u.proj_z[0] = cam->proj[10];
+    u.proj_z[1] = cam->proj[14];
+    u.history_valid = has_history ? 1.0f : 0.0f;
+    u.view_changed = cam_changed ? 1.0f : 0.0f;
+    return u;
+}
+
+int ensure_denoise_targets(gs_ctx* c) {
+    int rc = gs::ensure_stochastic_targets(c->st, c->width, c->height, c->stream);
+    if (rc) return fail(c, rc, "stochastic target allocation failed");
+    const size_t npix = (size_t)c->width * c->height;
+    if (c->features_pix != npix || !c->features) {
+        dfree(c->features);
+        dfree(c->fallback_tiles);
+        dfree(c->tile_error);
+        c->features_pix = 0;
+        GS_CUDA(c, dalloc(&c->features, npix * gs::dn::kInC * sizeof(__nv_bfloat16)));
+        GS_CUDA(c, dalloc(&c->fallback_tiles, (size_t)c->tiles_cap * sizeof(uint32_t)));
+        GS_CUDA(c, dalloc(&c->tile_error, (size_t)c->tiles_cap * sizeof(float)));
+        c->features_pix = npix;
+    }
+    return GS_OK;
+}
+
+// The stochastic half of a denoised frame: two un-jittered stochastic samples
+// per pixel (seeds frame_seed + 1, + 2) from the sorted tile lists, their TAA
+// history (shaders/accum.glsl:148-178) and the denoiser's input features.
+int render_denoise_inputs(gs_ctx* c, const gs_camera* cam) {
+    int rc = ensure_denoise_targets(c);
+    if (rc) return rc;
+    const size_t npix = (size_t)c->width * c->height;
+    const bool cam_changed = c->prev_cam_valid && std::memcmp(&c->prev_cam, cam, sizeof(gs_camera)) != 0;
+    const gs_camera prev_cam = c->prev_cam;
+    bool prev_valid = c->prev_cam_valid;
+    c->prev_cam = *cam;
+    c->prev_cam_valid = true;
+    float inv_view[16];
+    if (!gs::mat4_inverse(cam->view, inv_view)) {
+        c->taa_prev_valid = false;
+        std::memcpy(inv_view, cam->view, sizeof(inv_view));
+        prev_valid = false;
+    }
+    run_cull(c);
+    run_depth_sort(c);
+    run_binning(c, 0.0f, 0.0f, 0.0f);
+    {
+        StageScope sc(c, ST_RASTER);
+        gs::RasterParams r = raster_params(c, background(c));
+        r.frame_seed = (float)(c->frame_seed + 1u);
+        r.frame_seed2 = (float)(c->frame_seed + 2u);
+        c->frame_seed += 2u;
+        r.out_rgba32f = c->st.sample;
+        r.out_depth = c->st.depth;
+        sc.add(gs::launch_raster_stochastic2(r, c->stream));
+    }
+    StageScope sa(c, ST_ACCUM);
+    const uint32_t w = c->accum_write_index & 1u, rd = w ^ 1u;
+    const bool has_history = c->taa_prev_valid && prev_valid;
+    const gs::TaaUniforms u = taa_uniforms(cam, prev_cam, inv_view, has_history, cam_changed);
+    sa.add(gs::launch_taa(c->st.sample, c->st.depth, c->st.accum[rd], c->st.xyz[rd], c->width, c->height, u,
+                          c->st.accum[w], c->st.xyz[w], c->stream));
+    c->taa_prev_valid = true;
+    c->sample_count++;
+    c->accum_write_index = w ^ 1u;
+    sa.add(gs::dn::launch_features(c->st.sample, c->st.depth, c->st.accum[w], (int)npix, c->features, c->stream));
+    return GS_OK;
+}
+
+// Denoised stochastic mode: the denoiser's estimate of the sorted-alpha
+// frame; tiles whose estimated error exceeds the budget are rendered again
+// by the sorted-alpha rasterizer from the same tile lists.
+int render_denoised(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
+    if (!c->denoiser) return fail(c, GS_ERR_BAD_ARG, "denoised mode needs a denoiser (gs_set_denoiser)");
+    if ((c->width & 1) || (c->height & 1)) return fail(c, GS_ERR_BAD_ARG, "denoised mode needs an even viewport");
+    int rc = render_denoise_inputs(c, cam);
+    if (rc) return rc;
+    {
+        StageScope sd(c, ST_DENOISE);
+        rc = gs::dn::forward(c->denoiser, c->features, 1, c->height, c->width);
+        if (rc) return fail(c, rc, "denoiser forward failed");
+        sd.add(7);
+        sd.add(gs::dn::launch_output_tiles(gs::dn::output(c->denoiser), c->features, c->width, c->height, c->tiles_x,
+                                           c->tiles_y, c->denoise_fallback ? c->denoise_budget : 3.0e38f, out,
+                                           &c->fc->fallback_tiles, c->fallback_tiles, c->tile_error, c->stream));
+    }
+    if (c->denoise_fallback) {
+        StageScope sc(c, ST_RASTER);
+        gs::RasterParams r = raster_params(c, background(c));
+        r.tile_order = c->fallback_tiles;
+        r.tile_count = &c->fc->fallback_tiles;
+        r.out_rgba16f = out;
+        sc.add(gs::launch_raster_alpha(r, c->stream));
+    }
+    return GS_OK;
+}
+
 int render_gps(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
     int rc = gs::ensure_stochastic_targets(c->st, c->width, c->height, c->stream);
     if (rc) return fail(c, rc, "stochastic target allocation failed");
@@ -813,11 +950,14 @@ int gs_create(gs_ctx** out, int device, void* stream) {
     c->knobs.linear_color = 0;
     c->knobs.write_invisible_records = 0;
     if (cudaMallocHost(reinterpret_cast<void**>(&c->h_fc), sizeof(FrameCounters)) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->fc_event, cudaEventDisableTiming) != cudaSuccess) {
+        cudaMallocHost(reinterpret_cast<void**>(&c->h_bin_fc), sizeof(FrameCounters)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->fc_event, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->bin_event, cudaEventDisableTiming) != cudaSuccess) {
         gs_destroy(c);
         return GS_ERR_OOM;
     }
     std::memset(c->h_fc, 0, sizeof(FrameCounters));
+    std::memset(c->h_bin_fc, 0, sizeof(FrameCounters));
     *out = c;
     return GS_OK;
 }
@@ -830,10 +970,12 @@ void gs_destroy(gs_ctx* c) {
     release_targets(c);
     dfree(c->display_lut);
     if (c->h_fc) cudaFreeHost(c->h_fc);
+    if (c->h_bin_fc) cudaFreeHost(c->h_bin_fc);
     if (c->h_out16) cudaFreeHost(c->h_out16);
     for (auto e : c->chunk_events)
         if (e) cudaEventDestroy(e);
     if (c->fc_event) cudaEventDestroy(c->fc_event);
+    if (c->bin_event) cudaEventDestroy(c->bin_event);
     for (auto& p : c->pending) {
         cudaEventDestroy(p.a);
         cudaEventDestroy(p.b);
@@ -850,7 +992,7 @@ int gs_get_knobs(const gs_ctx* c, gs_knobs* out) {
 
 int gs_set_knobs(gs_ctx* c, const gs_knobs* k) {
     if (!c || !k) return GS_ERR_BAD_ARG;
-    if (k->render_mode < 0 || k->render_mode > 2 || k->sh_degree < 0 || k->sh_degree > 3)
+    if (k->render_mode < 0 || k->render_mode > 3 || k->sh_degree < 0 || k->sh_degree > 3)
         return fail(c, GS_ERR_BAD_ARG, "knob out of range");
     const bool reset = k->render_mode != c->knobs.render_mode ||
                        k->gps_supersample_factor != c->knobs.gps_supersample_factor ||
@@ -863,10 +1005,23 @@ int gs_set_knobs(gs_ctx* c, const gs_knobs* k) {
 }
 
 int gs_set_mode(gs_ctx* c, int mode) {
-    if (!c || mode < 0 || mode > 2) return GS_ERR_BAD_ARG;
+    if (!c || mode < 0 || mode > 3) return GS_ERR_BAD_ARG;
     gs_knobs k = c->knobs;
     k.render_mode = mode;
     return gs_set_knobs(c, &k);
+}
+
+int gs_set_denoiser(gs_ctx* c, gs_denoiser* d) {
+    if (!c) return GS_ERR_BAD_ARG;
+    c->denoiser = d;
+    return GS_OK;
+}
+
+int gs_set_denoise_budget(gs_ctx* c, float tile_mse, int fallback) {
+    if (!c || !(tile_mse >= 0.0f)) return GS_ERR_BAD_ARG;
+    c->denoise_budget = tile_mse;
+    c->denoise_fallback = fallback ? 1 : 0;
+    return GS_OK;
 }
 
 int gs_reset_accumulation(gs_ctx* c) {
@@ -1171,19 +1326,47 @@ int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
         rc = ensure_entries(c, default_entry_cap(c->n));
         if (rc) return rc;
     }
-    nvtxRangePushA("gs_render");
-    begin_frame(c, cam);
     uint16_t* o = static_cast<uint16_t*>(out);
-    switch (c->knobs.render_mode) {
-        case GS_MODE_ALPHA: rc = render_alpha(c, o); break;
-        case GS_MODE_STOCHASTIC: rc = render_stochastic(c, cam, o); break;
-        default: rc = render_gps(c, cam, o); break;
+    // The (tile, splat) entries of a frame are counted on the device.  The
+    // host reads the count back as soon as the binning has run (the rest of
+    // the frame stays queued behind it) and, if the entries did not fit,
+    // grows the buffers and renders the frame again, restoring the state a
+    // frame advances; so a frame that returns GS_OK is never truncated.
+    for (int attempt = 0;; ++attempt) {
+        const uint32_t seed = c->frame_seed, samples = c->sample_count, widx = c->accum_write_index;
+        const gs_camera pcam = c->prev_cam;
+        const bool pvalid = c->prev_cam_valid, tvalid = c->taa_prev_valid;
+        nvtxRangePushA("gs_render");
+        begin_frame(c, cam);
+        c->bin_recorded = false;
+        switch (c->knobs.render_mode) {
+            case GS_MODE_ALPHA: rc = render_alpha(c, o); break;
+            case GS_MODE_STOCHASTIC: rc = render_stochastic(c, cam, o); break;
+            case GS_MODE_DENOISED: rc = render_denoised(c, cam, o); break;
+            default: rc = render_gps(c, cam, o); break;
+        }
+        end_frame(c);
+        nvtxRangePop();
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+        if (rc || !c->bin_recorded) return rc;
+        GS_CUDA(c, cudaEventSynchronize(c->bin_event));
+        const uint32_t over = c->h_bin_fc->tile_overflow;
+        if (!over) return GS_OK;
+        GS_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->fc_pending = false;
+        const uint64_t need = (uint64_t)c->h_bin_fc->tile_entries + over;
+        if (attempt >= 3 || c->entry_cap >= 0x3FFFFFFFu)
+            return fail(c, GS_ERR_TOO_LARGE, "tile entries beyond the largest entry buffer: frame truncated");
+        rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(need + need / 4 + 1024, 0x3FFFFFFFull));
+        if (rc) return rc;
+        c->frame_seed = seed;
+        c->sample_count = samples;
+        c->accum_write_index = widx;
+        c->prev_cam = pcam;
+        c->prev_cam_valid = pvalid;
+        c->taa_prev_valid = tvalid;
     }
-    end_frame(c);
-    nvtxRangePop();
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
-    return rc;
 }
 
 int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
@@ -1207,56 +1390,78 @@ int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
         GS_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&c->h_out16), bytes));
         c->h_out16_bytes = bytes;
     }
-    for (int attempt = 0; attempt < 3; ++attempt) {
-        // A re-render replays the same frame: restore the state a frame advances.
+    // Alpha frames into page-locked memory: the rasterizer writes the pixels
+    // straight into the host buffer (mapped, over PCIe), so the transfer
+    // overlaps the raster instead of following it.  gs_render grows the tile
+    // entries and re-renders the frame itself when they overflow.
+    void* mapped = nullptr;
+    const bool direct = pinned_out && c->knobs.render_mode == GS_MODE_ALPHA &&
+                        cudaHostGetDevicePointer(&mapped, host_out, 0) == cudaSuccess && mapped;
+    cudaGetLastError();
+    rc = gs_render(c, cam, direct ? mapped : static_cast<void*>(c->out16));
+    if (rc) return rc;
+    if (direct) {
+        GS_CUDA(c, cudaStreamSynchronize(c->stream));   // written by the frame's kernels
+    } else if (pinned_out) {
+        GS_CUDA(c, cudaMemcpyAsync(host_out, c->out16, bytes, cudaMemcpyDeviceToHost, c->stream));
+        GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    } else {
+        // eight chunks, each with an event, so the host copies chunk i out of
+        // the staging buffer while the copy engine brings in chunk i + 1
+        for (int k = 0; k < 8; ++k) {
+            if (!c->chunk_events[k])
+                GS_CUDA(c, cudaEventCreateWithFlags(&c->chunk_events[k], cudaEventDisableTiming));
+            const size_t b0 = bytes * k / 8, b1 = bytes * (k + 1) / 8;
+            GS_CUDA(c, cudaMemcpyAsync(reinterpret_cast<char*>(c->h_out16) + b0,
+                                       reinterpret_cast<const char*>(c->out16) + b0, b1 - b0,
+                                       cudaMemcpyDeviceToHost, c->stream));
+            GS_CUDA(c, cudaEventRecord(c->chunk_events[k], c->stream));
+        }
+        for (int k = 0; k < 8; ++k) {
+            const size_t b0 = bytes * k / 8, b1 = bytes * (k + 1) / 8;
+            GS_CUDA(c, cudaEventSynchronize(c->chunk_events[k]));
+            std::memcpy(reinterpret_cast<char*>(host_out) + b0, reinterpret_cast<const char*>(c->h_out16) + b0,
+                        b1 - b0);
+        }
+    }
+    GS_CUDA(c, cudaEventSynchronize(c->fc_event));
+    c->fc_pending = false;
+    if (c->h_fc->error_flags & ~(uint32_t)gs::kErrTileOverflow)
+        return fail(c, GS_ERR_DEVICE_TIMEOUT, "a device-side wait ran out");
+    return GS_OK;
+}
+
+int gs_render_features(gs_ctx* c, const gs_camera* cam, void* features_out) {
+    if (!c || !cam || !features_out) return GS_ERR_BAD_ARG;
+    if (!gl_clip_convention(cam)) return fail(c, GS_ERR_BAD_ARG, "only the GL clip convention is drawn");
+    if (!c->n) return fail(c, GS_ERR_NO_SCENE, "no scene uploaded");
+    cudaSetDevice(c->device);
+    int w = 0, h = 0;
+    int rc = viewport_dims(c, cam, &w, &h);
+    if (rc) return rc;
+    if ((w & 1) || (h & 1)) return fail(c, GS_ERR_BAD_ARG, "the denoiser input needs an even viewport");
+    if ((rc = ensure_targets(c, w, h))) return rc;
+    if ((rc = check_previous_frame(c))) return rc;
+    if (!c->entry_cap && (rc = ensure_entries(c, default_entry_cap(c->n)))) return rc;
+    for (int attempt = 0;; ++attempt) {
         const uint32_t seed = c->frame_seed, samples = c->sample_count, widx = c->accum_write_index;
         const gs_camera pcam = c->prev_cam;
         const bool pvalid = c->prev_cam_valid, tvalid = c->taa_prev_valid;
-        // Alpha frames into page-locked memory: the rasterizer writes the
-        // pixels straight into the host buffer (mapped, over PCIe), so the
-        // transfer overlaps the raster instead of following it.
-        void* mapped = nullptr;
-        const bool direct = pinned_out && c->knobs.render_mode == GS_MODE_ALPHA &&
-                            cudaHostGetDevicePointer(&mapped, host_out, 0) == cudaSuccess && mapped;
-        cudaGetLastError();
-        rc = gs_render(c, cam, direct ? mapped : static_cast<void*>(c->out16));
+        begin_frame(c, cam);
+        c->bin_recorded = false;
+        rc = render_denoise_inputs(c, cam);
+        end_frame(c);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
         if (rc) return rc;
-        if (direct) {
-            // written by the frame's kernels
-        } else if (pinned_out) {
-            GS_CUDA(c, cudaMemcpyAsync(host_out, c->out16, bytes, cudaMemcpyDeviceToHost, c->stream));
-        } else {
-            // eight chunks, each with an event, so the host copies chunk i out of
-            // the staging buffer while the copy engine brings in chunk i + 1
-            for (int k = 0; k < 8; ++k) {
-                if (!c->chunk_events[k])
-                    GS_CUDA(c, cudaEventCreateWithFlags(&c->chunk_events[k], cudaEventDisableTiming));
-                const size_t b0 = bytes * k / 8, b1 = bytes * (k + 1) / 8;
-                GS_CUDA(c, cudaMemcpyAsync(reinterpret_cast<char*>(c->h_out16) + b0,
-                                           reinterpret_cast<const char*>(c->out16) + b0, b1 - b0,
-                                           cudaMemcpyDeviceToHost, c->stream));
-                GS_CUDA(c, cudaEventRecord(c->chunk_events[k], c->stream));
-            }
-        }
-        GS_CUDA(c, cudaEventSynchronize(c->fc_event));   // the frame's counters (recorded before the image copy)
-        c->fc_pending = false;
-        if (!c->h_fc->tile_overflow) {
-            if (!pinned_out) {
-                for (int k = 0; k < 8; ++k) {
-                    const size_t b0 = bytes * k / 8, b1 = bytes * (k + 1) / 8;
-                    GS_CUDA(c, cudaEventSynchronize(c->chunk_events[k]));
-                    std::memcpy(reinterpret_cast<char*>(host_out) + b0, reinterpret_cast<const char*>(c->h_out16) + b0,
-                                b1 - b0);
-                }
-            } else {
-                GS_CUDA(c, cudaStreamSynchronize(c->stream));
-            }
-            break;
-        }
+        GS_CUDA(c, cudaEventSynchronize(c->bin_event));
+        const uint32_t over = c->h_bin_fc->tile_overflow;
+        if (!over) break;
         GS_CUDA(c, cudaStreamSynchronize(c->stream));
-        uint64_t need = (uint64_t)c->h_fc->tile_entries + c->h_fc->tile_overflow;
-        rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(need + need / 4 + 1024, 0x3FFFFFFFull));
-        if (rc) return rc;
+        if (attempt >= 3 || c->entry_cap >= 0x3FFFFFFFu)
+            return fail(c, GS_ERR_TOO_LARGE, "tile entries beyond the largest entry buffer: frame truncated");
+        const uint64_t need = (uint64_t)c->h_bin_fc->tile_entries + over;
+        if ((rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(need + need / 4 + 1024, 0x3FFFFFFFull)))) return rc;
         c->frame_seed = seed;
         c->sample_count = samples;
         c->accum_write_index = widx;
@@ -1264,14 +1469,8 @@ int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
         c->prev_cam_valid = pvalid;
         c->taa_prev_valid = tvalid;
     }
-    if (c->h_fc->tile_overflow && !pinned_out) {
-        // still overflowing after the retries: hand back the last frame as is
-        // (gs_stats reports the overflow)
-        GS_CUDA(c, cudaStreamSynchronize(c->stream));
-        std::memcpy(host_out, c->h_out16, bytes);
-    }
-    if (c->h_fc->error_flags & ~(uint32_t)gs::kErrTileOverflow)
-        return fail(c, GS_ERR_DEVICE_TIMEOUT, "a device-side wait ran out");
+    GS_CUDA(c, cudaMemcpyAsync(features_out, c->features, c->features_pix * gs::dn::kInC * sizeof(__nv_bfloat16),
+                               cudaMemcpyDeviceToDevice, c->stream));
     return GS_OK;
 }
 
@@ -1293,6 +1492,7 @@ int gs_read_stats(gs_ctx* c, gs_stats* s) {
     s->frame_seed = c->frame_seed;
     s->error_flags = f.error_flags;
     s->kernel_launches = c->last_launches;
+    s->denoise_fallback_tiles = f.fallback_tiles;
     return (f.error_flags & ~(uint32_t)gs::kErrTileOverflow) ? GS_ERR_DEVICE_TIMEOUT : GS_OK;
 }
 

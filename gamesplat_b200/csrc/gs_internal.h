@@ -32,7 +32,8 @@ struct FrameCounters {
     uint32_t tile_overflow;      // entries that did not fit
     uint32_t gps_work[2];        // [0] requested work items, [1] overflow (gps.glsl work_count)
     uint32_t raster_ticket;
-    uint32_t pad[2];
+    uint32_t fallback_tiles;     // denoised mode: tiles over the error budget
+    uint32_t pad[1];
 };
 
 // Device-resident plan of one radix sort, written by its plan kernel from the
@@ -179,11 +180,13 @@ struct RasterParams {
     const SortPlan* tile_plan;       // tile-sorted entry values at tile_plan->vfinal
     const uint2* tile_ranges;        // [start, end) per tile
     const uint32_t* tile_order;      // tiles by descending work (CTA b rasterizes tile_order[b])
+    const uint32_t* tile_count;      // optional: CTAs b >= *tile_count do nothing (a tile list of the frame)
     int width, height, tiles_x, tiles_y;
     float bg;
     // stochastic mode (envelope records): the sample's jitter and seed, and
     // the viewport of the quad computation
     float jitter_x, jitter_y, frame_seed;
+    float frame_seed2;               // two-sample mode: the second sample's seed (frame_seed is the first's)
     float vp_w, vp_h, clip_y_sign;
     uint16_t* out_rgba16f;           // width*height*4 halves, top row first
     float4* out_rgba32f;             // optional float copy (stochastic sample), top row first
@@ -226,6 +229,7 @@ int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint3
 int launch_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order, cudaStream_t s);
 int launch_raster_alpha(const RasterParams& p, cudaStream_t s);
 int launch_raster_stochastic(const RasterParams& p, cudaStream_t s);
+int launch_raster_stochastic2(const RasterParams& p, cudaStream_t s);
 
 int launch_wait_probe(const unsigned long long* status, FrameCounters* fc, uint32_t epoch, int which, uint32_t limit,
                       cudaStream_t s);

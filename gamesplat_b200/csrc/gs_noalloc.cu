@@ -18,13 +18,18 @@
 // can reach host memory, silently use the wrong memory).  The device address
 // is looked up with cudaGetSymbolAddress once per device, with that device
 // current, on the first call made on that device; that first call should
-// therefore come before any stream capture.
+// therefore come before any stream capture.  The address is kept together
+// with the id of the CUDA context it belongs to: if the device's primary
+// context has been reset since (cudaDeviceReset), the module and its array
+// were loaded anew in a new context, so the next call looks the address up
+// again instead of using a stale one.
 //
 // All calls share the one array and it keeps the previous call's contents:
 // each call clears the parts that must start at zero (sort plan, histograms,
 // look-back words) on its stream before using them.  Calls that overlap on
 // the GPU (different streams or host threads) race on the array and corrupt
 // each other's results; callers must serialise them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -48,7 +53,33 @@ static __device__ __align__(256) unsigned char g_sort_scratch[kNoAllocScratchByt
 
 constexpr int kMaxDevices = 64;
 void* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};   // id of the context each address was looked up in
 std::mutex g_setup_mutex;
+
+// Driver entry points reached through the runtime (no link against libcuda).
+void* driver_entry(const char* name) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+// The unique id (cuCtxGetId; never reused within a process) of the context
+// current on this thread; 0 if there is none.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = reinterpret_cast<GetCurrent>(driver_entry("cuCtxGetCurrent"));
+    static GetId get_id = reinterpret_cast<GetId>(driver_entry("cuCtxGetId"));
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 
 }  // namespace
 
@@ -59,10 +90,18 @@ extern "C" int gs_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* va
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return GS_ERR_CUDA;
     if (dev < 0 || dev >= kMaxDevices) return GS_ERR_BAD_ARG;
+    // Make the device's primary context current (cudaSetDevice initialises
+    // it), so that the context read below is the one the sort will run in.
+    if (cudaSetDevice(dev) != cudaSuccess) {
+        cudaGetLastError();
+        return GS_ERR_CUDA;
+    }
+    const unsigned long long ctx = current_context_id();
+    if (!ctx) return GS_ERR_CUDA;
     void* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_addr[dev]) {
+        if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
             void* addr = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&addr, g_sort_scratch);
             if (e != cudaSuccess || !addr) {
@@ -70,6 +109,7 @@ extern "C" int gs_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* va
                 return GS_ERR_CUDA;
             }
             g_scratch_addr[dev] = addr;
+            g_scratch_ctx[dev] = ctx;
         }
         scratch = g_scratch_addr[dev];
     }

@@ -35,6 +35,13 @@
 // the bounds of RasterRecord; alpha = min(2^(s * -0.5 log2(e) + log2(opacity)),
 // 0.99) uses the hardware exp2.
 //
+// Two-sample mode (the input of the denoised mode): the stochastic sample
+// rule below for two seeds at once, on un-jittered records (the alpha
+// binning), alpha evaluated once per (pixel, splat) and hashed per seed; a
+// pixel stops when both samples are decided.  Writes the mean colour of the
+// two samples (background where none kept), the fraction that kept a
+// fragment and the mean window depth (1 where none kept), all in float.
+//
 // Stochastic mode: a fragment is kept iff hash13(fragcoord, id + seed) <
 // alpha; the depth test (LESS, writes on) keeps the kept fragment with the
 // smallest (D24 depth, instance index).  Walking front to back, a pixel stops
@@ -90,6 +97,65 @@ __device__ __forceinline__ void stoch_step(StochState& S, float s, float opacity
         S.g = g;
         S.b = b;
     }
+}
+
+// Two samples of one pixel (denoised mode): the kept fragment of each seed.
+struct Stoch2 {
+    StochState s[2];
+    bool done[2];
+};
+
+__device__ __forceinline__ void stoch2_init(Stoch2& P, bool inside) {
+    for (int k = 0; k < 2; ++k) {
+        P.s[k] = {16777215u, 0xFFFFFFFFu, 0.0f, 0.0f, 0.0f};
+        P.done[k] = !inside;
+    }
+}
+
+// One splat into both samples of a pixel: alpha once, one hash per seed.
+__device__ __forceinline__ void stoch2_step(Stoch2& P, bool live, float sq, float opacity, float fcx, float fcy,
+                                            float hz0, float hz1, uint32_t z24, uint32_t id, float r, float g,
+                                            float b) {
+    bool want[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+        want[k] = live && !P.done[k] &&
+                  (z24 < P.s[k].best_d24 || (z24 == P.s[k].best_d24 && id < P.s[k].best_id));
+    if (!(want[0] || want[1])) return;
+    const float alpha = g_min(mul(opacity, det_expf(mul(-0.5f, sq))), 0.99f);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (want[k] && hash13(fcx, fcy, k ? hz1 : hz0) < alpha) {
+            P.s[k].best_d24 = z24;
+            P.s[k].best_id = id;
+            P.s[k].r = r;
+            P.s[k].g = g;
+            P.s[k].b = b;
+        }
+    }
+}
+
+__device__ __forceinline__ void stoch2_retire(Stoch2& P, uint32_t z24, uint32_t margin) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+        if (P.s[k].best_id != 0xFFFFFFFFu && z24 > P.s[k].best_d24 + margin) P.done[k] = true;
+}
+
+__device__ __forceinline__ void write_pixel_stoch2(const RasterParams& p, int px, int py, const Stoch2& P) {
+    const size_t o = (size_t)(p.height - 1 - py) * p.width + px;
+    float c[2][3], a[2], d[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const bool kept = P.s[k].best_id != 0xFFFFFFFFu;
+        c[k][0] = kept ? P.s[k].r : p.bg;
+        c[k][1] = kept ? P.s[k].g : p.bg;
+        c[k][2] = kept ? P.s[k].b : p.bg;
+        a[k] = kept ? 1.0f : 0.0f;
+        d[k] = __fdiv_rn((float)P.s[k].best_d24, 16777215.0f);
+    }
+    p.out_rgba32f[o] = make_float4(mul(add(c[0][0], c[1][0]), 0.5f), mul(add(c[0][1], c[1][1]), 0.5f),
+                                   mul(add(c[0][2], c[1][2]), 0.5f), mul(add(a[0], a[1]), 0.5f));
+    p.out_depth[o] = mul(add(d[0], d[1]), 0.5f);
 }
 
 __device__ __forceinline__ void write_rgba16f(uint16_t* out, size_t o, float r, float g, float b, float a) {
@@ -152,7 +218,7 @@ __device__ __forceinline__ float min_q_box(float A, float B, float C, float X0, 
 // (w & 1, w >> 1); lane l shades pixels (l & 7, l >> 3) and (l & 7, (l >> 3) + 4)
 // of it: the two pixels share a column, hence dx, the column test and the
 // first term of the Gaussian exponent.
-template <int kMode>  // 0 = alpha, 1 = stochastic
+template <int kMode>  // 0 = alpha, 1 = stochastic, 2 = two un-jittered stochastic samples
 __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) {
     __shared__ __align__(128) RasterRecord s_rec[2][kBatch];
     __shared__ __align__(8) uint64_t s_bar[2];
@@ -160,6 +226,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     __shared__ uint8_t s_mask[kBatch];
     __shared__ float4 s_cen[kMode == 1 ? kBatch : 1];   // stochastic: jittered centre and hash z of the sample
 
+    if (p.tile_count && blockIdx.x >= *p.tile_count) return;
     const uint32_t tile = p.tile_order[blockIdx.x];
     const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -188,6 +255,11 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     float2 C0 = f2(0.0f), C1 = f2(0.0f), C2 = f2(0.0f);
     StochState S0 = {16777215u, 0xFFFFFFFFu, 0.0f, 0.0f, 0.0f}, S1 = S0;
     bool sdone0 = !in0, sdone1 = !in1;
+    Stoch2 P0, P1;
+    if (kMode == 2) {
+        stoch2_init(P0, in0);
+        stoch2_init(P1, in1);
+    }
     bool failed = false;
     const uint32_t nb = (n + kBatch - 1) / kBatch;
     uint32_t phase0 = 0, phase1 = 0;
@@ -204,6 +276,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     };
     auto pixels_done = [&]() -> bool {
         if (kMode == 0) return fmaxf(T.x, T.y) < kTransmittanceMin;
+        if (kMode == 2) return P0.done[0] && P0.done[1] && P1.done[0] && P1.done[1];
         return sdone0 && sdone1;
     };
 
@@ -348,6 +421,17 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
                     C2 = __ffma2_rn(w, f2(q2.y), C2);
                     T = __ffma2_rn(w, f2(-1.0f), T);
                     if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
+                } else if (kMode == 2) {
+                    const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
+                    const uint32_t z24 = q3.x, id = q3.y;
+                    stoch2_retire(P0, z24, kDepthMargin);
+                    stoch2_retire(P1, z24, kDepthMargin);
+                    if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
+                    const float2 q2 = reinterpret_cast<const float2*>(recs + j)[4];
+                    const float op = __uint_as_float(q3.w);
+                    const float hz0 = add((float)id, p.frame_seed), hz1 = add((float)id, p.frame_seed2);
+                    stoch2_step(P0, live0, sq.x, op, fcx, fcy0, hz0, hz1, z24, id, q1.w, q2.x, q2.y);
+                    stoch2_step(P1, live1, sq.y, op, fcx, fcy1, hz0, hz1, z24, id, q1.w, q2.x, q2.y);
                 } else {
                     const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
                     const uint32_t z24 = q3.x, id = q3.y;
@@ -381,6 +465,9 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         const float2 r = __ffma2_rn(T, bg, C0), g = __ffma2_rn(T, bg, C1), bb = __ffma2_rn(T, bg, C2);
         if (in0) write_rgba16f(p.out_rgba16f, o0, r.x, g.x, bb.x, 1.0f - T.x);
         if (in1) write_rgba16f(p.out_rgba16f, o1, r.y, g.y, bb.y, 1.0f - T.y);
+    } else if (kMode == 2) {
+        if (in0) write_pixel_stoch2(p, px, py0, P0);
+        if (in1) write_pixel_stoch2(p, px, py1, P1);
     } else {
         if (in0) write_pixel_stoch(p, px, py0, S0);
         if (in1) write_pixel_stoch(p, px, py1, S1);
@@ -391,6 +478,13 @@ int launch_raster_alpha(const RasterParams& p, cudaStream_t s) {
     const uint32_t tiles = (uint32_t)p.tiles_x * (uint32_t)p.tiles_y;
     if (tiles == 0) return 0;
     raster_kernel<0><<<tiles, kRasterThreads, 0, s>>>(p);
+    return 1;
+}
+
+int launch_raster_stochastic2(const RasterParams& p, cudaStream_t s) {
+    const uint32_t tiles = (uint32_t)p.tiles_x * (uint32_t)p.tiles_y;
+    if (tiles == 0) return 0;
+    raster_kernel<2><<<tiles, kRasterThreads, 0, s>>>(p);
     return 1;
 }
 

@@ -20,7 +20,8 @@ import numpy as np
 
 from . import _lib as L
 
-MODE_NAMES = {"alpha": L.GS_MODE_ALPHA, "stochastic": L.GS_MODE_STOCHASTIC, "gps": L.GS_MODE_GPS}
+MODE_NAMES = {"alpha": L.GS_MODE_ALPHA, "stochastic": L.GS_MODE_STOCHASTIC, "gps": L.GS_MODE_GPS,
+              "denoised": L.GS_MODE_DENOISED}
 KNOB_FIELDS = [f for f, _ in L.GsKnobs._fields_ if f != "reserved"]
 
 
@@ -215,6 +216,23 @@ class Renderer:
             return False
         L.check(st, "gs_set_gps_budget", self._ctx)
         return True
+
+    # -- denoised mode ---------------------------------------------------------
+    def set_denoiser(self, denoiser) -> None:
+        """Attach a gamesplat_b200.denoiser.Denoiser (kept alive by the caller) for the denoised mode."""
+        self._denoiser = denoiser
+        L.check(L.lib().gs_set_denoiser(self._ctx, denoiser.handle if denoiser is not None else None),
+                "gs_set_denoiser", self._ctx)
+
+    def set_denoise_budget(self, tile_mse: float = 1e-4, fallback: bool = True) -> None:
+        L.check(L.lib().gs_set_denoise_budget(self._ctx, float(tile_mse), int(bool(fallback))),
+                "gs_set_denoise_budget", self._ctx)
+
+    def render_features(self, cam, features_ptr: int) -> None:
+        """The denoiser input of the next frame into device memory (H x W x 16 bf16)."""
+        c = camera_from_array(cam)
+        L.check(L.lib().gs_render_features(self._ctx, C.byref(c), C.c_void_p(features_ptr)), "gs_render_features",
+                self._ctx)
 
     def reset_stochastic_accumulation(self) -> None:
         L.check(L.lib().gs_reset_accumulation(self._ctx), "gs_reset_accumulation", self._ctx)

@@ -51,7 +51,9 @@ typedef enum gs_status {
 typedef enum gs_render_mode {
     GS_MODE_ALPHA = 0,            /* AlphaBlendSorted */
     GS_MODE_STOCHASTIC = 1,       /* StochasticSplats */
-    GS_MODE_GPS = 2               /* GaussianPointSplatting */
+    GS_MODE_GPS = 2,              /* GaussianPointSplatting */
+    GS_MODE_DENOISED = 3          /* two-sample stochastic frame + denoiser (gs_set_denoiser), tiles over
+                                     the error budget rendered sorted-alpha; no counterpart in the reference */
 } gs_render_mode;
 
 /* CameraUniforms, byte for byte (src/camera.h:23-38): 40 floats, 160 bytes. */
@@ -98,7 +100,8 @@ typedef struct gs_stats {
     uint32_t gaussian_count;
     uint32_t visible_count;
     uint32_t tile_entries;               /* (16x16 tile, splat) pairs of the last frame */
-    uint32_t tile_overflow;              /* entries that did not fit (frame re-rendered by gs_render_host) */
+    uint32_t tile_overflow;              /* entries that did not fit in the frame's last pass (gs_render grows
+                                            the buffers and re-renders, so 0 after a GS_OK frame) */
     uint32_t diagnostics[8];             /* shaders/cull.glsl:296-318 counters, if enabled */
     uint32_t gps_requested_work_items;
     uint32_t gps_budget_exhausted;
@@ -107,7 +110,8 @@ typedef struct gs_stats {
     uint32_t frame_seed;
     uint32_t error_flags;                /* device error bits (bounded waits that ran out) */
     uint32_t kernel_launches;            /* kernels launched by the last gs_render */
-    uint32_t reserved[5];
+    uint32_t denoise_fallback_tiles;     /* denoised mode: 16x16 tiles rendered again sorted-alpha */
+    uint32_t reserved[4];
 } gs_stats;
 
 /* gs_debug_read selectors (reference buffers, src/renderer.cpp:922-1058). */
@@ -123,6 +127,7 @@ typedef enum gs_debug_buffer {
 } gs_debug_buffer;
 
 typedef struct gs_ctx gs_ctx;
+typedef struct gs_denoiser gs_denoiser;   /* the stochastic-splat denoiser, see gs_denoiser_create */
 
 /* renderer_init (src/renderer.h:249): create a context on `device`, issuing
  * work on `stream` (cudaStream_t, may be NULL).  Knobs get the reference
@@ -189,6 +194,24 @@ int gs_set_layer_weights(gs_ctx* ctx, const float* weights, uint32_t count);
  * (src/renderer.cpp:1076-1123). */
 int gs_set_gps_budget(gs_ctx* ctx, uint32_t max_work_items);
 
+/* Denoised mode (GS_MODE_DENOISED; no counterpart in the reference): the
+ * denoiser the context uses (not owned; NULL detaches), and the error
+ * budget: a 16x16 tile whose estimated mean squared error (over RGBA)
+ * reaches tile_mse (>= 0; default 1e-4, i.e. 40 dB PSNR) is rendered again by
+ * the sorted-alpha rasterizer when fallback != 0 (default); tile_mse 0 sends
+ * every tile to the sorted-alpha rasterizer. */
+int gs_set_denoiser(gs_ctx* ctx, gs_denoiser* denoiser);
+int gs_set_denoise_budget(gs_ctx* ctx, float tile_mse, int fallback);
+
+/* The denoiser's input of the next frame, without the denoiser: two
+ * un-jittered stochastic samples per pixel (seeds frame_seed + 1 and + 2,
+ * the kept-fragment rule of shaders/splat.glsl:127-145 on the sorted tile
+ * lists), their TAA history (shaders/accum.glsl:148-178, advanced as a
+ * denoised frame advances it) and the features, written to features_out
+ * (device, height x width x 16 bf16, top row first; even viewport).  For
+ * generating training pairs. */
+int gs_render_features(gs_ctx* ctx, const gs_camera* cam, void* features_out);
+
 /* renderer_reset_stochastic_accumulation (src/renderer.h:261). */
 int gs_reset_accumulation(gs_ctx* ctx);
 
@@ -210,7 +233,14 @@ uint64_t gs_scene_device_bytes(uint64_t count, uint32_t gps_work_items);
  * Only the GL clip convention (clip_y_sign 1, clip_z_01 0; the non-WGPU
  * branch of src/main.cpp:1275-1281) is drawn: other cameras return
  * GS_ERR_BAD_ARG, since the WGPU backend's top-left fragment origin is not
- * what the kernels rasterise. */
+ * what the kernels rasterise.
+ * Alpha and stochastic frames count their (tile, splat) entries on the
+ * device; the call waits for that count (read back right after the binning,
+ * with the rest of the frame still queued, as the reference's draw_frame
+ * reads back inside the frame) and, when the entries did not fit, grows the
+ * buffers and renders the frame again before returning.  A GS_OK frame is
+ * therefore complete; GS_ERR_TOO_LARGE if the entries exceed the largest
+ * buffer (2^30 - 1 entries), GS_ERR_OOM if growing fails. */
 int gs_render(gs_ctx* ctx, const gs_camera* cam, void* rgba16f_out);
 
 /* gs_render into host memory: includes the host->device camera copy and the
@@ -398,10 +428,81 @@ size_t gs_sort_pairs_scratch_bytes(uint32_t n);
  * [begin_bit, end_bit): the order of the reference's 8-bit LSD passes
  * (shaders/sort.glsl:26-163, driven by src/renderer.cpp:1873-1962).
  * keys_in/vals_in are left unchanged; results go to keys_out/vals_out.
- * scratch: device memory of gs_sort_pairs_scratch_bytes(n) bytes. */
+ * scratch: device memory of gs_sort_pairs_scratch_bytes(n) bytes.
+ * Stream-ordered and never synchronising, so a bounded device wait that ran
+ * out (a look-back that gave up, which needs a stalled GPU) is not reported
+ * here; renders report theirs through gs_stats.error_flags. */
 int gs_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                   uint32_t* vals_out, uint32_t n, int begin_bit, int end_bit, void* scratch,
                   size_t scratch_bytes, void* stream);
+
+/* ---- stochastic-splat denoiser (the learned half of the render modes) ---- */
+
+/* A 5-layer, 32-channel convolutional denoiser with a U-Net skip that turns
+ * a two-sample stochastic frame (shaders/splat.glsl:127-145 without the
+ * sort) plus its reprojected history (shaders/accum.glsl:148-178) into an
+ * estimate of the sorted-alpha frame.  No counterpart in the reference,
+ * which has no denoiser; its stochastic and sorted-alpha modes are the input
+ * and the training target.
+ *
+ * Tensors are NHWC in device memory.  Input x: n x h x w x 16 bf16 (noisy RGB,
+ * alpha, expected depth, reprojected history RGB, 8 zero channels); output:
+ * n x h x w x 16 f32 (RGBA residual over (history RGB, alpha), then the
+ * error estimate in channel 4, 1000 x the expected squared error); h, w even.
+ * Layers, each a 3x3 "same" convolution on the tensor cores (BF16 operands,
+ * FP32 accumulation):
+ *   e1 = relu(conv1(x)) 16->32;  p1 = avgpool2(e1);  e2 = relu(conv2(p1));
+ *   e3 = relu(conv3(e2));  d4 = relu(conv4(up2(e3) + e1));  o = conv5(d4) 32->16.
+ * Parameters (gs_denoiser_param_count floats): per layer the weights as
+ * [ky][kx][cin][cout] then the bias [cout].  All calls are stream-ordered
+ * on the denoiser's stream unless they return host data. */
+uint64_t gs_denoiser_param_count(void);
+int gs_denoiser_create(gs_denoiser** out, int device, void* stream);   /* seeded initial parameters */
+void gs_denoiser_destroy(gs_denoiser* d);
+int gs_denoiser_init_params(gs_denoiser* d, uint64_t seed);            /* He initialisation, zero bias */
+int gs_denoiser_set_params(gs_denoiser* d, const float* host, uint64_t count);   /* resets Adam's moments */
+int gs_denoiser_get_params(gs_denoiser* d, float* host, uint64_t count);
+int gs_denoiser_get_grads(gs_denoiser* d, float* host, uint64_t count);
+/* Forward pass; `out` (device, may be NULL) receives the 16-channel output. */
+int gs_denoiser_forward(gs_denoiser* d, const void* x_bf16, int n, int h, int w, float* out);
+/* Parameter gradients (gs_denoiser_get_grads) of sum(out * dout) for the last
+ * forward pass, which must have been on the same x; dout: n x h x w x 16 bf16. */
+int gs_denoiser_backward(gs_denoiser* d, const void* x_bf16, const void* dout_bf16, int n, int h, int w);
+/* Training loss of an output against a target RGBA (n x h x w x 4 f32):
+ *   L = mean |rgba - target| + ssim_weight (1 - mean SSIM(rgb)) + err_weight mean (o4 - 1000 e)^2,
+ * SSIM with an 11-tap Gaussian window (sigma 1.5) over pixels at least 5 from the border,
+ * e = mean over RGBA of (rgba - target)^2 (not differentiated).  Writes dL/dout
+ * (bf16, 16 channels) to dout_bf16; with parts != NULL waits and stores
+ * {mean L1, mean SSIM, error-head mean square, L}. */
+int gs_denoiser_loss(gs_denoiser* d, const void* x_bf16, const float* out, const float* target, int n, int h,
+                     int w, float ssim_weight, float err_weight, void* dout_bf16, float* parts);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected) with the last gradients. */
+int gs_denoiser_adam(gs_denoiser* d, float lr);
+/* forward + loss (ssim_weight 0.2, err_weight 0.01) + backward + Adam; with
+ * loss_parts != NULL waits and stores the loss parts as gs_denoiser_loss. */
+int gs_denoiser_train_step(gs_denoiser* d, const void* x_bf16, const float* target, int n, int h, int w, float lr,
+                           float* loss_parts);
+/* Waits; GS_ERR_DEVICE_TIMEOUT if a bounded device wait of a denoiser kernel ran out. */
+int gs_denoiser_status(gs_denoiser* d);
+
+/* One 3x3 "same" convolution of the denoiser on the tensor cores, NHWC bf16:
+ * out[c] = epilogue(sum_{ky,kx,ci} in[y+ky-1][x+kx-1][ci] * weights[ky][kx][ci][c] + bias[c]),
+ * epilogue = ReLU if relu, then 0 where mask <= 0 (mask: a tensor shaped like
+ * the output, or NULL).  weights: device f32 [3][3][cin][cout]; with
+ * transposed != 0 the convolution is the input gradient of that layer (input
+ * of cout channels, output of cin channels).  x_half != NULL: the input is
+ * x + the 2x nearest upsampling of x_half (n x h/2 x w/2).  Supported
+ * (input, output) channels: (16, 32), (32, 32), (32, 16), the last two with
+ * x_half only for (32, 32).  image_scratch: gs_conv3x3_scratch_bytes(cin, cout)
+ * device bytes; err: a device word, bit 0 set if a bounded wait ran out. */
+size_t gs_conv3x3_scratch_bytes(int cin, int cout);
+int gs_conv3x3_bf16(const void* x, const void* x_half, int n, int h, int w, int cin, int cout, const float* weights,
+                    const float* bias, int relu, int transposed, const void* mask, void* out_bf16, float* out_f32,
+                    void* image_scratch, uint32_t* err, void* stream);
+/* Weight gradient of that convolution: dw[ky][kx][ci][c] += sum over pixels of
+ * in[p + (ky-1, kx-1)][ci] * dy[p][c]; db[c] += sum of dy[p][c] (db may be NULL). */
+int gs_conv3x3_wgrad_bf16(const void* x, const void* x_half, int n, int h, int w, int cin, int cout, const void* dy,
+                          float* dw, float* db, uint32_t* err, void* stream);
 
 /* gs_sort_pairs without any allocation; no counterpart in the reference.
  * For callers that cannot allocate device memory through this library: a
@@ -412,7 +513,8 @@ int gs_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* ke
  * loads the library until exit, so n is limited to 1,048,576 pairs
  * (GS_ERR_TOO_LARGE beyond).  The first call on a device, with that device
  * current, looks up the array's device address; make it before any stream
- * capture.  Every call shares the array (each clears what must start at zero);
+ * capture.  After a reset of the device's context (cudaDeviceReset) the next
+ * call looks the address up again, in the new context.  Every call shares the array (each clears what must start at zero);
  * calls that overlap on the GPU race, so serialise them. */
 int gs_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                           uint32_t* vals_out, uint32_t n, int begin_bit, int end_bit, void* stream);

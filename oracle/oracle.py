@@ -51,11 +51,25 @@ _lib = None
 _ref = None
 
 
+def reference_dir():
+    """The reference checkout whose sources oracle/_ref is compiled from:
+    $GS_REFERENCE_DIR, else a directory named `reference` beside this
+    repository; None when neither holds the reference sources."""
+    for cand in (os.environ.get("GS_REFERENCE_DIR"), str(HERE.parent.parent / "reference")):
+        if cand and (Path(cand) / "src" / "gaussian.cpp").exists():
+            return str(Path(cand).resolve())
+    return None
+
+
 def build() -> None:
     """Compile liboracle.so (and _ref/libgsref.so when the reference tree is present)."""
     import subprocess
 
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    cmd = ["make", "-s", "-C", str(HERE)]
+    ref_dir = reference_dir()
+    if ref_dir:
+        cmd.append(f"REF={ref_dir}")
+    subprocess.run(cmd, check=True)
 
 
 def lib():
@@ -135,6 +149,9 @@ def ref():
         R.ref_camera_matrices.restype = None
         R.ref_camera_matrices.argtypes = [_f32p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                           C.c_int, C.c_float, C.c_float, C.c_float, _f32p, _f32p]
+        R.ref_camera_uniforms.restype = None
+        R.ref_camera_uniforms.argtypes = [_f32p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                          C.c_int, C.c_int, _f32p]
         vp = C.c_void_p
         R.ref_gsanim_open.restype = vp
         R.ref_gsanim_open.argtypes = [C.c_char_p]
@@ -177,6 +194,44 @@ def ref_cull_sort_seconds(rows: np.ndarray, cam: np.ndarray):
     sec = ref().ref_time_cull_sort_rows(rows.reshape(-1), rows.shape[0], np.ascontiguousarray(cam[0:16]),
                                         np.ascontiguousarray(cam[16:32]), float(cam[34]), C.byref(vis))
     return float(sec), int(vis.value)
+
+
+def ref_camera_uniforms(position, yaw: float, pitch: float, width: int, height: int,
+                        fov_y: float = np.pi / 3, near_plane: float = 0.1, far_plane: float = 100.0) -> np.ndarray:
+    """CameraUniforms (40 float32) of the reference fly camera, built by the
+    reference's own camera code (src/camera.cpp:137-245) and its frame setup
+    (src/main.cpp:1264-1281, GL branch)."""
+    out = np.zeros(40, np.float32)
+    pos = np.asarray(position, np.float32).reshape(3)
+    ref().ref_camera_uniforms(pos, float(yaw), float(pitch), float(fov_y), float(near_plane), float(far_plane),
+                              int(width), int(height), out)
+    return out
+
+
+def ref_rows_from_raw(raw: np.ndarray, tmpdir=None) -> np.ndarray:
+    """GpuGaussian rows of raw 3DGS attributes (N x 59, PLY property order)
+    through the reference's own PLY loader and pack_gpu_gaussians
+    (src/gaussian_loader_ply.cpp:14-228, src/gaussian.cpp:53-73): the
+    attributes are written as a binary PLY file and loaded back."""
+    import tempfile
+
+    raw = np.ascontiguousarray(raw, dtype="<f4")
+    names = ["x", "y", "z", "f_dc_0", "f_dc_1", "f_dc_2"] + [f"f_rest_{k}" for k in range(45)] + \
+            ["opacity", "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"]
+    header = "ply\nformat binary_little_endian 1.0\n" + f"element vertex {raw.shape[0]}\n" + \
+             "".join(f"property float {nm}\n" for nm in names) + "end_header\n"
+    with tempfile.TemporaryDirectory(dir=tmpdir) as d:
+        path = os.path.join(d, "scene.ply")
+        with open(path, "wb") as f:
+            f.write(header.encode())
+            f.write(raw.tobytes())
+        R = ref()
+        n = raw.shape[0]
+        rows = np.empty((n, 64), np.float32)
+        got = R.ref_load_ply_rows(path.encode(), rows.ctypes.data, n)
+    if got != n:
+        raise RuntimeError(f"reference PLY loader returned {got} rows for {n}")
+    return rows
 
 
 def ref_sog_rows(path):

@@ -5,13 +5,15 @@
 //   - gaussian_load_ply + pack_gpu_gaussians   (src/gaussian_loader_ply.cpp:14-228,
 //                                                src/gaussian.cpp:53-73)
 //   - cull_gaussians + sort_gaussians           (src/gaussian.cpp:77-181)
-//   - camera_get_view_matrix / camera_get_proj_matrix (src/camera.cpp:137-245)
+//   - camera_get_view_matrix / camera_get_proj_matrix (src/camera.cpp:137-245),
+//     and the CameraUniforms setup around them (src/main.cpp:1264-1281)
 //   - gaussian_load_gsanim, gsanim_sample, gsanim_layer_weights
 //                                               (src/gaussian_loader_gsanim.cpp:386-531)
 //   - gaussian_load_sog + pack_gpu_gaussians    (src/gaussian_loader_sog.cpp:126-551)
 //   - WebPGetInfo + WebPDecodeRGBA (the vendored libwebp decoder the SOG loader calls)
 // Never linked into the product.
 #include <SDL3/SDL.h>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <cstdlib>
@@ -166,6 +168,24 @@ void ref_camera_matrices(const float pos[3], float yaw, float pitch, float fov_y
     cam.z_up = z_up != 0; cam.ortho_size = ortho_size; cam.ortho_blend = ortho_blend;
     camera_get_view_matrix(&cam, view16);
     camera_get_proj_matrix(&cam, aspect, proj16);
+}
+
+// A whole CameraUniforms block (src/camera.h:23-38, 40 floats) of the
+// reference fly camera for a width x height GL target: view and projection
+// from camera_get_view_matrix / camera_get_proj_matrix, the rest as the
+// reference's frame setup fills it (src/main.cpp:1231, 1264-1281, GL branch).
+void ref_camera_uniforms(const float pos[3], float yaw, float pitch, float fov_y, float near_plane,
+                         float far_plane, int width, int height, float* out40) {
+    memset(out40, 0, 40 * sizeof(float));
+    const float aspect = (float)width / (float)height;
+    ref_camera_matrices(pos, yaw, pitch, fov_y, near_plane, far_plane, 0, 1.0f, 0.0f, aspect, out40, out40 + 16);
+    out40[32] = (float)width;
+    out40[33] = (float)height;
+    out40[34] = 0.0f;                                                  // orthographic blend
+    out40[35] = (1.0f / tanf(fov_y * 0.5f)) * (float)height * 0.5f;   // persp_focal
+    out40[36] = (float)height / (2.0f * 1.0f);                         // ortho_focal, ortho_size 1
+    out40[37] = 1.0f;                                                  // clip_y_sign (GL)
+    out40[38] = 0.0f;                                                  // clip_z_01 (GL)
 }
 
 // ---- gsanim archives --------------------------------------------------------

@@ -123,7 +123,7 @@ def test_nothing_visible():
 def test_single_gaussian_and_giant_splats_overflow_path():
     # 300 Gaussians just in front of the camera cover every tile of a 1080p
     # frame: 300 x 8160 entries exceed the initial entry capacity (1 Mi), so
-    # gs_render_host must grow the buffers and re-render.
+    # the frame must grow the buffers and re-render.
     raw = scene.small_scene(11, 300)
     raw[:, 0:3] *= 0.05
     raw[:, 52:55] = 0.0   # scale e^0 = 1 m
@@ -141,6 +141,33 @@ def test_single_gaussian_and_giant_splats_overflow_path():
     with make_renderer(one) as r:
         img1 = r.draw_frame(cam)
     assert image_gate(img1, ref1)["ok"]
+
+
+def test_overflowing_frame_through_stream_ordered_render():
+    """gs_render (device output, the drop-in renderer_draw_frame path) on the
+    giant-splat scene: the first frame's tile entries overflow the initial
+    buffers, and gs_render must grow them and re-render before it returns
+    GS_OK, so the image in device memory is the whole frame, not a truncated
+    one."""
+    import torch
+
+    raw = scene.small_scene(11, 300)
+    raw[:, 0:3] *= 0.05
+    raw[:, 52:55] = 0.0
+    rows = RR.pack_raw(raw)
+    W, H = 1920, 1080
+    cam = RR.camera_uniforms((0.0, 0.0, 1.2), float(np.pi), 0.0, W, H)
+    ref_img, _ = oracle_alpha(rows, cam, W, H)
+    out = torch.empty(W * H * 4, dtype=torch.float16, device="cuda")
+    with make_renderer(rows) as r:
+        for _ in range(2):   # the first call overflows and re-renders; the second fits
+            out.fill_(float("nan"))
+            r.draw_frame(cam, out_ptr=out.data_ptr())
+            st = r.stats()
+            assert st.tile_overflow == 0 and st.tile_entries > (1 << 20)
+            img = out.view(H, W, 4).cpu().numpy()
+            gate = image_gate(img, ref_img)
+            assert gate["ok"], gate
 
 
 def test_errors_are_status_codes():
