@@ -361,6 +361,162 @@ def denoised_mode(r, stream, out, frame, args, rank):
 _bench_rows_cache = []
 
 
+def batched_mode(r, stream, args):
+    """Batched variant on the benchmark scene: 64 cameras (4-8 m shell, aimed
+    within 1 m of the origin, viewports cycling 512x512 / 1280x720 /
+    1920x1080) in one gs_render_batch, against the same frames one gs_render
+    each; and gsanim appearance states (1M Gaussians x 256 int8 states, 32 per
+    gs_render_anim_batch) against one frame per state."""
+    import torch
+
+    from gamesplat_b200 import Renderer
+    from gamesplat_b200 import renderer as R
+    from gamesplat_b200 import scene
+
+    out = {}
+    cams = [R.camera_uniforms(p, y, pt, w, h) for p, y, pt, w, h in scene.batch_cameras(3, 64)]
+    bufs = [torch.empty(int(c[32]) * int(c[33]) * 4, dtype=torch.float16, device="cuda") for c in cams]
+    ptrs = [b.data_ptr() for b in bufs]
+    r.set(splat_render_mode="alpha", black_background=1)
+
+    def timed(fn, reps):
+        fn()
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    reps = 3
+    t_batch = timed(lambda: r.render_batch(cams, ptrs), reps)
+    t_seq = timed(lambda: [r.draw_frame(c, out_ptr=p) for c, p in zip(cams, ptrs)], reps)
+    mix = {}
+    for (w, h) in scene.BATCH_VIEWPORTS:
+        sel = [(c, p) for c, p in zip(cams, ptrs) if int(c[32]) == w and int(c[33]) == h]
+        tb = timed(lambda: r.render_batch([c for c, _ in sel], [p for _, p in sel]), reps)
+        mix[f"{w}x{h}"] = {"cameras": len(sel), "batch_frames_per_s": 1000.0 * len(sel) / tb}
+    out["cameras"] = {"count": len(cams), "viewports": "512x512 / 1280x720 / 1920x1080 cycling",
+                      "batch_ms": t_batch, "batch_frames_per_s": 1000.0 * len(cams) / t_batch,
+                      "sequential_ms": t_seq, "sequential_frames_per_s": 1000.0 * len(cams) / t_seq,
+                      "per_viewport": mix}
+    # gsanim states: 1M Gaussians x 256 states, 32 per launch
+    n_anim, states, per = args.anim_gaussians, 256, 32
+    if n_anim > 0:
+        rows = R.pack_raw(scene.room_scene(1, n_anim))
+        # round(N(0, 20)) clipped to [-127, 127], drawn on the device (12 GB: numpy would take minutes)
+        g = torch.Generator(device="cuda").manual_seed(3)
+        deltas = np.empty((states - 1, n_anim, 48), np.int8)
+        for sidx in range(states - 1):
+            d = torch.randn(n_anim, 48, device="cuda", generator=g).mul_(20.0).round_().clamp_(-127, 127)
+            deltas[sidx] = d.to(torch.int8).cpu().numpy()
+        ra = Renderer(0, stream=stream.cuda_stream)
+        ra.set(splat_render_mode="alpha", black_background=1)
+        ra.upload_gaussians(rows)
+        ra.upload_animation(deltas, np.full(48, 1.0 / 256.0, np.float32))
+        del deltas
+        cam = R.camera_uniforms(*scene.orbit_pose(0, FRAMES), WIDTH, HEIGHT)
+        imgs = [torch.empty(WIDTH * HEIGHT * 4, dtype=torch.float16, device="cuda") for _ in range(per)]
+        iptr = [b.data_ptr() for b in imgs]
+
+        def all_states_batched():
+            for b0 in range(0, states, per):
+                ra.render_anim_batch(cam, list(range(b0, b0 + per)), iptr)
+
+        def all_states_single():
+            for sidx in range(states):
+                ra.set_animation_state(sidx)
+                ra.draw_frame(cam, out_ptr=iptr[sidx % per])
+
+        tb = timed(all_states_batched, 1)
+        ts = timed(all_states_single, 1)
+        ra.destroy()
+        out["gsanim_states"] = {"gaussians": n_anim, "states": states, "states_per_launch": per,
+                                "viewport": f"{WIDTH}x{HEIGHT}", "batch_ms": tb,
+                                "batch_states_per_s": 1000.0 * states / tb, "sequential_ms": ts,
+                                "sequential_states_per_s": 1000.0 * states / ts}
+    return out
+
+
+def precision_variant(args):
+    """The FP16-SH row format on the larger workload: 6M Gaussians drawn as the
+    3M scene (seed 2), 3840x2160, 8 orbit cameras (frames 0, 15, ..., 105).
+    Frame time and the cull roofline with 144-byte rows beside the FP32 rows,
+    and the error of the FP16-SH frames against the FP32 frames of the same
+    cameras (the FP32 path's own distance from float64 is stated by the
+    test suite on reduced scenes)."""
+    import torch
+
+    from gamesplat_b200 import Renderer
+    from gamesplat_b200 import renderer as R
+    from gamesplat_b200 import scene
+
+    n = args.precision_gaussians
+    W, H = 3840, 2160
+    raw = scene.room_scene(2, n)
+    rows = R.pack_raw(raw)
+    del raw
+    cams = [R.camera_uniforms(*scene.orbit_pose(15 * k, FRAMES), W, H) for k in range(8)]
+    stream = torch.cuda.Stream()
+    imgs, out = {}, {}
+    hbm_peak = load_peaks()[0]
+    for fmt in ("fp32", "fp16_sh"):
+        r = Renderer(0, stream=stream.cuda_stream)
+        r.set(splat_render_mode="alpha", black_background=1)
+        r.set_row_format(fmt == "fp16_sh")
+        r.upload_gaussians(rows)
+        o = torch.empty(H * W * 4, dtype=torch.float16, device="cuda")
+        for c in cams[:3]:
+            r.draw_frame(c, out_ptr=o.data_ptr())
+        stream.synchronize()
+        r.profile(True)
+        r.stage_times(reset=True)
+        reps = 3
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            for c in cams:
+                r.draw_frame(c, out_ptr=o.data_ptr())
+        e1.record(stream)
+        stream.synchronize()
+        frames = reps * len(cams)
+        ms = e0.elapsed_time(e1) / frames
+        st = {k: v[0] / frames for k, v in r.stage_times(reset=True).items() if v[0] > 0}
+        r.profile(False)
+        vis = []
+        r.set(splat_diagnostics_enabled=0)
+        frames_img = []
+        for c in cams:
+            r.draw_frame(c, out_ptr=o.data_ptr())
+            vis.append(r.stats().visible_count)
+            frames_img.append(o.view(H, W, 4).float().clone())
+        imgs[fmt] = frames_img
+        n_vis = float(np.mean(vis))
+        row_rest = 240.0 if fmt == "fp32" else 128.0   # bytes of a visible row beyond its 16-byte head
+        alg = 16.0 * n + (row_rest + 64.0) * n_vis + 8.0 * n
+        ach = alg / (st["cull"] / 1000.0) / 1e9
+        out[fmt] = {"ms_per_frame": ms, "fps": 1000.0 / ms, "stages_ms_per_frame": {k: round(v, 4) for k, v in
+                                                                                     st.items()},
+                    "row_bytes": 256 if fmt == "fp32" else 144, "visible_per_frame": n_vis,
+                    "cull_roofline": {"achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                                      "algorithmic_bytes": alg}}
+        r.destroy()
+    errs = []
+    for a, b in zip(imgs["fp16_sh"], imgs["fp32"]):
+        d = (a - b).abs()
+        mse = float((d ** 2).mean())
+        errs.append({"max_abs": float(d.max()), "psnr_db": float("inf") if mse == 0 else 10 * np.log10(1 / mse),
+                     "frac_over_2^-9": float((d > 2.0 ** -9).float().mean())})
+    return {"workload": f"room{n // 1_000_000}m_sh3_2160p_8cams", "gaussians": n, "width": W, "height": H,
+            "formats": out, "fp16_vs_fp32_per_camera": errs,
+            "sh_eval": "SH3 basis (hi + lo FP16) x FP16 coefficients on the tensor cores (mma.m16n8k16, FP32 "
+                       "accumulation); covariance, conic and compositing FP32"}
+
+
 def run_ours(args):
     import torch
 
@@ -508,6 +664,11 @@ def run_ours(args):
             modes[mode] = entry
         r.set(splat_render_mode="alpha", black_background=1)
 
+    precision = None
+    if not args.no_modes and args.precision_gaussians > 0 and rank == 0:
+        precision = precision_variant(args)
+    if not args.no_modes and rank == 0:
+        modes["batched"] = batched_mode(r, stream, args)
     if not args.no_modes:
         den = denoised_mode(r, stream, out, frame, args, rank)
         if den is not None:
@@ -576,6 +737,7 @@ def run_ours(args):
         "dominant_stage": dominant,
         "raster": raster,
         "modes": modes or None,
+        "precision_variant": precision,
         "stages_ms_per_frame": per_frame,
         "hbm_stages": hbm_stages,
         "visible_per_frame": n_vis,
@@ -601,6 +763,10 @@ def main():
     ap.add_argument("--denoise-history", type=int, default=16,
                     help="frames along the orbit before each held-out camera (the TAA history)")
     ap.add_argument("--denoise-frames", type=int, default=None, help="timed denoised frames (default min(steps, 20))")
+    ap.add_argument("--precision-gaussians", type=int, default=6_000_000,
+                    help="scene size of the FP16-SH row format figures (0: skip)")
+    ap.add_argument("--anim-gaussians", type=int, default=1_000_000,
+                    help="scene size of the gsanim state batches (0: skip)")
     ap.add_argument("--gaussians", type=int, default=3_000_000,
                     help="scene size (the benchmark workload is 3M; smaller only for profiling captures)")
     args = ap.parse_args()

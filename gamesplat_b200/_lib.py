@@ -51,7 +51,8 @@ EXPORTS = (
     "gs_denoiser_set_params", "gs_denoiser_get_params", "gs_denoiser_get_grads", "gs_denoiser_forward",
     "gs_denoiser_backward", "gs_denoiser_loss", "gs_denoiser_adam", "gs_denoiser_train_step", "gs_denoiser_status",
     "gs_conv3x3_scratch_bytes", "gs_conv3x3_bf16", "gs_conv3x3_wgrad_bf16",
-    "gs_set_denoiser", "gs_set_denoise_budget", "gs_render_features",
+    "gs_set_denoiser", "gs_set_denoise_budget", "gs_render_features", "gs_set_row_format",
+    "gs_render_batch", "gs_render_anim_batch",
 )
 
 
@@ -216,6 +217,9 @@ def lib() -> C.CDLL:
         "gs_denoiser_status": (i32, [vp]),
         "gs_conv3x3_scratch_bytes": (C.c_size_t, [i32, i32]),
         "gs_set_denoiser": (i32, [vp, vp]),
+        "gs_set_row_format": (i32, [vp, i32]),
+        "gs_render_batch": (i32, [vp, vp, u32, vp]),
+        "gs_render_anim_batch": (i32, [vp, vp, vp, vp, vp, u32, vp]),
         "gs_set_denoise_budget": (i32, [vp, f32, i32]),
         "gs_render_features": (i32, [vp, C.POINTER(GsCamera), vp]),
         "gs_conv3x3_bf16": (i32, [vp, vp, i32, i32, i32, i32, i32, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp]),

@@ -120,9 +120,12 @@ __device__ __forceinline__ void sh_eval(const float4* row, float x, float y, flo
     }
 }
 
+// kGivenColour: the SH colour before the bias comes in sh_colour (FP16-SH rows)
+template <bool kGivenColour = false>
 __device__ __forceinline__ void project_visible(const float4* row, float4 c0, float vx, float vy, float vz,
                                                 const CamRegs& cam, int sh_degree, float sh_lod, float4* out,
-                                                float* quad_area, float* gps_points) {
+                                                float* quad_area, float* gps_points, float sc0 = 0.0f,
+                                                float sc1 = 0.0f, float sc2 = 0.0f) {
     const float t = cam.ortho;
     float4 c1 = row[1], c2 = row[2];
     float sx = c1.x, sy = c1.y, sz = c1.z;
@@ -208,7 +211,13 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
     int eff = sh_degree;
     if (sh_lod > 0.0f && (-vz) > sh_lod) eff = 0;
     float res[3];
-    sh_eval(row, x, y, z, eff, res);
+    if (kGivenColour) {
+        res[0] = sc0;
+        res[1] = sc1;
+        res[2] = sc2;
+    } else {
+        sh_eval(row, x, y, z, eff, res);
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) res[k] = g_max(add(res[k], 0.5f), 0.0f);
 
@@ -222,7 +231,7 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
 // kChunks 16-byte chunks of row ids[first + l] (if first + l < count) to
 // stage row l with one TMA bulk copy; completion is counted on `bar`.
 // Returns the lane's row id, or kSentinel past the end.
-template <int kChunks>
+template <int kChunks, int kRowChunks = 16>
 __device__ __forceinline__ uint32_t stage_group(const float4* rows, const uint32_t* ids, uint32_t first,
                                                 uint32_t count, float4* stage, uint64_t* bar, int lane,
                                                 uint64_t policy) {
@@ -235,7 +244,8 @@ __device__ __forceinline__ uint32_t stage_group(const float4* rows, const uint32
     // the in-place gsanim deltas) before the async-proxy refill
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (id != kSentinel)
-        bulk_g2s_hint(stage + lane * kStageStride, rows + (size_t)id * 16, (uint32_t)(kChunks * 16), bar, policy);
+        bulk_g2s_hint(stage + lane * kStageStride, rows + (size_t)id * kRowChunks, (uint32_t)(kChunks * 16), bar,
+                      policy);
     return id;
 }
 
@@ -270,16 +280,49 @@ __device__ void animate_row(const CullParams& p, uint32_t row, float4* staged, f
 
 // Copies the first 16 bytes of every row into the contiguous heads array
 // (run once per upload; the rows are written nowhere else).
-__global__ void gather_heads_kernel(const float4* __restrict__ rows, float4* __restrict__ heads, uint32_t n) {
+__global__ void gather_heads_kernel(const float4* __restrict__ rows, float4* __restrict__ heads, uint32_t n,
+                                    uint32_t stride) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        heads[i] = __ldg(rows + (size_t)i * 16);
+        heads[i] = __ldg(rows + (size_t)i * stride);
 }
 
-int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t num_sms, cudaStream_t s) {
+int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t num_sms, cudaStream_t s,
+                        uint32_t row_chunks) {
     if (n == 0) return 0;
     uint32_t grid = (n + 255) / 256;
     if (grid > num_sms * 8) grid = num_sms * 8;
-    gather_heads_kernel<<<grid, 256, 0, s>>>(rows, heads, n);
+    gather_heads_kernel<<<grid, 256, 0, s>>>(rows, heads, n, row_chunks);
+    return 1;
+}
+
+// 256-byte GpuGaussian rows -> 144-byte rows with FP16 SH: chunks 0..2
+// (position, opacity, scale, rotation) copied, then the 48 SH coefficients
+// (DC at floats 12..14, SH k = 1..15 at 16 + 3(k-1) + c) as IEEE half in the
+// order 3k + c (round to nearest even).
+__global__ void pack_half_rows_kernel(const float4* __restrict__ rows, float4* __restrict__ half_rows,
+                                      uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* r = reinterpret_cast<const float*>(rows + (size_t)i * 16);
+        float4* o = half_rows + (size_t)i * kHalfRowChunks;
+        o[0] = __ldg(rows + (size_t)i * 16);
+        o[1] = __ldg(rows + (size_t)i * 16 + 1);
+        o[2] = __ldg(rows + (size_t)i * 16 + 2);
+        __align__(16) __half h[48];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) h[c] = __float2half_rn(r[12 + c]);
+#pragma unroll
+        for (int j = 3; j < 48; ++j) h[j] = __float2half_rn(r[16 + (j - 3)]);
+        const float4* hv = reinterpret_cast<const float4*>(h);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) o[3 + q] = hv[q];
+    }
+}
+
+int launch_pack_half_rows(const float4* rows, float4* half_rows, uint32_t n, uint32_t num_sms, cudaStream_t s) {
+    if (n == 0) return 0;
+    uint32_t grid = (n + 255) / 256;
+    if (grid > num_sms * 8) grid = num_sms * 8;
+    pack_half_rows_kernel<<<grid, 256, 0, s>>>(rows, half_rows, n);
     return 1;
 }
 
@@ -486,6 +529,258 @@ __global__ void __launch_bounds__(kCullThreads, 6) cull_project_kernel(CullParam
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP16-SH rows (144 bytes: chunks 0..2 as the GpuGaussian row, then 48 IEEE
+// half SH coefficients in the order 3k + c).  The SH colour of a warp's 32
+// visible rows is evaluated on the tensor cores: per row the 16 SH basis
+// values Y_k(dir) (FP32, the weights of shaders/cull.glsl:355-408) split into
+// two FP16 terms (Y = hi + lo, so Y keeps ~22 bits) times the row's FP16
+// coefficients, accumulated in FP32.  Every row has its own coefficients,
+// so the product is a batch of 1 x 16 by 16 x 3 products: one
+// mma.m16n8k16 takes 16 rows' basis vectors (A, 16 x 16) against 8
+// (row, channel) columns of coefficients (B, 16 x 8) and keeps the 8 outputs
+// on its diagonal blocks; 2 x 6 x 2 instructions per 32 rows.  The warp-level
+// MMA fits the per-warp staging of this kernel; a CTA-wide tcgen05 MMA would
+// need 128-row tiles staged through shared memory and TMEM for the same
+// 48 useful outputs per 16 rows.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sh_basis(float x, float y, float z, int eff, bool valid, float* Y) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) Y[k] = 0.0f;
+    if (!valid) return;
+    Y[0] = SH_C0;
+    if (eff >= 1) {
+        Y[1] = mul(-SH_C1, y);
+        Y[2] = mul(SH_C1, z);
+        Y[3] = mul(-SH_C1, x);
+        if (eff >= 2) {
+            const float xx = mul(x, x), yy = mul(y, y), zz = mul(z, z);
+            const float xy = mul(x, y), yz = mul(y, z), xz = mul(z, x);
+            Y[4] = mul(SH_C2_0, xy);
+            Y[5] = mul(SH_C2_1, yz);
+            Y[6] = mul(SH_C2_2, sub(sub(mul(2.0f, zz), xx), yy));
+            Y[7] = mul(SH_C2_3, xz);
+            Y[8] = mul(SH_C2_4, sub(xx, yy));
+            if (eff >= 3) {
+                Y[9] = mul(mul(SH_C3_0, y), sub(mul(3.0f, xx), yy));
+                Y[10] = mul(mul(SH_C3_1, xy), z);
+                Y[11] = mul(mul(SH_C3_2, y), sub(sub(mul(4.0f, zz), xx), yy));
+                Y[12] = mul(mul(SH_C3_3, z), sub(sub(mul(2.0f, zz), mul(3.0f, xx)), mul(3.0f, yy)));
+                Y[13] = mul(mul(SH_C3_4, x), sub(sub(mul(4.0f, zz), xx), yy));
+                Y[14] = mul(mul(SH_C3_5, z), sub(xx, yy));
+                Y[15] = mul(mul(SH_C3_6, x), sub(xx, mul(3.0f, yy)));
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t pack_h2(__half a, __half b) {
+    return (uint32_t)__half_as_ushort(a) | ((uint32_t)__half_as_ushort(b) << 16);
+}
+
+__device__ __forceinline__ void mma_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                          uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// SH colour (before the +0.5 bias) of the warp's 32 staged half rows; lane l
+// passes the direction of its row and receives that row's colour.  s_y: 2 x
+// 32 x 16 halves of scratch, s_out: 32 x 3 floats of scratch (per warp).
+__device__ __forceinline__ void sh_eval_tc(const float4* stage, int lane, float x, float y, float z, int eff,
+                                           bool valid, __half* s_y, float* s_out, float* res) {
+    float Y[16];
+    sh_basis(x, y, z, eff, valid, Y);
+    __half* yh = s_y + lane * 16;
+    __half* yl = s_y + 512 + lane * 16;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const __half hi = __float2half_rn(Y[k]);
+        yh[k] = hi;
+        yl[k] = __float2half_rn(Y[k] - __half2float(hi));
+    }
+    __syncwarp();
+    const int gid = lane >> 2, tig = lane & 3;
+    const uint32_t* wy = reinterpret_cast<const uint32_t*>(s_y);
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const int r0 = 16 * t + gid, r1 = r0 + 8;
+        uint32_t ah[4], al[4];
+        ah[0] = wy[r0 * 8 + tig];
+        ah[1] = wy[r1 * 8 + tig];
+        ah[2] = wy[r0 * 8 + tig + 4];
+        ah[3] = wy[r1 * 8 + tig + 4];
+        al[0] = wy[256 + r0 * 8 + tig];
+        al[1] = wy[256 + r1 * 8 + tig];
+        al[2] = wy[256 + r0 * 8 + tig + 4];
+        al[3] = wy[256 + r1 * 8 + tig + 4];
+#pragma unroll
+        for (int b = 0; b < 6; ++b) {
+            const int q = 8 * b + gid, g = q / 3, c = q - 3 * g;
+            const __half* sh = reinterpret_cast<const __half*>(stage + (16 * t + g) * kStageStride + 3) + c;
+            const int k0 = 2 * tig;
+            const uint32_t b0 = pack_h2(sh[3 * k0], sh[3 * (k0 + 1)]);
+            const uint32_t b1 = pack_h2(sh[3 * (k0 + 8)], sh[3 * (k0 + 9)]);
+            float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            mma_16816(d, ah[0], ah[1], ah[2], ah[3], b0, b1);
+            mma_16816(d, al[0], al[1], al[2], al[3], b0, b1);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int row = gid + (e >> 1) * 8, col = 2 * tig + (e & 1);
+                const int qq = 8 * b + col;
+                if (qq / 3 == row) s_out[(16 * t + row) * 3 + (qq - 3 * row)] = d[e];
+            }
+        }
+    }
+    __syncwarp();
+    res[0] = s_out[lane * 3 + 0];
+    res[1] = s_out[lane * 3 + 1];
+    res[2] = s_out[lane * 3 + 2];
+    __syncwarp();
+}
+
+// The projection pass for FP16-SH rows: as cull_project_kernel, staging 144
+// bytes per visible row, with the SH colour from sh_eval_tc and everything
+// else (covariance, conic, radius, centre, depth) in FP32 as for full rows.
+__global__ void __launch_bounds__(kCullThreads, 6) cull_project_half_kernel(CullParams p) {
+    extern __shared__ float4 smem4[];
+    __shared__ __align__(8) uint64_t s_bar[kCullWarps];
+    __shared__ __align__(16) __half s_y[kCullWarps][1024];
+    __shared__ float s_out[kCullWarps][96];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        mbar_init(&s_bar[warp], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    float4* const stage0 = smem4 + (size_t)warp * 32 * kStageStride;
+    const uint32_t n_vis = p.fc->visible_count;
+    const uint32_t groups = (n_vis + 31) / 32;
+    const uint32_t wg = blockIdx.x * kCullWarps + warp, nw = gridDim.x * kCullWarps;
+    CamRegs cam;
+    load_cam(p.cam, cam);
+    const uint64_t stream_policy = l2_policy_evict_first();
+    bool stage_failed = false;
+    uint32_t phase = 0;
+    uint32_t d0 = 0, d2 = 0, d3 = 0, d4 = 0, d6 = 0, d7 = 0, m1 = 0, m5 = 0;
+    for (uint32_t g = wg; g < groups; g += nw) {
+        const uint32_t id = stage_group<kHalfRowChunks, kHalfRowChunks>(p.rows, p.ids_out, g * 32u, n_vis, stage0,
+                                                                        &s_bar[warp], lane, stream_policy);
+        if (!mbar_wait_bounded(&s_bar[warp], phase)) stage_failed = true;
+        phase ^= 1u;
+        const bool valid = id != kSentinel;
+        float4* row = stage0 + lane * kStageStride;
+        const float4 c0 = row[0];
+        float vx = 0.0f, vy = 0.0f, vz = 0.0f, dx = 0.0f, dy = 0.0f, dz = 0.0f;
+        int eff = 0;
+        if (valid) {
+            vx = add(add(add(mul(cam.V[0], c0.x), mul(cam.V[4], c0.y)), mul(cam.V[8], c0.z)), cam.V[12]);
+            vy = add(add(add(mul(cam.V[1], c0.x), mul(cam.V[5], c0.y)), mul(cam.V[9], c0.z)), cam.V[13]);
+            vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
+            // view direction and SH degree as in project_visible (shaders/cull.glsl:323-351)
+            const float ddx = sub(c0.x, cam.camw[0]), ddy = sub(c0.y, cam.camw[1]), ddz = sub(c0.z, cam.camw[2]);
+            const float len = __fsqrt_rn(add(add(mul(ddx, ddx), mul(ddy, ddy)), mul(ddz, ddz)));
+            dx = dv(ddx, len);
+            dy = dv(ddy, len);
+            dz = dv(ddz, len);
+            eff = p.sh_degree;
+            if (p.sh_lod_distance > 0.0f && (-vz) > p.sh_lod_distance) eff = 0;
+        }
+        float colour[3];
+        sh_eval_tc(stage0, lane, dx, dy, dz, eff, valid, s_y[warp], s_out[warp], colour);
+        if (valid) {
+            float4 rec[4];
+            float qa, gp;
+            project_visible<true>(row, c0, vx, vy, vz, cam, p.sh_degree, p.sh_lod_distance, rec, &qa, &gp, colour[0],
+                                  colour[1], colour[2]);
+            float4* dst = p.projected + (size_t)id * 4;
+            dst[0] = rec[0];
+            dst[1] = rec[1];
+            dst[2] = rec[2];
+            dst[3] = rec[3];
+            if (p.collect_stats) {
+                const uint32_t qpx = g_f2u_sat(g_min(g_max(0.0f, qa), 4294967295.0f));
+                const uint32_t gpx = g_f2u_sat(g_min(ceilf(gp), 4294967295.0f));
+                d0 += (uint32_t)(qpx + 1023u) >> 10u;
+                m1 = max(m1, qpx);
+                d2 += qpx > 1024u;
+                d3 += qpx > 16384u;
+                d4 += (uint32_t)(gpx + 1023u) >> 10u;
+                m5 = max(m5, gpx);
+                d6 += gpx > 1024u;
+                d7 += gpx > 16384u;
+            }
+        }
+        __syncwarp();
+    }
+    if (stage_failed) atomicOr(&p.fc->error_flags, kErrCullStage);
+    if (p.collect_stats) {
+        const uint32_t s0 = __reduce_add_sync(0xffffffffu, d0), s2 = __reduce_add_sync(0xffffffffu, d2);
+        const uint32_t s3 = __reduce_add_sync(0xffffffffu, d3), s4 = __reduce_add_sync(0xffffffffu, d4);
+        const uint32_t s6 = __reduce_add_sync(0xffffffffu, d6), s7 = __reduce_add_sync(0xffffffffu, d7);
+        const uint32_t x1 = __reduce_max_sync(0xffffffffu, m1), x5 = __reduce_max_sync(0xffffffffu, m5);
+        if (lane == 0) {
+            if (s0) atomicAdd(&p.fc->diag[0], s0);
+            if (x1) atomicMax(&p.fc->diag[1], x1);
+            if (s2) atomicAdd(&p.fc->diag[2], s2);
+            if (s3) atomicAdd(&p.fc->diag[3], s3);
+            if (s4) atomicAdd(&p.fc->diag[4], s4);
+            if (x5) atomicMax(&p.fc->diag[5], x5);
+            if (s6) atomicAdd(&p.fc->diag[6], s6);
+            if (s7) atomicAdd(&p.fc->diag[7], s7);
+        }
+    }
+}
+
+// Colours of a frame's binned records for another gsanim appearance state
+// (a frame of a state batch: the geometry, order and tiles of the frame stay,
+// the colours change).  Record i (sorted position) gets the colour the
+// projection pass would give its splat under the state of `p`: the same row,
+// deltas, view direction, SH degree and operations (animate_row, sh_eval,
+// shaders/cull.glsl:125-164, 323-417), bias and clamp.
+__global__ void __launch_bounds__(128) recolour_kernel(CullParams p, const RasterRecord* __restrict__ records,
+                                                       float4* __restrict__ colours) {
+    const uint32_t n_vis = p.fc->visible_count;
+    CamRegs cam;
+    load_cam(p.cam, cam);
+    const bool animated = p.anim_deltas != nullptr &&
+                          (p.anim_state_a != 0 || (p.anim_weight > 0.0f && p.anim_state_b != 0));
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_vis; i += gridDim.x * blockDim.x) {
+        const uint32_t id = records[i].splat_id;
+        if (id >= p.n) continue;
+        float4 row[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) row[k] = __ldg(p.rows + (size_t)id * 16 + k);
+        const float4 c0 = row[0];
+        const float vz = add(add(add(mul(cam.V[2], c0.x), mul(cam.V[6], c0.y)), mul(cam.V[10], c0.z)), cam.V[14]);
+        if (animated) {
+            float4 c3 = row[3];
+            animate_row(p, id, row, c3);
+        }
+        const float ddx = sub(c0.x, cam.camw[0]), ddy = sub(c0.y, cam.camw[1]), ddz = sub(c0.z, cam.camw[2]);
+        const float len = __fsqrt_rn(add(add(mul(ddx, ddx), mul(ddy, ddy)), mul(ddz, ddz)));
+        const float x = dv(ddx, len), y = dv(ddy, len), z = dv(ddz, len);
+        int eff = p.sh_degree;
+        if (p.sh_lod_distance > 0.0f && (-vz) > p.sh_lod_distance) eff = 0;
+        float res[3];
+        sh_eval(row, x, y, z, eff, res);
+        colours[i] = make_float4(g_max(add(res[0], 0.5f), 0.0f), g_max(add(res[1], 0.5f), 0.0f),
+                                 g_max(add(res[2], 0.5f), 0.0f), 0.0f);
+    }
+}
+
+int launch_recolour(const CullParams& p, const RasterRecord* records, float4* colours, uint32_t num_sms,
+                    cudaStream_t s) {
+    uint32_t grid = (p.n + 127) / 128;
+    if (grid > num_sms * 8) grid = num_sms * 8;
+    if (grid == 0) return 0;
+    recolour_kernel<<<grid, 128, 0, s>>>(p, records, colours);
+    return 1;
+}
+
 // Pass 3, gsanim 0.3 assets only (shaders/cull.glsl:141-148, 354-416): the
 // colour of every compacted visible row is the sum over the layers of
 // max(SH colour, 0) * the layer's RGB weight, without the +0.5 bias, where
@@ -535,6 +830,7 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
         cudaFuncSetAttribute(cull_project_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         cudaFuncSetAttribute(cull_project_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         cudaFuncSetAttribute(cull_project_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_project_half_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         attr_devices.fetch_or(bit);
     }
     int deg = p.sh_degree < 0 ? 0 : (p.sh_degree > 3 ? 3 : p.sh_degree);
@@ -546,6 +842,10 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
     const uint32_t groups_cap = (p.n + 31) / 32;
     uint32_t pgrid = num_sms * 6;
     if (pgrid * kCullWarps > groups_cap) pgrid = (groups_cap + kCullWarps - 1) / kCullWarps;
+    if (p.half_rows) {
+        cull_project_half_kernel<<<pgrid, kCullThreads, kCullSmem, s>>>(p);
+        return 2;
+    }
     switch (deg) {
         case 0: cull_project_kernel<4><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
         case 1: cull_project_kernel<7><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;

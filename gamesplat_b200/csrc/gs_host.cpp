@@ -44,6 +44,32 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// The buffers one frame's stages leave for its raster pass.  A batch keeps
+// one slot per frame and swaps it into the context while that frame's cull,
+// sort and binning run, so the stages need no batch-specific code.
+struct FrameSlot {
+    int width = 0, height = 0, tiles_x = 0, tiles_y = 0;
+    uint32_t tiles_cap = 0;
+    void* ctrl = nullptr;
+    size_t ctrl_bytes = 0;
+    FrameCounters* fc = nullptr;
+    SortPlan* depth_plan = nullptr;
+    SortPlan* tile_plan = nullptr;
+    uint32_t* depth_hist = nullptr;
+    uint32_t* tile_hist = nullptr;
+    uint2* tile_ranges = nullptr;
+    uint32_t* tile_order = nullptr;
+    RasterRecord* records = nullptr;
+    uint32_t entry_cap = 0;
+    uint32_t* ekeys[2] = {nullptr, nullptr};
+    uint32_t* evals[2] = {nullptr, nullptr};
+    uint32_t* chunk_first = nullptr;
+    uint32_t chunk_cap = 0;
+    unsigned long long* tsort_status = nullptr;
+    size_t tsort_status_stride = 0;
+    uint32_t record_cap = 0;
+};
+
 }  // namespace
 
 struct gs_ctx {
@@ -60,6 +86,8 @@ struct gs_ctx {
 
     // scene
     uint32_t n = 0;
+    int row_format = 0;                  // of the next upload: 0 GpuGaussian (256 B), 1 FP16 SH (144 B)
+    int half_rows = 0;                   // of the resident scene
     float4* rows = nullptr;
     float4* heads = nullptr;             // first 16 bytes of every row, contiguous (cull visibility pass)
     float4* projected = nullptr;
@@ -146,6 +174,19 @@ struct gs_ctx {
     bool prev_cam_valid = false;
     bool taa_prev_valid = false;
 
+    // batches (gs_render_batch, gs_render_anim_batch): one slot per frame
+    std::vector<FrameSlot> slots;
+    FrameCounters* h_slot_fc = nullptr;   // pinned, one per slot
+    uint32_t h_slot_fc_cap = 0;
+    gs::RasterParams* h_batch_params = nullptr;   // pinned
+    gs::RasterParams* batch_params = nullptr;     // device
+    uint32_t* batch_first = nullptr;              // device: prefix sums of tiles (+ the ticket word)
+    uint32_t* h_batch_first = nullptr;            // pinned
+    uint32_t batch_cap = 0;
+    float4* state_colours = nullptr;              // anim batches: n x states colours
+    size_t state_colours_cap = 0;
+    cudaEvent_t batch_event = nullptr;
+
     // profiling
     bool profiling = false;
     struct Pending { cudaEvent_t a, b; int stage; uint32_t launches; };
@@ -213,6 +254,54 @@ void dfree(T*& p) {
     p = nullptr;
 }
 
+void release_slot(FrameSlot& f) {
+    dfree(f.ctrl);
+    dfree(f.tile_order);
+    dfree(f.records);
+    for (int k = 0; k < 2; ++k) {
+        dfree(f.ekeys[k]);
+        dfree(f.evals[k]);
+    }
+    dfree(f.chunk_first);
+    dfree(f.tsort_status);
+    f = FrameSlot{};
+}
+
+void release_slots(gs_ctx* c) {
+    for (auto& f : c->slots) release_slot(f);
+    c->slots.clear();
+    dfree(c->state_colours);
+    c->state_colours_cap = 0;
+}
+
+// Exchange the per-frame buffers of the context with those of a slot.
+void swap_slot(gs_ctx* c, FrameSlot& f) {
+    std::swap(c->width, f.width);
+    std::swap(c->height, f.height);
+    std::swap(c->tiles_x, f.tiles_x);
+    std::swap(c->tiles_y, f.tiles_y);
+    std::swap(c->tiles_cap, f.tiles_cap);
+    std::swap(c->ctrl, f.ctrl);
+    std::swap(c->ctrl_bytes, f.ctrl_bytes);
+    std::swap(c->fc, f.fc);
+    std::swap(c->depth_plan, f.depth_plan);
+    std::swap(c->tile_plan, f.tile_plan);
+    std::swap(c->depth_hist, f.depth_hist);
+    std::swap(c->tile_hist, f.tile_hist);
+    std::swap(c->tile_ranges, f.tile_ranges);
+    std::swap(c->tile_order, f.tile_order);
+    std::swap(c->records, f.records);
+    std::swap(c->entry_cap, f.entry_cap);
+    for (int k = 0; k < 2; ++k) {
+        std::swap(c->ekeys[k], f.ekeys[k]);
+        std::swap(c->evals[k], f.evals[k]);
+    }
+    std::swap(c->chunk_first, f.chunk_first);
+    std::swap(c->chunk_cap, f.chunk_cap);
+    std::swap(c->tsort_status, f.tsort_status);
+    std::swap(c->tsort_status_stride, f.tsort_status_stride);
+}
+
 void release_scene(gs_ctx* c) {
     dfree(c->rows);
     dfree(c->heads);
@@ -244,6 +333,7 @@ void release_scene(gs_ctx* c) {
     c->layer_weights_host.clear();
     c->n = 0;
     c->entry_cap = 0;
+    release_slots(c);
 }
 
 void release_targets(gs_ctx* c) {
@@ -364,12 +454,10 @@ int ensure_entries(gs_ctx* c, uint32_t cap) {
     return GS_OK;
 }
 
-int ensure_targets(gs_ctx* c, int w, int h) {
-    if (w <= 0 || h <= 0) return fail(c, GS_ERR_BAD_ARG, "viewport must be positive");
-    if (w > 32767 || h > 32767) return fail(c, GS_ERR_TOO_LARGE, "viewport beyond 32767 pixels");
+// The per-frame control block of a w x h frame in the context's fields:
+// FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges, and the tile order.
+int alloc_control(gs_ctx* c, int w, int h) {
     const int tx = (w + gs::kTileW - 1) / gs::kTileW, ty = (h + gs::kTileH - 1) / gs::kTileH;
-    if (c->width == w && c->height == h && c->ctrl) return GS_OK;
-    release_targets(c);
     c->tiles_cap = (uint32_t)(tx * ty);
     // control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges
     size_t off = 0;
@@ -395,11 +483,25 @@ int ensure_targets(gs_ctx* c, int w, int h) {
     c->tile_ranges = reinterpret_cast<uint2*>(base + o_tr);
     GS_CUDA(c, cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream));
     GS_CUDA(c, dalloc(&c->tile_order, (size_t)c->tiles_cap * sizeof(uint32_t)));
-    GS_CUDA(c, dalloc(&c->out16, (size_t)w * h * 8));
     c->width = w;
     c->height = h;
     c->tiles_x = tx;
     c->tiles_y = ty;
+    return GS_OK;
+}
+
+int ensure_targets(gs_ctx* c, int w, int h) {
+    if (w <= 0 || h <= 0) return fail(c, GS_ERR_BAD_ARG, "viewport must be positive");
+    if (w > 32767 || h > 32767) return fail(c, GS_ERR_TOO_LARGE, "viewport beyond 32767 pixels");
+    if (c->width == w && c->height == h && c->ctrl) return GS_OK;
+    release_targets(c);
+    int rc = alloc_control(c, w, h);
+    if (rc) return rc;
+    const cudaError_t e = dalloc(&c->out16, (size_t)w * h * 8);
+    if (e != cudaSuccess) {
+        c->width = c->height = 0;   // the next frame allocates the targets again
+        return cuda_fail(c, e, "dalloc(out16)");
+    }
     c->sample_count = 0;
     c->accum_write_index = 0;
     c->taa_prev_valid = false;
@@ -434,8 +536,7 @@ void end_frame(gs_ctx* c) {
     c->last_launches = c->frame_launches;
 }
 
-void run_cull(gs_ctx* c) {
-    StageScope sc(c, ST_CULL);
+gs::CullParams cull_params(gs_ctx* c) {
     gs::CullParams p{};
     p.rows = c->rows;
     p.heads = c->heads;
@@ -463,8 +564,14 @@ void run_cull(gs_ctx* c) {
         p.layer_weights = c->layer_weights;
         p.layer_count = (int)c->layer_count;
     }
+    p.half_rows = c->half_rows;
     p.fc = c->fc;
-    sc.add(gs::launch_cull(p, c->num_sms, c->stream));
+    return p;
+}
+
+void run_cull(gs_ctx* c) {
+    StageScope sc(c, ST_CULL);
+    sc.add(gs::launch_cull(cull_params(c), c->num_sms, c->stream));
 }
 
 void run_depth_sort(gs_ctx* c) {
@@ -971,6 +1078,12 @@ void gs_destroy(gs_ctx* c) {
     dfree(c->display_lut);
     if (c->h_fc) cudaFreeHost(c->h_fc);
     if (c->h_bin_fc) cudaFreeHost(c->h_bin_fc);
+    if (c->h_slot_fc) cudaFreeHost(c->h_slot_fc);
+    if (c->h_batch_params) cudaFreeHost(c->h_batch_params);
+    if (c->h_batch_first) cudaFreeHost(c->h_batch_first);
+    dfree(c->batch_params);
+    dfree(c->batch_first);
+    if (c->batch_event) cudaEventDestroy(c->batch_event);
     if (c->h_out16) cudaFreeHost(c->h_out16);
     for (auto e : c->chunk_events)
         if (e) cudaEventDestroy(e);
@@ -1049,7 +1162,10 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
     }
     cudaStreamSynchronize(c->stream);
     release_scene(c);
-    GS_CUDA(c, dalloc(&c->rows, (size_t)n * 256));
+    const bool half = c->row_format == 1;
+    const size_t row_bytes = half ? (size_t)gs::kHalfRowChunks * 16 : 256;
+    c->half_rows = half ? 1 : 0;
+    GS_CUDA(c, dalloc(&c->rows, (size_t)n * row_bytes));
     GS_CUDA(c, dalloc(&c->heads, (size_t)n * 16));
     GS_CUDA(c, dalloc(&c->projected, (size_t)n * 64));
     for (int k = 0; k < 2; ++k) {
@@ -1068,8 +1184,19 @@ static int upload_common(gs_ctx* c, const float* rows, uint64_t count, cudaMemcp
     GS_CUDA(c, cudaMemsetAsync(c->sort_status, 0, c->sort_status_stride * 4 * 8, c->stream));
     GS_CUDA(c, cudaMemsetAsync(c->bin_status, 0, bin_tiles * 8, c->stream));
     GS_CUDA(c, cudaMemsetAsync(c->projected, 0, (size_t)n * 64, c->stream));
-    GS_CUDA(c, cudaMemcpyAsync(c->rows, rows, (size_t)n * 256, kind, c->stream));
-    gs::launch_gather_heads(c->rows, c->heads, n, c->num_sms, c->stream);
+    if (half) {
+        // the 256-byte rows pass through a temporary device copy into the FP16-SH rows
+        float4* full = nullptr;
+        GS_CUDA(c, dalloc(&full, (size_t)n * 256));
+        cudaError_t e = cudaMemcpyAsync(full, rows, (size_t)n * 256, kind, c->stream);
+        if (e == cudaSuccess) gs::launch_pack_half_rows(full, c->rows, n, c->num_sms, c->stream);
+        cudaStreamSynchronize(c->stream);
+        dfree(full);
+        GS_CUDA(c, e);
+    } else {
+        GS_CUDA(c, cudaMemcpyAsync(c->rows, rows, (size_t)n * 256, kind, c->stream));
+    }
+    gs::launch_gather_heads(c->rows, c->heads, n, c->num_sms, c->stream, half ? gs::kHalfRowChunks : 16);
     GS_CUDA(c, cudaGetLastError());
     int rc = ensure_entries(c, default_entry_cap(n));
     if (rc) return rc;   // the scene stays unloaded: every buffer must exist before n is set
@@ -1094,17 +1221,38 @@ int gs_upload_rows_range(gs_ctx* c, const float* rows, uint64_t first, uint64_t 
     if (!count) return GS_OK;
     cudaSetDevice(c->device);
     // stream-ordered after the frames already queued, which read the old rows
-    GS_CUDA(c, cudaMemcpyAsync(c->rows + first * 16, rows, count * 256, cudaMemcpyHostToDevice, c->stream));
-    gs::launch_gather_heads(c->rows + first * 16, c->heads + first, (uint32_t)count, c->num_sms, c->stream);
+    if (c->half_rows) {
+        float4* full = nullptr;
+        GS_CUDA(c, dalloc(&full, (size_t)count * 256));
+        cudaError_t e = cudaMemcpyAsync(full, rows, count * 256, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            gs::launch_pack_half_rows(full, c->rows + first * gs::kHalfRowChunks, (uint32_t)count, c->num_sms,
+                                      c->stream);
+        cudaStreamSynchronize(c->stream);
+        dfree(full);
+        GS_CUDA(c, e);
+        gs::launch_gather_heads(c->rows + first * gs::kHalfRowChunks, c->heads + first, (uint32_t)count, c->num_sms,
+                                c->stream, gs::kHalfRowChunks);
+    } else {
+        GS_CUDA(c, cudaMemcpyAsync(c->rows + first * 16, rows, count * 256, cudaMemcpyHostToDevice, c->stream));
+        gs::launch_gather_heads(c->rows + first * 16, c->heads + first, (uint32_t)count, c->num_sms, c->stream);
+    }
     GS_CUDA(c, cudaGetLastError());
     GS_CUDA(c, cudaStreamSynchronize(c->stream));   // the caller may reuse `rows` on return
     gs_reset_accumulation(c);
     return GS_OK;
 }
 
+int gs_set_row_format(gs_ctx* c, int format) {
+    if (!c || format < 0 || format > 1) return GS_ERR_BAD_ARG;
+    c->row_format = format;
+    return GS_OK;
+}
+
 int gs_upload_anim(gs_ctx* c, const int8_t* deltas, uint32_t num_states, const float* scales) {
     if (!c || (num_states && (!deltas || !scales))) return GS_ERR_BAD_ARG;
     if (!c->n) return fail(c, GS_ERR_NO_SCENE, "upload the Gaussians before their animation");
+    if (c->half_rows && num_states) return fail(c, GS_ERR_BAD_ARG, "animation needs GpuGaussian (FP32) rows");
     cudaSetDevice(c->device);
     if (num_states) {   // the old animation stays when the new one is refused
         const MemoryLimits lim = memory_limits(c);
@@ -1155,6 +1303,7 @@ int gs_upload_layers(gs_ctx* c, const uint16_t* halves, uint32_t layer_count) {
     if (!c || (layer_count && !halves)) return GS_ERR_BAD_ARG;
     if (!c->n) return fail(c, GS_ERR_NO_SCENE, "upload the Gaussians before their layers");
     if (layer_count > 256) return fail(c, GS_ERR_TOO_LARGE, "more than 256 layers");
+    if (c->half_rows && layer_count) return fail(c, GS_ERR_BAD_ARG, "appearance layers need GpuGaussian (FP32) rows");
     cudaSetDevice(c->device);
     if (layer_count) {   // the old layers stay when the new ones are refused
         const MemoryLimits lim = memory_limits(c);
@@ -1472,6 +1621,244 @@ int gs_render_features(gs_ctx* c, const gs_camera* cam, void* features_out) {
     GS_CUDA(c, cudaMemcpyAsync(features_out, c->features, c->features_pix * gs::dn::kInC * sizeof(__nv_bfloat16),
                                cudaMemcpyDeviceToDevice, c->stream));
     return GS_OK;
+}
+
+// ---- batches ---------------------------------------------------------------
+namespace {
+
+constexpr uint32_t kMaxBatch = 256;
+
+int ensure_batch(gs_ctx* c, uint32_t count) {
+    if (c->slots.size() < count) c->slots.resize(count);
+    if (c->batch_cap >= count) return GS_OK;
+    if (c->h_slot_fc) cudaFreeHost(c->h_slot_fc);
+    if (c->h_batch_params) cudaFreeHost(c->h_batch_params);
+    if (c->h_batch_first) cudaFreeHost(c->h_batch_first);
+    c->h_slot_fc = nullptr;
+    c->h_batch_params = nullptr;
+    c->h_batch_first = nullptr;
+    dfree(c->batch_params);
+    dfree(c->batch_first);
+    c->batch_cap = 0;
+    GS_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&c->h_slot_fc), kMaxBatch * sizeof(FrameCounters)));
+    GS_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&c->h_batch_params), kMaxBatch * sizeof(gs::RasterParams)));
+    GS_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&c->h_batch_first), (kMaxBatch + 2) * sizeof(uint32_t)));
+    GS_CUDA(c, dalloc(&c->batch_params, kMaxBatch * sizeof(gs::RasterParams)));
+    GS_CUDA(c, dalloc(&c->batch_first, (kMaxBatch + 2) * sizeof(uint32_t)));
+    if (!c->batch_event) GS_CUDA(c, cudaEventCreateWithFlags(&c->batch_event, cudaEventDisableTiming));
+    c->batch_cap = kMaxBatch;
+    return GS_OK;
+}
+
+// Make slot f (swapped into the context) ready for a w x h frame of the scene.
+int prepare_slot(gs_ctx* c, int w, int h, bool fresh_records) {
+    if (c->width != w || c->height != h || !c->ctrl) {
+        dfree(c->ctrl);
+        dfree(c->tile_order);
+        c->width = c->height = 0;
+        int rc = alloc_control(c, w, h);
+        if (rc) return rc;
+    }
+    if (fresh_records || !c->records) {
+        dfree(c->records);
+        GS_CUDA(c, dalloc(&c->records, (size_t)c->n * sizeof(RasterRecord)));
+    }
+    if (!c->entry_cap) return ensure_entries(c, default_entry_cap(c->n));
+    return GS_OK;
+}
+
+// The cull, depth sort and binning of frame k into slot k, and its raster
+// parameters; the slot's counters are read back into h_slot_fc[k].
+int stage_frame(gs_ctx* c, uint32_t k, const gs_camera* cam, void* out) {
+    FrameSlot& f = c->slots[k];
+    swap_slot(c, f);
+    int w = 0, h = 0;
+    int rc = viewport_dims(c, cam, &w, &h);
+    if (!rc) rc = prepare_slot(c, w, h, false);
+    if (!rc) {
+        begin_frame(c, cam);
+        run_cull(c);
+        run_depth_sort(c);
+        run_binning(c, 0.0f, 0.0f, 0.0f);
+        cudaMemcpyAsync(&c->h_slot_fc[k], c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
+        gs::RasterParams r = raster_params(c, background(c));
+        r.out_rgba16f = static_cast<uint16_t*>(out);
+        c->h_batch_params[k] = r;
+    }
+    swap_slot(c, f);
+    return rc;
+}
+
+// Grow the entries of every slot whose binning overflowed; returns the
+// number of such slots (< 0: error).
+int grow_overflowed(gs_ctx* c, uint32_t count, std::vector<uint32_t>& redo) {
+    GS_CUDA(c, cudaEventRecord(c->batch_event, c->stream));
+    GS_CUDA(c, cudaEventSynchronize(c->batch_event));
+    redo.clear();
+    for (uint32_t k = 0; k < count; ++k) {
+        const FrameCounters& fc = c->h_slot_fc[k];
+        if (!fc.tile_overflow) continue;
+        FrameSlot& f = c->slots[k];
+        if (f.entry_cap >= 0x3FFFFFFFu) return fail(c, GS_ERR_TOO_LARGE, "tile entries beyond the largest buffer");
+        const uint64_t need = (uint64_t)fc.tile_entries + fc.tile_overflow;
+        swap_slot(c, f);
+        const int rc = ensure_entries(c, (uint32_t)std::min<uint64_t>(need + need / 4 + 1024, 0x3FFFFFFFull));
+        swap_slot(c, f);
+        if (rc) return rc;
+        redo.push_back(k);
+    }
+    return GS_OK;
+}
+
+int raster_batch(gs_ctx* c, uint32_t count) {
+    uint32_t total = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        c->h_batch_first[k] = total;
+        total += (uint32_t)c->h_batch_params[k].tiles_x * (uint32_t)c->h_batch_params[k].tiles_y;
+    }
+    c->h_batch_first[count] = total;
+    c->h_batch_first[count + 1] = 0;   // the work ticket
+    GS_CUDA(c, cudaMemcpyAsync(c->batch_params, c->h_batch_params, count * sizeof(gs::RasterParams),
+                               cudaMemcpyHostToDevice, c->stream));
+    GS_CUDA(c, cudaMemcpyAsync(c->batch_first, c->h_batch_first, (count + 2) * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, c->stream));
+    static int blocks_per_sm = 0;
+    if (!blocks_per_sm) {
+        int b = 0;
+        gs::raster_batch_occupancy(&b);
+        blocks_per_sm = b > 0 ? b : 1;
+    }
+    StageScope sc(c, ST_RASTER);
+    sc.add(gs::launch_raster_batch_alpha(c->batch_params, c->batch_first, count, c->batch_first + count + 1,
+                                         c->num_sms * (uint32_t)blocks_per_sm, c->stream));
+    return GS_OK;
+}
+
+int batch_checks(gs_ctx* c, uint32_t count) {
+    if (!c->n) return fail(c, GS_ERR_NO_SCENE, "no scene uploaded");
+    if (count > kMaxBatch) return fail(c, GS_ERR_TOO_LARGE, "more than 256 frames in a batch");
+    if (c->knobs.render_mode != GS_MODE_ALPHA) return fail(c, GS_ERR_BAD_ARG, "batches render the alpha mode");
+    return GS_OK;
+}
+
+}  // namespace
+
+int gs_render_batch(gs_ctx* c, const gs_camera* cams, uint32_t count, void* const* outs) {
+    if (!c || (count && (!cams || !outs))) return GS_ERR_BAD_ARG;
+    for (uint32_t k = 0; k < count; ++k) {
+        if (!outs[k]) return GS_ERR_BAD_ARG;
+        if (!gl_clip_convention(&cams[k])) return fail(c, GS_ERR_BAD_ARG, "only the GL clip convention is drawn");
+    }
+    int rc = batch_checks(c, count);
+    if (rc || !count) return rc;
+    cudaSetDevice(c->device);
+    if ((rc = ensure_batch(c, count))) return rc;
+    nvtxRangePushA("gs_render_batch");
+    c->frame_launches = 0;
+    std::vector<uint32_t> redo(count);
+    for (uint32_t k = 0; k < count; ++k) redo[k] = k;
+    for (int attempt = 0; !redo.empty(); ++attempt) {
+        if (attempt > 3) {
+            nvtxRangePop();
+            return fail(c, GS_ERR_TOO_LARGE, "tile entries still overflowing");
+        }
+        for (uint32_t k : redo) {
+            if ((rc = stage_frame(c, k, &cams[k], outs[k]))) {
+                nvtxRangePop();
+                return rc;
+            }
+        }
+        if ((rc = grow_overflowed(c, count, redo))) {
+            nvtxRangePop();
+            return rc;
+        }
+    }
+    rc = raster_batch(c, count);
+    // the statistics of the batch's last frame
+    cudaMemcpyAsync(c->h_fc, c->slots[count - 1].fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
+    cudaEventRecord(c->fc_event, c->stream);
+    c->fc_pending = false;
+    c->last_launches = c->frame_launches;
+    nvtxRangePop();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    return rc;
+}
+
+int gs_render_anim_batch(gs_ctx* c, const gs_camera* cam, const int32_t* states_a, const int32_t* states_b,
+                         const float* weights, uint32_t count, void* const* outs) {
+    if (!c || !cam || (count && (!states_a || !outs))) return GS_ERR_BAD_ARG;
+    if (!gl_clip_convention(cam)) return fail(c, GS_ERR_BAD_ARG, "only the GL clip convention is drawn");
+    int rc = batch_checks(c, count);
+    if (rc || !count) return rc;
+    if (!c->anim_deltas) return fail(c, GS_ERR_BAD_ARG, "no gsanim appearance states uploaded");
+    for (uint32_t k = 0; k < count; ++k) {
+        const int a = states_a[k], b = states_b ? states_b[k] : 0;
+        const float wgt = weights ? weights[k] : 0.0f;
+        if (!outs[k] || a < 0 || a > (int)c->anim_states || b < 0 || b > (int)c->anim_states || !(wgt >= 0.0f) ||
+            wgt > 1.0f)
+            return fail(c, GS_ERR_BAD_ARG, "bad appearance state in the batch");
+    }
+    cudaSetDevice(c->device);
+    if ((rc = ensure_batch(c, count))) return rc;
+    const size_t need = (size_t)count * c->n;
+    if (c->state_colours_cap < need) {
+        dfree(c->state_colours);
+        c->state_colours_cap = 0;
+        GS_CUDA(c, dalloc(&c->state_colours, need * sizeof(float4)));
+        c->state_colours_cap = need;
+    }
+    nvtxRangePushA("gs_render_anim_batch");
+    c->frame_launches = 0;
+    // the geometry, order and tiles of the frame, once (slot 0)
+    std::vector<uint32_t> redo;
+    for (int attempt = 0;; ++attempt) {
+        if ((rc = stage_frame(c, 0, cam, outs[0]))) break;
+        if ((rc = grow_overflowed(c, 1, redo))) break;
+        if (redo.empty()) break;
+        if (attempt >= 3) {
+            rc = fail(c, GS_ERR_TOO_LARGE, "tile entries still overflowing");
+            break;
+        }
+    }
+    if (rc) {
+        nvtxRangePop();
+        return rc;
+    }
+    // per state: the colours of the frame's records, and the raster parameters
+    FrameSlot& f0 = c->slots[0];
+    swap_slot(c, f0);
+    const int sa = c->anim_a, sb = c->anim_b;
+    const float sw = c->anim_w;
+    const gs::RasterParams base = c->h_batch_params[0];
+    {
+        StageScope sc(c, ST_CULL);
+        for (uint32_t k = 0; k < count; ++k) {
+            c->anim_a = states_a[k];
+            c->anim_b = states_b ? states_b[k] : 0;
+            c->anim_w = weights ? weights[k] : 0.0f;
+            gs::CullParams p = cull_params(c);
+            float4* colours = c->state_colours + (size_t)k * c->n;
+            sc.add(gs::launch_recolour(p, c->records, colours, c->num_sms, c->stream));
+            gs::RasterParams r = base;
+            r.colours = colours;
+            r.out_rgba16f = static_cast<uint16_t*>(outs[k]);
+            c->h_batch_params[k] = r;
+        }
+    }
+    c->anim_a = sa;
+    c->anim_b = sb;
+    c->anim_w = sw;
+    swap_slot(c, f0);
+    rc = raster_batch(c, count);
+    cudaMemcpyAsync(c->h_fc, c->slots[0].fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
+    cudaEventRecord(c->fc_event, c->stream);
+    c->fc_pending = false;
+    c->last_launches = c->frame_launches;
+    nvtxRangePop();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    return rc;
 }
 
 int gs_read_stats(gs_ctx* c, gs_stats* s) {

@@ -69,6 +69,7 @@ constexpr int kCullVisThreads = 256;
 constexpr int kCullVisItems = 8;
 constexpr int kCullVisTile = kCullVisThreads * kCullVisItems;
 constexpr int kCullThreads = 128;
+constexpr int kHalfRowChunks = 9;   // 144-byte FP16-SH row: position/opacity, scale, rotation, 48 half SH
 
 // Binning configuration: 8 sorted splats per thread, 1024 per CTA tile; the
 // expansion takes the global entry range in chunks of 1024 entries.
@@ -128,6 +129,7 @@ struct CullParams {
     const uint16_t* layer_halves;   // [(l * n + row) * 48 + j] IEEE half bits
     const float* layer_weights;     // [l * 3 + c] (device)
     int layer_count;
+    int half_rows;               // rows are 144-byte FP16-SH rows (kHalfRowChunks float4 each)
     FrameCounters* fc;
 };
 
@@ -181,6 +183,7 @@ struct RasterParams {
     const uint2* tile_ranges;        // [start, end) per tile
     const uint32_t* tile_order;      // tiles by descending work (CTA b rasterizes tile_order[b])
     const uint32_t* tile_count;      // optional: CTAs b >= *tile_count do nothing (a tile list of the frame)
+    const float4* colours;           // optional: r, g, b per record, replacing the records' colour
     int width, height, tiles_x, tiles_y;
     float bg;
     // stochastic mode (envelope records): the sample's jitter and seed, and
@@ -221,7 +224,11 @@ cudaError_t device_malloc(void** p, size_t bytes);
 
 // Launchers (each returns the number of kernels it launched).
 int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s);
-int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t num_sms, cudaStream_t s);
+int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t num_sms, cudaStream_t s,
+                        uint32_t row_chunks = 16);
+int launch_pack_half_rows(const float4* rows, float4* half_rows, uint32_t n, uint32_t num_sms, cudaStream_t s);
+int launch_recolour(const CullParams& p, const RasterRecord* records, float4* colours, uint32_t num_sms,
+                    cudaStream_t s);
 int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s);
 int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s);
 int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint32_t entry_cap, uint2* ranges,
@@ -230,6 +237,11 @@ int launch_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order, 
 int launch_raster_alpha(const RasterParams& p, cudaStream_t s);
 int launch_raster_stochastic(const RasterParams& p, cudaStream_t s);
 int launch_raster_stochastic2(const RasterParams& p, cudaStream_t s);
+// alpha frames[f] for f < nframes in one persistent launch (first: nframes + 1
+// prefix sums of the frames' tile counts, device; ticket: a zeroed device word)
+int launch_raster_batch_alpha(const RasterParams* frames, const uint32_t* first, uint32_t nframes, uint32_t* ticket,
+                              uint32_t grid, cudaStream_t s);
+void raster_batch_occupancy(int* blocks_per_sm);
 
 int launch_wait_probe(const unsigned long long* status, FrameCounters* fc, uint32_t epoch, int which, uint32_t limit,
                       cudaStream_t s);

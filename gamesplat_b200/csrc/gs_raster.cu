@@ -218,16 +218,21 @@ __device__ __forceinline__ float min_q_box(float A, float B, float C, float X0, 
 // (w & 1, w >> 1); lane l shades pixels (l & 7, l >> 3) and (l & 7, (l >> 3) + 4)
 // of it: the two pixels share a column, hence dx, the column test and the
 // first term of the Gaussian exponent.
-template <int kMode>  // 0 = alpha, 1 = stochastic, 2 = two un-jittered stochastic samples
-__global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) {
-    __shared__ __align__(128) RasterRecord s_rec[2][kBatch];
-    __shared__ __align__(8) uint64_t s_bar[2];
-    __shared__ uint32_t s_bits[kBatch];
-    __shared__ uint8_t s_mask[kBatch];
-    __shared__ float4 s_cen[kMode == 1 ? kBatch : 1];   // stochastic: jittered centre and hash z of the sample
+// Shared memory of one CTA's tile: two staging buffers of records, their
+// barriers, the records' coverage bits and warp-block masks.
+template <int kMode>
+struct __align__(128) RasterShared {
+    RasterRecord rec[2][kBatch];
+    uint64_t bar[2];
+    uint32_t bits[kBatch];
+    uint8_t mask[kBatch];
+    float4 cen[kMode == 1 ? kBatch : 1];   // stochastic: jittered centre and hash z of the sample
+};
 
-    if (p.tile_count && blockIdx.x >= *p.tile_count) return;
-    const uint32_t tile = p.tile_order[blockIdx.x];
+// One 16x16 tile, the whole CTA (used by the per-frame kernel, one tile per
+// CTA, and by the batch kernel, many frames' tiles per CTA in turn).
+template <int kMode>  // 0 = alpha, 1 = stochastic, 2 = two un-jittered stochastic samples
+__device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_t tile, RasterShared<kMode>& sh) {
     const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int x0 = tx * kTileW, y0 = ty * kTileH;
@@ -241,8 +246,8 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     const uint32_t* __restrict__ vals = p.tile_plan->vfinal;
 
     if (threadIdx.x == 0) {
-        mbar_init(&s_bar[0], 1);
-        mbar_init(&s_bar[1], 1);
+        mbar_init(&sh.bar[0], 1);
+        mbar_init(&sh.bar[1], 1);
         mbar_fence_init();
     }
     __syncthreads();
@@ -267,11 +272,11 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     auto issue = [&](uint32_t b) {
         const uint32_t first = b * kBatch;
         const uint32_t cnt = min((uint32_t)kBatch, n - first);
-        uint64_t* bar = &s_bar[b & 1];
+        uint64_t* bar = &sh.bar[b & 1];
         if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, cnt * (uint32_t)sizeof(RasterRecord));
         for (uint32_t i = threadIdx.x; i < cnt; i += kRasterThreads) {
             const uint32_t s = min(vals[range.x + first + i], p.record_cap - 1u);
-            bulk_g2s(&s_rec[b & 1][i], p.records + s, (uint32_t)sizeof(RasterRecord), bar);
+            bulk_g2s(&sh.rec[b & 1][i], p.records + s, (uint32_t)sizeof(RasterRecord), bar);
         }
     };
     auto pixels_done = [&]() -> bool {
@@ -284,10 +289,10 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
     for (uint32_t b = 0; b < nb; ++b) {
         if (b + 1 < nb) issue(b + 1);
         const uint32_t ph = (b & 1) ? phase1 : phase0;
-        if (!mbar_wait_bounded(&s_bar[b & 1], ph)) failed = true;
+        if (!mbar_wait_bounded(&sh.bar[b & 1], ph)) failed = true;
         if (b & 1) phase1 ^= 1u; else phase0 ^= 1u;
         const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
-        const RasterRecord* recs = s_rec[b & 1];
+        const RasterRecord* recs = sh.rec[b & 1];
         // Coverage bits of each staged record and which of the four 8x8 warp
         // blocks it can shade (one thread per record): blocks its rectangle
         // touches, minus those where the splat's ellipse q(d) <= s_max misses
@@ -295,6 +300,16 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         // s_max, far above the rounding of q and of the exact per-pixel sum).
         for (uint32_t i = threadIdx.x; i < cnt; i += kRasterThreads) {
             const RasterRecord* R = recs + i;
+            if (p.colours) {
+                // per-frame colours (gsanim state batches): the record's r, g, b replaced
+                const uint32_t si = min(vals[range.x + b * kBatch + i], p.record_cap - 1u);
+                const float4 col = __ldg(p.colours + si);
+                RasterRecord* Rw = const_cast<RasterRecord*>(R);
+                Rw->r = col.x;
+                Rw->g = col.y;
+                Rw->b = col.z;
+                if (kMode != 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            }
             const uint2 rr = reinterpret_cast<const uint2*>(R)[5];
             uint32_t bits;
             float cen_x, cen_y;
@@ -310,13 +325,13 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
                            : 0u;
                 cen_x = add(R->cx, p.jitter_x);
                 cen_y = add(R->cy, p.jitter_y);
-                s_cen[i] = make_float4(cen_x, cen_y, add((float)R->splat_id, p.frame_seed), 0.0f);
+                sh.cen[i] = make_float4(cen_x, cen_y, add((float)R->splat_id, p.frame_seed), 0.0f);
             } else {
                 bits = rect_bits(rr.x, rr.y, x0, y0);
                 cen_x = R->cx;
                 cen_y = R->cy;
             }
-            s_bits[i] = bits;
+            sh.bits[i] = bits;
             if (kMode == 0) {
                 // coverage bits next to g, b: one 16-byte load per splat in the loop
                 const_cast<RasterRecord*>(R)->rect_x = bits;
@@ -341,13 +356,13 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
                     if (m > thr) blocks &= ~(1u << w);
                 }
             }
-            s_mask[i] = (uint8_t)blocks;
+            sh.mask[i] = (uint8_t)blocks;
         }
         __syncthreads();
         // Warp-uniform control flow only; per-pixel work is predicated.
         bool warp_done = __any_sync(0xffffffffu, failed) || __all_sync(0xffffffffu, pixels_done());
         for (uint32_t c = 0; c < cnt && !warp_done; c += 32) {
-            const bool mine = c + lane < cnt && ((s_mask[c + lane] >> warp) & 1u);
+            const bool mine = c + lane < cnt && ((sh.mask[c + lane] >> warp) & 1u);
             uint32_t todo = __ballot_sync(0xffffffffu, mine);
             if (kMode == 0) {
                 // one splat of the warp's list into both pixels' state
@@ -393,10 +408,10 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
                 todo &= todo - 1u;
                 float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
                 const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
-                const uint32_t bits = s_bits[j];
+                const uint32_t bits = sh.bits[j];
                 float hz = 0.0f;
                 if (kMode == 1) {
-                    const float4 cz = s_cen[j];
+                    const float4 cz = sh.cen[j];
                     q0.x = cz.x;
                     q0.y = cz.y;
                     hz = cz.z;
@@ -452,7 +467,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         if (all_done) {
             if (b + 1 < nb) {
                 const uint32_t ph2 = ((b + 1) & 1) ? phase1 : phase0;
-                if (!mbar_wait_bounded(&s_bar[(b + 1) & 1], ph2)) failed = true;
+                if (!mbar_wait_bounded(&sh.bar[(b + 1) & 1], ph2)) failed = true;
             }
             break;
         }
@@ -472,6 +487,51 @@ __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) 
         if (in0) write_pixel_stoch(p, px, py0, S0);
         if (in1) write_pixel_stoch(p, px, py1, S1);
     }
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) {
+    __shared__ RasterShared<kMode> sh;
+    if (p.tile_count && blockIdx.x >= *p.tile_count) return;
+    raster_tile<kMode>(p, p.tile_order[blockIdx.x], sh);
+}
+
+// Many frames in one persistent launch: work item w is tile
+// frames[f].tile_order[w - first[f]] of the frame f with first[f] <= w <
+// first[f + 1]; CTAs take items by ticket until all are done.
+template <int kMode>
+__global__ void __launch_bounds__(kRasterThreads) raster_batch_kernel(const RasterParams* __restrict__ frames,
+                                                                      const uint32_t* __restrict__ first,
+                                                                      uint32_t nframes, uint32_t* __restrict__ ticket) {
+    __shared__ RasterShared<kMode> sh;
+    __shared__ uint32_t s_item;
+    const uint32_t total = first[nframes];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const uint32_t w = s_item;
+        if (w >= total) break;
+        uint32_t lo = 0, hi = nframes;   // last f with first[f] <= w
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (first[mid] <= w) lo = mid;
+            else hi = mid;
+        }
+        const RasterParams p = frames[lo];
+        raster_tile<kMode>(p, p.tile_order[w - first[lo]], sh);
+        __syncthreads();
+    }
+}
+
+void raster_batch_occupancy(int* blocks_per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_batch_kernel<0>, kRasterThreads, 0);
+}
+
+int launch_raster_batch_alpha(const RasterParams* frames, const uint32_t* first, uint32_t nframes, uint32_t* ticket,
+                              uint32_t grid, cudaStream_t s) {
+    if (nframes == 0) return 0;
+    raster_batch_kernel<0><<<grid, kRasterThreads, 0, s>>>(frames, first, nframes, ticket);
+    return 1;
 }
 
 int launch_raster_alpha(const RasterParams& p, cudaStream_t s) {

@@ -217,6 +217,31 @@ class Renderer:
         L.check(st, "gs_set_gps_budget", self._ctx)
         return True
 
+    # -- batches ---------------------------------------------------------------
+    def render_batch(self, cams, out_ptrs) -> None:
+        """Alpha frames of several cameras (any viewports) into device images
+        (out_ptrs[k]: W_k * H_k * 4 halves), one persistent raster launch."""
+        n = len(cams)
+        arr = (L.GsCamera * n)(*[camera_from_array(c) for c in cams])
+        outs = (C.c_void_p * n)(*[C.c_void_p(p) for p in out_ptrs])
+        L.check(L.lib().gs_render_batch(self._ctx, arr, n, outs), "gs_render_batch", self._ctx)
+
+    def render_anim_batch(self, cam, states_a, out_ptrs, states_b=None, weights=None) -> None:
+        """gsanim appearance states of one camera into device images."""
+        n = len(states_a)
+        a = np.ascontiguousarray(states_a, np.int32)
+        b = np.ascontiguousarray(states_b if states_b is not None else np.zeros(n), np.int32)
+        w = np.ascontiguousarray(weights if weights is not None else np.zeros(n), np.float32)
+        outs = (C.c_void_p * n)(*[C.c_void_p(p) for p in out_ptrs])
+        c = camera_from_array(cam)
+        L.check(L.lib().gs_render_anim_batch(self._ctx, C.byref(c), a.ctypes.data, b.ctypes.data, w.ctypes.data, n,
+                                             outs), "gs_render_anim_batch", self._ctx)
+
+    def set_row_format(self, fp16_sh: bool) -> None:
+        """Row format of the next upload: FP16 SH coefficients (144-byte rows,
+        SH3 on the tensor cores) or the FP32 GpuGaussian rows."""
+        L.check(L.lib().gs_set_row_format(self._ctx, int(bool(fp16_sh))), "gs_set_row_format", self._ctx)
+
     # -- denoised mode ---------------------------------------------------------
     def set_denoiser(self, denoiser) -> None:
         """Attach a gamesplat_b200.denoiser.Denoiser (kept alive by the caller) for the denoised mode."""

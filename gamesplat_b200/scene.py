@@ -106,3 +106,45 @@ def orbit_pose(k: int, frames: int = 120, radius: float = 6.0):
     fwd = (math.sin(float(yaw)), 0.0, math.cos(float(yaw)))
     pos = tuple(float(np.float32(-radius * c)) for c in fwd)
     return pos, float(yaw), 0.0
+
+
+def look_at_pose(position, target):
+    """(yaw, pitch) of the reference fly camera (z_up off) at `position` looking
+    at `target`: forward = (cos p sin y, sin p, cos p cos y) (src/camera.cpp:22-33)."""
+    d = np.asarray(target, np.float64) - np.asarray(position, np.float64)
+    d /= np.linalg.norm(d)
+    return float(math.atan2(d[0], d[2])), float(math.asin(max(-1.0, min(1.0, d[1]))))
+
+
+BATCH_VIEWPORTS = ((512, 512), (1280, 720), (1920, 1080))
+
+
+def batch_cameras(seed: int = 3, count: int = 64):
+    """The batched workload's cameras: positions uniform on the 4-8 m shell
+    around the origin, each aimed at a point uniform in the 1 m ball, the
+    viewport cycling through 512x512, 1280x720 and 1920x1080.  Returns
+    [(position, yaw, pitch, width, height)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        r = rng.uniform(4.0, 8.0)
+        t = rng.normal(size=3)
+        t *= rng.uniform(0.0, 1.0) ** (1.0 / 3.0) / np.linalg.norm(t)
+        pos = tuple(float(np.float32(v)) for v in d * r)
+        yaw, pitch = look_at_pose(pos, t)
+        w, h = BATCH_VIEWPORTS[k % len(BATCH_VIEWPORTS)]
+        out.append((pos, yaw, pitch, w, h))
+    return out
+
+
+def anim_deltas(seed: int, n: int, states: int) -> np.ndarray:
+    """gsanim appearance states of the batched workload: int8 SH deltas
+    round(N(0, 20)) clipped to [-127, 127], (states, n, 48), for a scale of 1/256."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((states, n, 48), np.int8)
+    for s in range(states):
+        out[s] = np.clip(np.rint(rng.normal(0.0, 20.0, size=(n, 48))), -127, 127).astype(np.int8)
+    return out
+

@@ -147,6 +147,16 @@ int gs_set_mode(gs_ctx* ctx, int render_mode);
  * The caller keeps ownership of `rows`.  Replaces any previous scene. */
 int gs_upload_rows(gs_ctx* ctx, const float* rows, uint64_t count);
 
+/* Row format of the next upload (no counterpart in the reference, whose rows
+ * are always the FP32 GpuGaussian): 0 = GpuGaussian rows kept as uploaded
+ * (256 bytes, the default); 1 = 144-byte rows with the SH coefficients in
+ * IEEE half (position, opacity, scale and rotation stay FP32, as do the
+ * projected records and all arithmetic after the cull): the upload converts
+ * the GpuGaussian rows on the device, and the cull evaluates SH3 on the tensor
+ * cores (FP16 operands, FP32 accumulation).  Scenes in format 1 take no
+ * gsanim deltas or layers (GS_ERR_BAD_ARG). */
+int gs_set_row_format(gs_ctx* ctx, int format);
+
 /* As gs_upload_rows, from device memory (stream-ordered copy). */
 int gs_upload_rows_device(gs_ctx* ctx, const float* rows_dev, uint64_t count);
 
@@ -242,6 +252,30 @@ uint64_t gs_scene_device_bytes(uint64_t count, uint32_t gps_work_items);
  * therefore complete; GS_ERR_TOO_LARGE if the entries exceed the largest
  * buffer (2^30 - 1 entries), GS_ERR_OOM if growing fails. */
 int gs_render(gs_ctx* ctx, const gs_camera* cam, void* rgba16f_out);
+
+/* Batches (no counterpart in the reference, which draws one frame per call):
+ * `count` alpha-mode frames (at most 256) rendered as gs_render would render
+ * them one after another, each into its own device image outs[k]; cameras may
+ * differ in position and viewport size.  Every frame's cull, depth sort and
+ * binning run in turn into buffers the context keeps per frame slot, then one
+ * persistent rasterizer launch composites all frames' tiles, taking
+ * (frame, tile) work items by ticket.  Each image is identical to the
+ * frame's gs_render image.  Waits once for the frames' tile-entry counts
+ * (growing and re-binning overflowed frames, as gs_render does).  The slots
+ * hold each frame's raster records and tile entries (about 0.2 KB per
+ * Gaussian per frame), kept until the scene changes. */
+int gs_render_batch(gs_ctx* ctx, const gs_camera* cams, uint32_t count, void* const* outs);
+
+/* A batch of `count` gsanim appearance states of one camera (at most 256):
+ * frame k is what gs_render draws after gs_set_anim_state(states_a[k],
+ * states_b[k], weights[k]) (states_b / weights may be NULL for 0), into
+ * outs[k].  The states share the frame's geometry, depth order and tiles,
+ * computed once; per state only the colours of the visible splats are
+ * evaluated again (the SH of shaders/cull.glsl:125-164, 323-417 with that
+ * state's deltas), and one persistent rasterizer launch composites all
+ * states.  Needs gs_upload_anim; alpha mode. */
+int gs_render_anim_batch(gs_ctx* ctx, const gs_camera* cam, const int32_t* states_a, const int32_t* states_b,
+                         const float* weights, uint32_t count, void* const* outs);
 
 /* gs_render into host memory: includes the host->device camera copy and the
  * device->host image copy, and waits for them. */

@@ -1,0 +1,88 @@
+"""GPU tests of the FP16-SH row format (gs_set_row_format(ctx, 1)): 144-byte
+rows with the SH coefficients in IEEE half, SH3 evaluated on the tensor
+cores with FP32 accumulation, everything else FP32.
+
+- Projected records against the CPU oracle run on the same rows with their
+  SH rounded to half (oracle.sh_to_fp16): visibility, keys, centre, radius,
+  conic, depth and covariance bit-exact (those fields never touch SH); the
+  colour within 1e-4 (the tensor cores' sums in another order).
+- The frame against the oracle frame of those rows: within the RGBA16F parity
+  gate (max-abs 2^-9, PSNR >= 55 dB).
+- The frame against the float64 restatement of the splatting equations on
+  the original FP32 rows (oracle64), on 8 cameras: max-abs, PSNR and the
+  fraction of pixels over 2^-9 are stated, and must stay above 80 dB with no
+  pixel over 2^-9.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from gamesplat_b200 import Renderer, _lib as L
+from gamesplat_b200 import renderer as RR
+from oracle import oracle as O
+from oracle import oracle64 as O64
+
+from helpers import image_gate, oracle_alpha, psnr, small_rows
+
+pytestmark = pytest.mark.gpu
+
+W, H = 320, 180
+
+
+def cameras(k):
+    poses = []
+    for i in range(k):
+        a = np.pi + 0.35 * (i - k / 2) / k
+        r = 3.0 + 0.2 * (i % 3)
+        poses.append(((float(r * np.sin(a + np.pi) * 0.3), 0.15 * (i % 2), float(r)), float(a), -0.05 * (i % 3)))
+    return [RR.camera_uniforms(p, y, pt, W, H) for p, y, pt in poses]
+
+
+def _half_renderer(rows, **knobs):
+    r = Renderer(0)
+    r.set(splat_render_mode="alpha", black_background=1, **knobs)
+    r.set_row_format(True)
+    r.upload_gaussians(rows)
+    return r
+
+
+@pytest.mark.parametrize("sh_degree", [3, 1])
+def test_fp16_sh_records_match_the_oracle(sh_degree):
+    rows = small_rows(30_000, seed=2)
+    cam = RR.camera_uniforms((0.0, 0.0, 3.0), float(np.pi), 0.0, W, H)
+    with _half_renderer(rows, write_invisible_records=1, sh_degree=sh_degree) as r:
+        r.draw_frame(cam)
+        n = rows.shape[0]
+        keys = r.debug_read(L.GS_DEBUG_KEYS, n)
+        proj = r.debug_read(L.GS_DEBUG_PROJECTED, n * 16, np.float32, (n, 16))
+        st = r.stats()
+    ids, okeys, oproj, vc, _ = O.cull(O.sh_to_fp16(rows), cam, sh_degree=sh_degree)
+    assert st.visible_count == vc
+    assert np.array_equal(keys, okeys)
+    vis = ids != O.SENTINEL
+    assert np.array_equal(proj[vis][:, 3:].view(np.uint32), oproj[vis][:, 3:].view(np.uint32))
+    assert float(np.abs(proj[vis][:, :3] - oproj[vis][:, :3]).max()) <= 1e-4
+
+
+def test_fp16_sh_frame_in_the_parity_gate():
+    rows = small_rows(30_000, seed=3)
+    cam = RR.camera_uniforms((0.0, 0.0, 3.0), float(np.pi), 0.0, W, H)
+    ref, _ = oracle_alpha(O.sh_to_fp16(rows), cam, W, H)
+    with _half_renderer(rows) as r:
+        img = r.draw_frame(cam)
+    gate = image_gate(img, ref)
+    assert gate["ok"], gate
+
+
+def test_fp16_sh_error_against_fp64_on_8_cameras():
+    rows = small_rows(12_000, seed=4)
+    report = []
+    with _half_renderer(rows) as r:
+        for cam in cameras(8):
+            img = r.draw_frame(cam).astype(np.float64)
+            exact = O64.frame64(rows, cam, W, H)
+            err = np.abs(img - exact)
+            report.append((float(err.max()), psnr(img, exact), float((err > 2.0 ** -9).mean())))
+    for max_abs, db, over in report:
+        assert db > 80.0 and over == 0.0, report
