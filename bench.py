@@ -391,6 +391,20 @@ def batched_mode(r, stream, args):
         stream.synchronize()
         return e0.elapsed_time(e1) / reps
 
+    # the autotuner picks the tile shape and the frames per raster launch
+    import ctypes as C
+
+    from gamesplat_b200 import _lib as L
+
+    arr = (L.GsCamera * len(cams))(*[R.camera_from_array(c) for c in cams])
+    cptr = (C.c_void_p * len(cams))(*[C.c_void_p(p) for p in ptrs])
+    tune = L.GsTuneResult()
+    L.check(L.lib().gs_autotune_batch(r._ctx, arr, len(cams), cptr, C.byref(tune)), "gs_autotune_batch")
+    out["autotuner"] = {"tile": f"{tune.tile_w}x{tune.tile_h}", "batch_depth": int(tune.batch_depth),
+                        "best_ms": float(tune.best_ms),
+                        "tried": [{"tile": f"{tune.tried_tile_w[i]}x{tune.tried_tile_h[i]}",
+                                   "batch_depth": int(tune.tried_depth[i]), "ms": float(tune.tried_ms[i])}
+                                  for i in range(tune.tried)]}
     reps = 3
     t_batch = timed(lambda: r.render_batch(cams, ptrs), reps)
     t_seq = timed(lambda: [r.draw_frame(c, out_ptr=p) for c, p in zip(cams, ptrs)], reps)
@@ -669,6 +683,10 @@ def run_ours(args):
         precision = precision_variant(args)
     if not args.no_modes and rank == 0:
         modes["batched"] = batched_mode(r, stream, args)
+        from gamesplat_b200 import _lib as L
+
+        L.check(L.lib().gs_set_tile_shape(r._ctx, 16, 16), "gs_set_tile_shape")
+        L.check(L.lib().gs_set_batch_depth(r._ctx, 0), "gs_set_batch_depth")
     if not args.no_modes:
         den = denoised_mode(r, stream, out, frame, args, rank)
         if den is not None:

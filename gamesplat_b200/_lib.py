@@ -52,7 +52,7 @@ EXPORTS = (
     "gs_denoiser_backward", "gs_denoiser_loss", "gs_denoiser_adam", "gs_denoiser_train_step", "gs_denoiser_status",
     "gs_conv3x3_scratch_bytes", "gs_conv3x3_bf16", "gs_conv3x3_wgrad_bf16",
     "gs_set_denoiser", "gs_set_denoise_budget", "gs_render_features", "gs_set_row_format",
-    "gs_render_batch", "gs_render_anim_batch",
+    "gs_render_batch", "gs_render_anim_batch", "gs_set_tile_shape", "gs_set_batch_depth", "gs_autotune_batch",
 )
 
 
@@ -124,6 +124,22 @@ class GsGsanimInfo(C.Structure):
         ("log2_min", C.c_float),
         ("log2_max", C.c_float),
         ("duration_seconds", C.c_double),
+    ]
+
+
+class GsTuneResult(C.Structure):
+    """gs_tune_result (include/gs_api.h)."""
+
+    _fields_ = [
+        ("tile_w", C.c_int32),
+        ("tile_h", C.c_int32),
+        ("batch_depth", C.c_uint32),
+        ("best_ms", C.c_float),
+        ("tried", C.c_uint32),
+        ("tried_tile_w", C.c_int32 * 32),
+        ("tried_tile_h", C.c_int32 * 32),
+        ("tried_depth", C.c_uint32 * 32),
+        ("tried_ms", C.c_float * 32),
     ]
 
 
@@ -219,6 +235,9 @@ def lib() -> C.CDLL:
         "gs_set_denoiser": (i32, [vp, vp]),
         "gs_set_row_format": (i32, [vp, i32]),
         "gs_render_batch": (i32, [vp, vp, u32, vp]),
+        "gs_set_tile_shape": (i32, [vp, i32, i32]),
+        "gs_set_batch_depth": (i32, [vp, u32]),
+        "gs_autotune_batch": (i32, [vp, vp, u32, vp, C.POINTER(GsTuneResult)]),
         "gs_render_anim_batch": (i32, [vp, vp, vp, vp, vp, u32, vp]),
         "gs_set_denoise_budget": (i32, [vp, f32, i32]),
         "gs_render_features": (i32, [vp, C.POINTER(GsCamera), vp]),

@@ -79,10 +79,10 @@ __device__ __forceinline__ BinItem bin_one(const BinParams& p, uint32_t s, uint3
         rc.j1 = min(rc.j1, (int)fminf(fj1, 32767.0f) + 1);
     }
     if (rc.i0 >= rc.i1 || rc.j0 >= rc.j1) return it;
-    it.tx0 = rc.i0 / kTileW;
-    it.tx1 = (rc.i1 - 1) / kTileW;
-    it.ty0 = rc.j0 / kTileH;
-    it.ty1 = (rc.j1 - 1) / kTileH;
+    it.tx0 = rc.i0 >> p.tile_shift_x;
+    it.tx1 = (rc.i1 - 1) >> p.tile_shift_x;
+    it.ty0 = rc.j0 >> p.tile_shift_y;
+    it.ty1 = (rc.j1 - 1) >> p.tile_shift_y;
     it.count = (uint32_t)((it.tx1 - it.tx0 + 1) * (it.ty1 - it.ty0 + 1));
     RasterRecord rec;
     rec.cx = ccx;

@@ -49,6 +49,7 @@ struct DevBuf {
 // sort and binning run, so the stages need no batch-specific code.
 struct FrameSlot {
     int width = 0, height = 0, tiles_x = 0, tiles_y = 0;
+    int tile_w = 16, tile_h = 16;
     uint32_t tiles_cap = 0;
     void* ctrl = nullptr;
     size_t ctrl_bytes = 0;
@@ -148,6 +149,9 @@ struct gs_ctx {
 
     // image targets
     int width = 0, height = 0, tiles_x = 0, tiles_y = 0;
+    int tile_w = 16, tile_h = 16;            // tile shape of the targets
+    int alpha_tile_w = 16, alpha_tile_h = 16;   // tile shape of alpha frames (gs_set_tile_shape)
+    uint32_t batch_depth = 0;                // frames per persistent raster launch in batches (0: all)
     uint16_t* out16 = nullptr;     // internal RGBA16F (gs_render_host)
     uint16_t* h_out16 = nullptr;   // pinned
     size_t h_out16_bytes = 0;
@@ -186,6 +190,8 @@ struct gs_ctx {
     float4* state_colours = nullptr;              // anim batches: n x states colours
     size_t state_colours_cap = 0;
     cudaEvent_t batch_event = nullptr;
+    cudaEvent_t params_event = nullptr;           // after the last copy out of h_batch_params / h_batch_first
+    bool params_pending = false;
 
     // profiling
     bool profiling = false;
@@ -280,6 +286,8 @@ void swap_slot(gs_ctx* c, FrameSlot& f) {
     std::swap(c->height, f.height);
     std::swap(c->tiles_x, f.tiles_x);
     std::swap(c->tiles_y, f.tiles_y);
+    std::swap(c->tile_w, f.tile_w);
+    std::swap(c->tile_h, f.tile_h);
     std::swap(c->tiles_cap, f.tiles_cap);
     std::swap(c->ctrl, f.ctrl);
     std::swap(c->ctrl_bytes, f.ctrl_bytes);
@@ -456,8 +464,10 @@ int ensure_entries(gs_ctx* c, uint32_t cap) {
 
 // The per-frame control block of a w x h frame in the context's fields:
 // FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges, and the tile order.
-int alloc_control(gs_ctx* c, int w, int h) {
-    const int tx = (w + gs::kTileW - 1) / gs::kTileW, ty = (h + gs::kTileH - 1) / gs::kTileH;
+int alloc_control(gs_ctx* c, int w, int h, int tw, int th) {
+    const int tx = (w + tw - 1) / tw, ty = (h + th - 1) / th;
+    c->tile_w = tw;
+    c->tile_h = th;
     c->tiles_cap = (uint32_t)(tx * ty);
     // control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges
     size_t off = 0;
@@ -490,12 +500,21 @@ int alloc_control(gs_ctx* c, int w, int h) {
     return GS_OK;
 }
 
+// Tile shape of the context's frames: the alpha knob in alpha mode, 16x16 otherwise.
+void frame_tile_shape(const gs_ctx* c, int* tw, int* th) {
+    const bool alpha = c->knobs.render_mode == GS_MODE_ALPHA;
+    *tw = alpha ? c->alpha_tile_w : 16;
+    *th = alpha ? c->alpha_tile_h : 16;
+}
+
 int ensure_targets(gs_ctx* c, int w, int h) {
     if (w <= 0 || h <= 0) return fail(c, GS_ERR_BAD_ARG, "viewport must be positive");
     if (w > 32767 || h > 32767) return fail(c, GS_ERR_TOO_LARGE, "viewport beyond 32767 pixels");
-    if (c->width == w && c->height == h && c->ctrl) return GS_OK;
+    int tw = 16, th = 16;
+    frame_tile_shape(c, &tw, &th);
+    if (c->width == w && c->height == h && c->ctrl && c->tile_w == tw && c->tile_h == th) return GS_OK;
     release_targets(c);
-    int rc = alloc_control(c, w, h);
+    int rc = alloc_control(c, w, h, tw, th);
     if (rc) return rc;
     const cudaError_t e = dalloc(&c->out16, (size_t)w * h * 8);
     if (e != cudaSuccess) {
@@ -615,6 +634,8 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = fals
         p.height = c->height;
         p.tiles_x = c->tiles_x;
         p.tiles_y = c->tiles_y;
+        p.tile_shift_x = c->tile_w == 32 ? 5 : c->tile_w == 8 ? 3 : 4;
+        p.tile_shift_y = c->tile_h == 32 ? 5 : c->tile_h == 8 ? 3 : 4;
         p.records = c->records;
         p.entry_keys = c->ekeys[1];
         p.entry_vals = c->evals[1];
@@ -672,6 +693,8 @@ gs::RasterParams raster_params(gs_ctx* c, float bg) {
     r.height = c->height;
     r.tiles_x = c->tiles_x;
     r.tiles_y = c->tiles_y;
+    r.tile_w = c->tile_w;
+    r.tile_h = c->tile_h;
     r.bg = bg;
     r.fc = c->fc;
     return r;
@@ -1084,6 +1107,7 @@ void gs_destroy(gs_ctx* c) {
     dfree(c->batch_params);
     dfree(c->batch_first);
     if (c->batch_event) cudaEventDestroy(c->batch_event);
+    if (c->params_event) cudaEventDestroy(c->params_event);
     if (c->h_out16) cudaFreeHost(c->h_out16);
     for (auto e : c->chunk_events)
         if (e) cudaEventDestroy(e);
@@ -1646,17 +1670,18 @@ int ensure_batch(gs_ctx* c, uint32_t count) {
     GS_CUDA(c, dalloc(&c->batch_params, kMaxBatch * sizeof(gs::RasterParams)));
     GS_CUDA(c, dalloc(&c->batch_first, (kMaxBatch + 2) * sizeof(uint32_t)));
     if (!c->batch_event) GS_CUDA(c, cudaEventCreateWithFlags(&c->batch_event, cudaEventDisableTiming));
+    if (!c->params_event) GS_CUDA(c, cudaEventCreateWithFlags(&c->params_event, cudaEventDisableTiming));
     c->batch_cap = kMaxBatch;
     return GS_OK;
 }
 
 // Make slot f (swapped into the context) ready for a w x h frame of the scene.
-int prepare_slot(gs_ctx* c, int w, int h, bool fresh_records) {
-    if (c->width != w || c->height != h || !c->ctrl) {
+int prepare_slot(gs_ctx* c, int w, int h, int tw, int th, bool fresh_records) {
+    if (c->width != w || c->height != h || !c->ctrl || c->tile_w != tw || c->tile_h != th) {
         dfree(c->ctrl);
         dfree(c->tile_order);
         c->width = c->height = 0;
-        int rc = alloc_control(c, w, h);
+        int rc = alloc_control(c, w, h, tw, th);
         if (rc) return rc;
     }
     if (fresh_records || !c->records) {
@@ -1670,11 +1695,16 @@ int prepare_slot(gs_ctx* c, int w, int h, bool fresh_records) {
 // The cull, depth sort and binning of frame k into slot k, and its raster
 // parameters; the slot's counters are read back into h_slot_fc[k].
 int stage_frame(gs_ctx* c, uint32_t k, const gs_camera* cam, void* out) {
+    if (c->params_pending) {   // the pinned parameters of the last launch are copied before they are rewritten
+        GS_CUDA(c, cudaEventSynchronize(c->params_event));
+        c->params_pending = false;
+    }
     FrameSlot& f = c->slots[k];
+    const int tw = c->alpha_tile_w, th = c->alpha_tile_h;
     swap_slot(c, f);
     int w = 0, h = 0;
     int rc = viewport_dims(c, cam, &w, &h);
-    if (!rc) rc = prepare_slot(c, w, h, false);
+    if (!rc) rc = prepare_slot(c, w, h, tw, th, false);
     if (!rc) {
         begin_frame(c, cam);
         run_cull(c);
@@ -1722,6 +1752,8 @@ int raster_batch(gs_ctx* c, uint32_t count) {
                                cudaMemcpyHostToDevice, c->stream));
     GS_CUDA(c, cudaMemcpyAsync(c->batch_first, c->h_batch_first, (count + 2) * sizeof(uint32_t),
                                cudaMemcpyHostToDevice, c->stream));
+    GS_CUDA(c, cudaEventRecord(c->params_event, c->stream));
+    c->params_pending = true;
     static int blocks_per_sm = 0;
     if (!blocks_per_sm) {
         int b = 0;
@@ -1730,7 +1762,8 @@ int raster_batch(gs_ctx* c, uint32_t count) {
     }
     StageScope sc(c, ST_RASTER);
     sc.add(gs::launch_raster_batch_alpha(c->batch_params, c->batch_first, count, c->batch_first + count + 1,
-                                         c->num_sms * (uint32_t)blocks_per_sm, c->stream));
+                                         c->num_sms * (uint32_t)blocks_per_sm, c->h_batch_params[0].tile_w,
+                                         c->stream));
     return GS_OK;
 }
 
@@ -1752,37 +1785,116 @@ int gs_render_batch(gs_ctx* c, const gs_camera* cams, uint32_t count, void* cons
     int rc = batch_checks(c, count);
     if (rc || !count) return rc;
     cudaSetDevice(c->device);
-    if ((rc = ensure_batch(c, count))) return rc;
+    const uint32_t depth = c->batch_depth ? std::min(c->batch_depth, count) : count;
+    if ((rc = ensure_batch(c, depth))) return rc;
     nvtxRangePushA("gs_render_batch");
     c->frame_launches = 0;
-    std::vector<uint32_t> redo(count);
-    for (uint32_t k = 0; k < count; ++k) redo[k] = k;
-    for (int attempt = 0; !redo.empty(); ++attempt) {
-        if (attempt > 3) {
-            nvtxRangePop();
-            return fail(c, GS_ERR_TOO_LARGE, "tile entries still overflowing");
-        }
-        for (uint32_t k : redo) {
-            if ((rc = stage_frame(c, k, &cams[k], outs[k]))) {
-                nvtxRangePop();
-                return rc;
+    std::vector<uint32_t> redo;
+    // frames in chunks of `depth`: the stages of a chunk's frames into its
+    // slots, then one persistent raster launch for the chunk
+    for (uint32_t k0 = 0; k0 < count && !rc; k0 += depth) {
+        const uint32_t m = std::min(depth, count - k0);
+        redo.resize(m);
+        for (uint32_t k = 0; k < m; ++k) redo[k] = k;
+        for (int attempt = 0; !redo.empty() && !rc; ++attempt) {
+            if (attempt > 3) {
+                rc = fail(c, GS_ERR_TOO_LARGE, "tile entries still overflowing");
+                break;
             }
+            for (uint32_t k : redo)
+                if ((rc = stage_frame(c, k, &cams[k0 + k], outs[k0 + k]))) break;
+            if (!rc) rc = grow_overflowed(c, m, redo);
         }
-        if ((rc = grow_overflowed(c, count, redo))) {
-            nvtxRangePop();
-            return rc;
+        if (!rc) rc = raster_batch(c, m);
+        if (!rc) {
+            // the statistics of the batch's last frame
+            cudaMemcpyAsync(c->h_fc, c->slots[m - 1].fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
+            cudaEventRecord(c->fc_event, c->stream);
         }
     }
-    rc = raster_batch(c, count);
-    // the statistics of the batch's last frame
-    cudaMemcpyAsync(c->h_fc, c->slots[count - 1].fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
-    cudaEventRecord(c->fc_event, c->stream);
     c->fc_pending = false;
     c->last_launches = c->frame_launches;
     nvtxRangePop();
+    if (rc) return rc;
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
-    return rc;
+    return GS_OK;
+}
+
+int gs_set_tile_shape(gs_ctx* c, int tile_w, int tile_h) {
+    if (!c) return GS_ERR_BAD_ARG;
+    const bool ok = (tile_w == 16 && tile_h == 16) || (tile_w == 32 && tile_h == 8) || (tile_w == 8 && tile_h == 32);
+    if (!ok) return fail(c, GS_ERR_BAD_ARG, "tile shapes: 16x16, 32x8, 8x32");
+    c->alpha_tile_w = tile_w;
+    c->alpha_tile_h = tile_h;
+    return GS_OK;
+}
+
+int gs_set_batch_depth(gs_ctx* c, uint32_t depth) {
+    if (!c || depth > kMaxBatch) return GS_ERR_BAD_ARG;
+    c->batch_depth = depth;
+    return GS_OK;
+}
+
+int gs_autotune_batch(gs_ctx* c, const gs_camera* cams, uint32_t count, void* const* outs, gs_tune_result* res) {
+    if (!c || !cams || !outs || !count) return GS_ERR_BAD_ARG;
+    int rc = batch_checks(c, count);
+    if (rc) return rc;
+    static const int shapes[3][2] = {{16, 16}, {32, 8}, {8, 32}};
+    static const uint32_t depths[6] = {4, 8, 16, 32, 64, 128};
+    const int keep_w = c->alpha_tile_w, keep_h = c->alpha_tile_h;
+    const uint32_t keep_d = c->batch_depth;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    GS_CUDA(c, cudaEventCreate(&e0));
+    GS_CUDA(c, cudaEventCreate(&e1));
+    gs_tune_result r{};
+    r.best_ms = 3.0e38f;
+    int tried = 0;
+    for (int si = 0; si < 3 && !rc; ++si) {
+        for (int di = 0; di < 6 && !rc; ++di) {
+            const uint32_t d = depths[di];
+            if (d > count && di > 0 && depths[di - 1] >= count) break;
+            c->alpha_tile_w = shapes[si][0];
+            c->alpha_tile_h = shapes[si][1];
+            c->batch_depth = std::min(d, count);
+            if ((rc = gs_render_batch(c, cams, count, outs))) break;   // warm-up (and slot allocation)
+            cudaEventRecord(e0, c->stream);
+            for (int rep = 0; rep < 2 && !rc; ++rep) rc = gs_render_batch(c, cams, count, outs);
+            cudaEventRecord(e1, c->stream);
+            if (rc) break;
+            GS_CUDA(c, cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms *= 0.5f;
+            if (tried < 32) {
+                r.tried_tile_w[tried] = shapes[si][0];
+                r.tried_tile_h[tried] = shapes[si][1];
+                r.tried_depth[tried] = c->batch_depth;
+                r.tried_ms[tried] = ms;
+            }
+            ++tried;
+            if (ms < r.best_ms) {
+                r.best_ms = ms;
+                r.tile_w = shapes[si][0];
+                r.tile_h = shapes[si][1];
+                r.batch_depth = c->batch_depth;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) {
+        c->alpha_tile_w = keep_w;
+        c->alpha_tile_h = keep_h;
+        c->batch_depth = keep_d;
+        return rc;
+    }
+    r.tried = (uint32_t)std::min(tried, 32);
+    c->alpha_tile_w = r.tile_w;
+    c->alpha_tile_h = r.tile_h;
+    c->batch_depth = r.batch_depth;
+    if (res) *res = r;
+    return GS_OK;
 }
 
 int gs_render_anim_batch(gs_ctx* c, const gs_camera* cam, const int32_t* states_a, const int32_t* states_b,

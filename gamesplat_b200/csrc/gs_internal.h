@@ -158,6 +158,7 @@ struct BinParams {
     float jitter_x, jitter_y;
     float frame_seed;
     int width, height, tiles_x, tiles_y;
+    int tile_shift_x, tile_shift_y;  // log2 of the tile width and height
     RasterRecord* records;           // N_vis records (sorted order)
     uint32_t* entry_keys;            // tile id per entry
     uint32_t* entry_vals;            // sorted position per entry
@@ -185,6 +186,7 @@ struct RasterParams {
     const uint32_t* tile_count;      // optional: CTAs b >= *tile_count do nothing (a tile list of the frame)
     const float4* colours;           // optional: r, g, b per record, replacing the records' colour
     int width, height, tiles_x, tiles_y;
+    int tile_w, tile_h;              // tile shape: 16x16, or 32x8 / 8x32 (alpha mode)
     float bg;
     // stochastic mode (envelope records): the sample's jitter and seed, and
     // the viewport of the quad computation
@@ -240,7 +242,7 @@ int launch_raster_stochastic2(const RasterParams& p, cudaStream_t s);
 // alpha frames[f] for f < nframes in one persistent launch (first: nframes + 1
 // prefix sums of the frames' tile counts, device; ticket: a zeroed device word)
 int launch_raster_batch_alpha(const RasterParams* frames, const uint32_t* first, uint32_t nframes, uint32_t* ticket,
-                              uint32_t grid, cudaStream_t s);
+                              uint32_t grid, int tile_w, cudaStream_t s);
 void raster_batch_occupancy(int* blocks_per_sm);
 
 int launch_wait_probe(const unsigned long long* status, FrameCounters* fc, uint32_t epoch, int which, uint32_t limit,

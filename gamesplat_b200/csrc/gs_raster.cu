@@ -50,6 +50,8 @@
 // hash, so the kept set matches the oracle bit for bit.
 #include <cuda_fp16.h>
 
+#include <type_traits>
+
 #include "gs_common.cuh"
 #include "gs_internal.h"
 #include "gs_tma.cuh"
@@ -182,15 +184,31 @@ __device__ __forceinline__ void write_pixel_stoch(const RasterParams& p, int px,
     if (p.out_rgba16f) write_rgba16f(p.out_rgba16f, o, c.x, c.y, c.z, c.w);
 }
 
-// Tile-relative coverage of a record's pixel rectangle: column bits [15:0],
-// row bits [31:16] (bit k = tile column / GL row k).  Empty rectangles give 0.
-__device__ __forceinline__ uint32_t rect_bits(uint32_t rect_x, uint32_t rect_y, int x0, int y0) {
-    const int i0 = min(max((int)(rect_x & 0xFFFFu) - x0, 0), 16), i1 = min(max((int)(rect_x >> 16) - x0, 0), 16);
-    const int j0 = min(max((int)(rect_y & 0xFFFFu) - y0, 0), 16), j1 = min(max((int)(rect_y >> 16) - y0, 0), 16);
-    if (i1 <= i0 || j1 <= j0) return 0u;
-    const uint32_t cols = (1u << i1) - (1u << i0);
-    const uint32_t rows = (1u << j1) - (1u << j0);
-    return cols | (rows << 16);
+// Tile shapes: kTw x kTh pixels, four 8x8 warp blocks (16x16, 32x8, 8x32).
+// Coverage masks: column bits from bit 0, row bits from bit RowShift (16 for
+// 16x16 tiles, whose masks fit 32 bits; 32 for the others, in 64 bits).
+template <int kTw, int kTh>
+struct TileShape {
+    static_assert(kTw * kTh == 256 && kTw % 8 == 0 && kTh % 8 == 0, "four 8x8 blocks");
+    static constexpr int kBx = kTw / 8;          // blocks per row
+    static constexpr int kRowShift = kTw == 16 && kTh == 16 ? 16 : 32;
+    using Mask = typename std::conditional<kRowShift == 16, uint32_t, unsigned long long>::type;
+};
+
+// Tile-relative coverage of a record's pixel rectangle: column bits
+// [0, kTw), row bits [RowShift, RowShift + kTh) (bit k = tile column / GL row
+// k).  Empty rectangles give 0.
+template <int kTw, int kTh>
+__device__ __forceinline__ typename TileShape<kTw, kTh>::Mask rect_bits(uint32_t rect_x, uint32_t rect_y, int x0,
+                                                                        int y0) {
+    using S = TileShape<kTw, kTh>;
+    using M = typename S::Mask;
+    const int i0 = min(max((int)(rect_x & 0xFFFFu) - x0, 0), kTw), i1 = min(max((int)(rect_x >> 16) - x0, 0), kTw);
+    const int j0 = min(max((int)(rect_y & 0xFFFFu) - y0, 0), kTh), j1 = min(max((int)(rect_y >> 16) - y0, 0), kTh);
+    if (i1 <= i0 || j1 <= j0) return (M)0;
+    const unsigned long long cols = (1ull << i1) - (1ull << i0);
+    const unsigned long long rows = (1ull << j1) - (1ull << j0);
+    return (M)(cols | (rows << S::kRowShift));
 }
 
 // Lower bound of the splat's quadratic form q(d) = A dx^2 + B dx dy + C dy^2
@@ -220,27 +238,32 @@ __device__ __forceinline__ float min_q_box(float A, float B, float C, float X0, 
 // first term of the Gaussian exponent.
 // Shared memory of one CTA's tile: two staging buffers of records, their
 // barriers, the records' coverage bits and warp-block masks.
-template <int kMode>
+template <int kMode, int kTw = 16, int kTh = 16>
 struct __align__(128) RasterShared {
     RasterRecord rec[2][kBatch];
     uint64_t bar[2];
-    uint32_t bits[kBatch];
+    typename TileShape<kTw, kTh>::Mask bits[kBatch];
     uint8_t mask[kBatch];
     float4 cen[kMode == 1 ? kBatch : 1];   // stochastic: jittered centre and hash z of the sample
 };
 
 // One 16x16 tile, the whole CTA (used by the per-frame kernel, one tile per
 // CTA, and by the batch kernel, many frames' tiles per CTA in turn).
-template <int kMode>  // 0 = alpha, 1 = stochastic, 2 = two un-jittered stochastic samples
-__device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_t tile, RasterShared<kMode>& sh) {
+template <int kMode, int kTw = 16, int kTh = 16>  // kMode: 0 alpha, 1 stochastic, 2 two stochastic samples
+__device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_t tile,
+                                            RasterShared<kMode, kTw, kTh>& sh) {
+    using Shape = TileShape<kTw, kTh>;
+    using Mask = typename Shape::Mask;
+    constexpr int kRs = Shape::kRowShift;
+    static_assert(kMode == 0 || (kTw == 16 && kTh == 16), "the stochastic modes rasterize 16x16 tiles");
     const int tx = (int)(tile % (uint32_t)p.tiles_x), ty = (int)(tile / (uint32_t)p.tiles_x);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int x0 = tx * kTileW, y0 = ty * kTileH;
-    const int lx = (warp & 1) * 8 + (lane & 7), ly0 = (warp >> 1) * 8 + (lane >> 3), ly1 = ly0 + 4;
+    const int x0 = tx * kTw, y0 = ty * kTh;
+    const int lx = (warp % Shape::kBx) * 8 + (lane & 7), ly0 = (warp / Shape::kBx) * 8 + (lane >> 3), ly1 = ly0 + 4;
     const int px = x0 + lx, py0 = y0 + ly0, py1 = y0 + ly1;
     const bool in0 = px < p.width && py0 < p.height, in1 = px < p.width && py1 < p.height;
     // coverage bits a pixel needs: its tile column and its tile row
-    const uint32_t need0 = (1u << lx) | (1u << (16 + ly0)), need1 = (1u << lx) | (1u << (16 + ly1));
+    const Mask need0 = ((Mask)1 << lx) | ((Mask)1 << (kRs + ly0)), need1 = ((Mask)1 << lx) | ((Mask)1 << (kRs + ly1));
     const uint2 range = p.tile_ranges[tile];
     const uint32_t n = range.y > range.x ? range.y - range.x : 0u;
     const uint32_t* __restrict__ vals = p.tile_plan->vfinal;
@@ -311,7 +334,7 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                 if (kMode != 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             }
             const uint2 rr = reinterpret_cast<const uint2*>(R)[5];
-            uint32_t bits;
+            Mask bits;
             float cen_x, cen_y;
             if (kMode == 1) {
                 // envelope record: this sample's quad (same computation as
@@ -320,27 +343,31 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                 const bool qok = quad_rect(R->cx, R->cy, R->log2_opacity, __uint_as_float(rr.y), __uint_as_float(rr.x),
                                            p.jitter_x, p.jitter_y, p.vp_w, p.vp_h, p.clip_y_sign, p.width, p.height,
                                            &q);
-                bits = qok ? rect_bits((uint32_t)q.i0 | ((uint32_t)q.i1 << 16), (uint32_t)q.j0 | ((uint32_t)q.j1 << 16),
-                                       x0, y0)
-                           : 0u;
+                bits = qok ? rect_bits<kTw, kTh>((uint32_t)q.i0 | ((uint32_t)q.i1 << 16),
+                                                 (uint32_t)q.j0 | ((uint32_t)q.j1 << 16), x0, y0)
+                           : (Mask)0;
                 cen_x = add(R->cx, p.jitter_x);
                 cen_y = add(R->cy, p.jitter_y);
                 sh.cen[i] = make_float4(cen_x, cen_y, add((float)R->splat_id, p.frame_seed), 0.0f);
             } else {
-                bits = rect_bits(rr.x, rr.y, x0, y0);
+                bits = rect_bits<kTw, kTh>(rr.x, rr.y, x0, y0);
                 cen_x = R->cx;
                 cen_y = R->cy;
             }
             sh.bits[i] = bits;
             if (kMode == 0) {
                 // coverage bits next to g, b: one 16-byte load per splat in the loop
-                const_cast<RasterRecord*>(R)->rect_x = bits;
+                const_cast<RasterRecord*>(R)->rect_x = (uint32_t)bits;
+                if (kRs == 32) const_cast<RasterRecord*>(R)->rect_y = (uint32_t)((unsigned long long)bits >> 32);
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             }
-            const uint32_t c = (uint32_t)((bits & 0x00FFu) != 0u) | ((uint32_t)((bits & 0xFF00u) != 0u) << 1);
-            const uint32_t r = (uint32_t)((bits & 0x00FF0000u) != 0u) | ((uint32_t)((bits & 0xFF000000u) != 0u) << 1);
-            // block w = (w & 1, w >> 1): bit w set iff its column and row halves are covered
-            uint32_t blocks = (c & (r & 1u ? 3u : 0u)) | ((c & (r & 2u ? 3u : 0u)) << 2);
+            // block w = (w % kBx, w / kBx): bit w set iff its 8 columns and 8 rows are covered
+            uint32_t blocks = 0u;
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const int bxw = w % Shape::kBx, byw = w / Shape::kBx;
+                if (((bits >> (8 * bxw)) & 0xFFu) != 0u && ((bits >> (kRs + 8 * byw)) & 0xFFu) != 0u) blocks |= 1u << w;
+            }
             const float4 q0 = reinterpret_cast<const float4*>(R)[0];
             const float2 q1 = reinterpret_cast<const float2*>(R)[2];
             const float A = q0.z, B = q0.w, C = q1.x;
@@ -348,9 +375,11 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                 const float thr = fmaf(R->s_max, 1.02f, 0.02f);
                 for (uint32_t todo_w = blocks; todo_w; todo_w &= todo_w - 1u) {
                     const int w = __ffs(todo_w) - 1;
-                    const uint32_t cb = (bits >> (8 * (w & 1))) & 0xFFu, rb = (bits >> (16 + 8 * (w >> 1))) & 0xFFu;
-                    const float bx = (float)(x0 + 8 * (w & 1)) + 0.5f - cen_x;
-                    const float by = (float)(y0 + 8 * (w >> 1)) + 0.5f - cen_y;
+                    const int bxw = w % Shape::kBx, byw = w / Shape::kBx;
+                    const uint32_t cb = (uint32_t)(bits >> (8 * bxw)) & 0xFFu;
+                    const uint32_t rb = (uint32_t)(bits >> (kRs + 8 * byw)) & 0xFFu;
+                    const float bx = (float)(x0 + 8 * bxw) + 0.5f - cen_x;
+                    const float by = (float)(y0 + 8 * byw) + 0.5f - cen_y;
                     const float m = min_q_box(A, B, C, bx + (float)(__ffs(cb) - 1), bx + (float)(31 - __clz(cb)),
                                               by + (float)(__ffs(rb) - 1), by + (float)(31 - __clz(rb)));
                     if (m > thr) blocks &= ~(1u << w);
@@ -370,7 +399,9 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                     const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
                     const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
                     const uint4 q2u = reinterpret_cast<const uint4*>(recs + j)[2];
-                    const uint32_t bits = q2u.z;
+                    Mask bits;
+                    if (kRs == 32) bits = (Mask)((unsigned long long)q2u.z | ((unsigned long long)q2u.w << 32));
+                    else bits = (Mask)q2u.z;
                     const float dx = sub(fcx, q0.x);
                     const float t0 = mul(mul(q0.z, dx), dx);
                     const float m = mul(q0.w, dx);
@@ -408,7 +439,7 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                 todo &= todo - 1u;
                 float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
                 const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
-                const uint32_t bits = sh.bits[j];
+                const Mask bits = sh.bits[j];
                 float hz = 0.0f;
                 if (kMode == 1) {
                     const float4 cz = sh.cen[j];
@@ -489,21 +520,22 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
     }
 }
 
-template <int kMode>
+template <int kMode, int kTw = 16, int kTh = 16>
 __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) {
-    __shared__ RasterShared<kMode> sh;
+    __shared__ RasterShared<kMode, kTw, kTh> sh;
     if (p.tile_count && blockIdx.x >= *p.tile_count) return;
-    raster_tile<kMode>(p, p.tile_order[blockIdx.x], sh);
+    raster_tile<kMode, kTw, kTh>(p, p.tile_order[blockIdx.x], sh);
 }
 
 // Many frames in one persistent launch: work item w is tile
 // frames[f].tile_order[w - first[f]] of the frame f with first[f] <= w <
-// first[f + 1]; CTAs take items by ticket until all are done.
-template <int kMode>
+// first[f + 1]; CTAs take items by ticket until all are done.  Every frame of
+// a launch has the launch's tile shape.
+template <int kMode, int kTw = 16, int kTh = 16>
 __global__ void __launch_bounds__(kRasterThreads) raster_batch_kernel(const RasterParams* __restrict__ frames,
                                                                       const uint32_t* __restrict__ first,
                                                                       uint32_t nframes, uint32_t* __restrict__ ticket) {
-    __shared__ RasterShared<kMode> sh;
+    __shared__ RasterShared<kMode, kTw, kTh> sh;
     __shared__ uint32_t s_item;
     const uint32_t total = first[nframes];
     for (;;) {
@@ -518,26 +550,30 @@ __global__ void __launch_bounds__(kRasterThreads) raster_batch_kernel(const Rast
             else hi = mid;
         }
         const RasterParams p = frames[lo];
-        raster_tile<kMode>(p, p.tile_order[w - first[lo]], sh);
+        raster_tile<kMode, kTw, kTh>(p, p.tile_order[w - first[lo]], sh);
         __syncthreads();
     }
 }
 
 void raster_batch_occupancy(int* blocks_per_sm) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_batch_kernel<0>, kRasterThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, raster_batch_kernel<0, 16, 16>, kRasterThreads, 0);
 }
 
 int launch_raster_batch_alpha(const RasterParams* frames, const uint32_t* first, uint32_t nframes, uint32_t* ticket,
-                              uint32_t grid, cudaStream_t s) {
+                              uint32_t grid, int tile_w, cudaStream_t s) {
     if (nframes == 0) return 0;
-    raster_batch_kernel<0><<<grid, kRasterThreads, 0, s>>>(frames, first, nframes, ticket);
+    if (tile_w == 32) raster_batch_kernel<0, 32, 8><<<grid, kRasterThreads, 0, s>>>(frames, first, nframes, ticket);
+    else if (tile_w == 8) raster_batch_kernel<0, 8, 32><<<grid, kRasterThreads, 0, s>>>(frames, first, nframes, ticket);
+    else raster_batch_kernel<0, 16, 16><<<grid, kRasterThreads, 0, s>>>(frames, first, nframes, ticket);
     return 1;
 }
 
 int launch_raster_alpha(const RasterParams& p, cudaStream_t s) {
     const uint32_t tiles = (uint32_t)p.tiles_x * (uint32_t)p.tiles_y;
     if (tiles == 0) return 0;
-    raster_kernel<0><<<tiles, kRasterThreads, 0, s>>>(p);
+    if (p.tile_w == 32) raster_kernel<0, 32, 8><<<tiles, kRasterThreads, 0, s>>>(p);
+    else if (p.tile_w == 8) raster_kernel<0, 8, 32><<<tiles, kRasterThreads, 0, s>>>(p);
+    else raster_kernel<0><<<tiles, kRasterThreads, 0, s>>>(p);
     return 1;
 }
 

@@ -266,6 +266,32 @@ int gs_render(gs_ctx* ctx, const gs_camera* cam, void* rgba16f_out);
  * Gaussian per frame), kept until the scene changes. */
 int gs_render_batch(gs_ctx* ctx, const gs_camera* cams, uint32_t count, void* const* outs);
 
+/* Tile shape of alpha frames (the other modes use 16 x 16): 16 x 16 (default),
+ * 32 x 8 or 8 x 32 pixels; images are the same for every shape. */
+int gs_set_tile_shape(gs_ctx* ctx, int tile_w, int tile_h);
+
+/* Frames per persistent raster launch in gs_render_batch (0: the whole
+ * batch, the default); each launch's frames are staged, checked for
+ * tile-entry overflow and rasterized before the next ones. */
+int gs_set_batch_depth(gs_ctx* ctx, uint32_t depth);
+
+typedef struct gs_tune_result {
+    int32_t tile_w, tile_h;          /* the fastest configuration, now set on the context */
+    uint32_t batch_depth;
+    float best_ms;                   /* its time for the whole batch */
+    uint32_t tried;                  /* configurations measured (at most 32 listed) */
+    int32_t tried_tile_w[32], tried_tile_h[32];
+    uint32_t tried_depth[32];
+    float tried_ms[32];
+} gs_tune_result;
+
+/* Autotuner of the batched path (no counterpart in the reference): renders
+ * the batch (gs_render_batch, images into outs) with every tile shape
+ * (16x16, 32x8, 8x32) and batch depth (4, 8, ..., 128, up to the batch),
+ * times each on the device (CUDA events, two runs after a warm-up), and sets
+ * the fastest on the context; res (may be NULL) receives every timing. */
+int gs_autotune_batch(gs_ctx* ctx, const gs_camera* cams, uint32_t count, void* const* outs, gs_tune_result* res);
+
 /* A batch of `count` gsanim appearance states of one camera (at most 256):
  * frame k is what gs_render draws after gs_set_anim_state(states_a[k],
  * states_b[k], weights[k]) (states_b / weights may be NULL for 0), into

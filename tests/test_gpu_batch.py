@@ -107,3 +107,53 @@ def test_anim_state_batch_equals_single_frames():
         img = o.view(180, 320, 4).cpu().numpy()
         assert np.array_equal(img.view(np.uint16), s.view(np.uint16)), k
     assert not np.array_equal(singles[0].view(np.uint16), singles[1].view(np.uint16))
+
+
+@pytest.mark.parametrize("shape", [(16, 16), (32, 8), (8, 32)])
+def test_tile_shapes_in_the_parity_gate(shape):
+    """Every tile shape draws the frame within the alpha parity gate of the
+    oracle, single frames and batches alike."""
+    rows = RR.pack_raw(scene.small_scene(7, 40_000))
+    cams = _cams()[:3]
+    with Renderer(0) as r:
+        r.set(splat_render_mode="alpha", black_background=1)
+        r.upload_gaussians(rows)
+        import ctypes as C
+
+        from gamesplat_b200 import _lib as L
+        L.check(L.lib().gs_set_tile_shape(r._ctx, shape[0], shape[1]), "gs_set_tile_shape")
+        single = _render_single(r, cams[0])
+        batch = _render_batch(r, cams)
+    for cam, img in [(cams[0], single)] + list(zip(cams, batch)):
+        w, h = int(cam[32]), int(cam[33])
+        ref, _ = oracle_alpha(rows, cam, w, h)
+        gate = image_gate(img, ref)
+        assert gate["ok"], (shape, gate)
+
+
+def test_autotuner_picks_a_measured_configuration():
+    import ctypes as C
+
+    from gamesplat_b200 import _lib as L
+
+    rows = RR.pack_raw(scene.small_scene(7, 40_000))
+    cams = _cams()
+    outs = [torch.zeros(int(c[33]) * int(c[32]) * 4, dtype=torch.float16, device="cuda") for c in cams]
+    with Renderer(0) as r:
+        r.set(splat_render_mode="alpha", black_background=1)
+        r.upload_gaussians(rows)
+        n = len(cams)
+        arr = (L.GsCamera * n)(*[RR.camera_from_array(c) for c in cams])
+        ptrs = (C.c_void_p * n)(*[C.c_void_p(o.data_ptr()) for o in outs])
+        res = L.GsTuneResult()
+        L.check(L.lib().gs_autotune_batch(r._ctx, arr, n, ptrs, C.byref(res)), "gs_autotune_batch")
+        torch.cuda.synchronize()
+        tried = [(res.tried_tile_w[i], res.tried_tile_h[i], res.tried_depth[i], res.tried_ms[i])
+                 for i in range(res.tried)]
+        assert res.tried >= 3 and {(t[0], t[1]) for t in tried} == {(16, 16), (32, 8), (8, 32)}
+        assert (res.tile_w, res.tile_h, res.batch_depth) in [(t[0], t[1], t[2]) for t in tried]
+        assert res.best_ms == min(t[3] for t in tried) and res.best_ms > 0
+        batch = _render_batch(r, cams)   # with the chosen configuration
+    for cam, img in zip(cams, batch):
+        ref, _ = oracle_alpha(rows, cam, int(cam[32]), int(cam[33]))
+        assert image_gate(img, ref)["ok"]
