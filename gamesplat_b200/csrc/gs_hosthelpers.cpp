@@ -11,6 +11,8 @@
 #include <new>
 #include <string>
 #include <thread>
+
+#include "gs_parallel.h"
 #include <vector>
 
 #include "../../include/gs_api.h"
@@ -301,29 +303,23 @@ int64_t load_ply(const char* path, float* rows, uint64_t capacity) {
     };
     const unsigned hw = std::thread::hardware_concurrency();
     const unsigned workers = hw > 1 ? (hw - 1 < 15 ? hw - 1 : 15) : 0;
+    // one set of worker threads for the whole body (the other loaders use
+    // gs::parallel_ranges; here the calling thread also reads the next block)
+    gs::WorkerPool pool(n >= 2 * 2048 ? workers : 0);
     uint64_t cnt = n < batch ? n : batch;
     bool ok = std::fread(raw[0].data(), stride, cnt, f) == cnt;
     for (uint64_t i = 0, b = 0; ok && i < n; i += cnt, b ^= 1) {
         cnt = n - i < batch ? n - i : batch;
         const uint64_t next = n - (i + cnt) < batch ? n - (i + cnt) : batch;
         const unsigned char* buf = raw[b].data();
-        const uint64_t per = workers ? (cnt + workers - 1) / workers : cnt;
-        std::vector<std::thread> pool;
-        uint64_t inline_from = 0;   // rows no worker took (all of them without workers)
-        if (workers && cnt >= 2048) {
-            try {
-                pool.reserve(workers);
-                for (unsigned w = 0; w < workers && inline_from < cnt; ++w) {
-                    const uint64_t lo = inline_from, hi = lo + per < cnt ? lo + per : cnt;
-                    pool.emplace_back(transform, buf, i, lo, hi);
-                    inline_from = hi;
-                }
-            } catch (const std::exception&) {   // no memory or no more threads: the rest runs here
-            }
-        }
-        if (next) ok = std::fread(raw[b ^ 1].data(), stride, next, f) == next;
-        transform(buf, i, inline_from, cnt);
-        for (auto& t : pool) t.join();
+        bool next_ok = true;
+        // the workers transform this block while this thread reads the next
+        // one, then takes its own slice of the block
+        pool.run(cnt, [&](uint64_t lo, uint64_t hi) {
+            if (lo == 0 && next) next_ok = std::fread(raw[b ^ 1].data(), stride, next, f) == next;
+            transform(buf, i, lo, hi);
+        });
+        ok = next_ok;
     }
     return ok ? (int64_t)vertex_count : GS_ERR_BAD_ARG;
 }

@@ -6,8 +6,11 @@
 #pragma once
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdint>
 #include <exception>
+#include <functional>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -37,5 +40,80 @@ bool parallel_ranges(uint64_t n, uint64_t min_per_slice, F&& fn) {
     for (auto& t : pool) t.join();
     return std::all_of(ok.begin(), ok.end(), [](char c) { return c != 0; });
 }
+
+// A fixed set of worker threads for a loader that processes many blocks:
+// run(n, fn) calls fn(lo, hi) over [0, n) in one slice per worker plus one
+// for the calling thread, and returns when all slices are done.  The threads
+// are started once (as many as could be started, at most `workers`) and
+// joined by the destructor.  fn must not throw and must only write state
+// private to its slice.
+class WorkerPool {
+  public:
+    explicit WorkerPool(unsigned workers) {
+        try {
+            for (unsigned w = 0; w < workers; ++w) threads_.emplace_back([this, w] { loop(w); });
+        } catch (const std::exception&) {   // no memory or no more threads: fewer workers
+        }
+    }
+    ~WorkerPool() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : threads_) t.join();
+    }
+    WorkerPool(const WorkerPool&) = delete;
+    WorkerPool& operator=(const WorkerPool&) = delete;
+
+    void run(uint64_t n, const std::function<void(uint64_t, uint64_t)>& fn) {
+        const uint64_t slices = (uint64_t)threads_.size() + 1;
+        const uint64_t per = (n + slices - 1) / slices;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            fn_ = &fn;
+            n_ = n;
+            per_ = per;
+            pending_ = threads_.size();
+            ++generation_;
+        }
+        cv_.notify_all();
+        fn(0, std::min(n, per));   // the calling thread's slice
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [this] { return pending_ == 0; });
+        fn_ = nullptr;
+    }
+
+  private:
+    void loop(unsigned w) {
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(uint64_t, uint64_t)>* fn;
+            uint64_t lo, hi;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return stop_ || generation_ != seen; });
+                if (stop_) return;
+                seen = generation_;
+                fn = fn_;
+                lo = std::min(n_, (uint64_t)(w + 1) * per_);
+                hi = std::min(n_, lo + per_);
+            }
+            if (lo < hi) (*fn)(lo, hi);
+            {
+                std::lock_guard<std::mutex> lk(m_);
+                if (--pending_ == 0) done_.notify_one();
+            }
+        }
+    }
+
+    std::vector<std::thread> threads_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    const std::function<void(uint64_t, uint64_t)>* fn_ = nullptr;
+    uint64_t n_ = 0, per_ = 0, generation_ = 0;
+    size_t pending_ = 0;
+    bool stop_ = false;
+};
 
 }  // namespace gs
