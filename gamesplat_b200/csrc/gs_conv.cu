@@ -376,7 +376,9 @@ static int launch_fwd_t(const ConvArgs& a, cudaStream_t s) {
 
 template <int kCin, int kCout, int kLoad>
 static int launch_wgrad_t(const WgradArgs& a, int grid, cudaStream_t s) {
-    const size_t smem = (size_t)wgrad_mtiles(kCin) * 16 * kGroupBytes + (size_t)(kCout / 8) * kGroupBytes;
+    // + 2 groups: every address a descriptor can name, with either stride
+    // reading as either, stays inside the allocation
+    const size_t smem = (size_t)wgrad_mtiles(kCin) * 16 * kGroupBytes + (size_t)(kCout / 8 + 2) * kGroupBytes;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(conv_wgrad_kernel<kCin, kCout, kLoad>, cudaFuncAttributeMaxDynamicSharedMemorySize,
