@@ -139,12 +139,10 @@ static int ensure_train(gs_denoiser* d, size_t pix) {
     return GS_OK;
 }
 
-static void pack_images(gs_denoiser* d) {
+static void pack_images(gs_denoiser* d, cudaStream_t s) {
     for (int l = 0; l < gs::dn::kLayers; ++l) {
-        conv::launch_pack_weights(d->params + w_offset(l), kNet[l].cin, kNet[l].cout, 0, d->wimg[l],
-                                  d->stream);
-        conv::launch_pack_weights(d->params + w_offset(l), kNet[l].cin, kNet[l].cout, 1, d->wimg_t[l],
-                                  d->stream);
+        conv::launch_pack_weights(d->params + w_offset(l), kNet[l].cin, kNet[l].cout, 0, d->wimg[l], s);
+        conv::launch_pack_weights(d->params + w_offset(l), kNet[l].cin, kNet[l].cout, 1, d->wimg_t[l], s);
     }
     d->images_valid = true;
 }
@@ -157,7 +155,7 @@ static int rows_per_cta(const gs_denoiser* d, int n, int h, int w) {
 }
 
 static int conv_fwd(gs_denoiser* d, int l, bool transposed, const bf16* x, const bf16* xh, int n, int h, int w,
-                    const bf16* mask, bf16* out_bf16, float* out_f32) {
+                    const bf16* mask, bf16* out_bf16, float* out_f32, cudaStream_t s) {
     const Layer& L = kNet[l];
     conv::ConvArgs a{};
     a.x = x;
@@ -174,7 +172,7 @@ static int conv_fwd(gs_denoiser* d, int l, bool transposed, const bf16* x, const
     a.rows_per_cta = rows_per_cta(d, n, h, w);
     a.err = d->err;
     const int cin = transposed ? L.cout : L.cin, cout = transposed ? L.cin : L.cout;
-    return conv::launch_fwd(cin, cout, transposed ? 0 : L.load, a, d->stream) < 0 ? GS_ERR_BAD_ARG : GS_OK;
+    return conv::launch_fwd(cin, cout, transposed ? 0 : L.load, a, s) < 0 ? GS_ERR_BAD_ARG : GS_OK;
 }
 
 static int conv_wgrad(gs_denoiser* d, int l, const bf16* x, const bf16* xh, int n, int h, int w, const bf16* dy) {
@@ -194,19 +192,19 @@ static int conv_wgrad(gs_denoiser* d, int l, const bf16* x, const bf16* xh, int 
     return conv::launch_wgrad(L.cin, L.cout, L.load, a, grid, d->stream) < 0 ? GS_ERR_BAD_ARG : GS_OK;
 }
 
-int forward(gs_denoiser* d, const bf16* x, int n, int h, int w) {
+int forward(gs_denoiser* d, const bf16* x, int n, int h, int w, cudaStream_t s) {
     if (n <= 0 || h <= 0 || w <= 0 || (h & 1) || (w & 1)) return GS_ERR_BAD_ARG;
     const size_t pix = (size_t)n * h * w;
     int rc = ensure_acts(d, pix);
     if (rc) return rc;
-    if (!d->images_valid) pack_images(d);
+    if (!d->images_valid) pack_images(d, s);
     const int hh = h / 2, hw = w / 2;
-    if ((rc = conv_fwd(d, 0, false, x, nullptr, n, h, w, nullptr, d->e1, nullptr))) return rc;
-    launch_avgpool2(d->e1, n, h, w, d->p1, d->stream);
-    if ((rc = conv_fwd(d, 1, false, d->p1, nullptr, n, hh, hw, nullptr, d->e2, nullptr))) return rc;
-    if ((rc = conv_fwd(d, 2, false, d->e2, nullptr, n, hh, hw, nullptr, d->e3, nullptr))) return rc;
-    if ((rc = conv_fwd(d, 3, false, d->e1, d->e3, n, h, w, nullptr, d->d4, nullptr))) return rc;
-    if ((rc = conv_fwd(d, 4, false, d->d4, nullptr, n, h, w, nullptr, nullptr, d->out))) return rc;
+    if ((rc = conv_fwd(d, 0, false, x, nullptr, n, h, w, nullptr, d->e1, nullptr, s))) return rc;
+    launch_avgpool2(d->e1, n, h, w, d->p1, s);
+    if ((rc = conv_fwd(d, 1, false, d->p1, nullptr, n, hh, hw, nullptr, d->e2, nullptr, s))) return rc;
+    if ((rc = conv_fwd(d, 2, false, d->e2, nullptr, n, hh, hw, nullptr, d->e3, nullptr, s))) return rc;
+    if ((rc = conv_fwd(d, 3, false, d->e1, d->e3, n, h, w, nullptr, d->d4, nullptr, s))) return rc;
+    if ((rc = conv_fwd(d, 4, false, d->d4, nullptr, n, h, w, nullptr, nullptr, d->out, s))) return rc;
     d->last_n = n;
     d->last_h = h;
     d->last_w = w;
@@ -223,16 +221,16 @@ int backward(gs_denoiser* d, const bf16* x, const bf16* dout, int n, int h, int 
     cudaMemsetAsync(d->grads, 0, param_count() * sizeof(float), d->stream);
     // conv5
     if ((rc = conv_wgrad(d, 4, d->d4, nullptr, n, h, w, dout))) return rc;
-    if ((rc = conv_fwd(d, 4, true, dout, nullptr, n, h, w, d->d4, d->dz4, nullptr))) return rc;
+    if ((rc = conv_fwd(d, 4, true, dout, nullptr, n, h, w, d->d4, d->dz4, nullptr, d->stream))) return rc;
     // conv4 (input up2(e3) + e1)
     if ((rc = conv_wgrad(d, 3, d->e1, d->e3, n, h, w, d->dz4))) return rc;
-    if ((rc = conv_fwd(d, 3, true, d->dz4, nullptr, n, h, w, nullptr, d->du, nullptr))) return rc;
+    if ((rc = conv_fwd(d, 3, true, d->dz4, nullptr, n, h, w, nullptr, d->du, nullptr, d->stream))) return rc;
     launch_upsample_grad(d->du, d->e3, n, h, w, d->dz3, d->stream);
     // conv3, conv2 at half resolution
     if ((rc = conv_wgrad(d, 2, d->e2, nullptr, n, hh, hw, d->dz3))) return rc;
-    if ((rc = conv_fwd(d, 2, true, d->dz3, nullptr, n, hh, hw, d->e2, d->dz2, nullptr))) return rc;
+    if ((rc = conv_fwd(d, 2, true, d->dz3, nullptr, n, hh, hw, d->e2, d->dz2, nullptr, d->stream))) return rc;
     if ((rc = conv_wgrad(d, 1, d->p1, nullptr, n, hh, hw, d->dz2))) return rc;
-    if ((rc = conv_fwd(d, 1, true, d->dz2, nullptr, n, hh, hw, nullptr, d->dp1, nullptr))) return rc;
+    if ((rc = conv_fwd(d, 1, true, d->dz2, nullptr, n, hh, hw, nullptr, d->dp1, nullptr, d->stream))) return rc;
     launch_skip_pool_grad(d->du, d->dp1, d->e1, n, h, w, d->dz1, d->stream);
     // conv1
     return conv_wgrad(d, 0, x, nullptr, n, h, w, d->dz1);
@@ -393,7 +391,12 @@ int gs_denoiser_set_params(gs_denoiser* d, const float* host, uint64_t count) {
         return GS_ERR_CUDA;
     }
     d->adam_t = 0;
-    pack_images(d);
+    pack_images(d, d->stream);
+    // a renderer may run the network on its own stream next
+    if (cudaStreamSynchronize(d->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return GS_ERR_CUDA;
+    }
     return launched(d, GS_OK);
 }
 
@@ -419,7 +422,7 @@ int gs_denoiser_get_grads(gs_denoiser* d, float* host, uint64_t count) {
 int gs_denoiser_forward(gs_denoiser* d, const void* x, int n, int h, int w, float* out) {
     if (!d || !x) return GS_ERR_BAD_ARG;
     cudaSetDevice(d->device);
-    int rc = launched(d, forward(d, static_cast<const bf16*>(x), n, h, w));
+    int rc = launched(d, forward(d, static_cast<const bf16*>(x), n, h, w, d->stream));
     if (rc) return rc;
     if (out) {
         if (cudaMemcpyAsync(out, d->out, (size_t)n * h * w * kOutC * sizeof(float), cudaMemcpyDeviceToDevice,
@@ -461,7 +464,7 @@ int gs_denoiser_adam(gs_denoiser* d, float lr) {
     const float bc1 = 1.0f - (float)std::pow(b1, d->adam_t), bc2 = 1.0f - (float)std::pow(b2, d->adam_t);
     launch_adam(d->params, d->grads, d->adam_m, d->adam_v, (int)param_count(), lr, b1, b2, 1e-8f, bc1, bc2,
                 d->stream);
-    pack_images(d);
+    pack_images(d, d->stream);
     return launched(d, GS_OK);
 }
 

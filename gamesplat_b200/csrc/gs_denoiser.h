@@ -3,6 +3,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_bf16.h>
+#include <cuda_runtime.h>
 
 #include "../../include/gs_api.h"
 
@@ -15,8 +16,9 @@ constexpr float kTrainErrWeight = 0.01f;
 
 uint64_t parameter_count();
 // Forward pass of the last-layer output (16 channels, f32) into the
-// denoiser's own buffer, returned by output().
-int forward(gs_denoiser* d, const __nv_bfloat16* x, int n, int h, int w);
+// denoiser's own buffer, returned by output(), issued on stream s (the
+// renderer's, whose kernels produced x).
+int forward(gs_denoiser* d, const __nv_bfloat16* x, int n, int h, int w, cudaStream_t s);
 const float* output(const gs_denoiser* d);
 
 }  // namespace dn

@@ -931,7 +931,7 @@ int render_denoised(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
     if (rc) return rc;
     {
         StageScope sd(c, ST_DENOISE);
-        rc = gs::dn::forward(c->denoiser, c->features, 1, c->height, c->width);
+        rc = gs::dn::forward(c->denoiser, c->features, 1, c->height, c->width, c->stream);
         if (rc) return fail(c, rc, "denoiser forward failed");
         sd.add(7);
         sd.add(gs::dn::launch_output_tiles(gs::dn::output(c->denoiser), c->features, c->width, c->height, c->tiles_x,
