@@ -551,6 +551,19 @@ def run_ours(args):
     def frame(i):
         return cams[replicas.frame_index(rank, world, i, FRAMES)]
 
+    if args.only_mode:
+        # one secondary figure alone (for profiling captures): no headline line
+        if args.only_mode == "denoised":
+            res = denoised_mode(r, stream, out, frame, args, rank)
+        elif args.only_mode == "precision":
+            res = precision_variant(args)
+        else:
+            res = batched_mode(r, stream, args)
+        r.destroy()
+        if rank == 0:
+            print(json.dumps({"only_mode": args.only_mode, "result": res}), flush=True)
+        return
+
     # untimed warm-up (also sizes the tile-entry buffers via the host path)
     r.draw_frame(frame(0))
     for i in range(args.warmup):
@@ -776,6 +789,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-modes", action="store_true", help="skip the stochastic and GPS mode figures")
+    ap.add_argument("--only-mode", choices=["denoised", "precision", "batched"], default=None,
+                    help="run one secondary figure alone and print it (profiling captures), no headline line")
     ap.add_argument("--denoise-eval-cameras", type=int, default=200,
                     help="held-out cameras of the denoised mode's quality figures (0: skip)")
     ap.add_argument("--denoise-history", type=int, default=16,
