@@ -339,12 +339,13 @@ __global__ void __launch_bounds__(kThreads) conv_wgrad_kernel(WgradArgs a) {
 // the forward convolution, or of the transposed convolution that gives the
 // input gradient (cin' = cout, cout' = cin, tap' = 8 - tap).
 // ---------------------------------------------------------------------------
-__global__ void pack_weights_kernel(const float* __restrict__ w, int cin, int cout, int transposed,
+__global__ void pack_weights_kernel(const float* __restrict__ w, int cin, int cout, int transposed, int cut_cout,
                                     uint8_t* __restrict__ image) {
     const int total = 9 * cin * cout;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const int co = i % cout, ci = (i / cout) % cin, tap = i / (cin * cout);
-        const float v = w[i];
+        // cut_cout: the output channel whose gradient stops at this layer (zero in the transposed image)
+        const float v = (transposed && co == cut_cout) ? 0.0f : w[i];
         int k, nn, cdim;
         if (!transposed) {
             k = tap * cin + ci;
@@ -413,9 +414,10 @@ int launch_wgrad(int cin, int cout, int load_mode, const WgradArgs& a, int grid,
     return -1;
 }
 
-int launch_pack_weights(const float* w, int cin, int cout, int transposed, uint8_t* image, cudaStream_t s) {
+int launch_pack_weights(const float* w, int cin, int cout, int transposed, uint8_t* image, cudaStream_t s,
+                        int cut_cout) {
     const int total = 9 * cin * cout;
-    pack_weights_kernel<<<(total + 255) / 256, 256, 0, s>>>(w, cin, cout, transposed, image);
+    pack_weights_kernel<<<(total + 255) / 256, 256, 0, s>>>(w, cin, cout, transposed, cut_cout, image);
     return 1;
 }
 

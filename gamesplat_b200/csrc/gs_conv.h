@@ -40,7 +40,10 @@ struct WgradArgs {
 // Return the number of kernels launched, or -1 for an unsupported shape.
 int launch_fwd(int cin, int cout, int load_mode, const ConvArgs& a, cudaStream_t s);
 int launch_wgrad(int cin, int cout, int load_mode, const WgradArgs& a, int grid, cudaStream_t s);
-int launch_pack_weights(const float* w, int cin, int cout, int transposed, uint8_t* image, cudaStream_t s);
+// transposed: the image of the layer's input gradient; cut_cout >= 0 leaves that
+// output channel out of it (its gradient stops at the layer)
+int launch_pack_weights(const float* w, int cin, int cout, int transposed, uint8_t* image, cudaStream_t s,
+                        int cut_cout = -1);
 size_t weight_image_bytes(int cin, int cout);
 
 }  // namespace conv

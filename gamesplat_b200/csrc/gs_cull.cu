@@ -30,8 +30,10 @@
 namespace gs {
 
 constexpr int kStageStride = 17;  // float4 per staged row (16 + 1 pad)
+constexpr int kHalfStageStride = 9;   // float4 per staged 144-byte FP16-SH row
 constexpr int kCullWarps = kCullThreads / 32;
 constexpr size_t kCullSmem = (size_t)kCullWarps * 32 * kStageStride * sizeof(float4);  // one stage per warp
+constexpr size_t kCullHalfSmem = (size_t)kCullWarps * 32 * kHalfStageStride * sizeof(float4);
 
 struct CamRegs {
     float V[16];
@@ -231,7 +233,7 @@ __device__ __forceinline__ void project_visible(const float4* row, float4 c0, fl
 // kChunks 16-byte chunks of row ids[first + l] (if first + l < count) to
 // stage row l with one TMA bulk copy; completion is counted on `bar`.
 // Returns the lane's row id, or kSentinel past the end.
-template <int kChunks, int kRowChunks = 16>
+template <int kChunks, int kRowChunks = 16, int kStride = kStageStride>
 __device__ __forceinline__ uint32_t stage_group(const float4* rows, const uint32_t* ids, uint32_t first,
                                                 uint32_t count, float4* stage, uint64_t* bar, int lane,
                                                 uint64_t policy) {
@@ -244,8 +246,7 @@ __device__ __forceinline__ uint32_t stage_group(const float4* rows, const uint32
     // the in-place gsanim deltas) before the async-proxy refill
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (id != kSentinel)
-        bulk_g2s_hint(stage + lane * kStageStride, rows + (size_t)id * kRowChunks, (uint32_t)(kChunks * 16), bar,
-                      policy);
+        bulk_g2s_hint(stage + lane * kStride, rows + (size_t)id * kRowChunks, (uint32_t)(kChunks * 16), bar, policy);
     return id;
 }
 
@@ -297,8 +298,9 @@ int launch_gather_heads(const float4* rows, float4* heads, uint32_t n, uint32_t 
 
 // 256-byte GpuGaussian rows -> 144-byte rows with FP16 SH: chunks 0..2
 // (position, opacity, scale, rotation) copied, then the 48 SH coefficients
-// (DC at floats 12..14, SH k = 1..15 at 16 + 3(k-1) + c) as IEEE half in the
-// order 3k + c (round to nearest even).
+// (DC at floats 12..14, SH k = 1..15 at 16 + 3(k-1) + c) as IEEE half, one
+// channel after the other: half 16c + k (k = 0 the DC term), so that the
+// coefficients k, k + 1 of a channel are one 32-bit word (round to nearest even).
 __global__ void pack_half_rows_kernel(const float4* __restrict__ rows, float4* __restrict__ half_rows,
                                       uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -309,9 +311,11 @@ __global__ void pack_half_rows_kernel(const float4* __restrict__ rows, float4* _
         o[2] = __ldg(rows + (size_t)i * 16 + 2);
         __align__(16) __half h[48];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) h[c] = __float2half_rn(r[12 + c]);
+        for (int c = 0; c < 3; ++c) {
+            h[16 * c] = __float2half_rn(r[12 + c]);
 #pragma unroll
-        for (int j = 3; j < 48; ++j) h[j] = __float2half_rn(r[16 + (j - 3)]);
+            for (int k = 1; k < 16; ++k) h[16 * c + k] = __float2half_rn(r[16 + 3 * (k - 1) + c]);
+        }
         const float4* hv = reinterpret_cast<const float4*>(h);
 #pragma unroll
         for (int q = 0; q < 6; ++q) o[3 + q] = hv[q];
@@ -594,14 +598,19 @@ __device__ __forceinline__ void sh_eval_tc(const float4* stage, int lane, float 
                                            bool valid, __half* s_y, float* s_out, float* res) {
     float Y[16];
     sh_basis(x, y, z, eff, valid, Y);
-    __half* yh = s_y + lane * 16;
-    __half* yl = s_y + 512 + lane * 16;
+    uint32_t hw[8], lw[8];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const __half hi = __float2half_rn(Y[k]);
-        yh[k] = hi;
-        yl[k] = __float2half_rn(Y[k] - __half2float(hi));
+    for (int k = 0; k < 8; ++k) {
+        const __half h0 = __float2half_rn(Y[2 * k]), h1 = __float2half_rn(Y[2 * k + 1]);
+        hw[k] = pack_h2(h0, h1);
+        lw[k] = pack_h2(__float2half_rn(Y[2 * k] - __half2float(h0)), __float2half_rn(Y[2 * k + 1] - __half2float(h1)));
     }
+    uint4* yh = reinterpret_cast<uint4*>(s_y) + lane * 2;
+    uint4* yl = reinterpret_cast<uint4*>(s_y + 512) + lane * 2;
+    yh[0] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    yh[1] = make_uint4(hw[4], hw[5], hw[6], hw[7]);
+    yl[0] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    yl[1] = make_uint4(lw[4], lw[5], lw[6], lw[7]);
     __syncwarp();
     const int gid = lane >> 2, tig = lane & 3;
     const uint32_t* wy = reinterpret_cast<const uint32_t*>(s_y);
@@ -619,11 +628,11 @@ __device__ __forceinline__ void sh_eval_tc(const float4* stage, int lane, float 
         al[3] = wy[256 + r1 * 8 + tig + 4];
 #pragma unroll
         for (int b = 0; b < 6; ++b) {
+            // column gid of this 8-column block: coefficients of channel c of row g
             const int q = 8 * b + gid, g = q / 3, c = q - 3 * g;
-            const __half* sh = reinterpret_cast<const __half*>(stage + (16 * t + g) * kStageStride + 3) + c;
-            const int k0 = 2 * tig;
-            const uint32_t b0 = pack_h2(sh[3 * k0], sh[3 * (k0 + 1)]);
-            const uint32_t b1 = pack_h2(sh[3 * (k0 + 8)], sh[3 * (k0 + 9)]);
+            const uint32_t* shw =
+                reinterpret_cast<const uint32_t*>(stage + (16 * t + g) * kHalfStageStride + 3) + 8 * c;
+            const uint32_t b0 = shw[tig], b1 = shw[tig + 4];
             float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             mma_16816(d, ah[0], ah[1], ah[2], ah[3], b0, b1);
             mma_16816(d, al[0], al[1], al[2], al[3], b0, b1);
@@ -656,7 +665,7 @@ __global__ void __launch_bounds__(kCullThreads, 6) cull_project_half_kernel(Cull
         mbar_fence_init();
     }
     __syncthreads();
-    float4* const stage0 = smem4 + (size_t)warp * 32 * kStageStride;
+    float4* const stage0 = smem4 + (size_t)warp * 32 * kHalfStageStride;
     const uint32_t n_vis = p.fc->visible_count;
     const uint32_t groups = (n_vis + 31) / 32;
     const uint32_t wg = blockIdx.x * kCullWarps + warp, nw = gridDim.x * kCullWarps;
@@ -667,12 +676,12 @@ __global__ void __launch_bounds__(kCullThreads, 6) cull_project_half_kernel(Cull
     uint32_t phase = 0;
     uint32_t d0 = 0, d2 = 0, d3 = 0, d4 = 0, d6 = 0, d7 = 0, m1 = 0, m5 = 0;
     for (uint32_t g = wg; g < groups; g += nw) {
-        const uint32_t id = stage_group<kHalfRowChunks, kHalfRowChunks>(p.rows, p.ids_out, g * 32u, n_vis, stage0,
-                                                                        &s_bar[warp], lane, stream_policy);
+        const uint32_t id = stage_group<kHalfRowChunks, kHalfRowChunks, kHalfStageStride>(
+            p.rows, p.ids_out, g * 32u, n_vis, stage0, &s_bar[warp], lane, stream_policy);
         if (!mbar_wait_bounded(&s_bar[warp], phase)) stage_failed = true;
         phase ^= 1u;
         const bool valid = id != kSentinel;
-        float4* row = stage0 + lane * kStageStride;
+        float4* row = stage0 + lane * kHalfStageStride;
         const float4 c0 = row[0];
         float vx = 0.0f, vy = 0.0f, vz = 0.0f, dx = 0.0f, dy = 0.0f, dz = 0.0f;
         int eff = 0;
@@ -830,7 +839,8 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
         cudaFuncSetAttribute(cull_project_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         cudaFuncSetAttribute(cull_project_kernel<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
         cudaFuncSetAttribute(cull_project_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
-        cudaFuncSetAttribute(cull_project_half_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCullSmem);
+        cudaFuncSetAttribute(cull_project_half_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kCullHalfSmem);
         attr_devices.fetch_or(bit);
     }
     int deg = p.sh_degree < 0 ? 0 : (p.sh_degree > 3 ? 3 : p.sh_degree);
@@ -843,7 +853,7 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
     uint32_t pgrid = num_sms * 6;
     if (pgrid * kCullWarps > groups_cap) pgrid = (groups_cap + kCullWarps - 1) / kCullWarps;
     if (p.half_rows) {
-        cull_project_half_kernel<<<pgrid, kCullThreads, kCullSmem, s>>>(p);
+        cull_project_half_kernel<<<pgrid, kCullThreads, kCullHalfSmem, s>>>(p);
         return 2;
     }
     switch (deg) {

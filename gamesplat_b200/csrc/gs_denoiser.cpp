@@ -26,6 +26,8 @@ constexpr Layer kNet[gs::dn::kLayers] = {
     {gs::dn::kInC, gs::dn::kHidC, 1, 0}, {gs::dn::kHidC, gs::dn::kHidC, 1, 0}, {gs::dn::kHidC, gs::dn::kHidC, 1, 0},
     {gs::dn::kHidC, gs::dn::kHidC, 1, 1}, {gs::dn::kHidC, gs::dn::kOutC, 0, 0}};
 
+constexpr int kErrChannel = 4;   // output channel of the error estimate
+
 constexpr size_t w_count(int l) { return (size_t)9 * kNet[l].cin * kNet[l].cout; }
 size_t w_offset(int l) {
     size_t o = 0;
@@ -142,7 +144,10 @@ static int ensure_train(gs_denoiser* d, size_t pix) {
 static void pack_images(gs_denoiser* d, cudaStream_t s) {
     for (int l = 0; l < gs::dn::kLayers; ++l) {
         conv::launch_pack_weights(d->params + w_offset(l), kNet[l].cin, kNet[l].cout, 0, d->wimg[l], s);
-        conv::launch_pack_weights(d->params + w_offset(l), kNet[l].cin, kNet[l].cout, 1, d->wimg_t[l], s);
+        // the error estimate (channel 4 of the last layer) trains the last layer only: its gradient
+        // does not reach the trunk, whose features would otherwise chase their own growing error
+        conv::launch_pack_weights(d->params + w_offset(l), kNet[l].cin, kNet[l].cout, 1, d->wimg_t[l], s,
+                                  l == gs::dn::kLayers - 1 ? kErrChannel : -1);
     }
     d->images_valid = true;
 }

@@ -526,7 +526,10 @@ int gs_denoiser_get_grads(gs_denoiser* d, float* host, uint64_t count);
 /* Forward pass; `out` (device, may be NULL) receives the 16-channel output. */
 int gs_denoiser_forward(gs_denoiser* d, const void* x_bf16, int n, int h, int w, float* out);
 /* Parameter gradients (gs_denoiser_get_grads) of sum(out * dout) for the last
- * forward pass, which must have been on the same x; dout: n x h x w x 16 bf16. */
+ * forward pass, which must have been on the same x; dout: n x h x w x 16 bf16.
+ * The error estimate (output channel 4) is a head of the last layer alone: its
+ * gradient trains conv5 and stops there (the trunk's features would otherwise
+ * grow to chase their own error). */
 int gs_denoiser_backward(gs_denoiser* d, const void* x_bf16, const void* dout_bf16, int n, int h, int w);
 /* Training loss of an output against a target RGBA (n x h x w x 4 f32):
  *   L = mean |rgba - target| + ssim_weight (1 - mean SSIM(rgb)) + err_weight mean (o4 - 1000 e)^2,

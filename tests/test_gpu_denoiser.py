@@ -8,9 +8,10 @@ checker only):
 - its weight gradient against conv2d_weight: <= 1e-3 relative;
 - the whole network forward against a torch model that rounds its
   activations to bf16 where the kernels store bf16: <= 1e-2 relative;
-- the parameter gradients of the whole network against torch autograd: each
-  layer's relative L2 error <= 3e-2 (the kernels also store the gradients of
-  the activations in bf16);
+- the parameter gradients of the whole network against torch autograd through
+  the same bf16 forward (error channel detached from the trunk, as in the
+  kernels): each layer's relative L2 error <= 3e-2 (the kernels also store the
+  gradients of the activations in bf16);
 - the L1 + SSIM + error-head loss and its gradient: value within 1e-4, the
   bf16 gradient within 1e-2 relative;
 - Adam against torch.optim.Adam: 1e-6 relative;
@@ -195,21 +196,27 @@ def test_network_forward_and_backward_match_torch():
     layers = params
 
     def net(xx):
-        e1 = _conv_ref(xx, *layers[0]).clamp_min(0)
-        p1 = F.avg_pool2d(e1.permute(0, 3, 1, 2), 2).permute(0, 2, 3, 1)
-        e2 = _conv_ref(p1, *layers[1]).clamp_min(0)
-        e3 = _conv_ref(e2, *layers[2]).clamp_min(0)
-        d4 = _conv_ref(_up2(e3) + e1, *layers[3]).clamp_min(0)
-        return _conv_ref(d4, *layers[4])
+        # the kernels' forward: activations stored in bf16 (so the ReLU masks are the kernels'
+        # masks; with an fp32 forward ~0.2 % of them flip, which moves a random-sign gradient
+        # sum by ~sqrt(0.2 %) = 5 %), and the error channel 4 trained by the last layer only
+        e1 = _bf(_conv_ref(xx, *layers[0]).clamp_min(0))
+        p1 = _bf(F.avg_pool2d(e1.permute(0, 3, 1, 2), 2).permute(0, 2, 3, 1))
+        e2 = _bf(_conv_ref(p1, *layers[1]).clamp_min(0))
+        e3 = _bf(_conv_ref(e2, *layers[2]).clamp_min(0))
+        d4 = _bf(_conv_ref(_bf(_up2(e3) + e1), *layers[3]).clamp_min(0))
+        o = _conv_ref(d4, *layers[4])
+        o_err = _conv_ref(d4.detach(), *layers[4])
+        return torch.cat([o[..., :4], o_err[..., 4:5], o[..., 5:]], dim=-1)
 
     (net(x.float()) * dout.float()).sum().backward()
     got = DN.split_params(grads)
-    for k, ((gw, gb), (pw, pb)) in enumerate(zip(got, params)):
+    errs = []
+    for (gw, gb), (pw, pb) in zip(got, params):
         rw = pw.grad.cpu().numpy()
         rb = pb.grad.cpu().numpy()
-        ew = np.linalg.norm(gw - rw) / np.linalg.norm(rw)
-        eb = np.linalg.norm(gb - rb) / max(np.linalg.norm(rb), 1e-12)
-        assert ew <= 3e-2 and eb <= 3e-2, (k, ew, eb)
+        errs.append((float(np.linalg.norm(gw - rw) / np.linalg.norm(rw)),
+                     float(np.linalg.norm(gb - rb) / max(np.linalg.norm(rb), 1e-12))))
+    assert all(ew <= 3e-2 and eb <= 3e-2 for ew, eb in errs), errs
 
 
 def _torch_loss(out, x, target, ssim_w, err_w):
