@@ -42,16 +42,20 @@ constexpr uint32_t kWaitLimit = 1u << 22;
 
 __host__ __device__ constexpr int wimage_bytes(int cin, int cout) { return 9 * cin * cout * 2; }
 
-// Dynamic shared memory of the forward kernel: the three halo rows, then the
-// weight image, padded so that every address an A-operand descriptor can
-// name (16 row groups and 2 K columns from any start, with either stride
-// reading as either) lies inside the allocation.
+constexpr int kSlots = 4;   // halo rows resident: the three a row needs and the one being loaded
+
+// Dynamic shared memory of the forward kernel: the halo rows, then the weight image.
 __host__ __device__ constexpr int fwd_smem_bytes(int cin, int cout) {
-    const int slot = (cin / 8) * kColBytes;
-    const int worst = 2 * slot + 2 * (cin / 16 - 1) * kColBytes + 2 * 16 + 16 * kColBytes + 2 * kColBytes;
-    const int used = 3 * slot + wimage_bytes(cin, cout);
-    return used > worst ? used : worst;
+    return kSlots * (cin / 8) * kColBytes + wimage_bytes(cin, cout);
 }
+
+// 16-byte asynchronous global -> shared copy (zero-filled when src_bytes is 0).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // Byte offset of weight (k = tap * cin + ci, n = co) in the K-major B image.
 __host__ __device__ constexpr int wimage_offset(int k, int n, int cout) {
@@ -93,8 +97,8 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     constexpr int kW = wimage_bytes(kCin, kCout);
     constexpr uint32_t kIdesc = umma::idesc_bf16(128, kCout, 0, 0);
     extern __shared__ __align__(128) uint8_t smem[];
-    uint8_t* s_halo = smem;                              // 3 slots
-    uint8_t* s_w = smem + 3 * kSlot;
+    uint8_t* s_halo = smem;                              // kSlots rows: row yy in slot (yy + 4) & 3
+    uint8_t* s_w = smem + kSlots * kSlot;
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ uint32_t s_taddr;
 
@@ -116,16 +120,39 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     }
     if (warp == 0) umma::tmem_alloc(&s_taddr, 32);
 
+    // Load mode 0: rows come in by cp.async, one row ahead of the MMAs (the
+    // copy of row y + 2 is in flight while row y is multiplied).  Load mode 1
+    // (a sum of two tensors) loads and adds through registers, row y + 1 at
+    // the start of row y.
+    auto slot_of = [&](int yy) { return s_halo + ((yy + 4) & 3) * kSlot; };
     auto load_row = [&](int yy) {
-        uint8_t* slot = s_halo + ((yy + 3) % 3) * kSlot;
+        uint8_t* slot = slot_of(yy);
         for (int q = tid; q < 130 * kG; q += kThreads) {
             const int hp = q / kG, g = q - hp * kG;
             const uint4 v = load_granule<kCin, kLoad>(a, n, yy, x0 - 1 + hp, g);
             *reinterpret_cast<uint4*>(slot + g * kColBytes + hp * 16) = v;
         }
     };
-    load_row(y0 - 1);
-    load_row(y0);
+    auto issue_row = [&](int yy) {
+        uint8_t* slot = slot_of(yy);
+        const bool row_in = yy >= 0 && yy < a.h;
+        const __nv_bfloat16* rowp = a.x + ((size_t)n * a.h + (row_in ? yy : 0)) * a.w * kCin;
+        for (int q = tid; q < 130 * kG; q += kThreads) {
+            const int hp = q / kG, g = q - hp * kG;
+            const int x = x0 - 1 + hp;
+            const bool in = row_in && x >= 0 && x < a.w;
+            cp_async16(slot + g * kColBytes + hp * 16, in ? rowp + (size_t)x * kCin + g * 8 : a.x, in ? 16u : 0u);
+        }
+        cp_async_commit();
+    };
+    if (kLoad == 0) {
+        issue_row(y0 - 1);
+        issue_row(y0);
+        issue_row(y0 + 1);
+    } else {
+        load_row(y0 - 1);
+        load_row(y0);
+    }
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
@@ -135,7 +162,12 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     bool failed = false;
 
     for (int y = y0; y < y1; ++y) {
-        load_row(y + 1);
+        if (kLoad == 0) {
+            issue_row(y + 2);               // into the slot of row y - 2, free since the last row's MMAs
+            cp_async_wait_all_but_one();    // rows up to y + 1 have landed
+        } else {
+            load_row(y + 1);
+        }
         umma::fence_smem_to_async();
         __syncthreads();
         if (tid == 0) {
@@ -143,7 +175,7 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
             uint32_t acc = 0;
 #pragma unroll
             for (int ky = 0; ky < 3; ++ky) {
-                const uint32_t slot = halo_base + (uint32_t)(((y - 1 + ky + 3) % 3) * kSlot);
+                const uint32_t slot = halo_base + (uint32_t)(((y - 1 + ky + 4) & 3) * kSlot);
 #pragma unroll
                 for (int kx = 0; kx < 3; ++kx) {
 #pragma unroll
@@ -215,6 +247,7 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
             break;
         }
     }
+    if (kLoad == 0) asm volatile("cp.async.wait_all;" ::: "memory");   // the prefetched rows past the run
     if (failed && tid == 0) atomicOr(a.err, 1u);
     __syncthreads();
     if (warp == 0) umma::tmem_dealloc(taddr, 32);

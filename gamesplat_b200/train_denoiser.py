@@ -7,7 +7,8 @@ frame of the same camera (the target).  Cameras are random positions on the
 benchmark orbit (radius 6 m around the origin, looking at it); the history
 comes from `history_frames` frames that approach the camera along the orbit
 at the benchmark's speed (3 degrees per frame).  Each training step renders
-one pair at full resolution and takes a batch of random crops from it.
+one pair at full resolution every `batches_per_pair` steps and takes a batch of
+random crops from it at every step.
 
 All compute runs in libgs_cuda.so (renderer and the denoiser's kernels);
 torch only holds device buffers and slices the crops.
@@ -70,9 +71,11 @@ class PairSource:
 
 
 def train(rows, pairs: int = 2000, epochs: int = 2, batch: int = 8, crop: int = 256, lr: float = 1e-3,
-          width: int = 1920, height: int = 1080, seed: int = 4, log_every: int = 200, denoiser=None):
+          width: int = 1920, height: int = 1080, seed: int = 4, log_every: int = 500, denoiser=None,
+          batches_per_pair: int = 4):
     """Train a denoiser (new, seeded, unless one is given) on `pairs` random
-    orbit cameras; returns (denoiser, loss history)."""
+    orbit cameras, `batches_per_pair` batches of random crops from each
+    rendered pair; returns (denoiser, loss history)."""
     import torch
 
     from .denoiser import Denoiser
@@ -87,9 +90,10 @@ def train(rows, pairs: int = 2000, epochs: int = 2, batch: int = 8, crop: int = 
     tb = torch.zeros(batch, crop, crop, 4, dtype=torch.float32, device="cuda")
     history = []
     t0 = time.perf_counter()
-    steps = pairs * epochs
+    steps = pairs * epochs * batches_per_pair
     for it in range(steps):
-        feats, target = src.render(float(angles[it % pairs]))
+        if it % batches_per_pair == 0:
+            feats, target = src.render(float(angles[(it // batches_per_pair) % pairs]))
         ys = rng.integers(0, height - crop + 1, size=batch)
         xs = rng.integers(0, width - crop + 1, size=batch)
         for b in range(batch):
@@ -111,6 +115,7 @@ def main():
     ap.add_argument("--out", required=True, help="where to write the parameters (float32, little-endian)")
     ap.add_argument("--pairs", type=int, default=2000)
     ap.add_argument("--epochs", type=int, default=2)
+    ap.add_argument("--batches-per-pair", type=int, default=4)
     ap.add_argument("--gaussians", type=int, default=3_000_000)
     ap.add_argument("--lr", type=float, default=1e-3)
     args = ap.parse_args()
@@ -118,7 +123,7 @@ def main():
     from . import scene
 
     rows = R.pack_raw(scene.room_scene(1, args.gaussians))
-    d, hist = train(rows, pairs=args.pairs, epochs=args.epochs, lr=args.lr)
+    d, hist = train(rows, pairs=args.pairs, epochs=args.epochs, lr=args.lr, batches_per_pair=args.batches_per_pair)
     for it, loss, l1, ssim, t in hist:
         print(f"step {it:6d}  loss {loss:.5f}  l1 {l1:.5f}  ssim {ssim:.4f}  {t:7.1f} s", flush=True)
     d.params().astype("<f4").tofile(args.out)
