@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     uint8_t* s_w = smem + kSlots * kSlot;
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ uint32_t s_taddr;
+    __shared__ float s_bias[kCout];
 
     const int strips_x = (a.w + 127) / 128;
     const int segs = (a.h + a.rows_per_cta - 1) / a.rows_per_cta;
@@ -111,9 +112,10 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     const int y0 = seg * a.rows_per_cta, y1 = min(a.h, y0 + a.rows_per_cta);
     const int tid = threadIdx.x, warp = tid >> 5;
 
-    // weights: the packed image, copied verbatim
+    // weights: the packed image, copied verbatim; the bias
     for (int i = tid; i < kW / 16; i += kThreads)
         reinterpret_cast<uint4*>(s_w)[i] = __ldg(reinterpret_cast<const uint4*>(a.wimage) + i);
+    if (tid < kCout) s_bias[tid] = a.bias ? __ldg(a.bias + tid) : 0.0f;
     if (tid == 0) {
         mbar_init(&s_bar, 1);
         mbar_fence_init();
@@ -206,7 +208,7 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
         if (x < a.w && !failed) {
             if (a.bias) {
 #pragma unroll
-                for (int c = 0; c < kCout; ++c) v[c] += __ldg(a.bias + c);
+                for (int c = 0; c < kCout; ++c) v[c] += s_bias[c];
             }
             if (a.relu) {
 #pragma unroll

@@ -154,7 +154,7 @@ static void pack_images(gs_denoiser* d, cudaStream_t s) {
 
 static int rows_per_cta(const gs_denoiser* d, int n, int h, int w) {
     const long strips = (long)n * ((w + 127) / 128);
-    const long want = (long)d->num_sms * 4;
+    const long want = (long)d->num_sms * 8;   // enough CTAs for every SM's occupancy, a few rows each
     long rows = (strips * h + want - 1) / want;
     return (int)std::max(2L, std::min(64L, rows));
 }

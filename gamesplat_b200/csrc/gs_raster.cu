@@ -88,10 +88,14 @@ struct StochState {
     float r, g, b;
 };
 
+// alpha = min(opacity * exp(power), 0.99) with power <= 0 (exp <= 1 there, also
+// for the deterministic exp) never exceeds min(opacity, 0.99): a fragment whose
+// hash is at or above that bound is rejected without evaluating exp.
 __device__ __forceinline__ void stoch_step(StochState& S, float s, float opacity, float fcx, float fcy,
                                            float hz, uint32_t z24, uint32_t id, float r, float g, float b) {
-    const float alpha = g_min(mul(opacity, det_expf(mul(-0.5f, s))), 0.99f);
     const float rnd = hash13(fcx, fcy, hz);
+    if (!(rnd < g_min(opacity, 0.99f))) return;
+    const float alpha = g_min(mul(opacity, det_expf(mul(-0.5f, s))), 0.99f);
     if (rnd < alpha) {
         S.best_d24 = z24;
         S.best_id = id;
@@ -124,10 +128,20 @@ __device__ __forceinline__ void stoch2_step(Stoch2& P, bool live, float sq, floa
         want[k] = live && !P.done[k] &&
                   (z24 < P.s[k].best_d24 || (z24 == P.s[k].best_d24 && id < P.s[k].best_id));
     if (!(want[0] || want[1])) return;
+    // hashes first: exp only when one of them is below alpha's bound (see stoch_step)
+    const float bound = g_min(opacity, 0.99f);
+    float rnd[2];
+    bool cand[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        rnd[k] = want[k] ? hash13(fcx, fcy, k ? hz1 : hz0) : 1.0f;
+        cand[k] = want[k] && rnd[k] < bound;
+    }
+    if (!(cand[0] || cand[1])) return;
     const float alpha = g_min(mul(opacity, det_expf(mul(-0.5f, sq))), 0.99f);
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-        if (want[k] && hash13(fcx, fcy, k ? hz1 : hz0) < alpha) {
+        if (cand[k] && rnd[k] < alpha) {
             P.s[k].best_d24 = z24;
             P.s[k].best_id = id;
             P.s[k].r = r;
