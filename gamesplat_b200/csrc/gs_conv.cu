@@ -44,9 +44,12 @@ __host__ __device__ constexpr int wimage_bytes(int cin, int cout) { return 9 * c
 
 constexpr int kSlots = 4;   // halo rows resident: the three a row needs and the one being loaded
 
-// Dynamic shared memory of the forward kernel: the halo rows, then the weight image.
-__host__ __device__ constexpr int fwd_smem_bytes(int cin, int cout) {
-    return kSlots * (cin / 8) * kColBytes + wimage_bytes(cin, cout);
+constexpr int kHalfPix = 66;   // half-resolution pixels under a 130-pixel halo row
+
+// Dynamic shared memory of the forward kernel: the halo rows, the weight
+// image, and (load mode 1) the half-resolution rows staged beside them.
+__host__ __device__ constexpr int fwd_smem_bytes(int cin, int cout, int load = 0) {
+    return kSlots * (cin / 8) * kColBytes + wimage_bytes(cin, cout) + (load ? kSlots * kHalfPix * cin * 2 : 0);
 }
 
 // 16-byte asynchronous global -> shared copy (zero-filled when src_bytes is 0).
@@ -99,6 +102,8 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* s_halo = smem;                              // kSlots rows: row yy in slot (yy + 4) & 3
     uint8_t* s_w = smem + kSlots * kSlot;
+    constexpr int kHalfSlot = kHalfPix * kG * 16;
+    uint8_t* s_hstage = s_w + kW;                        // load mode 1: kSlots half rows
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ uint32_t s_taddr;
     __shared__ float s_bias[kCout];
@@ -122,19 +127,12 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     }
     if (warp == 0) umma::tmem_alloc(&s_taddr, 32);
 
-    // Load mode 0: rows come in by cp.async, one row ahead of the MMAs (the
-    // copy of row y + 2 is in flight while row y is multiplied).  Load mode 1
-    // (a sum of two tensors) loads and adds through registers, row y + 1 at
-    // the start of row y.
+    // Rows come in by cp.async, one row ahead of the MMAs (the copy of row
+    // y + 2 is in flight while row y is multiplied).  Load mode 1 also copies
+    // the half-resolution row under the halo into a staging buffer, and a
+    // pass over the landed row adds it in (FP32 sum rounded to bf16).
     auto slot_of = [&](int yy) { return s_halo + ((yy + 4) & 3) * kSlot; };
-    auto load_row = [&](int yy) {
-        uint8_t* slot = slot_of(yy);
-        for (int q = tid; q < 130 * kG; q += kThreads) {
-            const int hp = q / kG, g = q - hp * kG;
-            const uint4 v = load_granule<kCin, kLoad>(a, n, yy, x0 - 1 + hp, g);
-            *reinterpret_cast<uint4*>(slot + g * kColBytes + hp * 16) = v;
-        }
-    };
+    auto hstage_of = [&](int yy) { return s_hstage + ((yy + 4) & 3) * kHalfSlot; };
     auto issue_row = [&](int yy) {
         uint8_t* slot = slot_of(yy);
         const bool row_in = yy >= 0 && yy < a.h;
@@ -145,15 +143,41 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
             const bool in = row_in && x >= 0 && x < a.w;
             cp_async16(slot + g * kColBytes + hp * 16, in ? rowp + (size_t)x * kCin + g * 8 : a.x, in ? 16u : 0u);
         }
+        if (kLoad == 1) {
+            const int hh = a.h >> 1, hw = a.w >> 1, hx0 = (x0 - 1) >> 1;
+            uint8_t* hs = hstage_of(yy);
+            const __nv_bfloat16* hrow = a.xh + ((size_t)n * hh + (row_in ? min(yy >> 1, hh - 1) : 0)) * hw * kCin;
+            for (int q = tid; q < kHalfPix * kG; q += kThreads) {
+                const int hp = q / kG, g = q - hp * kG;
+                // clamped like the row: an odd width's last pixel takes the last half pixel
+                const int hx = min(max(hx0 + hp, 0), hw - 1);
+                cp_async16(hs + q * 16, row_in ? hrow + (size_t)hx * kCin + g * 8 : a.xh, row_in ? 16u : 0u);
+            }
+        }
         cp_async_commit();
     };
-    if (kLoad == 0) {
-        issue_row(y0 - 1);
-        issue_row(y0);
-        issue_row(y0 + 1);
-    } else {
-        load_row(y0 - 1);
-        load_row(y0);
+    // load mode 1: row yy's landed halo += its upsampled half-resolution row
+    auto combine_row = [&](int yy) {
+        if (yy < 0 || yy >= a.h) return;
+        uint8_t* slot = slot_of(yy);
+        const uint8_t* hs = hstage_of(yy);
+        const int hx0 = (x0 - 1) >> 1;
+        for (int q = tid; q < 130 * kG; q += kThreads) {
+            const int hp = q / kG, g = q - hp * kG;
+            const int x = x0 - 1 + hp;
+            if (x < 0 || x >= a.w) continue;
+            uint4* dst = reinterpret_cast<uint4*>(slot + g * kColBytes + hp * 16);
+            *dst = bf16x8_add(*dst, *reinterpret_cast<const uint4*>(hs + (((x >> 1) - hx0) * kG + g) * 16));
+        }
+    };
+    issue_row(y0 - 1);
+    issue_row(y0);
+    issue_row(y0 + 1);
+    if (kLoad == 1) {
+        asm volatile("cp.async.wait_group 1;" ::: "memory");   // rows y0 - 1 and y0
+        __syncthreads();
+        combine_row(y0 - 1);
+        combine_row(y0);
     }
     umma::fence_before_sync();
     __syncthreads();
@@ -164,11 +188,11 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     bool failed = false;
 
     for (int y = y0; y < y1; ++y) {
-        if (kLoad == 0) {
-            issue_row(y + 2);               // into the slot of row y - 2, free since the last row's MMAs
-            cp_async_wait_all_but_one();    // rows up to y + 1 have landed
-        } else {
-            load_row(y + 1);
+        issue_row(y + 2);               // into the slot of row y - 2, free since the last row's MMAs
+        cp_async_wait_all_but_one();    // rows up to y + 1 have landed
+        if (kLoad == 1) {
+            __syncthreads();            // every thread's copies of row y + 1 are visible
+            combine_row(y + 1);
         }
         umma::fence_smem_to_async();
         __syncthreads();
@@ -249,7 +273,7 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
             break;
         }
     }
-    if (kLoad == 0) asm volatile("cp.async.wait_all;" ::: "memory");   // the prefetched rows past the run
+    asm volatile("cp.async.wait_all;" ::: "memory");   // the prefetched rows past the run
     if (failed && tid == 0) atomicOr(a.err, 1u);
     __syncthreads();
     if (warp == 0) umma::tmem_dealloc(taddr, 32);
@@ -399,7 +423,7 @@ template <int kCin, int kCout, int kLoad>
 static int launch_fwd_t(const ConvArgs& a, cudaStream_t s) {
     const int strips = a.n * ((a.w + 127) / 128);
     const int segs = (a.h + a.rows_per_cta - 1) / a.rows_per_cta;
-    const size_t smem = (size_t)fwd_smem_bytes(kCin, kCout);
+    const size_t smem = (size_t)fwd_smem_bytes(kCin, kCout, kLoad);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(conv_fwd_kernel<kCin, kCout, kLoad>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -498,6 +498,7 @@ int gs_conv3x3_bf16(const void* x, const void* x_half, int n, int h, int w, int 
                     const float* bias, int relu, int transposed, const void* mask, void* out_bf16, float* out_f32,
                     void* image_scratch, uint32_t* err, void* stream) {
     if (!x || !weights || !image_scratch || !err || n <= 0 || h <= 0 || w <= 0) return GS_ERR_BAD_ARG;
+    if (x_half && (h < 2 || w < 2)) return GS_ERR_BAD_ARG;   // the half-resolution input has no pixels
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // weights are [tap][cin][cout] of the layer; transposed: the input gradient
     // of that layer (an input of cout channels, an output of cin channels)
@@ -524,6 +525,7 @@ int gs_conv3x3_bf16(const void* x, const void* x_half, int n, int h, int w, int 
 int gs_conv3x3_wgrad_bf16(const void* x, const void* x_half, int n, int h, int w, int cin, int cout, const void* dy,
                           float* dw, float* db, uint32_t* err, void* stream) {
     if (!x || !dy || !dw || !err || n <= 0 || h <= 0 || w <= 0) return GS_ERR_BAD_ARG;
+    if (x_half && (h < 2 || w < 2)) return GS_ERR_BAD_ARG;
     gs::conv::WgradArgs a{};
     a.x = static_cast<const bf16*>(x);
     a.xh = static_cast<const bf16*>(x_half);

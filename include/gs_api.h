@@ -554,7 +554,8 @@ int gs_denoiser_status(gs_denoiser* d);
  * the output, or NULL).  weights: device f32 [3][3][cin][cout]; with
  * transposed != 0 the convolution is the input gradient of that layer (input
  * of cout channels, output of cin channels).  x_half != NULL: the input is
- * x + the 2x nearest upsampling of x_half (n x h/2 x w/2).  Supported
+ * x + the 2x nearest upsampling of x_half (n x h/2 x w/2, h and w >= 2; an
+ * odd size's last row / column takes the last half-resolution one).  Supported
  * (input, output) channels: (16, 32), (32, 32), (32, 16), the last two with
  * x_half only for (32, 32).  image_scratch: gs_conv3x3_scratch_bytes(cin, cout)
  * device bytes; err: a device word, bit 0 set if a bounded wait ran out. */

@@ -47,8 +47,17 @@ def _conv_ref(x_nhwc, w, b=None):
     return y.permute(0, 2, 3, 1)
 
 
-def _up2(t_nhwc):
-    return t_nhwc.repeat_interleave(2, dim=1).repeat_interleave(2, dim=2)
+def _up2(t_nhwc, h=None, w=None):
+    """Nearest 2x upsample to h x w; an odd size's last row / column repeats
+    the last half-resolution one."""
+    up = t_nhwc.repeat_interleave(2, dim=1).repeat_interleave(2, dim=2)
+    h = h or up.shape[1]
+    w = w or up.shape[2]
+    if h > up.shape[1]:
+        up = torch.cat([up, up[:, -1:]], dim=1)
+    if w > up.shape[2]:
+        up = torch.cat([up, up[:, :, -1:]], dim=2)
+    return up
 
 
 @pytest.mark.parametrize("cin,cout", [(16, 32), (32, 32), (32, 16)])
@@ -97,10 +106,10 @@ def test_conv_input_gradient_matches_torch(cin, cout):
     assert float((out - ref).abs().max()) <= 1e-4 * float(ref.abs().max()) + 1e-6
 
 
-def test_conv_upsample_add_input_matches_torch():
+@pytest.mark.parametrize("n,h,w", [(1, 8, 260), (2, 9, 301)])
+def test_conv_upsample_add_input_matches_torch(n, h, w):
     """x_half: the decoder input up2(x_half) + x, rounded to bf16 as the kernel stores it."""
-    g = torch.Generator(device="cuda").manual_seed(5)
-    n, h, w = 1, 8, 260
+    g = torch.Generator(device="cuda").manual_seed(5 + w)
     x = torch.randn(n, h, w, 32, device="cuda", generator=g).bfloat16()
     xh = torch.randn(n, h // 2, w // 2, 32, device="cuda", generator=g).bfloat16()
     wt = (torch.randn(3, 3, 32, 32, device="cuda", generator=g) * 0.2).float()
@@ -110,7 +119,7 @@ def test_conv_upsample_add_input_matches_torch():
     L.check(L.lib().gs_conv3x3_bf16(_p(x), _p(xh), n, h, w, 32, 32, _p(wt), None, 0, 0, None, None, _p(out),
                                     _p(scratch), _p(err), None), "gs_conv3x3_bf16")
     torch.cuda.synchronize()
-    ref = _conv_ref(_bf(x.float() + _up2(xh.float())), _bf(wt))
+    ref = _conv_ref(_bf(x.float() + _up2(xh.float(), h, w)), _bf(wt))
     assert float((out - ref).abs().max()) <= 1e-4 * float(ref.abs().max()) + 1e-6
 
 
