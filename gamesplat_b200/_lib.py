@@ -38,7 +38,7 @@ GS_DEBUG_DEPTH = 7
 # Every function include/gs_api.h declares (checked by the CPU test suite).
 EXPORTS = (
     "gs_create", "gs_destroy", "gs_get_knobs", "gs_set_knobs", "gs_set_mode", "gs_upload_rows",
-    "gs_upload_rows_device", "gs_set_gps_budget", "gs_reset_accumulation", "gs_render", "gs_render_host",
+    "gs_upload_rows_device", "gs_set_gps_budget", "gs_reset_accumulation", "gs_render", "gs_render_host", "gs_render_host_submit", "gs_render_host_wait",
     "gs_read_stats", "gs_debug_read", "gs_profile_enable", "gs_stage_times", "gs_stage_names", "gs_status_str",
     "gs_last_error", "gs_camera_uniforms", "gs_load_ply", "gs_pack_raw", "gs_sort_pairs_scratch_bytes",
     "gs_sort_pairs", "gs_sort_pairs_noalloc", "gs_upload_anim", "gs_set_anim_state", "gs_set_display_lut",
@@ -180,6 +180,8 @@ def lib() -> C.CDLL:
         "gs_reset_accumulation": (i32, [vp]),
         "gs_render": (i32, [vp, C.POINTER(GsCamera), vp]),
         "gs_render_host": (i32, [vp, C.POINTER(GsCamera), vp]),
+        "gs_render_host_submit": (i32, [vp, C.POINTER(GsCamera), vp]),
+        "gs_render_host_wait": (i32, [vp, vp]),
         "gs_read_stats": (i32, [vp, C.POINTER(GsStats)]),
         "gs_debug_read": (i32, [vp, i32, vp, u64]),
         "gs_profile_enable": (i32, [vp, i32]),

@@ -156,6 +156,19 @@ struct gs_ctx {
     uint16_t* h_out16 = nullptr;   // pinned
     size_t h_out16_bytes = 0;
     cudaEvent_t chunk_events[8] = {};   // gs_render_host: readback chunks of a pageable destination
+    // streamed readback (gs_render_host_submit / gs_render_host_wait): two
+    // device images; each frame's image is copied to its caller's page-locked
+    // buffer on copy_stream while the next frame renders on `stream`
+    struct StreamSlot {
+        uint16_t* image = nullptr;          // device RGBA16F
+        size_t bytes = 0;                   // its capacity
+        const uint16_t* host = nullptr;     // destination of the frame in flight (null: slot free)
+        FrameCounters* h_fc = nullptr;      // pinned: that frame's counters
+        cudaEvent_t rendered = nullptr, copied = nullptr;
+    };
+    StreamSlot sslot[2];
+    int sslot_next = 0;                     // the slot the next frame takes (the older one when both are busy)
+    cudaStream_t copy_stream = nullptr;
     gs::StochasticTargets st{};
     gs::GpsTargets gps{};
     uint32_t gps_max_work_items = 16u * 1024u * 1024u;
@@ -1111,6 +1124,14 @@ void gs_destroy(gs_ctx* c) {
     if (c->h_out16) cudaFreeHost(c->h_out16);
     for (auto e : c->chunk_events)
         if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    for (auto& ss : c->sslot) {
+        dfree(ss.image);
+        if (ss.h_fc) cudaFreeHost(ss.h_fc);
+        if (ss.rendered) cudaEventDestroy(ss.rendered);
+        if (ss.copied) cudaEventDestroy(ss.copied);
+    }
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->fc_event) cudaEventDestroy(c->fc_event);
     if (c->bin_event) cudaEventDestroy(c->bin_event);
     for (auto& p : c->pending) {
@@ -1602,6 +1623,80 @@ int gs_render_host(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
     if (c->h_fc->error_flags & ~(uint32_t)gs::kErrTileOverflow)
         return fail(c, GS_ERR_DEVICE_TIMEOUT, "a device-side wait ran out");
     return GS_OK;
+}
+
+// Waits for the copy of a streamed frame and frees its slot; the frame's
+// device-side waits are checked on the counters it read back.
+static int retire_stream_slot(gs_ctx* c, gs_ctx::StreamSlot& ss) {
+    if (!ss.host) return GS_OK;
+    ss.host = nullptr;
+    GS_CUDA(c, cudaEventSynchronize(ss.copied));
+    if (ss.h_fc->error_flags & ~(uint32_t)gs::kErrTileOverflow)
+        return fail(c, GS_ERR_DEVICE_TIMEOUT, "a device-side wait ran out");
+    return GS_OK;
+}
+
+int gs_render_host_submit(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
+    if (!c || !cam || !host_out) return GS_ERR_BAD_ARG;
+    if (!gl_clip_convention(cam)) return fail(c, GS_ERR_BAD_ARG, "only the GL clip convention is drawn");
+    cudaSetDevice(c->device);
+    int w = 0, h = 0;
+    int rc = viewport_dims(c, cam, &w, &h);
+    if (rc) return rc;
+    const size_t bytes = (size_t)w * h * 8;
+    cudaPointerAttributes pa{};
+    const bool pinned_out = cudaPointerGetAttributes(&pa, host_out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (!pinned_out) return fail(c, GS_ERR_BAD_ARG, "gs_render_host_submit needs a page-locked destination");
+    if (!c->copy_stream) GS_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    // a destination still in flight is delivered before it is written again
+    int first_err = GS_OK;
+    for (auto& o : c->sslot)
+        if (o.host == host_out) {
+            rc = retire_stream_slot(c, o);
+            if (rc && !first_err) first_err = rc;
+        }
+    gs_ctx::StreamSlot& ss = c->sslot[c->sslot_next];
+    rc = retire_stream_slot(c, ss);   // the older frame: at most two in flight
+    if (rc && !first_err) first_err = rc;
+    if (first_err) return first_err;
+    if (!ss.h_fc) {
+        GS_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(&ss.h_fc), sizeof(FrameCounters)));
+        std::memset(ss.h_fc, 0, sizeof(FrameCounters));
+    }
+    if (!ss.rendered) GS_CUDA(c, cudaEventCreateWithFlags(&ss.rendered, cudaEventDisableTiming));
+    if (!ss.copied) GS_CUDA(c, cudaEventCreateWithFlags(&ss.copied, cudaEventDisableTiming));
+    if (ss.bytes < bytes) {
+        dfree(ss.image);
+        ss.image = nullptr;
+        ss.bytes = 0;
+        const cudaError_t e = dalloc(&ss.image, bytes);
+        if (e != cudaSuccess) return cuda_fail(c, e, "dalloc(stream image)");
+        ss.bytes = bytes;
+    }
+    rc = gs_render(c, cam, ss.image);
+    if (rc) return rc;
+    GS_CUDA(c, cudaMemcpyAsync(ss.h_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream));
+    GS_CUDA(c, cudaEventRecord(ss.rendered, c->stream));
+    GS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ss.rendered, 0));
+    GS_CUDA(c, cudaMemcpyAsync(host_out, ss.image, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+    GS_CUDA(c, cudaEventRecord(ss.copied, c->copy_stream));
+    ss.host = host_out;
+    c->sslot_next ^= 1;
+    return GS_OK;
+}
+
+int gs_render_host_wait(gs_ctx* c, const uint16_t* host_out) {
+    if (!c) return GS_ERR_BAD_ARG;
+    cudaSetDevice(c->device);
+    int first_err = GS_OK;
+    for (int k = 0; k < 2; ++k) {   // oldest first
+        gs_ctx::StreamSlot& ss = c->sslot[(c->sslot_next + k) & 1];
+        if (!ss.host || (host_out && ss.host != host_out)) continue;
+        const int rc = retire_stream_slot(c, ss);
+        if (rc && !first_err) first_err = rc;
+    }
+    return first_err;
 }
 
 int gs_render_features(gs_ctx* c, const gs_camera* cam, void* features_out) {

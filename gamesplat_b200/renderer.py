@@ -25,6 +25,11 @@ MODE_NAMES = {"alpha": L.GS_MODE_ALPHA, "stochastic": L.GS_MODE_STOCHASTIC, "gps
 KNOB_FIELDS = [f for f, _ in L.GsKnobs._fields_ if f != "reserved"]
 
 
+def _host_ptr(buf) -> int:
+    """Address of a host buffer: a torch tensor (data_ptr) or a numpy array."""
+    return int(buf.data_ptr()) if hasattr(buf, "data_ptr") else int(buf.ctypes.data)
+
+
 def camera_from_array(cam) -> L.GsCamera:
     if isinstance(cam, L.GsCamera):
         return cam
@@ -293,6 +298,20 @@ class Renderer:
         img = np.empty((h, w, 4), np.float16)
         L.check(L.lib().gs_render_host(self._ctx, C.byref(c), img.ctypes.data), "gs_render_host", self._ctx)
         return img
+
+    def submit_frame(self, cam, host_image) -> None:
+        """Queue a frame whose RGBA16F image is copied into the page-locked
+        host tensor host_image (H x W x 4 float16, e.g. torch.empty(...,
+        pin_memory=True)) while the next frame renders (gs_render_host_submit);
+        the image is there after wait_frames(host_image)."""
+        c = camera_from_array(cam)
+        L.check(L.lib().gs_render_host_submit(self._ctx, C.byref(c), C.c_void_p(_host_ptr(host_image))),
+                "gs_render_host_submit", self._ctx)
+
+    def wait_frames(self, host_image=None) -> None:
+        """Wait until the submitted frame(s) for host_image (None: all) are in host memory."""
+        ptr = None if host_image is None else C.c_void_p(_host_ptr(host_image))
+        L.check(L.lib().gs_render_host_wait(self._ctx, ptr), "gs_render_host_wait", self._ctx)
 
     def stats(self) -> L.GsStats:
         s = L.GsStats()

@@ -16,7 +16,8 @@
  *    (src/renderer.cpp:860-1073).
  *  - All calls on one gs_ctx must be serialised by the caller, as the
  *    reference renderer is used from one thread (src/main.cpp:1963).
- *  - Work is stream-ordered; only gs_render_host, gs_read_stats and
+ *  - Work is stream-ordered; only gs_render_host, gs_render_host_wait (and a
+ *    gs_render_host_submit that retires an older frame), gs_read_stats and
  *    gs_debug_read synchronise.
  *  - Images are RGBA16F (IEEE half, 4 channels), row-major, top row first
  *    (the orientation of the reference harness's linear_capture,
@@ -306,6 +307,22 @@ int gs_render_anim_batch(gs_ctx* ctx, const gs_camera* cam, const int32_t* state
 /* gs_render into host memory: includes the host->device camera copy and the
  * device->host image copy, and waits for them. */
 int gs_render_host(gs_ctx* ctx, const gs_camera* cam, uint16_t* rgba16f_out_host);
+
+/* Streamed readback, for a frame loop that displays or stores every frame on
+ * the host (the reference's renderer_draw_frame + present, src/main.cpp's
+ * frame loop): gs_render_host_submit queues the frame of `cam` (gs_render
+ * into one of two device images of the context), then the copy of its image
+ * into rgba16f_out_host on a copy stream of the context, and returns once
+ * both are queued; the copy of frame i overlaps the kernels of frame i + 1.
+ * rgba16f_out_host must be page-locked (cudaMallocHost / cudaHostRegister),
+ * else GS_ERR_BAD_ARG.  Two frames are in flight at most: a submit first
+ * waits for the copy of the older one, and for an earlier frame to the same
+ * buffer.  The image is in the buffer once gs_render_host_wait(ctx, buffer)
+ * returns (NULL: every frame in flight); a device-side wait that ran out in a
+ * frame is reported (GS_ERR_DEVICE_TIMEOUT) by the call that retires it.
+ * Same image as gs_render_host. */
+int gs_render_host_submit(gs_ctx* ctx, const gs_camera* cam, uint16_t* rgba16f_out_host);
+int gs_render_host_wait(gs_ctx* ctx, const uint16_t* rgba16f_out_host);
 
 /* gsanim 0.3 display LUT: the scene's display_lut, lut_size, log2_min and
  * log2_max (src/gsanim.h:33-35), uploaded by the renderer at

@@ -71,7 +71,8 @@ def test_every_context_entry_rejects_a_null_context():
     lib = L.lib()
     bad = L.GS_ERR_BAD_ARG
     calls = {
-        "gs_render_host": (None, None, None), "gs_upload_rows_device": (None, None, 0),
+        "gs_render_host": (None, None, None), "gs_render_host_submit": (None, None, None),
+        "gs_render_host_wait": (None, None), "gs_upload_rows_device": (None, None, 0),
         "gs_upload_rows_range": (None, None, 0, 0), "gs_upload_anim": (None, None, 0, None),
         "gs_set_anim_state": (None, 0, 0, 0.0), "gs_upload_layers": (None, None, 0),
         "gs_set_layer_weights": (None, None, 0), "gs_get_knobs": (None, None), "gs_set_knobs": (None, None),

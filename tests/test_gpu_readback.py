@@ -2,7 +2,9 @@
 page-locked destination (alpha mode: the rasterizer writes the pixels into
 it through its mapped device address; other modes: one copy into it) and a
 pageable destination (chunked copy through pinned staging, overlapped with
-the host copy), at sizes that are not multiples of the tile size."""
+the host copy), at sizes that are not multiples of the tile size; and the
+streamed readback (gs_render_host_submit / gs_render_host_wait), frame by
+frame."""
 from __future__ import annotations
 
 import ctypes as C
@@ -12,7 +14,7 @@ import pytest
 import torch
 
 from gamesplat_b200 import Renderer, _lib as L
-from gamesplat_b200.renderer import camera_from_array
+from gamesplat_b200.renderer import camera_from_array, camera_uniforms
 
 from helpers import small_cam, small_rows
 
@@ -48,3 +50,51 @@ def test_readback_paths_agree(w, h, mode):
                     assert np.isfinite(img).all()
                     assert img[..., 3].min() >= 0.0 and img[..., 3].max() <= 1.0
                     assert (img[..., 3] > 0).mean() > 0.05
+
+
+def _cams(sizes):
+    """A camera per frame, each from another position near (0, 0, 3)."""
+    return [camera_uniforms((0.05 * i, 0.02 * i, 3.0), np.pi, 0.0, w, h) for i, (w, h) in enumerate(sizes)]
+
+
+def test_streamed_readback_matches_gs_render():
+    """gs_render_host_submit / gs_render_host_wait: every frame's image lands in
+    its own page-locked buffer bit-identical to gs_render's, with two frames
+    in flight, a viewport change mid-stream and a buffer reused at once."""
+    rows = small_rows(20_000, seed=14)
+    sizes = [(320, 180)] * 4 + [(333, 211)] * 3
+    cams = _cams(sizes)
+    with Renderer(0) as r:
+        r.set(splat_render_mode="alpha", black_background=1)
+        r.upload_gaussians(rows)
+        refs = []
+        for cam, (w, h) in zip(cams, sizes):
+            dev = torch.empty((h, w, 4), dtype=torch.float16, device="cuda")
+            r.draw_frame(cam, out_ptr=dev.data_ptr())
+            torch.cuda.synchronize()
+            refs.append(dev.cpu().numpy())
+        bufs = [torch.full((h, w, 4), float("nan"), dtype=torch.float16, pin_memory=True) for w, h in sizes]
+        for cam, buf in zip(cams, bufs):
+            r.submit_frame(cam, buf)
+        r.wait_frames()
+        for k, (buf, ref) in enumerate(zip(bufs, refs)):
+            assert np.array_equal(buf.numpy().view(np.uint16), ref.view(np.uint16)), k
+        # the same buffer twice in a row: the second frame is what it holds
+        one = torch.empty((180, 320, 4), dtype=torch.float16, pin_memory=True)
+        r.submit_frame(cams[0], one)
+        r.submit_frame(cams[3], one)
+        r.wait_frames(one)
+        assert np.array_equal(one.numpy().view(np.uint16), refs[3].view(np.uint16))
+        r.wait_frames(one)   # nothing in flight for it: returns at once
+
+
+def test_streamed_readback_refuses_pageable_memory():
+    rows = small_rows(5_000, seed=15)
+    cam = small_cam(64, 48)
+    with Renderer(0) as r:
+        r.set(splat_render_mode="alpha", black_background=1)
+        r.upload_gaussians(rows)
+        pageable = np.empty((48, 64, 4), np.float16)
+        assert L.lib().gs_render_host_submit(r._ctx, C.byref(camera_from_array(cam)),
+                                             pageable.ctypes.data) == L.GS_ERR_BAD_ARG
+        assert L.lib().gs_render_host_wait(r._ctx, None) == L.GS_OK
