@@ -11,8 +11,11 @@
 //                           histograms (passes whose digit is the same for all
 //                           keys are skipped: identity for a stable sort;
 //                           ping-pong assignment of the active passes), then
-//                           persistent CTAs take 4096-key tiles in
-//                           ticket order, rank keys within each warp (lanes
+//                           persistent CTAs (3 per SM) take 4096-key tiles in
+//                           ticket order, copy the tile's values into shared
+//                           memory (cp.async: registers hold only keys and
+//                           ranks, which is what lets 3 CTAs share an SM),
+//                           rank keys within each warp (lanes
 //                           of equal digit found by per-bit ballots), publish
 //                           per-digit counts,
 //                           reorder the tile by digit in shared memory, then
@@ -24,6 +27,7 @@
 // the host.
 #include "gs_common.cuh"
 #include "gs_internal.h"
+#include "gs_tma.cuh"
 
 namespace gs {
 
@@ -37,6 +41,20 @@ size_t sort_status_words(uint32_t count_cap) {
     if (tiles == 0) tiles = 1;
     return tiles * kRadix;
 }
+
+// Asynchronous global -> shared copies of 4 and 16 bytes (zero-filled past src_bytes).
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+// Dynamic shared memory of the pass kernel: the reordered keys and values and
+// the tile's values in input order.
+constexpr int kPassSmem = 3 * kSortTile * 4;
 
 __device__ __forceinline__ uint32_t digit_of(uint32_t key, int shift, uint32_t dmask) { return (key >> shift) & dmask; }
 
@@ -132,11 +150,13 @@ __device__ PassIO plan_passes(const SortParams& p, int npasses, int pass, uint32
     return io;
 }
 
-__global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p, int pass, int npasses) {
+__global__ void __launch_bounds__(kSortThreads, 3) sort_pass_kernel(SortParams p, int pass, int npasses) {
     pdl_wait();
     pdl_trigger();
-    __shared__ uint32_t s_keys[kSortTile];
-    __shared__ uint32_t s_vals[kSortTile];
+    extern __shared__ __align__(16) uint32_t s_dyn[];
+    uint32_t* s_keys = s_dyn;                    // the tile reordered by digit
+    uint32_t* s_vals = s_dyn + kSortTile;
+    uint32_t* s_vstage = s_dyn + 2 * kSortTile;  // the tile's values in input order
     __shared__ uint32_t warp_hist[kSortWarps][kRadix];
     __shared__ uint32_t s_global_base[kRadix];
     __shared__ uint32_t scan_tmp[33];
@@ -170,13 +190,31 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
         const uint32_t base = tile * kSortTile;
         const uint32_t wbase = base + warp * (kSortItems * 32);
 
-        uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+        uint32_t key[kSortItems], rank[kSortItems];
+        // The warp's 512 values go to shared memory in input order (item k of
+        // lane l at k * 32 + l), 16 bytes per copy when the values are
+        // 16-byte aligned; they are read once, at the reorder.
+        uint32_t* vst = s_vstage + warp * (kSortItems * 32);
+        if ((reinterpret_cast<uintptr_t>(vin) & 15u) == 0u) {
+#pragma unroll
+            for (int q = 0; q < kSortItems / 4; ++q) {
+                const uint32_t e = (uint32_t)(q * 128 + lane * 4);
+                const uint32_t idx = wbase + e;
+                const uint32_t left = idx < n ? min(n - idx, 4u) : 0u;
+                cp_async16(vst + e, left ? vin + idx : vin, left * 4u);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kSortItems; ++k) {
+                const uint32_t idx = wbase + k * 32 + lane;
+                cp_async4(vst + k * 32 + lane, idx < n ? vin + idx : vin, idx < n ? 4u : 0u);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
 #pragma unroll
         for (int k = 0; k < kSortItems; ++k) {
             uint32_t idx = wbase + k * 32 + lane;
-            bool ok = idx < n;
-            key[k] = ok ? kin[idx] : 0u;
-            val[k] = ok ? vin[idx] : 0u;
+            key[k] = idx < n ? kin[idx] : 0u;
         }
         // Warp ranking in index order (item k, then lane): the lanes holding a
         // digit find each other; their leader reads and advances the warp's
@@ -207,7 +245,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
             rank[k] = before + __popc(peers & lt_mask);
             __syncwarp();
         }
-        __syncthreads();
+        asm volatile("cp.async.wait_all;" ::: "memory");   // this thread's value copies
+        __syncthreads();                                      // ... and every other thread's
         // One thread per digit: tile count, published at once; then every
         // warp's start of the digit's run in the reordered tile.
         const uint32_t d = threadIdx.x;
@@ -236,7 +275,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) sort_pass_kernel(SortParams p
             if (idx < n) {
                 const uint32_t lp = warp_hist[warp][digit_of(key[k], shift, dmask)] + rank[k];
                 s_keys[lp] = key[k];
-                s_vals[lp] = val[k];
+                s_vals[lp] = vst[k * 32 + lane];
             }
         }
         // Global offset of each digit's run: decoupled look-back.
@@ -274,13 +313,19 @@ __global__ void sort_copy_kernel(SortParams p) {
     }
 }
 
-static int g_pass_blocks_per_sm = 0;
+// Per device: the pass kernel's shared-memory opt-in, then its occupancy.
+constexpr int kMaxDevices = 64;
+static int g_pass_blocks_per_sm[kMaxDevices] = {};
 
 int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s) {
-    if (g_pass_blocks_per_sm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& blocks_per_sm = g_pass_blocks_per_sm[dev >= 0 && dev < kMaxDevices ? dev : 0];
+    if (blocks_per_sm == 0 || dev >= kMaxDevices) {
+        cudaFuncSetAttribute(sort_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPassSmem);
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sort_pass_kernel, kSortThreads, 0);
-        g_pass_blocks_per_sm = b > 0 ? b : 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sort_pass_kernel, kSortThreads, kPassSmem);
+        blocks_per_sm = b > 0 ? b : 1;
     }
     const int npasses = sort_passes(p.begin_bit, p.end_bit);
     int launches = 0;
@@ -292,15 +337,15 @@ int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s) {
         sort_hist_kernel<<<hist_grid, kSortThreads, 0, s>>>(p, npasses);
         ++launches;
     }
-    uint32_t pass_grid = num_sms * (uint32_t)g_pass_blocks_per_sm;
+    uint32_t pass_grid = num_sms * (uint32_t)blocks_per_sm;
     if (pass_grid > tiles_cap) pass_grid = tiles_cap > 0 ? tiles_cap : 1;
     for (int ps = 0; ps < npasses; ++ps) {
         // Passes after the first overlap their launch with the previous pass's
         // tail (programmatic dependent launch).  Across stage boundaries
         // (cull -> sort, bin -> tile sort) it measured slower, so the first
         // pass is an ordinary launch.
-        if (ps == 0) sort_pass_kernel<<<pass_grid, kSortThreads, 0, s>>>(p, ps, npasses);
-        else launch_pdl(sort_pass_kernel, dim3(pass_grid), dim3(kSortThreads), 0, s, p, ps, npasses);
+        if (ps == 0) sort_pass_kernel<<<pass_grid, kSortThreads, kPassSmem, s>>>(p, ps, npasses);
+        else launch_pdl(sort_pass_kernel, dim3(pass_grid), dim3(kSortThreads), kPassSmem, s, p, ps, npasses);
         ++launches;
     }
     if (p.land_in_buf0) {
