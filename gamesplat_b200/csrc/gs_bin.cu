@@ -276,9 +276,21 @@ __global__ void __launch_bounds__(kBinThreads) expand_kernel(BinParams p) {
         own4[0] = make_int4(max(a.x, pre), max(a.y, pre), max(a.z, pre), max(a.w, pre));
         own4[1] = make_int4(max(bq.x, pre), max(bq.y, pre), max(bq.z, pre), max(bq.w, pre));
         __syncthreads();
-        for (uint32_t i = t; i < e1 - e0; i += kBinThreads) {
+        // the owners' item records first (all in flight at once), then the entries
+        static_assert(kBinChunk == 8 * kBinThreads, "eight entries per thread");
+        const uint32_t ne = e1 - e0;
+        uint4 infs[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const uint32_t i = (uint32_t)(t + r * kBinThreads);
+            if (i < ne) infs[r] = __ldg(p.item_info + qa + (uint32_t)s_own[i]);
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const uint32_t i = (uint32_t)(t + r * kBinThreads);
+            if (i >= ne) break;
             const uint32_t q = qa + (uint32_t)s_own[i];
-            const uint4 inf = p.item_info[q];
+            const uint4 inf = infs[r];
             const uint32_t k = e0 + i - inf.x;
             const uint32_t w = max(inf.z, 1u);
             const uint32_t ty = (inf.y >> 16) + k / w, tx = (inf.y & 0xFFFFu) + k % w;
