@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     uint8_t* s_w = smem + kSlots * kSlot;
     constexpr int kHalfSlot = kHalfPix * kG * 16;
     uint8_t* s_hstage = s_w + kW;                        // load mode 1: kSlots half rows
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar[2];   // MMA completion, one per accumulator
     __shared__ uint32_t s_taddr;
     __shared__ float s_bias[kCout];
 
@@ -122,10 +122,11 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
         reinterpret_cast<uint4*>(s_w)[i] = __ldg(reinterpret_cast<const uint4*>(a.wimage) + i);
     if (tid < kCout) s_bias[tid] = a.bias ? __ldg(a.bias + tid) : 0.0f;
     if (tid == 0) {
-        mbar_init(&s_bar, 1);
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
         mbar_fence_init();
     }
-    if (warp == 0) umma::tmem_alloc(&s_taddr, 32);
+    if (warp == 0) umma::tmem_alloc(&s_taddr, 64);   // two accumulators of 32 columns
 
     // Rows come in by cp.async, one row ahead of the MMAs (the copy of row
     // y + 2 is in flight while row y is multiplied).  Load mode 1 also copies
@@ -184,20 +185,18 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     umma::fence_after_sync();
     const uint32_t taddr = s_taddr;
     const uint32_t halo_base = smem_u32(s_halo), w_base = smem_u32(s_w);
-    uint32_t phase = 0;
+    uint32_t phase0 = 0, phase1 = 0;
     bool failed = false;
-
-    for (int y = y0; y < y1; ++y) {
-        issue_row(y + 2);               // into the slot of row y - 2, free since the last row's MMAs
-        cp_async_wait_all_but_one();    // rows up to y + 1 have landed
-        if (kLoad == 1) {
-            __syncthreads();            // every thread's copies of row y + 1 are visible
-            combine_row(y + 1);
-        }
-        umma::fence_smem_to_async();
-        __syncthreads();
+    // Two TMEM accumulators: the MMAs of row y (accumulator y & 1) run while
+    // the epilogue of row y - 1 reads the other one.
+    auto wait_mma = [&](int y) {   // row y's MMAs are done (every thread waits)
+        if (!mbar_wait_bounded(&s_bar[y & 1], (y & 1) ? phase1 : phase0, kWaitLimit)) failed = true;
+        if (y & 1) phase1 ^= 1u; else phase0 ^= 1u;
+    };
+    auto mma_row = [&](int y) {
         if (tid == 0) {
             umma::fence_after_sync();
+            const uint32_t acc_addr = taddr + (uint32_t)((y & 1) * 32);
             uint32_t acc = 0;
 #pragma unroll
             for (int ky = 0; ky < 3; ++ky) {
@@ -211,23 +210,24 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
                         const int k0 = (ky * 3 + kx) * kCin + kb * 16;
                         const uint64_t bd =
                             umma::smem_desc(w_base + (uint32_t)((k0 >> 3) * kCout * 16), (uint32_t)(kCout * 16), 128u);
-                        umma::mma_bf16(taddr, ad, bd, kIdesc, acc);
+                        umma::mma_bf16(acc_addr, ad, bd, kIdesc, acc);
                         acc = 1;
                     }
                 }
             }
-            umma::commit(&s_bar);
+            umma::commit(&s_bar[y & 1]);
         }
-        if (!mbar_wait_bounded(&s_bar, phase, kWaitLimit)) failed = true;
-        phase ^= 1u;
+    };
+    auto epilogue = [&](int y) {   // row y's MMAs waited for
         umma::fence_after_sync();
+        const uint32_t acc_addr = taddr + (uint32_t)((y & 1) * 32) + ((uint32_t)(warp * 32) << 16);
         const int x = x0 + tid;
         const size_t o = ((size_t)n * a.h + y) * a.w + x;
         float v[32];
         if (kCout == 32) {
-            umma::tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16), *reinterpret_cast<float(*)[32]>(v));
+            umma::tmem_ld32(acc_addr, *reinterpret_cast<float(*)[32]>(v));
         } else {
-            umma::tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16), *reinterpret_cast<float(*)[16]>(v));
+            umma::tmem_ld16(acc_addr, *reinterpret_cast<float(*)[16]>(v));
         }
         if (x < a.w && !failed) {
             if (a.bias) {
@@ -268,15 +268,33 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
             }
         }
         umma::fence_before_sync();
+    };
+
+    bool broke = false;   // uniform over the CTA (from __syncthreads_or)
+    for (int y = y0; y < y1; ++y) {
+        if (y > y0) wait_mma(y - 1);    // its MMAs were the last readers of row y - 2's slot
+        issue_row(y + 2);               // into that slot
+        asm volatile("cp.async.wait_group 1;" ::: "memory");   // rows up to y + 1 have landed
+        if (kLoad == 1) {
+            __syncthreads();            // every thread's copies of row y + 1 are visible
+            combine_row(y + 1);
+        }
+        umma::fence_smem_to_async();
         if (__syncthreads_or(failed)) {
-            failed = true;
+            failed = broke = true;
             break;
         }
+        mma_row(y);
+        if (y > y0) epilogue(y - 1);
+    }
+    if (!broke) {   // the whole CTA: the epilogue's TMEM loads are warp-collective
+        wait_mma(y1 - 1);
+        epilogue(y1 - 1);
     }
     asm volatile("cp.async.wait_all;" ::: "memory");   // the prefetched rows past the run
     if (failed && tid == 0) atomicOr(a.err, 1u);
     __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(taddr, 32);
+    if (warp == 0) umma::tmem_dealloc(taddr, 64);
 }
 
 // ---------------------------------------------------------------------------
