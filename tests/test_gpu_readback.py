@@ -98,3 +98,34 @@ def test_streamed_readback_refuses_pageable_memory():
         assert L.lib().gs_render_host_submit(r._ctx, C.byref(camera_from_array(cam)),
                                              pageable.ctypes.data) == L.GS_ERR_BAD_ARG
         assert L.lib().gs_render_host_wait(r._ctx, None) == L.GS_OK
+
+
+def test_streamed_readback_of_an_overflowing_frame():
+    """The giant-splat scene overflows the initial tile-entry buffers on its
+    first frame: the streamed frame's image must be the re-rendered whole
+    frame (within the parity gate of the oracle's), and so must the next one,
+    which fits."""
+    from gamesplat_b200 import renderer as RR
+    from gamesplat_b200 import scene
+
+    from helpers import image_gate, oracle_alpha
+
+    raw = scene.small_scene(11, 300)
+    raw[:, 0:3] *= 0.05
+    raw[:, 52:55] = 0.0   # scale e^0 = 1 m: every splat covers the whole frame
+    rows = RR.pack_raw(raw)
+    W, H = 1920, 1080
+    cam = RR.camera_uniforms((0.0, 0.0, 1.2), float(np.pi), 0.0, W, H)
+    ref_img, _ = oracle_alpha(rows, cam, W, H)
+    with Renderer(0) as r:
+        r.set(splat_render_mode="alpha", black_background=1)
+        r.upload_gaussians(rows)
+        bufs = [torch.full((H, W, 4), float("nan"), dtype=torch.float16, pin_memory=True) for _ in range(2)]
+        for b in bufs:
+            r.submit_frame(cam, b)
+        r.wait_frames()
+        st = r.stats()
+        assert st.tile_overflow == 0 and st.tile_entries > (1 << 20)
+        for b in bufs:
+            gate = image_gate(b.numpy(), ref_img)
+            assert gate["ok"], gate
