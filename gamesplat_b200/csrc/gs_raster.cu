@@ -252,9 +252,18 @@ __device__ __forceinline__ float min_q_box(float A, float B, float C, float X0, 
 // first term of the Gaussian exponent.
 // Shared memory of one CTA's tile: two staging buffers of records, their
 // barriers, the records' coverage bits and warp-block masks.
+// A staged record and 16 bytes of padding: at an 80-byte stride the 16-byte
+// loads of 8 consecutive records (one record per thread in the staging pass)
+// fall in distinct banks, and a 32-bit field of 32 consecutive records spreads
+// over 8 banks instead of 2.
+struct __align__(16) StagedRecord {
+    RasterRecord r;
+    uint4 pad;
+};
+
 template <int kMode, int kTw = 16, int kTh = 16>
 struct __align__(128) RasterShared {
-    RasterRecord rec[2][kBatch];
+    StagedRecord rec[2][kBatch];
     uint64_t bar[2];
     typename TileShape<kTw, kTh>::Mask bits[kBatch];
     uint8_t mask[kBatch];
@@ -313,7 +322,7 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
         if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, cnt * (uint32_t)sizeof(RasterRecord));
         for (uint32_t i = threadIdx.x; i < cnt; i += kRasterThreads) {
             const uint32_t s = min(vals[range.x + first + i], p.record_cap - 1u);
-            bulk_g2s(&sh.rec[b & 1][i], p.records + s, (uint32_t)sizeof(RasterRecord), bar);
+            bulk_g2s(&sh.rec[b & 1][i].r, p.records + s, (uint32_t)sizeof(RasterRecord), bar);
         }
     };
     auto pixels_done = [&]() -> bool {
@@ -329,14 +338,14 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
         if (!mbar_wait_bounded(&sh.bar[b & 1], ph)) failed = true;
         if (b & 1) phase1 ^= 1u; else phase0 ^= 1u;
         const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
-        const RasterRecord* recs = sh.rec[b & 1];
+        const StagedRecord* recs = sh.rec[b & 1];
         // Coverage bits of each staged record and which of the four 8x8 warp
         // blocks it can shade (one thread per record): blocks its rectangle
         // touches, minus those where the splat's ellipse q(d) <= s_max misses
         // every covered pixel centre (tested with a 2 % + 0.02 margin over
         // s_max, far above the rounding of q and of the exact per-pixel sum).
         for (uint32_t i = threadIdx.x; i < cnt; i += kRasterThreads) {
-            const RasterRecord* R = recs + i;
+            const RasterRecord* R = &recs[i].r;
             if (p.colours) {
                 // per-frame colours (gsanim state batches): the record's r, g, b replaced
                 const uint32_t si = min(vals[range.x + b * kBatch + i], p.record_cap - 1u);
@@ -410,9 +419,9 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
             if (kMode == 0) {
                 // one splat of the warp's list into both pixels' state
                 auto alpha_one = [&](uint32_t j) {
-                    const float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
-                    const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
-                    const uint4 q2u = reinterpret_cast<const uint4*>(recs + j)[2];
+                    const float4 q0 = reinterpret_cast<const float4*>(&recs[j].r)[0];
+                    const float4 q1 = reinterpret_cast<const float4*>(&recs[j].r)[1];
+                    const uint4 q2u = reinterpret_cast<const uint4*>(&recs[j].r)[2];
                     Mask bits;
                     if (kRs == 32) bits = (Mask)((unsigned long long)q2u.z | ((unsigned long long)q2u.w << 32));
                     else bits = (Mask)q2u.z;
@@ -451,8 +460,8 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
             while (todo) {
                 const uint32_t j = c + (uint32_t)(__ffs(todo) - 1);
                 todo &= todo - 1u;
-                float4 q0 = reinterpret_cast<const float4*>(recs + j)[0];
-                const float4 q1 = reinterpret_cast<const float4*>(recs + j)[1];
+                float4 q0 = reinterpret_cast<const float4*>(&recs[j].r)[0];
+                const float4 q1 = reinterpret_cast<const float4*>(&recs[j].r)[1];
                 const Mask bits = sh.bits[j];
                 float hz = 0.0f;
                 if (kMode == 1) {
@@ -471,7 +480,7 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                 const bool live0 = (bits & need0) == need0 && sq.x >= -__int_as_float(1) && sq.x <= q1.z;
                 const bool live1 = (bits & need1) == need1 && sq.y >= -__int_as_float(1) && sq.y <= q1.z;
                 if (kMode == 0) {
-                    const float2 q2 = reinterpret_cast<const float2*>(recs + j)[4];
+                    const float2 q2 = reinterpret_cast<const float2*>(&recs[j].r)[4];
                     const float2 arg = __ffma2_rn(sq, f2(kNegHalfLog2e), f2(q1.y));
                     const float a0 = live0 ? fminf(ex2_approx(arg.x), 0.99f) : 0.0f;
                     const float a1 = live1 ? fminf(ex2_approx(arg.y), 0.99f) : 0.0f;
@@ -482,18 +491,18 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                     T = __ffma2_rn(w, f2(-1.0f), T);
                     if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
                 } else if (kMode == 2) {
-                    const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
+                    const uint4 q3 = reinterpret_cast<const uint4*>(&recs[j].r)[3];
                     const uint32_t z24 = q3.x, id = q3.y;
                     stoch2_retire(P0, z24, kDepthMargin);
                     stoch2_retire(P1, z24, kDepthMargin);
                     if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
-                    const float2 q2 = reinterpret_cast<const float2*>(recs + j)[4];
+                    const float2 q2 = reinterpret_cast<const float2*>(&recs[j].r)[4];
                     const float op = __uint_as_float(q3.w);
                     const float hz0 = add((float)id, p.frame_seed), hz1 = add((float)id, p.frame_seed2);
                     stoch2_step(P0, live0, sq.x, op, fcx, fcy0, hz0, hz1, z24, id, q1.w, q2.x, q2.y);
                     stoch2_step(P1, live1, sq.y, op, fcx, fcy1, hz0, hz1, z24, id, q1.w, q2.x, q2.y);
                 } else {
-                    const uint4 q3 = reinterpret_cast<const uint4*>(recs + j)[3];
+                    const uint4 q3 = reinterpret_cast<const uint4*>(&recs[j].r)[3];
                     const uint32_t z24 = q3.x, id = q3.y;
                     // a pixel stops once splats are beyond its kept depth (+ margin)
                     if (S0.best_id != 0xFFFFFFFFu && z24 > S0.best_d24 + kDepthMargin) sdone0 = true;
@@ -501,7 +510,7 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                     if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
                     const bool b0 = z24 < S0.best_d24 || (z24 == S0.best_d24 && id < S0.best_id);
                     const bool b1 = z24 < S1.best_d24 || (z24 == S1.best_d24 && id < S1.best_id);
-                    const float2 q2 = reinterpret_cast<const float2*>(recs + j)[4];
+                    const float2 q2 = reinterpret_cast<const float2*>(&recs[j].r)[4];
                     const float op = __uint_as_float(q3.w);
                     if (live0 && !sdone0 && b0) stoch_step(S0, sq.x, op, fcx, fcy0, hz, z24, id, q1.w, q2.x, q2.y);
                     if (live1 && !sdone1 && b1) stoch_step(S1, sq.y, op, fcx, fcy1, hz, z24, id, q1.w, q2.x, q2.y);
