@@ -129,3 +129,26 @@ def test_streamed_readback_of_an_overflowing_frame():
         for b in bufs:
             gate = image_gate(b.numpy(), ref_img)
             assert gate["ok"], gate
+
+
+@pytest.mark.parametrize("mode", ["stochastic", "gps"])
+def test_streamed_frames_keep_the_render_state(mode):
+    """Stochastic and GPS frames carry state from frame to frame (sample
+    seeds, running accumulation, TAA history): six streamed frames equal, bit
+    for bit, the frames of a second context that draws the same cameras one
+    gs_render_host call at a time."""
+    rows = small_rows(20_000, seed=16)
+    W, H = 200, 120
+    cams = [camera_uniforms((0.03 * (i % 3), 0.0, 3.0), np.pi, 0.0, W, H) for i in range(6)]
+    knobs = dict(splat_render_mode=mode, black_background=1)
+    with Renderer(0) as a, Renderer(0) as b:
+        for r in (a, b):
+            r.set(**knobs)
+            r.upload_gaussians(rows)
+        ref = [a.draw_frame(cam) for cam in cams]
+        bufs = [torch.empty((H, W, 4), dtype=torch.float16, pin_memory=True) for _ in cams]
+        for cam, buf in zip(cams, bufs):
+            b.submit_frame(cam, buf)
+        b.wait_frames()
+        for k, (buf, img) in enumerate(zip(bufs, ref)):
+            assert np.array_equal(buf.numpy().view(np.uint16), img.view(np.uint16)), k
