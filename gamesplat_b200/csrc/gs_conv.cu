@@ -37,7 +37,13 @@ namespace conv {
 
 constexpr int kThreads = 128;
 constexpr int kHaloRows = 136;                  // 130 used (pixels x0-1 .. x0+128)
-constexpr int kColBytes = kHaloRows * 16 + 16;  // one 8-channel column of a halo row (+16: bank spread)
+// One 8-channel column of a halo row (kHaloRows pixels of 16 bytes) plus
+// padding.  Consecutive threads copy the kG columns of a pixel, then the next
+// pixel's; a quarter warp's eight 16-byte copies hit distinct banks when the
+// columns are 8 banks apart for kG = 4 (stride = 32 mod 128 bytes) and 16
+// banks apart for kG = 2 (64 mod 128).  It is also the MMA descriptors'
+// K-direction stride.
+__host__ __device__ constexpr int col_bytes(int cin) { return kHaloRows * 16 + (cin / 8 == 2 ? 64 : 32); }
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 __host__ __device__ constexpr int wimage_bytes(int cin, int cout) { return 9 * cin * cout * 2; }
@@ -49,7 +55,7 @@ constexpr int kHalfPix = 66;   // half-resolution pixels under a 130-pixel halo 
 // Dynamic shared memory of the forward kernel: the halo rows, the weight
 // image, and (load mode 1) the half-resolution rows staged beside them.
 __host__ __device__ constexpr int fwd_smem_bytes(int cin, int cout, int load = 0) {
-    return kSlots * (cin / 8) * kColBytes + wimage_bytes(cin, cout) + (load ? kSlots * kHalfPix * cin * 2 : 0);
+    return kSlots * (cin / 8) * col_bytes(cin) + wimage_bytes(cin, cout) + (load ? kSlots * kHalfPix * cin * 2 : 0);
 }
 
 // 16-byte asynchronous global -> shared copy (zero-filled when src_bytes is 0).
@@ -96,6 +102,7 @@ template <int kCin, int kCout, int kLoad>
 __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     static_assert(kCin % 16 == 0 && (kCout == 16 || kCout == 32), "channel counts");
     constexpr int kG = kCin / 8;                         // 16-byte columns per pixel
+    constexpr int kColBytes = col_bytes(kCin);
     constexpr int kSlot = kG * kColBytes;                // one halo row
     constexpr int kW = wimage_bytes(kCin, kCout);
     constexpr uint32_t kIdesc = umma::idesc_bf16(128, kCout, 0, 0);
