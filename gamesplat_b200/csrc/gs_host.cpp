@@ -788,16 +788,24 @@ int render_stochastic(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
             r.vp_w = c->cam.viewport[0];
             r.vp_h = c->cam.viewport[1];
             r.clip_y_sign = c->cam.clip_y_sign;
-            r.out_rgba32f = c->st.sample;
-            r.out_depth = c->st.depth;
+            // TAA with several samples: the rasterizer folds each sample into
+            // the frame average itself; only the last sample's colour and
+            // depth are kept (the TAA pass and the debug reads use those)
+            const bool fold = use_taa && render_samples > 1, last = i + 1 == render_samples;
+            r.out_rgba32f = !fold || last ? c->st.sample : nullptr;
+            r.out_depth = !fold || last ? c->st.depth : nullptr;
+            if (fold) {
+                const uint32_t w = i & 1u, rd = w ^ 1u;
+                r.accum_in = i == 0 ? nullptr : c->st.frame_avg[rd];
+                r.accum_out = c->st.frame_avg[w];
+                r.accum_n = (float)(i + 1);
+            }
             r.rgba8 = c->knobs.linear_color ? 0 : 1;
             sc.add(gs::launch_raster_stochastic(r, c->stream));
         }
         StageScope sa(c, ST_ACCUM);
         if (use_taa && render_samples > 1) {
-            uint32_t w = i & 1u, rd = w ^ 1u;
-            sa.add(gs::launch_accum(c->st.sample, i == 0 ? c->st.sample : c->st.frame_avg[rd], (float)(i + 1),
-                                    c->st.frame_avg[w], npix, c->stream));
+            // folded into the rasterizer above
         } else if (!use_taa && (c->knobs.stochastic_accumulation_enabled || render_samples > 1)) {
             const bool acc = c->knobs.stochastic_accumulation_enabled != 0;
             uint32_t next = acc ? c->sample_count + 1 : i + 1;

@@ -196,6 +196,11 @@ struct RasterParams {
     uint16_t* out_rgba16f;           // width*height*4 halves, top row first
     float4* out_rgba32f;             // optional float copy (stochastic sample), top row first
     float* out_depth;                // optional window depth (stochastic), top row first
+    // optional running mean of the samples (stochastic): accum_out = h + (sample - h) / max(accum_n, 1)
+    // with h = accum_in, or the sample itself when accum_in is null (accum_kernel's arithmetic)
+    const float4* accum_in;
+    float4* accum_out;
+    float accum_n;
     int rgba8;                       // quantise stochastic sample like RGBA8 UNORM
     FrameCounters* fc;
 };

@@ -195,6 +195,12 @@ __device__ __forceinline__ void write_pixel_stoch(const RasterParams& p, int px,
     }
     if (p.out_rgba32f) p.out_rgba32f[o] = c;
     if (p.out_depth) p.out_depth[o] = (float)S.best_d24 / 16777215.0f;
+    if (p.accum_out) {   // the frame's running mean, as accum_kernel computes it from the sample
+        const float nn = g_max(p.accum_n, 1.0f);
+        const float4 h = p.accum_in ? p.accum_in[o] : c;
+        p.accum_out[o] = make_float4(add(h.x, dv(sub(c.x, h.x), nn)), add(h.y, dv(sub(c.y, h.y), nn)),
+                                     add(h.z, dv(sub(c.z, h.z), nn)), add(h.w, dv(sub(c.w, h.w), nn)));
+    }
     if (p.out_rgba16f) write_rgba16f(p.out_rgba16f, o, c.x, c.y, c.z, c.w);
 }
 
