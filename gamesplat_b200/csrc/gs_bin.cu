@@ -314,6 +314,8 @@ __global__ void __launch_bounds__(kBinThreads) expand_kernel(BinParams p) {
 // takes 8 consecutive keys (two 16-byte loads) and the keys either side.
 __global__ void tile_ranges_kernel(const SortPlan* plan, const FrameCounters* fc, uint2* ranges,
                                    uint32_t num_tiles) {
+    pdl_wait();
+    pdl_trigger();
     const uint32_t E = fc->tile_entries;
     const uint32_t* keys = plan->kfinal;
     const uint32_t groups = (E + 7) / 8;
@@ -347,6 +349,8 @@ __global__ void tile_ranges_kernel(const SortPlan* plan, const FrameCounters* fc
 // (each tile's CTA writes only its own pixels).
 __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* __restrict__ ranges, uint32_t num_tiles,
                                                           uint32_t* __restrict__ order) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ uint32_t s_cnt[129], s_start[129];
     const int t = threadIdx.x;
     if (t < 129) s_cnt[t] = 0u;
@@ -374,7 +378,9 @@ __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* __restric
 
 int launch_tile_order(const uint2* ranges, uint32_t num_tiles, uint32_t* order, cudaStream_t s) {
     if (num_tiles == 0) return 0;
-    tile_order_kernel<<<1, 1024, 0, s>>>(ranges, num_tiles, order);
+    // programmatic dependent launch (as the ranges and the raster after it): the kernel is scheduled while its
+    // predecessor drains and waits for it (griddepcontrol.wait) before it reads anything
+    launch_pdl(tile_order_kernel, dim3(1), dim3(1024), 0, s, ranges, num_tiles, order);
     return 1;
 }
 
@@ -393,7 +399,7 @@ int launch_tile_ranges(const SortPlan* tile_plan, const FrameCounters* fc, uint3
     uint32_t grid = (entry_cap / 8 + 255) / 256;
     if (grid > num_sms * 8) grid = num_sms * 8;
     if (grid == 0) grid = 1;
-    tile_ranges_kernel<<<grid, 256, 0, s>>>(tile_plan, fc, ranges, num_tiles);
+    launch_pdl(tile_ranges_kernel, dim3(grid), dim3(256), 0, s, tile_plan, (const FrameCounters*)fc, ranges, num_tiles);
     return 1;
 }
 

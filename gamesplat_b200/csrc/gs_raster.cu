@@ -551,6 +551,7 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
 
 template <int kMode, int kTw = 16, int kTh = 16>
 __global__ void __launch_bounds__(kRasterThreads) raster_kernel(RasterParams p) {
+    pdl_wait();
     __shared__ RasterShared<kMode, kTw, kTh> sh;
     if (p.tile_count && blockIdx.x >= *p.tile_count) return;
     raster_tile<kMode, kTw, kTh>(p, p.tile_order[blockIdx.x], sh);
@@ -602,7 +603,7 @@ int launch_raster_alpha(const RasterParams& p, cudaStream_t s) {
     if (tiles == 0) return 0;
     if (p.tile_w == 32) raster_kernel<0, 32, 8><<<tiles, kRasterThreads, 0, s>>>(p);
     else if (p.tile_w == 8) raster_kernel<0, 8, 32><<<tiles, kRasterThreads, 0, s>>>(p);
-    else raster_kernel<0><<<tiles, kRasterThreads, 0, s>>>(p);
+    else launch_pdl(raster_kernel<0, 16, 16>, dim3(tiles), dim3(kRasterThreads), 0, s, p);
     return 1;
 }
 
