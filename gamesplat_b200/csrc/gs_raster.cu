@@ -64,15 +64,31 @@ constexpr float kTransmittanceMin = 1.0f / 8192.0f;
 constexpr uint32_t kDepthMargin = 8;
 constexpr float kNegHalfLog2e = -0.72134752044448170368f;   // -0.5 / ln(2)
 
-__device__ __forceinline__ float hash13(float p0, float p1, float p2) {
-    p0 = g_fract(mul(p0, 0.1031f));
-    p1 = g_fract(mul(p1, 0.1031f));
-    p2 = g_fract(mul(p2, 0.1031f));
-    float d = add(add(mul(p0, add(p1, 33.33f)), mul(p1, add(p2, 33.33f))), mul(p2, add(p0, 33.33f)));
-    p0 = add(p0, d);
-    p1 = add(p1, d);
-    p2 = add(p2, d);
-    return g_fract(mul(add(p0, p1), p2));
+// hash13(x, y, z) (shaders/splat.glsl:121-125), split by what its terms
+// depend on: p0 = fract(0.1031 x), p1 = fract(0.1031 y) and the products that
+// hold only them belong to the pixel (computed once per tile), p2 =
+// fract(0.1031 z) to the splat and sample (once per splat for all the pixels of
+// a warp); the rest, per (pixel, splat, sample), is the same operations in the
+// same order:  d = p0 (p1 + 33.33) + p1 (p2 + 33.33) + p2 (p0 + 33.33),
+// hash = fract((p0 + d + p1 + d) (p2 + d)).
+struct PixelHash {
+    float p0, p1, t1, p0c;   // p0, p1, p0 (p1 + 33.33), p0 + 33.33
+};
+
+__device__ __forceinline__ PixelHash pixel_hash(float x, float y) {
+    PixelHash h;
+    h.p0 = g_fract(mul(x, 0.1031f));
+    h.p1 = g_fract(mul(y, 0.1031f));
+    h.t1 = mul(h.p0, add(h.p1, 33.33f));
+    h.p0c = add(h.p0, 33.33f);
+    return h;
+}
+
+__device__ __forceinline__ float hash_z(float z) { return g_fract(mul(z, 0.1031f)); }
+
+__device__ __forceinline__ float hash13(const PixelHash& h, float p2) {
+    const float d = add(add(h.t1, mul(h.p1, add(p2, 33.33f))), mul(p2, h.p0c));
+    return g_fract(mul(add(add(h.p0, d), add(h.p1, d)), add(p2, d)));
 }
 
 __device__ __forceinline__ float ex2_approx(float x) {
@@ -91,9 +107,10 @@ struct StochState {
 // alpha = min(opacity * exp(power), 0.99) with power <= 0 (exp <= 1 there, also
 // for the deterministic exp) never exceeds min(opacity, 0.99): a fragment whose
 // hash is at or above that bound is rejected without evaluating exp.
-__device__ __forceinline__ void stoch_step(StochState& S, float s, float opacity, float fcx, float fcy,
-                                           float hz, uint32_t z24, uint32_t id, float r, float g, float b) {
-    const float rnd = hash13(fcx, fcy, hz);
+// ph: the pixel's hash terms, hz: hash_z(splat id + sample seed).
+__device__ __forceinline__ void stoch_step(StochState& S, float s, float opacity, const PixelHash& ph, float hz,
+                                           uint32_t z24, uint32_t id, float r, float g, float b) {
+    const float rnd = hash13(ph, hz);
     if (!(rnd < g_min(opacity, 0.99f))) return;
     const float alpha = g_min(mul(opacity, det_expf(mul(-0.5f, s))), 0.99f);
     if (rnd < alpha) {
@@ -119,7 +136,7 @@ __device__ __forceinline__ void stoch2_init(Stoch2& P, bool inside) {
 }
 
 // One splat into both samples of a pixel: alpha once, one hash per seed.
-__device__ __forceinline__ void stoch2_step(Stoch2& P, bool live, float sq, float opacity, float fcx, float fcy,
+__device__ __forceinline__ void stoch2_step(Stoch2& P, bool live, float sq, float opacity, const PixelHash& ph,
                                             float hz0, float hz1, uint32_t z24, uint32_t id, float r, float g,
                                             float b) {
     bool want[2];
@@ -134,7 +151,7 @@ __device__ __forceinline__ void stoch2_step(Stoch2& P, bool live, float sq, floa
     bool cand[2];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-        rnd[k] = want[k] ? hash13(fcx, fcy, k ? hz1 : hz0) : 1.0f;
+        rnd[k] = want[k] ? hash13(ph, k ? hz1 : hz0) : 1.0f;
         cand[k] = want[k] && rnd[k] < bound;
     }
     if (!(cand[0] || cand[1])) return;
@@ -306,6 +323,8 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
 
     const float fcx = (float)px + 0.5f, fcy0 = (float)py0 + 0.5f, fcy1 = (float)py1 + 0.5f;
     const float2 fcy = make_float2(fcy0, fcy1);
+    // the stochastic modes' hash terms of the two pixels
+    const PixelHash ph0 = pixel_hash(fcx, fcy0), ph1 = pixel_hash(fcx, fcy1);
     // alpha state of the two pixels (x: pixel 0, y: pixel 1); pixels outside
     // the image start "done" (T = 0) and are never written
     float2 T = make_float2(in0 ? 1.0f : 0.0f, in1 ? 1.0f : 0.0f);
@@ -504,9 +523,9 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                     if (__all_sync(0xffffffffu, pixels_done())) { warp_done = true; break; }
                     const float2 q2 = reinterpret_cast<const float2*>(&recs[j].r)[4];
                     const float op = __uint_as_float(q3.w);
-                    const float hz0 = add((float)id, p.frame_seed), hz1 = add((float)id, p.frame_seed2);
-                    stoch2_step(P0, live0, sq.x, op, fcx, fcy0, hz0, hz1, z24, id, q1.w, q2.x, q2.y);
-                    stoch2_step(P1, live1, sq.y, op, fcx, fcy1, hz0, hz1, z24, id, q1.w, q2.x, q2.y);
+                    const float hz0 = hash_z(add((float)id, p.frame_seed)), hz1 = hash_z(add((float)id, p.frame_seed2));
+                    stoch2_step(P0, live0, sq.x, op, ph0, hz0, hz1, z24, id, q1.w, q2.x, q2.y);
+                    stoch2_step(P1, live1, sq.y, op, ph1, hz0, hz1, z24, id, q1.w, q2.x, q2.y);
                 } else {
                     const uint4 q3 = reinterpret_cast<const uint4*>(&recs[j].r)[3];
                     const uint32_t z24 = q3.x, id = q3.y;
@@ -518,8 +537,9 @@ __device__ __forceinline__ void raster_tile(const RasterParams& p, const uint32_
                     const bool b1 = z24 < S1.best_d24 || (z24 == S1.best_d24 && id < S1.best_id);
                     const float2 q2 = reinterpret_cast<const float2*>(&recs[j].r)[4];
                     const float op = __uint_as_float(q3.w);
-                    if (live0 && !sdone0 && b0) stoch_step(S0, sq.x, op, fcx, fcy0, hz, z24, id, q1.w, q2.x, q2.y);
-                    if (live1 && !sdone1 && b1) stoch_step(S1, sq.y, op, fcx, fcy1, hz, z24, id, q1.w, q2.x, q2.y);
+                    const float hzf = hash_z(hz);
+                    if (live0 && !sdone0 && b0) stoch_step(S0, sq.x, op, ph0, hzf, z24, id, q1.w, q2.x, q2.y);
+                    if (live1 && !sdone1 && b1) stoch_step(S1, sq.y, op, ph1, hzf, z24, id, q1.w, q2.x, q2.y);
                 }
             }
         }
