@@ -116,12 +116,13 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     __shared__ float s_bias[kCout];
 
     const int strips_x = (a.w + 127) / 128;
-    const int segs = (a.h + a.rows_per_cta - 1) / a.rows_per_cta;
+    const int segs = (a.h + a.row_offset + a.rows_per_cta - 1) / a.rows_per_cta;
     const int item = blockIdx.x;
     if (item >= a.n * strips_x * segs) return;
     const int seg = item % segs, strip = item / segs;
     const int n = strip / strips_x, x0 = (strip % strips_x) * 128;
-    const int y0 = seg * a.rows_per_cta, y1 = min(a.h, y0 + a.rows_per_cta);
+    const int y0 = max(0, seg * a.rows_per_cta - a.row_offset);
+    const int y1 = min(a.h, seg * a.rows_per_cta - a.row_offset + a.rows_per_cta);
     const int tid = threadIdx.x, warp = tid >> 5;
 
     // weights: the packed image, copied verbatim; the bias
@@ -194,6 +195,7 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     const uint32_t halo_base = smem_u32(s_halo), w_base = smem_u32(s_w);
     uint32_t phase0 = 0, phase1 = 0;
     bool failed = false;
+    float err_sum = 0.0f, err_cnt = 0.0f;   // head mode: this thread's column of the band, in row order
     // Two TMEM accumulators: the MMAs of row y (accumulator y & 1) run while
     // the epilogue of row y - 1 reads the other one.
     auto wait_mma = [&](int y) {   // row y's MMAs are done (every thread waits)
@@ -256,6 +258,20 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
                         if (!(__bfloat162float(mb[e]) > 0.0f)) v[q * 8 + e] = 0.0f;
                 }
             }
+            if (kCout == 16 && a.head_x) {
+                // the denoised frame's pixel (head_rgba of the output step) and its error estimate
+                const uint4 xv = __ldg(reinterpret_cast<const uint4*>(a.head_x + o * 16));
+                const __nv_bfloat16* xb = reinterpret_cast<const __nv_bfloat16*>(&xv);
+                const float4 px = make_float4(__bfloat162float(xb[5]) + v[0], __bfloat162float(xb[6]) + v[1],
+                                              __bfloat162float(xb[7]) + v[2], __bfloat162float(xb[3]) + v[3]);
+                __half2 h01 = __floats2half2_rn(px.x, px.y), h23 = __floats2half2_rn(px.z, px.w);
+                uint2 pk;
+                pk.x = *reinterpret_cast<uint32_t*>(&h01);
+                pk.y = *reinterpret_cast<uint32_t*>(&h23);
+                reinterpret_cast<uint2*>(a.head_out16)[o] = pk;
+                err_sum += fmaxf(v[4], 0.0f);
+                err_cnt += 1.0f;
+            }
             if (a.out_bf16) {
                 uint4* op = reinterpret_cast<uint4*>(a.out_bf16 + o * kCout);
 #pragma unroll
@@ -297,6 +313,23 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     if (!broke) {   // the whole CTA: the epilogue's TMEM loads are warp-collective
         wait_mma(y1 - 1);
         epilogue(y1 - 1);
+    }
+    if (kCout == 16 && a.head_x && !broke) {
+        // per tile (16 threads = 16 columns of the band): the sum of the error estimates and the
+        // pixel count, each over 16 lanes in a fixed order, then the tile's mean
+#pragma unroll
+        for (int off = 8; off; off >>= 1) {
+            err_sum += __shfl_xor_sync(0xffffffffu, err_sum, off);
+            err_cnt += __shfl_xor_sync(0xffffffffu, err_cnt, off);
+        }
+        const int tx = (x0 >> 4) + (tid >> 4);
+        if ((tid & 15) == 0 && tx < a.tiles_x && err_cnt > 0.0f) {
+            const int ty = (a.h + a.row_offset) / 16 - 1 - seg;   // GL tile row of this band
+            const uint32_t tile = (uint32_t)(ty * a.tiles_x + tx);
+            const float mse = err_sum / err_cnt * 0.001f;
+            if (a.tile_err) a.tile_err[tile] = mse;
+            if (mse >= a.err_budget) a.fallback_tiles[atomicAdd(a.fallback_count, 1u)] = tile;
+        }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");   // the prefetched rows past the run
     if (failed && tid == 0) atomicOr(a.err, 1u);
@@ -447,7 +480,7 @@ __global__ void pack_weights_kernel(const float* __restrict__ w, int cin, int co
 template <int kCin, int kCout, int kLoad>
 static int launch_fwd_t(const ConvArgs& a, cudaStream_t s) {
     const int strips = a.n * ((a.w + 127) / 128);
-    const int segs = (a.h + a.rows_per_cta - 1) / a.rows_per_cta;
+    const int segs = (a.h + a.row_offset + a.rows_per_cta - 1) / a.rows_per_cta;
     const size_t smem = (size_t)fwd_smem_bytes(kCin, kCout, kLoad);
     static bool attr = false;
     if (!attr) {

@@ -22,6 +22,18 @@ struct ConvArgs {
     float* out_f32;             // Cout channels, or null
     int rows_per_cta;
     uint32_t* err;              // bit 0 set if a bounded wait ran out
+    int row_offset;             // the row bands of the CTAs start at -row_offset (0: at row 0)
+    // Denoised-mode head (Cout = 16, forward, head_x set): the epilogue writes head_out16 =
+    // RGBA16F (head_x[5..7] + o[0..2], head_x[3] + o[3]) instead of the outputs above and,
+    // per 16x16 tile of GL rows (rows_per_cta = 16 and row_offset aligning the bands with
+    // them), tile_err = mean(max(o[4], 0)) * 0.001, listing tiles at or above err_budget.
+    const __nv_bfloat16* head_x;   // the network input (16 channels per pixel)
+    uint16_t* head_out16;
+    float* tile_err;
+    uint32_t* fallback_count;
+    uint32_t* fallback_tiles;
+    float err_budget;
+    int tiles_x;
 };
 
 // dw[tap * Cin + cin][cout] += sum over pixels of X[p + tap][cin] * dy[p][cout],

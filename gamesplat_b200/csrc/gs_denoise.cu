@@ -1,8 +1,10 @@
 // Elementwise and reduction kernels of the stochastic-splat denoiser: input
 // features, 2x average pooling and the backward passes of pooling and
-// upsampling, the output head, the L1 + SSIM training loss with its
-// gradient, Adam, and the per-tile error estimate that picks the tiles the
-// sorted-alpha rasterizer renders again.  The convolutions are in gs_conv.cu.
+// upsampling, the output head of training, the L1 + SSIM training loss with
+// its gradient and Adam.  The convolutions are in gs_conv.cu; in the denoised
+// render mode the last convolution's epilogue writes the frame and the
+// per-tile error estimate that picks the tiles the sorted-alpha rasterizer
+// renders again (conv::ConvArgs::head_x).
 //
 // Network (NHWC bf16 activations, FP32 accumulation):
 //   x   16 ch  = noisy RGB, alpha, expected depth, reprojected history RGB, 8 zero channels
@@ -285,53 +287,6 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
 }
 
 // ---------------------------------------------------------------------------
-// Rendering: the denoised frame into RGBA16F (top row first) and the tiles
-// whose estimated error is over budget.
-// ---------------------------------------------------------------------------
-__global__ void output_tiles_kernel(const float* __restrict__ o, const __nv_bfloat16* __restrict__ x, int width,
-                                    int height, int tiles_x, float err_budget, uint16_t* __restrict__ out16,
-                                    uint32_t* __restrict__ fallback_count, uint32_t* __restrict__ fallback_tiles,
-                                    float* __restrict__ tile_err) {
-    // one 256-thread CTA per 16x16 tile; pixel (tx*16 + t%16, ty*16 + t/16) in GL rows
-    const int tile = blockIdx.x;
-    const int tx = tile % tiles_x, ty = tile / tiles_x;
-    const int gx = tx * 16 + (threadIdx.x & 15), gy = ty * 16 + (threadIdx.x >> 4);
-    float err = 0.0f, cnt = 0.0f;
-    if (gx < width && gy < height) {
-        const size_t i = (size_t)(height - 1 - gy) * width + gx;   // top row first
-        const float* oi = o + i * kOutC;
-        const float4 p = head_rgba(oi, x + i * kInC);
-        err = fmaxf(oi[4], 0.0f);
-        cnt = 1.0f;
-        __half2 h01 = __floats2half2_rn(p.x, p.y), h23 = __floats2half2_rn(p.z, p.w);
-        uint2 pk;
-        pk.x = *reinterpret_cast<uint32_t*>(&h01);
-        pk.y = *reinterpret_cast<uint32_t*>(&h23);
-        reinterpret_cast<uint2*>(out16)[i] = pk;
-    }
-    __shared__ float s_e[8], s_c[8];
-    for (int off = 16; off; off >>= 1) {
-        err += __shfl_xor_sync(0xffffffffu, err, off);
-        cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        s_e[threadIdx.x >> 5] = err;
-        s_c[threadIdx.x >> 5] = cnt;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float te = 0.0f, tc = 0.0f;
-        for (int k = 0; k < 8; ++k) {
-            te += s_e[k];
-            tc += s_c[k];
-        }
-        const float mse = tc > 0.0f ? te / tc * 0.001f : 0.0f;
-        if (tile_err) tile_err[tile] = mse;
-        if (mse >= err_budget) fallback_tiles[atomicAdd(fallback_count, 1u)] = (uint32_t)tile;
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
 static int grid_for(size_t n, int threads = 256) {
@@ -392,13 +347,5 @@ int launch_adam(float* w, const float* g, float* m, float* v, int count, float l
     adam_kernel<<<grid_for(count), 256, 0, s>>>(w, g, m, v, count, lr, b1, b2, eps, bc1, bc2);
     return 1;
 }
-int launch_output_tiles(const float* o, const __nv_bfloat16* x, int width, int height, int tiles_x, int tiles_y,
-                        float err_budget, uint16_t* out16, uint32_t* fallback_count, uint32_t* fallback_tiles,
-                        float* tile_err, cudaStream_t s) {
-    output_tiles_kernel<<<tiles_x * tiles_y, 256, 0, s>>>(o, x, width, height, tiles_x, err_budget, out16,
-                                                          fallback_count, fallback_tiles, tile_err);
-    return 1;
-}
-
 }  // namespace dn
 }  // namespace gs

@@ -30,9 +30,6 @@ int launch_loss_grad(const float* o, const float4* pred, const float4* target, c
                      cudaStream_t s);
 int launch_adam(float* w, const float* g, float* m, float* v, int count, float lr, float b1, float b2, float eps,
                 float bc1, float bc2, cudaStream_t s);
-int launch_output_tiles(const float* o, const __nv_bfloat16* x, int width, int height, int tiles_x, int tiles_y,
-                        float err_budget, uint16_t* out16, uint32_t* fallback_count, uint32_t* fallback_tiles,
-                        float* tile_err, cudaStream_t s);
 
 }  // namespace dn
 }  // namespace gs

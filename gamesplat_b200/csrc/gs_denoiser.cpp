@@ -217,6 +217,43 @@ int forward(gs_denoiser* d, const bf16* x, int n, int h, int w, cudaStream_t s) 
     return GS_OK;
 }
 
+int forward_frame(gs_denoiser* d, const bf16* x, int h, int w, uint16_t* out16, int tiles_x, float err_budget,
+                  uint32_t* fallback_count, uint32_t* fallback_tiles, float* tile_err, cudaStream_t s) {
+    if (h <= 0 || w <= 0 || (h & 1) || (w & 1) || !out16 || !fallback_count || !fallback_tiles) return GS_ERR_BAD_ARG;
+    int rc = ensure_acts(d, (size_t)h * w);
+    if (rc) return rc;
+    d->last_x = nullptr;   // the activations are this frame's now: no backward pass follows
+    d->last_n = 0;
+    if (!d->images_valid) pack_images(d, s);
+    const int hh = h / 2, hw = w / 2;
+    if ((rc = conv_fwd(d, 0, false, x, nullptr, 1, h, w, nullptr, d->e1, nullptr, s))) return rc;
+    launch_avgpool2(d->e1, 1, h, w, d->p1, s);
+    if ((rc = conv_fwd(d, 1, false, d->p1, nullptr, 1, hh, hw, nullptr, d->e2, nullptr, s))) return rc;
+    if ((rc = conv_fwd(d, 2, false, d->e2, nullptr, 1, hh, hw, nullptr, d->e3, nullptr, s))) return rc;
+    if ((rc = conv_fwd(d, 3, false, d->e1, d->e3, 1, h, w, nullptr, d->d4, nullptr, s))) return rc;
+    // the last layer with the output step in its epilogue: row bands of 16 rows aligned with the tiles
+    const Layer& L = kNet[4];
+    conv::ConvArgs a{};
+    a.x = d->d4;
+    a.n = 1;
+    a.h = h;
+    a.w = w;
+    a.wimage = d->wimg[4];
+    a.bias = d->params + b_offset(4);
+    a.relu = L.relu;
+    a.rows_per_cta = 16;
+    a.row_offset = (16 - h % 16) % 16;
+    a.err = d->err;
+    a.head_x = x;
+    a.head_out16 = out16;
+    a.tile_err = tile_err;
+    a.fallback_count = fallback_count;
+    a.fallback_tiles = fallback_tiles;
+    a.err_budget = err_budget;
+    a.tiles_x = tiles_x;
+    return conv::launch_fwd(L.cin, L.cout, L.load, a, s) < 0 ? GS_ERR_BAD_ARG : GS_OK;
+}
+
 int backward(gs_denoiser* d, const bf16* x, const bf16* dout, int n, int h, int w) {
     if (d->last_x != x || d->last_n != n || d->last_h != h || d->last_w != w) return GS_ERR_BAD_ARG;
     const size_t pix = (size_t)n * h * w;

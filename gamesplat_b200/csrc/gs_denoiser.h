@@ -21,5 +21,15 @@ uint64_t parameter_count();
 int forward(gs_denoiser* d, const __nv_bfloat16* x, int n, int h, int w, cudaStream_t s);
 const float* output(const gs_denoiser* d);
 
+// The denoised mode's frame: the forward pass of one h x w frame whose last
+// layer writes the RGBA16F image out16 (the input's history RGB and alpha plus
+// the network's correction) and, per 16x16 tile (tiles_x across, GL rows from
+// the bottom), tile_err = the estimated mean squared error; tiles at or above
+// err_budget are appended to fallback_tiles (count in *fallback_count).  The
+// last layer's 16 output channels are not stored.
+int forward_frame(gs_denoiser* d, const __nv_bfloat16* x, int h, int w, uint16_t* out16, int tiles_x,
+                  float err_budget, uint32_t* fallback_count, uint32_t* fallback_tiles, float* tile_err,
+                  cudaStream_t s);
+
 }  // namespace dn
 }  // namespace gs

@@ -952,12 +952,12 @@ int render_denoised(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
     if (rc) return rc;
     {
         StageScope sd(c, ST_DENOISE);
-        rc = gs::dn::forward(c->denoiser, c->features, 1, c->height, c->width, c->stream);
+        // the network, its last layer writing the frame and the tiles' error estimates
+        rc = gs::dn::forward_frame(c->denoiser, c->features, c->height, c->width, out, c->tiles_x,
+                                   c->denoise_fallback ? c->denoise_budget : 3.0e38f, &c->fc->fallback_tiles,
+                                   c->fallback_tiles, c->tile_error, c->stream);
         if (rc) return fail(c, rc, "denoiser forward failed");
-        sd.add(7);
-        sd.add(gs::dn::launch_output_tiles(gs::dn::output(c->denoiser), c->features, c->width, c->height, c->tiles_x,
-                                           c->tiles_y, c->denoise_fallback ? c->denoise_budget : 3.0e38f, out,
-                                           &c->fc->fallback_tiles, c->fallback_tiles, c->tile_error, c->stream));
+        sd.add(6);
     }
     if (c->denoise_fallback) {
         StageScope sc(c, ST_RASTER);
