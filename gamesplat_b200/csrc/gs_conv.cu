@@ -114,6 +114,8 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     __shared__ __align__(8) uint64_t s_bar[2];   // MMA completion, one per accumulator
     __shared__ uint32_t s_taddr;
     __shared__ float s_bias[kCout];
+    constexpr bool kPool = kCin == 16 && kCout == 32;   // the pooled output (conv1 of the denoiser)
+    __shared__ __align__(16) uint4 s_pool[kPool ? kThreads * 4 : 1];   // an even row's bf16 outputs
 
     const int strips_x = (a.w + 127) / 128;
     const int segs = (a.h + a.row_offset + a.rows_per_cta - 1) / a.rows_per_cta;
@@ -290,6 +292,46 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
                     op[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
             }
         }
+        if (kPool && a.pool_out) {
+            // 2x2 average of the bf16 outputs: (0 + (y, x) + (y, x + 1) + (y + 1, x) + (y + 1, x + 1)) * 0.25,
+            // the even row parked in shared memory, the right neighbour's by a lane shuffle
+            uint32_t pk[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+                pk[e] = *reinterpret_cast<uint32_t*>(&b2);
+            }
+            if ((y & 1) == 0) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) s_pool[tid * 4 + q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
+            } else {
+                uint32_t nb[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e) nb[e] = __shfl_xor_sync(0xffffffffu, pk[e], 1);
+                if ((x & 1) == 0 && x < a.w && !failed) {
+                    const uint32_t* up = reinterpret_cast<const uint32_t*>(&s_pool[tid * 4]);
+                    const uint32_t* un = reinterpret_cast<const uint32_t*>(&s_pool[(tid + 1) * 4]);
+                    uint32_t res[16];
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const uint32_t t4[4] = {up[e], un[e], pk[e], nb[e]};
+                        float acc0 = 0.0f, acc1 = 0.0f;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&t4[k]));
+                            acc0 += f.x;
+                            acc1 += f.y;
+                        }
+                        __nv_bfloat162 r2 = __floats2bfloat162_rn(0.25f * acc0, 0.25f * acc1);
+                        res[e] = *reinterpret_cast<uint32_t*>(&r2);
+                    }
+                    const int hw2 = a.w >> 1;
+                    uint4* dp = reinterpret_cast<uint4*>(a.pool_out + (((size_t)n * (a.h >> 1) + (y >> 1)) * hw2 + (x >> 1)) * kCout);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) dp[q] = make_uint4(res[4 * q], res[4 * q + 1], res[4 * q + 2], res[4 * q + 3]);
+                }
+            }
+        }
         umma::fence_before_sync();
     };
 
@@ -312,6 +354,7 @@ __global__ void __launch_bounds__(kThreads) conv_fwd_kernel(ConvArgs a) {
     }
     if (!broke) {   // the whole CTA: the epilogue's TMEM loads are warp-collective
         wait_mma(y1 - 1);
+        if (kPool && a.pool_out) __syncthreads();   // the even row parked by the previous epilogue
         epilogue(y1 - 1);
     }
     if (kCout == 16 && a.head_x && !broke) {

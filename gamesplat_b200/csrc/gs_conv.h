@@ -23,6 +23,9 @@ struct ConvArgs {
     int rows_per_cta;
     uint32_t* err;              // bit 0 set if a bounded wait ran out
     int row_offset;             // the row bands of the CTAs start at -row_offset (0: at row 0)
+    // (Cin = 16, Cout = 32, forward): also the 2x2 average of the bf16 output, n x h/2 x w/2 (h, w
+    // and rows_per_cta even), summed and rounded as the denoiser's pooling kernel does
+    __nv_bfloat16* pool_out;
     // Denoised-mode head (Cout = 16, forward, head_x set): the epilogue writes head_out16 =
     // RGBA16F (head_x[5..7] + o[0..2], head_x[3] + o[3]) instead of the outputs above and,
     // per 16x16 tile of GL rows (rows_per_cta = 16 and row_offset aligning the bands with

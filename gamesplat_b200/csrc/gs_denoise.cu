@@ -1,6 +1,6 @@
 // Elementwise and reduction kernels of the stochastic-splat denoiser: input
-// features, 2x average pooling and the backward passes of pooling and
-// upsampling, the output head of training, the L1 + SSIM training loss with
+// features, the backward passes of pooling and upsampling (the 2x average
+// pooling itself is in conv1's epilogue), the output head of training, the L1 + SSIM training loss with
 // its gradient and Adam.  The convolutions are in gs_conv.cu; in the denoised
 // render mode the last convolution's epilogue writes the frame and the
 // per-tile error estimate that picks the tiles the sorted-alpha rasterizer
@@ -44,38 +44,6 @@ __global__ void features_kernel(const float4* __restrict__ sample, const float* 
         uint4* o = reinterpret_cast<uint4*>(x + (size_t)i * kInC);
         o[0] = lo;
         o[1] = hi;
-    }
-}
-
-// 2x2 average pooling, 32 channels (h, w even).
-__global__ void avgpool2_kernel(const __nv_bfloat16* __restrict__ in, int n, int h, int w,
-                                __nv_bfloat16* __restrict__ out) {
-    const int hh = h / 2, hw = w / 2;
-    const size_t total = (size_t)n * hh * hw * 4;   // 4 granules of 8 channels
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        const int g = (int)(i & 3);
-        const size_t op = i >> 2;
-        const int ox = (int)(op % hw), oy = (int)((op / hw) % hh), b = (int)(op / ((size_t)hw * hh));
-        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-            for (int dx = 0; dx < 2; ++dx) {
-                const size_t ip = ((size_t)b * h + 2 * oy + dy) * w + 2 * ox + dx;
-                const uint4 v = reinterpret_cast<const uint4*>(in + ip * kHidC)[g];
-                const __nv_bfloat162* pv = reinterpret_cast<const __nv_bfloat162*>(&v);
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const float2 f = __bfloat1622float2(pv[e]);
-                    acc[2 * e] += f.x;
-                    acc[2 * e + 1] += f.y;
-                }
-            }
-        uint4 r;
-        __nv_bfloat162* pr = reinterpret_cast<__nv_bfloat162*>(&r);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) pr[e] = __floats2bfloat162_rn(0.25f * acc[2 * e], 0.25f * acc[2 * e + 1]);
-        reinterpret_cast<uint4*>(out + op * kHidC)[g] = r;
     }
 }
 
@@ -307,10 +275,6 @@ void set_gauss_window(cudaStream_t s) {
 int launch_features(const float4* sample, const float* depth, const float4* history, int npix, __nv_bfloat16* x,
                     cudaStream_t s) {
     features_kernel<<<grid_for(npix), 256, 0, s>>>(sample, depth, history, npix, x);
-    return 1;
-}
-int launch_avgpool2(const __nv_bfloat16* in, int n, int h, int w, __nv_bfloat16* out, cudaStream_t s) {
-    avgpool2_kernel<<<grid_for((size_t)n * (h / 2) * (w / 2) * 4), 256, 0, s>>>(in, n, h, w, out);
     return 1;
 }
 int launch_upsample_grad(const __nv_bfloat16* du, const __nv_bfloat16* e3, int n, int h, int w, __nv_bfloat16* dz3,

@@ -176,6 +176,10 @@ static int conv_fwd(gs_denoiser* d, int l, bool transposed, const bf16* x, const
     a.out_f32 = out_f32;
     a.rows_per_cta = rows_per_cta(d, n, h, w);
     a.err = d->err;
+    if (l == 0 && !transposed) {   // conv1 also writes p1 = avgpool2(e1): row bands of an even number of rows
+        a.pool_out = d->p1;
+        a.rows_per_cta = (a.rows_per_cta + 1) & ~1;
+    }
     const int cin = transposed ? L.cout : L.cin, cout = transposed ? L.cin : L.cout;
     return conv::launch_fwd(cin, cout, transposed ? 0 : L.load, a, s) < 0 ? GS_ERR_BAD_ARG : GS_OK;
 }
@@ -204,8 +208,7 @@ int forward(gs_denoiser* d, const bf16* x, int n, int h, int w, cudaStream_t s) 
     if (rc) return rc;
     if (!d->images_valid) pack_images(d, s);
     const int hh = h / 2, hw = w / 2;
-    if ((rc = conv_fwd(d, 0, false, x, nullptr, n, h, w, nullptr, d->e1, nullptr, s))) return rc;
-    launch_avgpool2(d->e1, n, h, w, d->p1, s);
+    if ((rc = conv_fwd(d, 0, false, x, nullptr, n, h, w, nullptr, d->e1, nullptr, s))) return rc;   // e1 and p1
     if ((rc = conv_fwd(d, 1, false, d->p1, nullptr, n, hh, hw, nullptr, d->e2, nullptr, s))) return rc;
     if ((rc = conv_fwd(d, 2, false, d->e2, nullptr, n, hh, hw, nullptr, d->e3, nullptr, s))) return rc;
     if ((rc = conv_fwd(d, 3, false, d->e1, d->e3, n, h, w, nullptr, d->d4, nullptr, s))) return rc;
@@ -226,8 +229,7 @@ int forward_frame(gs_denoiser* d, const bf16* x, int h, int w, uint16_t* out16, 
     d->last_n = 0;
     if (!d->images_valid) pack_images(d, s);
     const int hh = h / 2, hw = w / 2;
-    if ((rc = conv_fwd(d, 0, false, x, nullptr, 1, h, w, nullptr, d->e1, nullptr, s))) return rc;
-    launch_avgpool2(d->e1, 1, h, w, d->p1, s);
+    if ((rc = conv_fwd(d, 0, false, x, nullptr, 1, h, w, nullptr, d->e1, nullptr, s))) return rc;   // e1 and p1
     if ((rc = conv_fwd(d, 1, false, d->p1, nullptr, 1, hh, hw, nullptr, d->e2, nullptr, s))) return rc;
     if ((rc = conv_fwd(d, 2, false, d->e2, nullptr, 1, hh, hw, nullptr, d->e3, nullptr, s))) return rc;
     if ((rc = conv_fwd(d, 3, false, d->e1, d->e3, 1, h, w, nullptr, d->d4, nullptr, s))) return rc;

@@ -957,7 +957,7 @@ int render_denoised(gs_ctx* c, const gs_camera* cam, uint16_t* out) {
                                    c->denoise_fallback ? c->denoise_budget : 3.0e38f, &c->fc->fallback_tiles,
                                    c->fallback_tiles, c->tile_error, c->stream);
         if (rc) return fail(c, rc, "denoiser forward failed");
-        sd.add(6);
+        sd.add(5);
     }
     if (c->denoise_fallback) {
         StageScope sc(c, ST_RASTER);
