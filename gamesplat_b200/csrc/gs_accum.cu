@@ -4,6 +4,7 @@
 // stored top row first; the kernels address texel (x, y) in GL orientation
 // at buffer row height-1-y.  Arithmetic uses unfused intrinsics in GLSL
 // operand order to match the CPU oracle bit for bit.
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include <cstring>
@@ -61,7 +62,8 @@ __device__ float4 bilinear(const float4* img, int w, int h, float u, float v) {
 
 __global__ void taa_kernel(const float4* __restrict__ cur_color, const float* __restrict__ cur_depth,
                            const float4* __restrict__ hist_color, const float4* __restrict__ hist_xyz, int w, int h,
-                           TaaUniforms U, float4* __restrict__ out_color, float4* __restrict__ out_xyz) {
+                           TaaUniforms U, float4* __restrict__ out_color, float4* __restrict__ out_xyz,
+                           __nv_bfloat16* __restrict__ features) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
@@ -115,16 +117,30 @@ __global__ void taa_kernel(const float4* __restrict__ cur_color, const float* __
         valid = hc.w > 0.0f && (U.view_changed == 0.0f || len < 100.0f);
     }
     const size_t o = (size_t)(h - 1 - y) * w + x;
+    float4 oc;
     if (valid) {
         float n = g_min(hc.w, 128.0f);
         float n1 = add(n, 1.0f);
-        out_color[o] = make_float4(dv(add(mul(hc.x, n), cc.x), n1), dv(add(mul(hc.y, n), cc.y), n1),
-                                   dv(add(mul(hc.z, n), cc.z), n1), g_min(n1, 128.0f));
+        oc = make_float4(dv(add(mul(hc.x, n), cc.x), n1), dv(add(mul(hc.y, n), cc.y), n1),
+                         dv(add(mul(hc.z, n), cc.z), n1), g_min(n1, 128.0f));
         out_xyz[o] = make_float4(dv(add(mul(hx.x, n), world[0]), n1), dv(add(mul(hx.y, n), world[1]), n1),
                                  dv(add(mul(hx.z, n), world[2]), n1), 1.0f);
     } else {
-        out_color[o] = make_float4(cc.x, cc.y, cc.z, 1.0f);
+        oc = make_float4(cc.x, cc.y, cc.z, 1.0f);
         out_xyz[o] = make_float4(world[0], world[1], world[2], 1.0f);
+    }
+    out_color[o] = oc;
+    if (features) {
+        // the denoiser's input: current RGBA, depth, the new history RGB (bf16 pairs), 8 zero channels
+        uint4 lo, hi = make_uint4(0u, 0u, 0u, 0u);
+        __nv_bfloat162* pp = reinterpret_cast<__nv_bfloat162*>(&lo);
+        pp[0] = __floats2bfloat162_rn(cc.x, cc.y);
+        pp[1] = __floats2bfloat162_rn(cc.z, cc.w);
+        pp[2] = __floats2bfloat162_rn(depth, oc.x);
+        pp[3] = __floats2bfloat162_rn(oc.y, oc.z);
+        uint4* fo = reinterpret_cast<uint4*>(features + o * 16);
+        fo[0] = lo;
+        fo[1] = hi;
     }
 }
 
@@ -145,9 +161,11 @@ int launch_to_half(const float4* src, uint16_t* dst, size_t npix, cudaStream_t s
 }
 
 int launch_taa(const float4* cur_color, const float* cur_depth, const float4* hist_color, const float4* hist_xyz,
-               int w, int h, const TaaUniforms& u, float4* out_color, float4* out_xyz, cudaStream_t s) {
+               int w, int h, const TaaUniforms& u, float4* out_color, float4* out_xyz, cudaStream_t s,
+               void* features) {
     dim3 block(16, 16), grid((w + 15) / 16, (h + 15) / 16);
-    taa_kernel<<<grid, block, 0, s>>>(cur_color, cur_depth, hist_color, hist_xyz, w, h, u, out_color, out_xyz);
+    taa_kernel<<<grid, block, 0, s>>>(cur_color, cur_depth, hist_color, hist_xyz, w, h, u, out_color, out_xyz,
+                                      static_cast<__nv_bfloat16*>(features));
     return 1;
 }
 

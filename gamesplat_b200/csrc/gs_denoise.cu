@@ -1,6 +1,7 @@
-// Elementwise and reduction kernels of the stochastic-splat denoiser: input
-// features, the backward passes of pooling and upsampling (the 2x average
-// pooling itself is in conv1's epilogue), the output head of training, the L1 + SSIM training loss with
+// Elementwise and reduction kernels of the stochastic-splat denoiser: the
+// backward passes of pooling and upsampling (the input features are written by
+// the TAA pass, the 2x average pooling by conv1's epilogue), the output head
+// of training, the L1 + SSIM training loss with
 // its gradient and Adam.  The convolutions are in gs_conv.cu; in the denoised
 // render mode the last convolution's epilogue writes the frame and the
 // per-tile error estimate that picks the tiles the sorted-alpha rasterizer
@@ -23,29 +24,6 @@ namespace gs {
 namespace dn {
 
 __device__ __forceinline__ float bf(const __nv_bfloat16& v) { return __bfloat162float(v); }
-
-// ---------------------------------------------------------------------------
-// Input features from the two-sample stochastic frame and the TAA history.
-// sample: float4 (mean RGB, alpha), depth: mean window depth, history: float4
-// (TAA colour), all top row first, width x height.
-// ---------------------------------------------------------------------------
-__global__ void features_kernel(const float4* __restrict__ sample, const float* __restrict__ depth,
-                                const float4* __restrict__ history, int npix, __nv_bfloat16* __restrict__ x) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
-        const float4 s = sample[i];
-        const float4 h = history ? history[i] : s;
-        const float d = depth[i];
-        uint4 lo, hi = make_uint4(0u, 0u, 0u, 0u);
-        __nv_bfloat162* p = reinterpret_cast<__nv_bfloat162*>(&lo);
-        p[0] = __floats2bfloat162_rn(s.x, s.y);
-        p[1] = __floats2bfloat162_rn(s.z, s.w);
-        p[2] = __floats2bfloat162_rn(d, h.x);
-        p[3] = __floats2bfloat162_rn(h.y, h.z);
-        uint4* o = reinterpret_cast<uint4*>(x + (size_t)i * kInC);
-        o[0] = lo;
-        o[1] = hi;
-    }
-}
 
 // Backward of the decoder input u = up2(e3) + e1 for its e3 term, with the
 // ReLU of e3: dz3[q] = (e3[q] > 0) * sum of du over the 2x2 block of q.
@@ -272,11 +250,6 @@ void set_gauss_window(cudaStream_t s) {
     cudaMemcpyToSymbolAsync(c_gauss, g, sizeof(g), 0, cudaMemcpyHostToDevice, s);
 }
 
-int launch_features(const float4* sample, const float* depth, const float4* history, int npix, __nv_bfloat16* x,
-                    cudaStream_t s) {
-    features_kernel<<<grid_for(npix), 256, 0, s>>>(sample, depth, history, npix, x);
-    return 1;
-}
 int launch_upsample_grad(const __nv_bfloat16* du, const __nv_bfloat16* e3, int n, int h, int w, __nv_bfloat16* dz3,
                          cudaStream_t s) {
     upsample_grad_kernel<<<grid_for((size_t)n * (h / 2) * (w / 2) * kHidC), 256, 0, s>>>(du, e3, n, h, w, dz3);

@@ -14,8 +14,6 @@ constexpr int kHidC = 32;   // hidden channels
 constexpr int kOutC = 16;   // output channels (5 used)
 
 void set_gauss_window(cudaStream_t s);
-int launch_features(const float4* sample, const float* depth, const float4* history, int npix, __nv_bfloat16* x,
-                    cudaStream_t s);
 int launch_upsample_grad(const __nv_bfloat16* du, const __nv_bfloat16* e3, int n, int h, int w, __nv_bfloat16* dz3,
                          cudaStream_t s);
 int launch_skip_pool_grad(const __nv_bfloat16* du, const __nv_bfloat16* dp1, const __nv_bfloat16* e1, int n, int h,

@@ -39,8 +39,11 @@ struct TaaUniforms {
 
 int launch_accum(const float4* sample, const float4* history, float sample_count, float4* out, size_t npix,
                  cudaStream_t s);
+// features (optional, 16 bf16 per pixel, top row first): the denoiser's input,
+// (current RGBA, depth, the new history RGB, 8 zeros), written beside the history
 int launch_taa(const float4* cur_color, const float* cur_depth, const float4* hist_color, const float4* hist_xyz,
-               int width, int height, const TaaUniforms& u, float4* out_color, float4* out_xyz, cudaStream_t s);
+               int width, int height, const TaaUniforms& u, float4* out_color, float4* out_xyz, cudaStream_t s,
+               void* features = nullptr);
 int launch_to_half(const float4* src, uint16_t* dst, size_t npix, cudaStream_t s);
 
 bool mat4_inverse(const float m[16], float out[16]);

@@ -933,12 +933,12 @@ int render_denoise_inputs(gs_ctx* c, const gs_camera* cam) {
     const uint32_t w = c->accum_write_index & 1u, rd = w ^ 1u;
     const bool has_history = c->taa_prev_valid && prev_valid;
     const gs::TaaUniforms u = taa_uniforms(cam, prev_cam, inv_view, has_history, cam_changed);
+    // the TAA pass also writes the denoiser's input features
     sa.add(gs::launch_taa(c->st.sample, c->st.depth, c->st.accum[rd], c->st.xyz[rd], c->width, c->height, u,
-                          c->st.accum[w], c->st.xyz[w], c->stream));
+                          c->st.accum[w], c->st.xyz[w], c->stream, c->features));
     c->taa_prev_valid = true;
     c->sample_count++;
     c->accum_write_index = w ^ 1u;
-    sa.add(gs::dn::launch_features(c->st.sample, c->st.depth, c->st.accum[w], (int)npix, c->features, c->stream));
     return GS_OK;
 }
 
