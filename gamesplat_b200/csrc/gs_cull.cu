@@ -468,8 +468,10 @@ __global__ void __launch_bounds__(kCullThreads, 6) cull_project_kernel(CullParam
     const uint32_t wg = blockIdx.x * kCullWarps + warp, nw = gridDim.x * kCullWarps;
     CamRegs cam;
     load_cam(p.cam, cam);
-    const bool animated = p.anim_deltas != nullptr &&
-                          (p.anim_state_a != 0 || (p.anim_weight > 0.0f && p.anim_state_b != 0));
+    // the shader blends whenever the weight is positive, states 0 and 0
+    // included (gsanim_sample returns {0, 0, w} between two linear keys of
+    // the base state), and (1 - w) x + w x need not round to x
+    const bool animated = p.anim_deltas != nullptr && (p.anim_state_a != 0 || p.anim_weight > 0.0f);
     const uint64_t stream_policy = l2_policy_evict_first();
     bool stage_failed = false;
     uint32_t phase = 0;   // parity of the next completion of the warp's barrier
@@ -755,8 +757,10 @@ __global__ void __launch_bounds__(128) recolour_kernel(CullParams p, const Raste
     const uint32_t n_vis = p.fc->visible_count;
     CamRegs cam;
     load_cam(p.cam, cam);
-    const bool animated = p.anim_deltas != nullptr &&
-                          (p.anim_state_a != 0 || (p.anim_weight > 0.0f && p.anim_state_b != 0));
+    // the shader blends whenever the weight is positive, states 0 and 0
+    // included (gsanim_sample returns {0, 0, w} between two linear keys of
+    // the base state), and (1 - w) x + w x need not round to x
+    const bool animated = p.anim_deltas != nullptr && (p.anim_state_a != 0 || p.anim_weight > 0.0f);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_vis; i += gridDim.x * blockDim.x) {
         const uint32_t id = records[i].splat_id;
         if (id >= p.n) continue;

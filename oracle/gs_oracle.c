@@ -381,7 +381,10 @@ void oc_cull_anim(const float* rows, uint32_t n, const oc_camera* cam, int sh_de
     for (int k = 0; k < 8; ++k) diag[k] = 0;
     for (uint32_t i = 0; i < n; ++i) { ids[i] = OC_SENTINEL; keys[i] = OC_SENTINEL; }
     oc_anim a = {deltas, n, scales, state_a, state_b, weight};
-    const int animated = deltas != NULL && (state_a != 0 || (weight > 0.0f && state_b != 0));
+    /* shaders/cull.glsl:155-160 blends whenever the weight is positive, also
+     * between two keys of state 0 (gsanim_sample returns {0, 0, w} there,
+     * src/gaussian_loader_gsanim.cpp:495-508): (1 - w) x + w x need not be x */
+    const int animated = deltas != NULL && (state_a != 0 || weight > 0.0f);
     float tmp[64];
     for (uint32_t i = 0; i < n; ++i) {
         const float* row = rows + (size_t)i * 64;

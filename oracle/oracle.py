@@ -1,5 +1,7 @@
-"""ctypes wrapper around the CPU oracle (liboracle.so) and the reference's own
-CPU code (_ref/libgsref.so).
+"""ctypes wrapper around the CPU oracle (liboracle.so), the reference's own
+CPU code (_ref/libgsref.so) and the reference's shader stages run on the CPU
+(_ref/libglslref.so: shaders/*.glsl translated by glsl/extract.py and run by
+glsl/harness.cpp).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py, always as the checker.  The product package
@@ -49,6 +51,7 @@ def camera_struct(cam: np.ndarray) -> OcCamera:
 
 _lib = None
 _ref = None
+_glsl = None
 
 
 def reference_dir():
@@ -183,6 +186,44 @@ def ref():
         R.ref_webp_decode.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, C.c_size_t]
         _ref = R
     return _ref
+
+
+def glsl_available() -> bool:
+    return (HERE / "_ref" / "libglslref.so").exists()
+
+
+def glsl():
+    """The reference's shader stages (shaders/cull.glsl, splat.glsl, gps.glsl,
+    accum.glsl) compiled from their own source for the CPU; entry points
+    mirror the oracle's oc_cull, oc_composite_alpha, oc_stochastic_sample,
+    oc_gps_frame, oc_accum and oc_taa."""
+    global _glsl
+    if _glsl is None:
+        path = HERE / "_ref" / "libglslref.so"
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (needs the reference sources)")
+        G = C.CDLL(str(path))
+        vp = C.c_void_p
+        G.glsl_cull.restype = None
+        G.glsl_cull.argtypes = [_f32p, C.c_uint32, _f32p, C.c_int, C.c_float, C.c_int, vp, C.c_int, C.c_int,
+                                C.c_int, C.c_float, vp, C.c_int, vp, _u32p, _u32p, _f32p, _u32p, _u32p]
+        G.glsl_composite_alpha.restype = C.c_uint64
+        G.glsl_composite_alpha.argtypes = [_u32p, C.c_uint32, _f32p, C.c_int, C.c_int, C.c_float, C.c_float,
+                                           C.c_float, C.c_float, C.c_float, C.c_float, _f32p]
+        G.glsl_stochastic_sample.restype = C.c_uint64
+        G.glsl_stochastic_sample.argtypes = [_u32p, C.c_uint32, _f32p, C.c_int, C.c_int, C.c_float, C.c_float,
+                                             C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                             _f32p, _f32p]
+        G.glsl_gps_frame.restype = None
+        G.glsl_gps_frame.argtypes = [_u32p, C.c_uint32, _f32p, C.c_int, C.c_int, C.c_int, C.c_uint32,
+                                     C.c_float, C.c_int, C.c_float, C.c_float, _f32p, _f32p, _u32p]
+        G.glsl_accum.restype = None
+        G.glsl_accum.argtypes = [_f32p, _f32p, C.c_float, C.c_int, C.c_int, _f32p]
+        G.glsl_taa.restype = None
+        G.glsl_taa.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p,
+                               _f32p, _f32p, C.c_float, C.c_float, _f32p, _f32p]
+        _glsl = G
+    return _glsl
 
 
 def ref_cull_sort_seconds(rows: np.ndarray, cam: np.ndarray):
@@ -478,3 +519,103 @@ def _vp(cam, width, height):
 def to_f16(img: np.ndarray) -> np.ndarray:
     """Round an FP32 image to RGBA16F (round-to-nearest-even), once."""
     return img.astype(np.float16)
+
+
+# --------------------------------------------------------------------------
+# the reference's shader stages on the CPU (libglslref.so), same calls and
+# outputs as the oracle helpers above
+# --------------------------------------------------------------------------
+def glsl_cull(rows: np.ndarray, cam: np.ndarray, sh_degree: int = 3, sh_lod_distance: float = 0.0,
+              collect_stats: bool = True, deltas=None, scales=None, state_a: int = 0, state_b: int = 0,
+              weight: float = 0.0, halves=None, layer_weights=None):
+    """cull_reset_cs + cull_cs; deltas: (states, N, 48) int8 with 48 scales, or
+    halves: (layers, N, 48) uint16 half bits with (layers, 3) weights."""
+    rows = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1, 64)
+    n = rows.shape[0]
+    ids = np.empty(n, np.uint32)
+    keys = np.empty(n, np.uint32)
+    proj = np.empty((n, 16), np.float32)
+    vc = np.zeros(1, np.uint32)
+    diag = np.zeros(8, np.uint32)
+    cam = np.ascontiguousarray(cam, np.float32)
+    words, states, layers, sc, lw = None, 0, 0, None, None
+    if halves is not None:
+        words = np.ascontiguousarray(halves, np.uint16).reshape(-1)
+        if words.size % 2:
+            words = np.concatenate([words, np.zeros(1, np.uint16)])
+        words = words.view(np.uint32)
+        lw = np.ascontiguousarray(layer_weights, np.float32).reshape(-1)
+        layers = int(np.asarray(halves).shape[0])
+    elif deltas is not None:
+        d = np.ascontiguousarray(deltas, np.int8).reshape(-1)
+        pad = (-d.size) % 4
+        if pad:
+            d = np.concatenate([d, np.zeros(pad, np.int8)])
+        words = d.view(np.uint32)
+        states = int(np.asarray(deltas).shape[0])
+        sc = np.ascontiguousarray(scales, np.float32).reshape(48)
+    ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+    glsl().glsl_cull(rows.reshape(-1), n, cam, int(sh_degree), float(sh_lod_distance), int(bool(collect_stats)),
+                     ptr(words), states, int(state_a), int(state_b), float(weight), ptr(sc), layers, ptr(lw),
+                     ids, keys, proj.reshape(-1), vc, diag)
+    return ids, keys, proj, int(vc[0]), diag
+
+
+def glsl_composite_alpha(sorted_ids: np.ndarray, projected: np.ndarray, width: int, height: int,
+                         cam: np.ndarray | None = None, bg: float = 0.0, jitter=(0.0, 0.0)):
+    vp_w, vp_h, ysign = _vp(cam, width, height)
+    out = np.empty((height, width, 4), np.float32)
+    sorted_ids = np.ascontiguousarray(sorted_ids, dtype=np.uint32)
+    frags = glsl().glsl_composite_alpha(sorted_ids, sorted_ids.size,
+                                        np.ascontiguousarray(projected, np.float32).reshape(-1), width, height,
+                                        vp_w, vp_h, ysign, float(bg), float(jitter[0]), float(jitter[1]),
+                                        out.reshape(-1))
+    return out, int(frags)
+
+
+def glsl_stochastic_sample(ids: np.ndarray, projected: np.ndarray, width: int, height: int, frame_seed: float,
+                           cam: np.ndarray | None = None, bg: float = 0.0, jitter=(0.0, 0.0), rgba8: bool = True):
+    vp_w, vp_h, ysign = _vp(cam, width, height)
+    out = np.empty((height, width, 4), np.float32)
+    depth = np.empty((height, width), np.float32)
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    kept = glsl().glsl_stochastic_sample(ids, ids.size, np.ascontiguousarray(projected, np.float32).reshape(-1),
+                                         width, height, vp_w, vp_h, ysign, float(bg), float(jitter[0]),
+                                         float(jitter[1]), float(frame_seed), int(bool(rgba8)), out.reshape(-1),
+                                         depth.reshape(-1))
+    return out, depth, int(kept)
+
+
+def glsl_gps_frame(ids: np.ndarray, projected: np.ndarray, width: int, height: int, supersample: int,
+                   max_work_items: int, frame_seed: float, clip_z_01: float = 0.0, linear_color: bool = False,
+                   bg: float = 0.0):
+    out = np.empty((height, width, 4), np.float32)
+    depth = np.empty((height, width), np.float32)
+    stats = np.zeros(2, np.uint32)
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    glsl().glsl_gps_frame(ids, ids.size, np.ascontiguousarray(projected, np.float32).reshape(-1), width, height,
+                          int(supersample), int(max_work_items), float(clip_z_01), int(bool(linear_color)),
+                          float(frame_seed), float(bg), out.reshape(-1), depth.reshape(-1), stats)
+    return out, depth, int(stats[0]), int(stats[1])
+
+
+def glsl_accum(sample: np.ndarray, history: np.ndarray, n: float):
+    """accum_fs over an (H, W, 4) frame."""
+    sample = np.ascontiguousarray(sample, np.float32)
+    history = np.ascontiguousarray(history, np.float32)
+    h, w = sample.shape[:2]
+    out = np.empty_like(sample)
+    glsl().glsl_accum(sample.reshape(-1), history.reshape(-1), float(n), w, h, out.reshape(-1))
+    return out
+
+
+def glsl_taa(cur_color, cur_depth, hist_color, hist_xyz, inv_view, prev_view, viewport_ortho, focal_clip,
+             prev_focal_clip, proj_z, history_valid: float, view_changed: float):
+    h, w = cur_depth.shape
+    oc = np.empty((h, w, 4), np.float32)
+    ox = np.empty((h, w, 4), np.float32)
+    f = lambda a: np.ascontiguousarray(a, np.float32).reshape(-1)  # noqa: E731
+    glsl().glsl_taa(f(cur_color), f(cur_depth), f(hist_color), f(hist_xyz), w, h, f(inv_view), f(prev_view),
+                    f(viewport_ortho), f(focal_clip), f(prev_focal_clip), f(proj_z), float(history_valid),
+                    float(view_changed), oc.reshape(-1), ox.reshape(-1))
+    return oc, ox

@@ -27,7 +27,9 @@ def anim():
     return rows, deltas, scales
 
 
-@pytest.mark.parametrize("state", [(0, 0, 0.0), (2, 0, 0.0), (1, 3, 0.375)])
+# (0, 0, 0.3): between two linear keys of the base state the shader still
+# blends the row with itself, (1 - w) x + w x, which need not round to x
+@pytest.mark.parametrize("state", [(0, 0, 0.0), (2, 0, 0.0), (1, 3, 0.375), (0, 0, 0.3), (2, 2, 0.7)])
 def test_anim_records_and_image(anim, state):
     rows, deltas, scales = anim
     cam = small_cam(W, H)
