@@ -11,7 +11,8 @@ never committed.  Nothing is changed in what the stage computes:
     blocks a pointer per unsized array (`T name[];` -> `T* name`), opaque
     uniforms (texture2D, sampler) plain variables;
   - stage inputs and outputs (`in`/`out`, `flat`) become variables the
-    harness sets and reads;
+    harness sets and reads; `shared` variables plain variables (the harness
+    runs one workgroup at a time);
   - GLSL array constructors `T[n](a, b, ...)` become brace initialisers;
   - float literals get an `f` suffix (GLSL literals are single precision,
     C++ ones double);
@@ -86,6 +87,7 @@ def translate(lines: list[str]) -> str:
                     line = f"{m.group(1)}{m.group(2)}* {m.group(3)} = nullptr;"
             out.append(line)
             continue
+        line = re.sub(r"^(\s*)shared\s+", r"\1", line)
         m = _OPAQUE.match(line)
         if m:
             line = f"{m.group(1)} {m.group(2)};"

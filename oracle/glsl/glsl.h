@@ -388,6 +388,7 @@ inline float uintBitsToFloat(uint u) {
     std::memcpy(&f, &u, 4);
     return f;
 }
+inline int bitCount(uint v) { return __builtin_popcount(v); }
 inline vec2 unpackHalf2x16(uint v) {
     return vec2(oc_half_to_float((uint16_t)(v & 0xFFFFu)), oc_half_to_float((uint16_t)(v >> 16)));
 }

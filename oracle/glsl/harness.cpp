@@ -1,5 +1,5 @@
-// Runs the reference's own shader stages (shaders/cull.glsl, splat.glsl,
-// gps.glsl, accum.glsl), translated to C++ by extract.py and compiled against
+// Runs the reference's own shader stages (shaders/cull.glsl, sort.glsl,
+// splat.glsl, gps.glsl, accum.glsl), translated to C++ by extract.py and compiled against
 // glsl.h, over whole frames on the CPU.
 //
 // TEST INFRASTRUCTURE ONLY: built into oracle/_ref/libglslref.so from the
@@ -7,7 +7,8 @@
 // (gs_oracle.c), and through the oracle with the CUDA path.
 //
 // Each entry point mirrors the oracle function of the same name (oc_cull,
-// oc_composite_alpha, oc_stochastic_sample, oc_gps_frame, oc_accum, oc_taa):
+// oc_sort_pairs, oc_composite_alpha, oc_stochastic_sample, oc_gps_frame,
+// oc_accum, oc_taa):
 // same arguments, same output layout.  Only the fixed-function steps between
 // the stages are written here, as the oracle defines them: the quad's
 // rasterization (viewport transform, 1/256-pixel snap, pixel centres at
@@ -17,11 +18,87 @@
 // varyings that are constant over a primitive passed through unchanged.
 #include "glsl.h"
 
+#include <ucontext.h>
+
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+
+// Workgroups of compute stages with barrier(): each of the 256 invocations
+// is a fiber (ucontext) on its own stack; the scheduler resumes them in
+// invocation order, each running to its next barrier() or its end, until all
+// have ended.  One phase thus completes for every invocation before any
+// starts the next, as barrier() requires, with no concurrency (atomics on
+// shared variables are plain read-modify-writes).
+namespace wg {
+constexpr int kLocal = 256;
+constexpr size_t kStack = 64 * 1024;
+struct Fiber {
+    ucontext_t ctx;
+    bool done;
+};
+ucontext_t sched;
+Fiber fibers[kLocal];
+std::vector<char> stacks;
+int cur = 0;
+void (*entry)() = nullptr;
+
+void trampoline() {
+    entry();
+    fibers[cur].done = true;   // returns to uc_link: the scheduler
+}
+inline void barrier() { swapcontext(&fibers[cur].ctx, &sched); }
+
+// Runs one workgroup of main_fn; set_ids(i) sets the stage's built-in ids
+// for invocation i before each resume.
+template <typename SetIds> void run(void (*main_fn)(), SetIds set_ids) {
+    if (stacks.empty()) stacks.resize((size_t)kLocal * kStack);
+    entry = main_fn;
+    for (int i = 0; i < kLocal; ++i) {
+        getcontext(&fibers[i].ctx);
+        fibers[i].ctx.uc_stack.ss_sp = stacks.data() + (size_t)i * kStack;
+        fibers[i].ctx.uc_stack.ss_size = kStack;
+        fibers[i].ctx.uc_link = &sched;
+        makecontext(&fibers[i].ctx, trampoline, 0);
+        fibers[i].done = false;
+    }
+    for (bool live = true; live;) {
+        live = false;
+        for (int i = 0; i < kLocal; ++i) {
+            if (fibers[i].done) continue;
+            cur = i;
+            set_ids(i);
+            swapcontext(&sched, &fibers[i].ctx);
+            live = true;
+        }
+    }
+}
+}  // namespace wg
+
+#define GLSL_WORKGROUP_BUILTINS                             \
+    uvec3 gl_GlobalInvocationID, gl_LocalInvocationID, gl_WorkGroupID; \
+    inline void barrier() { wg::barrier(); }                \
+    inline void memoryBarrierShared() {}
+
+namespace st_radix_hist {
+using namespace glsl;
+GLSL_WORKGROUP_BUILTINS
+#include "radix_hist_cs.inc"
+}  // namespace st_radix_hist
+
+namespace st_radix_prefix {
+using namespace glsl;
+GLSL_WORKGROUP_BUILTINS
+#include "radix_prefix_cs.inc"
+}  // namespace st_radix_prefix
+
+namespace st_radix_scatter {
+using namespace glsl;
+GLSL_WORKGROUP_BUILTINS
+#include "radix_scatter_cs.inc"
+}  // namespace st_radix_scatter
 
 namespace st_cull_reset {
 using namespace glsl;
@@ -525,6 +602,58 @@ void glsl_taa(const float* cur_color, const float* cur_depth, const float* hist_
     }
     flip_rows(oc.data(), out_color, width, height, 4);
     flip_rows(ox.data(), out_xyz, width, height, 4);
+}
+
+// radix_hist_cs, radix_prefix_cs and radix_scatter_cs for the four 8-bit
+// passes of the reference's sort driver (src/renderer.cpp:1873-1962): every
+// pass over all n entries, ceil(n / 256) workgroups, ping-pong buffers.
+void glsl_sort_pairs(const uint32_t* keys_in, const uint32_t* ids_in, uint32_t n, uint32_t* keys_out,
+                     uint32_t* ids_out) {
+    namespace RH = st_radix_hist;
+    namespace RP = st_radix_prefix;
+    namespace RS = st_radix_scatter;
+    std::vector<uint32_t> keys[2] = {std::vector<uint32_t>(keys_in, keys_in + n), std::vector<uint32_t>(n)};
+    std::vector<uint32_t> ids[2] = {std::vector<uint32_t>(ids_in, ids_in + n), std::vector<uint32_t>(n)};
+    if (n > 1) {   // renderer_sort_gaussians_gpu returns for a capacity of 0 or 1
+        const uint32_t groups = (n + 255u) / 256u;
+        std::vector<uint32_t> hist((size_t)groups * 256u);
+        for (uint32_t pass = 0; pass < 4u; ++pass) {
+            const int shift = (int)(pass * 8u);
+            const uint32_t src = pass & 1u, dst = src ^ 1u;
+            RH::sort_count = (int)n;
+            RH::shift = shift;
+            RH::hist_keys = reinterpret_cast<RH::RadixUIntData*>(keys[src].data());
+            RH::histograms = reinterpret_cast<RH::RadixUIntData*>(hist.data());
+            for (uint32_t g = 0; g < groups; ++g)
+                wg::run(RH::stage_main, [&](int i) {
+                    RH::gl_LocalInvocationID = glsl::uvec3((uint32_t)i, 0u, 0u);
+                    RH::gl_GlobalInvocationID = glsl::uvec3(g * 256u + (uint32_t)i, 0u, 0u);
+                    RH::gl_WorkGroupID = glsl::uvec3(g, 0u, 0u);
+                });
+            RP::group_count = (int)groups;
+            RP::histograms = reinterpret_cast<RP::RadixPrefixUIntData*>(hist.data());
+            wg::run(RP::stage_main, [&](int i) {
+                RP::gl_LocalInvocationID = glsl::uvec3((uint32_t)i, 0u, 0u);
+                RP::gl_GlobalInvocationID = glsl::uvec3((uint32_t)i, 0u, 0u);
+                RP::gl_WorkGroupID = glsl::uvec3(0u, 0u, 0u);
+            });
+            RS::sort_count = (int)n;
+            RS::shift = shift;
+            RS::keys_in = reinterpret_cast<RS::RadixScatterUIntData*>(keys[src].data());
+            RS::keys_out = reinterpret_cast<RS::RadixScatterUIntData*>(keys[dst].data());
+            RS::ids_in = reinterpret_cast<RS::RadixScatterUIntData*>(ids[src].data());
+            RS::ids_out = reinterpret_cast<RS::RadixScatterUIntData*>(ids[dst].data());
+            RS::histograms = reinterpret_cast<RS::RadixScatterUIntData*>(hist.data());
+            for (uint32_t g = 0; g < groups; ++g)
+                wg::run(RS::stage_main, [&](int i) {
+                    RS::gl_LocalInvocationID = glsl::uvec3((uint32_t)i, 0u, 0u);
+                    RS::gl_GlobalInvocationID = glsl::uvec3(g * 256u + (uint32_t)i, 0u, 0u);
+                    RS::gl_WorkGroupID = glsl::uvec3(g, 0u, 0u);
+                });
+        }
+    }
+    std::memcpy(keys_out, keys[0].data(), (size_t)n * 4);
+    std::memcpy(ids_out, ids[0].data(), (size_t)n * 4);
 }
 
 }  // extern "C"

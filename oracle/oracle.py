@@ -193,10 +193,10 @@ def glsl_available() -> bool:
 
 
 def glsl():
-    """The reference's shader stages (shaders/cull.glsl, splat.glsl, gps.glsl,
-    accum.glsl) compiled from their own source for the CPU; entry points
-    mirror the oracle's oc_cull, oc_composite_alpha, oc_stochastic_sample,
-    oc_gps_frame, oc_accum and oc_taa."""
+    """The reference's shader stages (shaders/cull.glsl, sort.glsl, splat.glsl,
+    gps.glsl, accum.glsl) compiled from their own source for the CPU; entry
+    points mirror the oracle's oc_cull, oc_sort_pairs, oc_composite_alpha,
+    oc_stochastic_sample, oc_gps_frame, oc_accum and oc_taa."""
     global _glsl
     if _glsl is None:
         path = HERE / "_ref" / "libglslref.so"
@@ -207,6 +207,8 @@ def glsl():
         G.glsl_cull.restype = None
         G.glsl_cull.argtypes = [_f32p, C.c_uint32, _f32p, C.c_int, C.c_float, C.c_int, vp, C.c_int, C.c_int,
                                 C.c_int, C.c_float, vp, C.c_int, vp, _u32p, _u32p, _f32p, _u32p, _u32p]
+        G.glsl_sort_pairs.restype = None
+        G.glsl_sort_pairs.argtypes = [_u32p, _u32p, C.c_uint32, _u32p, _u32p]
         G.glsl_composite_alpha.restype = C.c_uint64
         G.glsl_composite_alpha.argtypes = [_u32p, C.c_uint32, _f32p, C.c_int, C.c_int, C.c_float, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_float, _f32p]
@@ -559,6 +561,16 @@ def glsl_cull(rows: np.ndarray, cam: np.ndarray, sh_degree: int = 3, sh_lod_dist
                      ptr(words), states, int(state_a), int(state_b), float(weight), ptr(sc), layers, ptr(lw),
                      ids, keys, proj.reshape(-1), vc, diag)
     return ids, keys, proj, int(vc[0]), diag
+
+
+def glsl_sort_pairs(keys: np.ndarray, ids: np.ndarray):
+    """radix_hist_cs, radix_prefix_cs and radix_scatter_cs over four 8-bit passes."""
+    keys = np.ascontiguousarray(keys, dtype=np.uint32)
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    ko = np.empty_like(keys)
+    io = np.empty_like(ids)
+    glsl().glsl_sort_pairs(keys, ids, keys.size, ko, io)
+    return ko, io
 
 
 def glsl_composite_alpha(sorted_ids: np.ndarray, projected: np.ndarray, width: int, height: int,

@@ -1,5 +1,5 @@
 """Generate tests/golden/shader_small.npz from the reference's own shader
-stages (shaders/cull.glsl, splat.glsl, gps.glsl), compiled from their source
+stages (shaders/cull.glsl, sort.glsl, splat.glsl, gps.glsl), compiled from their source
 for the CPU by oracle/Makefile into oracle/_ref/libglslref.so.
 
 Run in a checkout that has the reference sources:
@@ -22,6 +22,11 @@ inside the scene, which culls about half of it):
   gps_k, zgps_k, gpsw_k : gps_clear/expand/splat/resolve, supersample 2,
              frame seed 1, 16M work items; RGBA8 values (uint8), depth
              (float32), requested work items
+  sort_in_t, sort_out_t : radix_hist_cs / radix_prefix_cs / radix_scatter_cs
+             over the four 8-bit passes of the reference's driver; (key, id)
+             pairs in and out (2 x n uint32) for t = cull (camera 3's keys and
+             ids, invisible rows' sentinels included) and t = ties (5000 keys
+             of 40 values with every byte varying, ids in index order)
   anim_ids, anim_proj_s : cull_cs with int8 deltas (`scene.anim_deltas(5, N,
              3)`, scales anim_scales) for camera 0 and the (state a, state b,
              weight) of anim_states[s]
@@ -79,6 +84,12 @@ def main() -> None:
         out[f"gps_{k}"] = np.rint(g * 255.0).astype(np.uint8)
         out[f"zgps_{k}"] = gz
         out[f"gpsw_{k}"] = np.uint32(requested)
+    ids, keys, _, _, _ = O.glsl_cull(rows, cams[3])
+    ties = np.random.default_rng(12).integers(0, 40, 5000).astype(np.uint32) * np.uint32(0x01010101)
+    for name, k, i in (("cull", keys, ids), ("ties", ties, np.arange(ties.size, dtype=np.uint32))):
+        ko, io = O.glsl_sort_pairs(k, i)
+        out[f"sort_in_{name}"] = np.stack([k, i])
+        out[f"sort_out_{name}"] = np.stack([ko, io])
     deltas = scene.anim_deltas(5, N, 3)
     scales = np.linspace(0.002, 0.02, 48, dtype=np.float32)
     out["anim_scales"] = scales

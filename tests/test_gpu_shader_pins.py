@@ -1,9 +1,9 @@
 """GPU parity against the reference's own shader stages: the CUDA path,
 through the C ABI, compared with tests/golden/shader_small.npz, the outputs of
-shaders/cull.glsl, splat.glsl and gps.glsl compiled from their source for the
+shaders/cull.glsl, sort.glsl, splat.glsl and gps.glsl compiled from their source for the
 CPU (tests/golden/make_shader_golden.py).
 
-Projected records, the stochastic sample (colour and D24 depth), GPS work
+Projected records, the sort permutation (gs_sort_pairs), the stochastic sample (colour and D24 depth), GPS work
 counts and depth, and the gsanim delta decode are compared bit for bit; the
 alpha frame within the RGBA16F gate (the CUDA compositor evaluates exp with
 the ex2 unit and blends front to back); GPS colours where two splats share a
@@ -18,6 +18,7 @@ import numpy as np
 import pytest
 
 from gamesplat_b200 import Renderer, _lib as L
+from gamesplat_b200 import renderer as RR
 from gamesplat_b200 import scene
 
 from helpers import image_gate
@@ -96,3 +97,21 @@ def test_gsanim_deltas_match_shaders(fx):
             r.draw_frame(fx["cams"][0])
             got = r.debug_read(L.GS_DEBUG_PROJECTED, n * 16, np.float32, (n, 16))
             assert np.array_equal(got[vis].view(np.uint32), fx[f"anim_proj_{s}"][vis].view(np.uint32)), (a, b, w)
+
+
+@pytest.mark.parametrize("case", ["cull", "ties"])
+def test_sort_pairs_matches_shaders(fx, case):
+    import torch
+
+    k, i = fx[f"sort_in_{case}"]
+    n = k.size
+    dk = torch.from_numpy(k.view(np.int32)).cuda()
+    dv = torch.from_numpy(i.view(np.int32)).cuda()
+    ok, ov = torch.empty_like(dk), torch.empty_like(dv)
+    nbytes = RR.sort_pairs_scratch_bytes(n)
+    scratch = torch.empty(max(nbytes, 1), dtype=torch.uint8, device="cuda")
+    RR.sort_pairs(dk.data_ptr(), dv.data_ptr(), ok.data_ptr(), ov.data_ptr(), n, scratch.data_ptr(), nbytes, 0, 32,
+                  torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    got = np.stack([ok.cpu().numpy().view(np.uint32), ov.cpu().numpy().view(np.uint32)])
+    assert np.array_equal(got, fx[f"sort_out_{case}"])

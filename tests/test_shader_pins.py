@@ -1,5 +1,5 @@
 """CPU tests: pin the oracle against the reference's own shader stages
-(shaders/cull.glsl, splat.glsl, gps.glsl, accum.glsl), compiled from their
+(shaders/cull.glsl, sort.glsl, splat.glsl, gps.glsl, accum.glsl), compiled from their
 source for the CPU into oracle/_ref/libglslref.so (oracle/Makefile, with
 oracle/glsl/extract.py and oracle/glsl/harness.cpp), through the committed
 fixture tests/golden/shader_small.npz (tests/golden/make_shader_golden.py)
@@ -80,6 +80,13 @@ def test_oracle_frames_match_shader_fixture(fx, k):
     _gps_colour_ties(g, fx[f"gps_{k}"].astype(np.float32) / 255.0, limit=W * H // 500)
 
 
+@pytest.mark.parametrize("case", ["cull", "ties"])
+def test_oracle_sort_matches_shader_fixture(fx, case):
+    k, i = fx[f"sort_in_{case}"]
+    ko, io = O.sort_pairs(k, i)
+    assert np.array_equal(np.stack([ko, io]), fx[f"sort_out_{case}"])
+
+
 def test_oracle_anim_matches_shader_fixture(fx):
     deltas = scene.anim_deltas(5, fx["rows"].shape[0], 3)
     for s, (a, b, w) in enumerate(fx["anim_states"]):
@@ -129,6 +136,29 @@ def test_cull_sweep_matches_shader():
             assert _same_cull(a, b), (seed, deg, lod, cam[32:40])
             visible += a[3]
     assert visible > 100_000
+
+
+@live
+def test_sort_matches_shader():
+    """The radix sort shaders (four 8-bit passes of hist / prefix / scatter,
+    workgroups run with their barriers) against the oracle's sort: the same
+    permutation, ties in index order, for partial, single and many
+    workgroups, tie-heavy keys, random keys and a cull's output."""
+    rng = np.random.default_rng(17)
+    for n in (1, 2, 255, 256, 257, 4099, 70_001):
+        k = rng.integers(0, 40, n).astype(np.uint32) * np.uint32(0x01010101)
+        i = np.arange(n, dtype=np.uint32)
+        a, b = O.sort_pairs(k, i), O.glsl_sort_pairs(k, i)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), n
+    k = rng.integers(0, 2 ** 32, 30_000, dtype=np.uint64).astype(np.uint32)
+    i = rng.permutation(30_000).astype(np.uint32)
+    a, b = O.sort_pairs(k, i), O.glsl_sort_pairs(k, i)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    rows = R.pack_raw(scene.small_scene(4, 20_000))
+    ids, keys, _, vc, _ = O.cull(rows, R.camera_uniforms((0.0, 0.0, 0.3), 3.0, -0.1, 320, 180, fov_y=1.9))
+    assert 0 < vc < 20_000
+    a, b = O.sort_pairs(keys, ids), O.glsl_sort_pairs(keys, ids)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
 @live
