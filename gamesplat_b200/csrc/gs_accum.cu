@@ -7,6 +7,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <cmath>
 #include <cstring>
 
 #include "gs_common.cuh"
@@ -201,48 +202,38 @@ void release_stochastic_targets(StochasticTargets& t) {
     t = StochasticTargets{};
 }
 
-// General 4x4 inverse by cofactor expansion along 2x2 minors (column-major);
-// false when the matrix is singular.  Used for the TAA inverse view matrix
-// (src/renderer.cpp:2322-2328).
 bool mat4_inverse(const float m[16], float out[16]) {
-    // m[c*4 + r]; work with a[r][c]
-    float a[4][4];
-    for (int c = 0; c < 4; ++c)
-        for (int r = 0; r < 4; ++r) a[r][c] = m[c * 4 + r];
-    float s0 = a[0][0] * a[1][1] - a[1][0] * a[0][1];
-    float s1 = a[0][0] * a[1][2] - a[1][0] * a[0][2];
-    float s2 = a[0][0] * a[1][3] - a[1][0] * a[0][3];
-    float s3 = a[0][1] * a[1][2] - a[1][1] * a[0][2];
-    float s4 = a[0][1] * a[1][3] - a[1][1] * a[0][3];
-    float s5 = a[0][2] * a[1][3] - a[1][2] * a[0][3];
-    float c5 = a[2][2] * a[3][3] - a[3][2] * a[2][3];
-    float c4 = a[2][1] * a[3][3] - a[3][1] * a[2][3];
-    float c3 = a[2][1] * a[3][2] - a[3][1] * a[2][2];
-    float c2 = a[2][0] * a[3][3] - a[3][0] * a[2][3];
-    float c1 = a[2][0] * a[3][2] - a[3][0] * a[2][2];
-    float c0 = a[2][0] * a[3][1] - a[3][0] * a[2][1];
-    float det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
-    if (det == 0.0f || !(det == det)) return false;
-    float id = 1.0f / det;
-    float b[4][4];
-    b[0][0] = (a[1][1] * c5 - a[1][2] * c4 + a[1][3] * c3) * id;
-    b[0][1] = (-a[0][1] * c5 + a[0][2] * c4 - a[0][3] * c3) * id;
-    b[0][2] = (a[3][1] * s5 - a[3][2] * s4 + a[3][3] * s3) * id;
-    b[0][3] = (-a[2][1] * s5 + a[2][2] * s4 - a[2][3] * s3) * id;
-    b[1][0] = (-a[1][0] * c5 + a[1][2] * c2 - a[1][3] * c1) * id;
-    b[1][1] = (a[0][0] * c5 - a[0][2] * c2 + a[0][3] * c1) * id;
-    b[1][2] = (-a[3][0] * s5 + a[3][2] * s2 - a[3][3] * s1) * id;
-    b[1][3] = (a[2][0] * s5 - a[2][2] * s2 + a[2][3] * s1) * id;
-    b[2][0] = (a[1][0] * c4 - a[1][1] * c2 + a[1][3] * c0) * id;
-    b[2][1] = (-a[0][0] * c4 + a[0][1] * c2 - a[0][3] * c0) * id;
-    b[2][2] = (a[3][0] * s4 - a[3][1] * s2 + a[3][3] * s0) * id;
-    b[2][3] = (-a[2][0] * s4 + a[2][1] * s2 - a[2][3] * s0) * id;
-    b[3][0] = (-a[1][0] * c3 + a[1][1] * c1 - a[1][2] * c0) * id;
-    b[3][1] = (a[0][0] * c3 - a[0][1] * c1 + a[0][2] * c0) * id;
-    b[3][2] = (-a[3][0] * s3 + a[3][1] * s1 - a[3][2] * s0) * id;
-    b[3][3] = (a[2][0] * s3 - a[2][1] * s1 + a[2][2] * s0) * id;
-    for (int c = 0; c < 4; ++c)
-        for (int r = 0; r < 4; ++r) out[c * 4 + r] = b[r][c];
+    // The reference's inverse (src/renderer.cpp:86-206, used for the TAA's
+    // inv_view at :2324): the adjugate by cofactor expansion, with the same
+    // products in the same order so the uniforms match bit for bit.  Entry
+    // k = 4c + r (m is column-major, m[4 * col + row]) is (-1)^(c+r) times the
+    // 3x3 determinant over rows R != c and columns Q != r, summed as six
+    // triple products m[a][R0] * m[b][Rx] * m[d][Ry] left to right: a runs
+    // over Q in order (signs +, -, + per a), b < d are the other two columns,
+    // (Rx, Ry) = (R1, R2) then (R2, R1) with the opposite sign.
+    float inv[16];
+    for (int k = 0; k < 16; ++k) {
+        const int c = k >> 2, r = k & 3;
+        int R[3], Q[3];
+        for (int i = 0, n = 0; i < 4; ++i)
+            if (i != c) R[n++] = i;
+        for (int i = 0, n = 0; i < 4; ++i)
+            if (i != r) Q[n++] = i;
+        const bool flip = ((c + r) & 1) != 0;
+        float acc = 0.0f;
+        for (int t = 0; t < 6; ++t) {
+            const int ai = t >> 1, sw = t & 1;
+            const int a = Q[ai], b = Q[ai == 0 ? 1 : 0], d = Q[ai == 2 ? 1 : 2];
+            const float p = (m[a * 4 + R[0]] * m[b * 4 + (sw ? R[2] : R[1])]) * m[d * 4 + (sw ? R[1] : R[2])];
+            const bool minus = ((ai == 1) != (sw == 1)) != flip;
+            acc = t == 0 ? (minus ? -p : p) : (minus ? acc - p : acc + p);
+        }
+        inv[k] = acc;
+    }
+    float det = ((m[0] * inv[0] + m[1] * inv[4]) + m[2] * inv[8]) + m[3] * inv[12];
+    if (std::fabs(det) <= 1.0e-8f) return false;
+    det = 1.0f / det;
+    for (int i = 0; i < 16; ++i) out[i] = inv[i] * det;
     return true;
 }
 

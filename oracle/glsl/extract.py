@@ -19,7 +19,12 @@ never committed.  Nothing is changed in what the stage computes:
   - `uint(x)` and `int(x)` become the saturating conversions u32_of / i32_of;
   - `discard;` sets gl_discarded and returns; `main` is renamed stage_main.
 
+A second mode cuts one C function out of a reference source file unchanged
+(from its signature line to the brace that closes its body), for functions
+the harness runs that live in files too entangled to compile whole:
+
 Usage: python extract.py SHADER.glsl STAGE OUT.inc
+       python extract.py --function SOURCE.cpp NAME OUT.inc
 """
 from __future__ import annotations
 
@@ -105,9 +110,30 @@ def translate(lines: list[str]) -> str:
     return src
 
 
+def c_function(text: str, name: str) -> str:
+    m = re.search(r"^[^\n;{}]*\b" + re.escape(name) + r"\s*\([^)]*\)\s*\{", text, re.M)
+    if not m:
+        raise ValueError(f"function {name} not found")
+    depth, j = 1, m.end()
+    while depth:
+        c = text[j]
+        depth += (c == "{") - (c == "}")
+        j += 1
+    return text[m.start():j] + "\n"
+
+
 def main(argv: list[str]) -> int:
+    if len(argv) == 5 and argv[1] == "--function":
+        path, name, dst = argv[2:]
+        with open(path, encoding="utf-8") as f:
+            body = c_function(f.read(), name)
+        with open(dst, "w", encoding="utf-8") as f:
+            f.write(f"// Cut by oracle/glsl/extract.py from the reference's {path.split('/')[-1]}, "
+                    f"function {name}.  Do not edit.\n")
+            f.write(body)
+        return 0
     if len(argv) != 4:
-        print(__doc__.strip().splitlines()[-1], file=sys.stderr)
+        print(__doc__.strip().splitlines()[-2:], file=sys.stderr)
         return 2
     path, stage, dst = argv[1:]
     with open(path, encoding="utf-8") as f:

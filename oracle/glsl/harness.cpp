@@ -176,6 +176,12 @@ bool gl_discarded;
 #include "taa_accum_fs.inc"
 }  // namespace st_taa
 
+// The reference's mat4_inverse (src/renderer.cpp:86-206), cut from its
+// source unchanged.
+namespace ref_renderer {
+#include "mat4_inverse.inc"
+}  // namespace ref_renderer
+
 namespace {
 
 using glsl::mat4;
@@ -289,6 +295,8 @@ void flip_rows(const float* src, float* dst, int width, int height, int ch) {
 }  // namespace
 
 extern "C" {
+
+int ref_mat4_inverse(const float* m, float* out) { return ref_renderer::mat4_inverse(m, out) ? 1 : 0; }
 
 // cull_reset_cs then cull_cs over n rows (shaders/cull.glsl:3-476).  cam is
 // the 40-float CameraUniforms block (view, proj, viewport, orthographic,

@@ -891,6 +891,39 @@ void oc_taa(const float* cur_color, const float* cur_depth, const float* hist_co
     }
 }
 
+/* The TAA's inverse view matrix as the reference computes it
+ * (src/renderer.cpp:86-206): the adjugate by cofactor expansion divided by
+ * the determinant, returning 0 when |det| <= 1e-8.  Entry k = 4c + r of the
+ * column-major result is (-1)^(c+r) times the 3x3 determinant over rows != c
+ * and columns != r of m, summed as six triple products left to right: the
+ * first factor's column a runs over the remaining columns in order at the
+ * first remaining row, the other two columns take the other two rows in
+ * order, then swapped (sign pattern + - - + + -). */
+int oc_mat4_inverse(const float* m, float* out) {
+    float inv[16];
+    for (int k = 0; k < 16; ++k) {
+        int c = k >> 2, r = k & 3, R[3], Q[3], n = 0;
+        for (int i = 0; i < 4; ++i) if (i != c) R[n++] = i;
+        n = 0;
+        for (int i = 0; i < 4; ++i) if (i != r) Q[n++] = i;
+        int flip = (c + r) & 1;
+        float acc = 0.0f;
+        for (int t = 0; t < 6; ++t) {
+            int ai = t >> 1, sw = t & 1;
+            int a = Q[ai], b = Q[ai == 0 ? 1 : 0], d = Q[ai == 2 ? 1 : 2];
+            float p = (m[a * 4 + R[0]] * m[b * 4 + (sw ? R[2] : R[1])]) * m[d * 4 + (sw ? R[1] : R[2])];
+            int minus = ((ai == 1) ^ sw) ^ flip;
+            acc = t == 0 ? (minus ? -p : p) : (minus ? acc - p : acc + p);
+        }
+        inv[k] = acc;
+    }
+    float det = ((m[0] * inv[0] + m[1] * inv[4]) + m[2] * inv[8]) + m[3] * inv[12];
+    if (fabsf(det) <= 1.0e-8f) return 0;
+    det = 1.0f / det;
+    for (int i = 0; i < 16; ++i) out[i] = inv[i] * det;
+    return 1;
+}
+
 float oc_halton(uint32_t index, uint32_t base) {              /* src/renderer.cpp:246-255 */
     float f = 1.0f, r = 0.0f;
     while (index > 0) {

@@ -142,6 +142,7 @@ void oc_display(const uint16_t* in_half, int width, int height, const uint16_t* 
 float oc_half_to_float(uint16_t h);
 
 /* Halton radical inverse (src/renderer.cpp:246-255). */
+int oc_mat4_inverse(const float* m, float* out);  /* src/renderer.cpp:86-206 */
 float oc_halton(uint32_t index, uint32_t base);
 
 #ifdef __cplusplus

@@ -119,6 +119,8 @@ def lib():
         L.oc_taa.restype = None
         L.oc_taa.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p,
                              _f32p, _f32p, C.c_float, C.c_float, _f32p, _f32p]
+        L.oc_mat4_inverse.restype = C.c_int
+        L.oc_mat4_inverse.argtypes = [_f32p, _f32p]
         L.oc_halton.restype = C.c_float
         L.oc_halton.argtypes = [C.c_uint32, C.c_uint32]
         L.oc_display.restype = None
@@ -207,6 +209,8 @@ def glsl():
         G.glsl_cull.restype = None
         G.glsl_cull.argtypes = [_f32p, C.c_uint32, _f32p, C.c_int, C.c_float, C.c_int, vp, C.c_int, C.c_int,
                                 C.c_int, C.c_float, vp, C.c_int, vp, _u32p, _u32p, _f32p, _u32p, _u32p]
+        G.ref_mat4_inverse.restype = C.c_int
+        G.ref_mat4_inverse.argtypes = [_f32p, _f32p]
         G.glsl_sort_pairs.restype = None
         G.glsl_sort_pairs.argtypes = [_u32p, _u32p, C.c_uint32, _u32p, _u32p]
         G.glsl_composite_alpha.restype = C.c_uint64
@@ -501,6 +505,24 @@ def taa(cur_color, cur_depth, hist_color, hist_xyz, inv_view, prev_view, viewpor
                  f(viewport_ortho), f(focal_clip), f(prev_focal_clip), f(proj_z), float(history_valid),
                  float(view_changed), oc.reshape(-1), ox.reshape(-1))
     return oc, ox
+
+
+def mat4_inverse(m: np.ndarray):
+    """(ok, inverse) of a column-major 4x4 float32 matrix, as the reference's
+    TAA computes its inverse view (src/renderer.cpp:86-206)."""
+    m = np.ascontiguousarray(m, np.float32).reshape(16)
+    out = np.zeros(16, np.float32)
+    ok = lib().oc_mat4_inverse(m, out)
+    return bool(ok), out
+
+
+def ref_mat4_inverse(m: np.ndarray):
+    """The reference's own mat4_inverse (cut from src/renderer.cpp at build
+    time into oracle/_ref/libglslref.so): (ok, inverse)."""
+    m = np.ascontiguousarray(m, np.float32).reshape(16)
+    out = np.zeros(16, np.float32)
+    ok = glsl().ref_mat4_inverse(m, out)
+    return bool(ok), out
 
 
 def quad_rect(projected16: np.ndarray, width: int, height: int, cam=None, jitter=(0.0, 0.0)):

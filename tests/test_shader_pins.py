@@ -226,6 +226,26 @@ def test_gps_frames_match_shader(ss):
 
 
 @live
+def test_mat4_inverse_matches_reference():
+    """The TAA's inverse view: the oracle's cofactor inverse against the
+    reference's own mat4_inverse (cut from src/renderer.cpp at build time) on
+    view and projection matrices of fly cameras and on scaled general
+    matrices: same refusals, same bits."""
+    rng = np.random.default_rng(21)
+    for k in range(1500):
+        if k % 3 == 0:
+            m = rng.normal(size=16).astype(np.float32) * np.float32(10.0 ** rng.uniform(-3, 3))
+        else:
+            cam = R.camera_uniforms(rng.uniform(-50, 50, 3), rng.uniform(-7, 7), rng.uniform(-1.5, 1.5), 64, 48,
+                                    z_up=bool(k % 2), ortho_blend=float(rng.choice([0.0, 0.5, 1.0])))
+            m = cam[:16] if k % 3 == 1 else cam[16:32]
+        a, b = O.mat4_inverse(m), O.ref_mat4_inverse(m)
+        assert a[0] == b[0] and (not a[0] or np.array_equal(_bits(a[1]), _bits(b[1]))), k
+    for m in (np.zeros(16, np.float32), np.diag(np.float32([1e-3, 1e-3, 1e-3, 1e-3])).reshape(16)):
+        assert O.mat4_inverse(m)[0] is False and O.ref_mat4_inverse(m)[0] is False
+
+
+@live
 def test_accum_and_taa_match_shader():
     """accum_fs on random frames; taa_accum_fs over a chain of frames whose
     camera moves, returns and holds, every output bit for bit."""
@@ -247,7 +267,8 @@ def test_accum_and_taa_match_shader():
         for i in range(2):
             smp, depth, _ = O.stochastic_sample(ids, proj, w, h, float(10 * k + i + 1), cam, jitter=(0.2 * i, -0.1))
             avg = O.accum(smp, smp if avg is None else avg, float(i + 1))
-        inv = np.linalg.inv(cam[:16].reshape(4, 4).T.astype(np.float64)).T.reshape(-1).astype(np.float32)
+        ok, inv = O.mat4_inverse(cam[:16])
+        assert ok
         has = prev is not None
         pv = prev if has else cam
         vo = np.array([cam[32], cam[33], cam[34], pv[34]], np.float32)
