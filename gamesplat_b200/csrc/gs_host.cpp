@@ -121,6 +121,26 @@ struct gs_ctx {
     uint2* tile_ranges = nullptr;
     uint32_t* tile_order = nullptr;      // raster CTA -> tile (heaviest first)
     uint32_t tiles_cap = 0;
+    // the last host read of this block's counters (on fc_stream) is queued:
+    // the block is zeroed again only after it (a device-side wait)
+    cudaEvent_t ctrl_read = nullptr;
+    bool ctrl_read_pending = false;
+    // The other control block of the frames drawn by gs_render (same layout):
+    // consecutive frames take the two blocks in turn, so a frame's counters are
+    // copied to the host on fc_stream while the next frame runs, instead of a
+    // copy between two kernels of the render stream.
+    struct CtrlBlock {
+        void* ctrl = nullptr;
+        FrameCounters* fc = nullptr;
+        SortPlan* depth_plan = nullptr;
+        SortPlan* tile_plan = nullptr;
+        uint32_t* depth_hist = nullptr;
+        uint32_t* tile_hist = nullptr;
+        uint2* tile_ranges = nullptr;
+        cudaEvent_t read = nullptr;
+        bool read_pending = false;
+    };
+    CtrlBlock alt;
 
     // gsanim appearance deltas (renderer animation buffer, src/renderer.cpp:824-841)
     int8_t* anim_deltas = nullptr;
@@ -145,6 +165,10 @@ struct gs_ctx {
     FrameCounters* h_bin_fc = nullptr;
     cudaEvent_t bin_event = nullptr;
     bool bin_recorded = false;
+    // small device-to-host copies of the frame counters, off the render stream
+    cudaStream_t fc_stream = nullptr;
+    cudaEvent_t binned = nullptr, frame_done = nullptr;
+    FrameCounters* fc_extra = nullptr;   // a second destination of the next end-of-frame copy
     uint32_t epoch = 0;
 
     // image targets
@@ -358,8 +382,17 @@ void release_scene(gs_ctx* c) {
 }
 
 void release_targets(gs_ctx* c) {
+    // copies of the counters may still read the blocks
+    if (c->fc_stream) cudaStreamSynchronize(c->fc_stream);
     dfree(c->out16);
     dfree(c->ctrl);
+    if (c->alt.ctrl) {
+        void* p = c->alt.ctrl;
+        dfree(p);
+        c->alt.ctrl = nullptr;
+        c->alt.fc = nullptr;
+    }
+    c->ctrl_read_pending = c->alt.read_pending = false;
     dfree(c->tile_order);
     dfree(c->features);
     dfree(c->fallback_tiles);
@@ -477,40 +510,93 @@ int ensure_entries(gs_ctx* c, uint32_t cap) {
 
 // The per-frame control block of a w x h frame in the context's fields:
 // FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges, and the tile order.
-int alloc_control(gs_ctx* c, int w, int h, int tw, int th) {
-    const int tx = (w + tw - 1) / tw, ty = (h + th - 1) / th;
-    c->tile_w = tw;
-    c->tile_h = th;
-    c->tiles_cap = (uint32_t)(tx * ty);
-    // control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile ranges
+// Control block layout: FrameCounters | SortPlan x2 | hist x2 (4x256) | tile
+// ranges; each part 256-byte aligned.
+struct CtrlLayout {
+    size_t fc, dp, tp, dh, th, tr, bytes;
+};
+
+CtrlLayout ctrl_layout(uint32_t tiles) {
+    CtrlLayout L{};
     size_t off = 0;
     auto place = [&](size_t bytes) {
         size_t o = off;
         off = (off + bytes + 255) & ~(size_t)255;
         return o;
     };
-    size_t o_fc = place(sizeof(FrameCounters));
-    size_t o_dp = place(sizeof(SortPlan));
-    size_t o_tp = place(sizeof(SortPlan));
-    size_t o_dh = place(4 * 256 * 4);
-    size_t o_th = place(4 * 256 * 4);
-    size_t o_tr = place((size_t)c->tiles_cap * sizeof(uint2));
-    c->ctrl_bytes = off;
-    GS_CUDA(c, dalloc(reinterpret_cast<char**>(&c->ctrl), c->ctrl_bytes));
-    char* base = static_cast<char*>(c->ctrl);
-    c->fc = reinterpret_cast<FrameCounters*>(base + o_fc);
-    c->depth_plan = reinterpret_cast<SortPlan*>(base + o_dp);
-    c->tile_plan = reinterpret_cast<SortPlan*>(base + o_tp);
-    c->depth_hist = reinterpret_cast<uint32_t*>(base + o_dh);
-    c->tile_hist = reinterpret_cast<uint32_t*>(base + o_th);
-    c->tile_ranges = reinterpret_cast<uint2*>(base + o_tr);
+    L.fc = place(sizeof(FrameCounters));
+    L.dp = place(sizeof(SortPlan));
+    L.tp = place(sizeof(SortPlan));
+    L.dh = place(4 * 256 * 4);
+    L.th = place(4 * 256 * 4);
+    L.tr = place((size_t)tiles * sizeof(uint2));
+    L.bytes = off;
+    return L;
+}
+
+template <typename B> void carve_ctrl(B& b, void* ctrl, const CtrlLayout& L) {
+    char* base = static_cast<char*>(ctrl);
+    b.ctrl = ctrl;
+    b.fc = reinterpret_cast<FrameCounters*>(base + L.fc);
+    b.depth_plan = reinterpret_cast<SortPlan*>(base + L.dp);
+    b.tile_plan = reinterpret_cast<SortPlan*>(base + L.tp);
+    b.depth_hist = reinterpret_cast<uint32_t*>(base + L.dh);
+    b.tile_hist = reinterpret_cast<uint32_t*>(base + L.th);
+    b.tile_ranges = reinterpret_cast<uint2*>(base + L.tr);
+}
+
+// The context's control block (and, with_alt, the second block of gs_render's
+// frames) for a w x h viewport of tw x th tiles.
+int alloc_control(gs_ctx* c, int w, int h, int tw, int th, bool with_alt = true) {
+    const int tx = (w + tw - 1) / tw, ty = (h + th - 1) / th;
+    c->tile_w = tw;
+    c->tile_h = th;
+    c->tiles_cap = (uint32_t)(tx * ty);
+    const CtrlLayout L = ctrl_layout(c->tiles_cap);
+    c->ctrl_bytes = L.bytes;
+    void* block = nullptr;
+    GS_CUDA(c, dalloc(reinterpret_cast<char**>(&block), c->ctrl_bytes));
+    carve_ctrl(*c, block, L);
     GS_CUDA(c, cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream));
+    if (with_alt) {
+        void* other = nullptr;
+        GS_CUDA(c, dalloc(reinterpret_cast<char**>(&other), c->ctrl_bytes));
+        carve_ctrl(c->alt, other, L);
+        GS_CUDA(c, cudaMemsetAsync(c->alt.ctrl, 0, c->ctrl_bytes, c->stream));
+    }
     GS_CUDA(c, dalloc(&c->tile_order, (size_t)c->tiles_cap * sizeof(uint32_t)));
     c->width = w;
     c->height = h;
     c->tiles_x = tx;
     c->tiles_y = ty;
     return GS_OK;
+}
+
+// gs_render's frames alternate between the two control blocks: this one's
+// counters may still be on their way to the host while the next frame runs.
+void swap_ctrl(gs_ctx* c) {
+    if (!c->alt.ctrl) return;
+    gs_ctx::CtrlBlock cur;
+    cur.ctrl = c->ctrl;
+    cur.fc = c->fc;
+    cur.depth_plan = c->depth_plan;
+    cur.tile_plan = c->tile_plan;
+    cur.depth_hist = c->depth_hist;
+    cur.tile_hist = c->tile_hist;
+    cur.tile_ranges = c->tile_ranges;
+    cur.read = c->ctrl_read;
+    cur.read_pending = c->ctrl_read_pending;
+    const gs_ctx::CtrlBlock nxt = c->alt;
+    c->alt = cur;
+    c->ctrl = nxt.ctrl;
+    c->fc = nxt.fc;
+    c->depth_plan = nxt.depth_plan;
+    c->tile_plan = nxt.tile_plan;
+    c->depth_hist = nxt.depth_hist;
+    c->tile_hist = nxt.tile_hist;
+    c->tile_ranges = nxt.tile_ranges;
+    c->ctrl_read = nxt.read;
+    c->ctrl_read_pending = nxt.read_pending;
 }
 
 // Tile shape of the context's frames: the alpha knob in alpha mode, 16x16 otherwise.
@@ -561,9 +647,26 @@ void begin_frame(gs_ctx* c, const gs_camera* cam) {
     c->frame_launches = 0;
 }
 
+// A frame of gs_render / gs_render_features: it takes the other control
+// block, once the host read of that block's last counters is done.
+void begin_render_frame(gs_ctx* c, const gs_camera* cam) {
+    swap_ctrl(c);
+    if (c->ctrl_read_pending) cudaStreamWaitEvent(c->stream, c->ctrl_read, 0);
+    c->ctrl_read_pending = false;
+    begin_frame(c, cam);
+}
+
+// The frame's counters go to the host on fc_stream, behind the frame's last
+// operation but off the render stream (and, when set, to fc_extra as well).
 void end_frame(gs_ctx* c) {
-    cudaMemcpyAsync(c->h_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
-    cudaEventRecord(c->fc_event, c->stream);
+    cudaEventRecord(c->frame_done, c->stream);
+    cudaStreamWaitEvent(c->fc_stream, c->frame_done, 0);
+    cudaMemcpyAsync(c->h_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->fc_stream);
+    if (c->fc_extra)
+        cudaMemcpyAsync(c->fc_extra, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->fc_stream);
+    cudaEventRecord(c->fc_event, c->fc_stream);
+    cudaEventRecord(c->ctrl_read, c->fc_stream);
+    c->ctrl_read_pending = true;
     c->fc_pending = true;
     c->last_launches = c->frame_launches;
 }
@@ -631,7 +734,9 @@ void run_depth_sort(gs_ctx* c) {
 }
 
 // Binning, tile sort and tile ranges for one raster pass.
-void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = false) {
+// readback: copy the counters to h_bin_fc once the expansion has run (on
+// fc_stream, so the tile sort does not queue behind the copy).
+void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = false, bool readback = true) {
     {
         StageScope sc(c, ST_BIN);
         gs::BinParams p{};
@@ -662,10 +767,13 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = fals
         p.fc = c->fc;
         p.envelope = envelope ? 1 : 0;
         sc.add(gs::launch_bin(p, c->n, c->num_sms, c->stream));
-        // the entry count is final once the expansion ran
-        cudaMemcpyAsync(c->h_bin_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
-        cudaEventRecord(c->bin_event, c->stream);
-        c->bin_recorded = true;
+        if (readback) {   // the entry count is final once the expansion ran
+            cudaEventRecord(c->binned, c->stream);
+            cudaStreamWaitEvent(c->fc_stream, c->binned, 0);
+            cudaMemcpyAsync(c->h_bin_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->fc_stream);
+            cudaEventRecord(c->bin_event, c->fc_stream);
+            c->bin_recorded = true;
+        }
     }
     {
         StageScope sc(c, ST_TILE_SORT);
@@ -1103,7 +1211,12 @@ int gs_create(gs_ctx** out, int device, void* stream) {
     if (cudaMallocHost(reinterpret_cast<void**>(&c->h_fc), sizeof(FrameCounters)) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void**>(&c->h_bin_fc), sizeof(FrameCounters)) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->fc_event, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->bin_event, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->bin_event, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->binned, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->frame_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ctrl_read, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->alt.read, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->fc_stream, cudaStreamNonBlocking) != cudaSuccess) {
         gs_destroy(c);
         return GS_ERR_OOM;
     }
@@ -1117,6 +1230,7 @@ void gs_destroy(gs_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    if (c->fc_stream) cudaStreamSynchronize(c->fc_stream);
     release_scene(c);
     release_targets(c);
     dfree(c->display_lut);
@@ -1142,6 +1256,9 @@ void gs_destroy(gs_ctx* c) {
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->fc_event) cudaEventDestroy(c->fc_event);
     if (c->bin_event) cudaEventDestroy(c->bin_event);
+    for (cudaEvent_t e : {c->binned, c->frame_done, c->ctrl_read, c->alt.read})
+        if (e) cudaEventDestroy(e);
+    if (c->fc_stream) cudaStreamDestroy(c->fc_stream);
     for (auto& p : c->pending) {
         cudaEventDestroy(p.a);
         cudaEventDestroy(p.b);
@@ -1539,7 +1656,7 @@ int gs_render(gs_ctx* c, const gs_camera* cam, void* out) {
         const gs_camera pcam = c->prev_cam;
         const bool pvalid = c->prev_cam_valid, tvalid = c->taa_prev_valid;
         nvtxRangePushA("gs_render");
-        begin_frame(c, cam);
+        begin_render_frame(c, cam);
         c->bin_recorded = false;
         switch (c->knobs.render_mode) {
             case GS_MODE_ALPHA: rc = render_alpha(c, o); break;
@@ -1682,12 +1799,14 @@ int gs_render_host_submit(gs_ctx* c, const gs_camera* cam, uint16_t* host_out) {
         if (e != cudaSuccess) return cuda_fail(c, e, "dalloc(stream image)");
         ss.bytes = bytes;
     }
+    c->fc_extra = ss.h_fc;   // the frame's counters, copied on fc_stream by end_frame
     rc = gs_render(c, cam, ss.image);
+    c->fc_extra = nullptr;
     if (rc) return rc;
-    GS_CUDA(c, cudaMemcpyAsync(ss.h_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream));
     GS_CUDA(c, cudaEventRecord(ss.rendered, c->stream));
     GS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ss.rendered, 0));
     GS_CUDA(c, cudaMemcpyAsync(host_out, ss.image, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+    GS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, c->fc_event, 0));   // ss.copied covers the counters too
     GS_CUDA(c, cudaEventRecord(ss.copied, c->copy_stream));
     ss.host = host_out;
     c->sslot_next ^= 1;
@@ -1723,7 +1842,7 @@ int gs_render_features(gs_ctx* c, const gs_camera* cam, void* features_out) {
         const uint32_t seed = c->frame_seed, samples = c->sample_count, widx = c->accum_write_index;
         const gs_camera pcam = c->prev_cam;
         const bool pvalid = c->prev_cam_valid, tvalid = c->taa_prev_valid;
-        begin_frame(c, cam);
+        begin_render_frame(c, cam);
         c->bin_recorded = false;
         rc = render_denoise_inputs(c, cam);
         end_frame(c);
@@ -1784,7 +1903,7 @@ int prepare_slot(gs_ctx* c, int w, int h, int tw, int th, bool fresh_records) {
         dfree(c->ctrl);
         dfree(c->tile_order);
         c->width = c->height = 0;
-        int rc = alloc_control(c, w, h, tw, th);
+        int rc = alloc_control(c, w, h, tw, th, /*with_alt*/ false);
         if (rc) return rc;
     }
     if (fresh_records || !c->records) {
@@ -1812,7 +1931,7 @@ int stage_frame(gs_ctx* c, uint32_t k, const gs_camera* cam, void* out) {
         begin_frame(c, cam);
         run_cull(c);
         run_depth_sort(c);
-        run_binning(c, 0.0f, 0.0f, 0.0f);
+        run_binning(c, 0.0f, 0.0f, 0.0f, false, /*readback*/ false);
         cudaMemcpyAsync(&c->h_slot_fc[k], c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
         gs::RasterParams r = raster_params(c, background(c));
         r.out_rgba16f = static_cast<uint16_t*>(out);
@@ -1911,6 +2030,7 @@ int gs_render_batch(gs_ctx* c, const gs_camera* cams, uint32_t count, void* cons
         if (!rc) rc = raster_batch(c, m);
         if (!rc) {
             // the statistics of the batch's last frame
+            cudaStreamWaitEvent(c->stream, c->fc_event, 0);   // after gs_render's copy of h_fc
             cudaMemcpyAsync(c->h_fc, c->slots[m - 1].fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
             cudaEventRecord(c->fc_event, c->stream);
         }
@@ -2066,6 +2186,7 @@ int gs_render_anim_batch(gs_ctx* c, const gs_camera* cam, const int32_t* states_
     c->anim_w = sw;
     swap_slot(c, f0);
     rc = raster_batch(c, count);
+    cudaStreamWaitEvent(c->stream, c->fc_event, 0);   // after gs_render's copy of h_fc
     cudaMemcpyAsync(c->h_fc, c->slots[0].fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
     cudaEventRecord(c->fc_event, c->stream);
     c->fc_pending = false;
@@ -2079,6 +2200,7 @@ int gs_render_anim_batch(gs_ctx* c, const gs_camera* cam, const int32_t* states_
 int gs_read_stats(gs_ctx* c, gs_stats* s) {
     if (!c || !s) return GS_ERR_BAD_ARG;
     GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    GS_CUDA(c, cudaStreamSynchronize(c->fc_stream));   // gs_render's counters come on fc_stream
     c->fc_pending = false;
     std::memset(s, 0, sizeof(*s));
     const FrameCounters& f = *c->h_fc;
