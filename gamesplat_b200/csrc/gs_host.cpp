@@ -639,21 +639,32 @@ int check_previous_frame(gs_ctx* c) {
     return GS_OK;
 }
 
-void begin_frame(gs_ctx* c, const gs_camera* cam) {
+void begin_frame(gs_ctx* c, const gs_camera* cam, bool zero_ctrl = true) {
     c->cam = *cam;
-    cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream);
+    if (zero_ctrl) cudaMemsetAsync(c->ctrl, 0, c->ctrl_bytes, c->stream);
     ++c->epoch;
     if (c->epoch == 0) ++c->epoch;
     c->frame_launches = 0;
 }
 
 // A frame of gs_render / gs_render_features: it takes the other control
-// block, once the host read of that block's last counters is done.
+// block, zeroed on fc_stream after its last counters went to the host (the
+// render stream waits for that, long done by now), and the block it leaves
+// is zeroed the same way while this frame runs.  The last frame's block stays
+// intact until the next frame begins, for gs_debug_read.
 void begin_render_frame(gs_ctx* c, const gs_camera* cam) {
+    if (!c->alt.ctrl) {
+        begin_frame(c, cam);
+        return;
+    }
     swap_ctrl(c);
     if (c->ctrl_read_pending) cudaStreamWaitEvent(c->stream, c->ctrl_read, 0);
     c->ctrl_read_pending = false;
-    begin_frame(c, cam);
+    if (c->alt.read_pending) {   // queued behind the copy of its counters on fc_stream
+        cudaMemsetAsync(c->alt.ctrl, 0, c->ctrl_bytes, c->fc_stream);
+        cudaEventRecord(c->alt.read, c->fc_stream);
+    }
+    begin_frame(c, cam, /*zero_ctrl*/ false);
 }
 
 // The frame's counters go to the host on fc_stream, behind the frame's last
