@@ -128,6 +128,7 @@ __device__ __forceinline__ BinItem bin_one(const BinParams& p, uint32_t s, uint3
 // entries).
 
 __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
+    pdl_wait();
     __shared__ uint32_t scan_tmp[33];
     __shared__ uint32_t s_tile, s_excl, s_total;
     __shared__ uint32_t s_off[kBinTile];    // exclusive entry offset of each splat in the CTA tile
@@ -241,6 +242,7 @@ __global__ void __launch_bounds__(kBinThreads) bin_kernel(BinParams p) {
 // whichever CTA expands a chunk; the tile ids' digit histograms for the tile
 // sort are accumulated here.
 __global__ void __launch_bounds__(kBinThreads) expand_kernel(BinParams p) {
+    pdl_wait();
     __shared__ uint32_t scan_tmp[33];
     __shared__ uint32_t s_hist[3][256];
     __shared__ __align__(16) int32_t s_own[kBinChunk];
@@ -389,8 +391,8 @@ int launch_bin(const BinParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_
     uint32_t grid = num_sms * (1024 / kBinThreads);
     if (grid > tiles) grid = tiles;
     if (grid == 0) grid = 1;
-    bin_kernel<<<grid, kBinThreads, 0, s>>>(p);
-    expand_kernel<<<num_sms * (1024 / kBinThreads), kBinThreads, 0, s>>>(p);
+    launch_pdl(bin_kernel, dim3(grid), dim3(kBinThreads), 0, s, p);
+    launch_pdl(expand_kernel, dim3(num_sms * (1024 / kBinThreads)), dim3(kBinThreads), 0, s, p);
     return 2;
 }
 

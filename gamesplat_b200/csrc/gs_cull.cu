@@ -342,6 +342,7 @@ int launch_pack_half_rows(const float4* rows, float4* half_rows, uint32_t n, uin
 // values in a scene) is aggregated per warp first, since 32 lanes adding to
 // one shared word would serialize.
 __global__ void __launch_bounds__(kCullVisThreads) cull_visible_kernel(CullParams p) {
+    pdl_wait();
     constexpr int kWarps = kCullVisThreads / 32;
     static_assert(kCullVisItems * kWarps == 64, "the count scan gives each lane two (row group, warp) counts");
     __shared__ uint32_t s_hist[4][256];
@@ -454,6 +455,7 @@ __global__ void __launch_bounds__(kCullVisThreads) cull_visible_kernel(CullParam
 // wait (measured faster than two stages per warp at 3 CTAs per SM).
 template <int kChunks>  // 16-byte chunks of a row the SH degree needs: 4, 7, 10 or 16
 __global__ void __launch_bounds__(kCullThreads, 6) cull_project_kernel(CullParams p) {
+    pdl_wait();
     extern __shared__ float4 smem4[];
     __shared__ __align__(8) uint64_t s_bar[kCullWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -851,7 +853,7 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
     if (p.anim_deltas) deg = 3;   // the delta pass touches every SH slot of the staged row
     const uint32_t tiles = (p.n + kCullVisTile - 1) / kCullVisTile;
     if (tiles == 0) return 0;
-    cull_visible_kernel<<<tiles, kCullVisThreads, 0, s>>>(p);   // one CTA per tile
+    launch_pdl(cull_visible_kernel, dim3(tiles), dim3(kCullVisThreads), 0, s, p);
     // projection: persistent, as many CTAs as fit (6 per SM) for the largest possible visible count
     const uint32_t groups_cap = (p.n + 31) / 32;
     uint32_t pgrid = num_sms * 6;
@@ -861,10 +863,10 @@ int launch_cull(const CullParams& p, uint32_t num_sms, cudaStream_t s) {
         return 2;
     }
     switch (deg) {
-        case 0: cull_project_kernel<4><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
-        case 1: cull_project_kernel<7><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
-        case 2: cull_project_kernel<10><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
-        default: cull_project_kernel<16><<<pgrid, kCullThreads, kCullSmem, s>>>(p); break;
+        case 0: launch_pdl(cull_project_kernel<4>, dim3(pgrid), dim3(kCullThreads), kCullSmem, s, p); break;
+        case 1: launch_pdl(cull_project_kernel<7>, dim3(pgrid), dim3(kCullThreads), kCullSmem, s, p); break;
+        case 2: launch_pdl(cull_project_kernel<10>, dim3(pgrid), dim3(kCullThreads), kCullSmem, s, p); break;
+        default: launch_pdl(cull_project_kernel<16>, dim3(pgrid), dim3(kCullThreads), kCullSmem, s, p); break;
     }
     if (p.layer_count > 0) {
         uint32_t lgrid = (p.n + 255) / 256;

@@ -741,12 +741,13 @@ void run_depth_sort(gs_ctx* c) {
     p.status_stride = c->sort_status_stride;
     p.epoch = c->epoch;
     p.error_flags = &c->fc->error_flags;
+    p.first_pdl = 1;
     sc.add(gs::launch_sort(p, c->num_sms, c->stream));
 }
 
 // Binning, tile sort and tile ranges for one raster pass.
-// readback: copy the counters to h_bin_fc once the expansion has run (on
-// fc_stream, so the tile sort does not queue behind the copy).
+// readback: copy the counters to h_bin_fc on fc_stream once the tile sort has
+// run (the entry count is final after the expansion).
 void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = false, bool readback = true) {
     {
         StageScope sc(c, ST_BIN);
@@ -778,13 +779,6 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = fals
         p.fc = c->fc;
         p.envelope = envelope ? 1 : 0;
         sc.add(gs::launch_bin(p, c->n, c->num_sms, c->stream));
-        if (readback) {   // the entry count is final once the expansion ran
-            cudaEventRecord(c->binned, c->stream);
-            cudaStreamWaitEvent(c->fc_stream, c->binned, 0);
-            cudaMemcpyAsync(c->h_bin_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->fc_stream);
-            cudaEventRecord(c->bin_event, c->fc_stream);
-            c->bin_recorded = true;
-        }
     }
     {
         StageScope sc(c, ST_TILE_SORT);
@@ -807,7 +801,18 @@ void run_binning(gs_ctx* c, float jx, float jy, float seed, bool envelope = fals
         p.status_stride = c->tsort_status_stride;
         p.epoch = c->epoch;
         p.error_flags = &c->fc->error_flags;
+        p.first_pdl = 1;
         sc.add(gs::launch_sort(p, c->num_sms, c->stream));
+        // The entry count is final once the expansion ran; the readback is
+        // queued behind the tile sort so that the expansion and the sort's
+        // first pass stay adjacent (programmatic dependent launch between them).
+        if (readback) {
+            cudaEventRecord(c->binned, c->stream);
+            cudaStreamWaitEvent(c->fc_stream, c->binned, 0);
+            cudaMemcpyAsync(c->h_bin_fc, c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->fc_stream);
+            cudaEventRecord(c->bin_event, c->fc_stream);
+            c->bin_recorded = true;
+        }
         sc.add(gs::launch_tile_ranges(c->tile_plan, c->fc, c->entry_cap, c->tile_ranges, c->tiles_cap, c->num_sms,
                                        c->stream));
         sc.add(gs::launch_tile_order(c->tile_ranges, c->tiles_cap, c->tile_order, c->stream));

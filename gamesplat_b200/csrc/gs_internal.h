@@ -149,6 +149,7 @@ struct SortParams {
     size_t status_stride;        // words per pass
     uint32_t epoch;
     uint32_t* error_flags;
+    int first_pdl = 0;           // 1: the first pass too is a programmatic dependent launch
 };
 
 struct BinParams {

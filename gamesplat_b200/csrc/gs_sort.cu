@@ -341,10 +341,11 @@ int launch_sort(const SortParams& p, uint32_t num_sms, cudaStream_t s) {
     if (pass_grid > tiles_cap) pass_grid = tiles_cap > 0 ? tiles_cap : 1;
     for (int ps = 0; ps < npasses; ++ps) {
         // Passes after the first overlap their launch with the previous pass's
-        // tail (programmatic dependent launch).  Across stage boundaries
-        // (cull -> sort, bin -> tile sort) it measured slower, so the first
-        // pass is an ordinary launch.
-        if (ps == 0) sort_pass_kernel<<<pass_grid, kSortThreads, kPassSmem, s>>>(p, ps, npasses);
+        // tail (programmatic dependent launch); so does the first pass when the
+        // caller asks (the frame's sorts: every kernel of a frame starts with
+        // griddepcontrol.wait).  The stage-level entry points launch it
+        // ordinarily behind the caller's work.
+        if (ps == 0 && !p.first_pdl) sort_pass_kernel<<<pass_grid, kSortThreads, kPassSmem, s>>>(p, ps, npasses);
         else launch_pdl(sort_pass_kernel, dim3(pass_grid), dim3(kSortThreads), kPassSmem, s, p, ps, npasses);
         ++launches;
     }
