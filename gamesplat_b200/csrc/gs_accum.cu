@@ -17,6 +17,7 @@ namespace gs {
 
 __global__ void accum_kernel(const float4* __restrict__ sample, const float4* __restrict__ history, float n,
                              float4* __restrict__ out, size_t npix) {
+    pdl_wait();   // launched as a programmatic dependent of the frame's previous kernel
     const float nn = g_max(n, 1.0f);
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npix; i += (size_t)gridDim.x * blockDim.x) {
         float4 s = sample[i], h = history[i];
@@ -30,6 +31,7 @@ __global__ void accum_kernel(const float4* __restrict__ sample, const float4* __
 }
 
 __global__ void to_half_kernel(const float4* __restrict__ src, uint2* __restrict__ dst, size_t npix) {
+    pdl_wait();   // launched as a programmatic dependent of the frame's previous kernel
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npix; i += (size_t)gridDim.x * blockDim.x) {
         float4 c = src[i];
         __half2 a = __floats2half2_rn(c.x, c.y), b = __floats2half2_rn(c.z, c.w);
@@ -65,6 +67,7 @@ __global__ void taa_kernel(const float4* __restrict__ cur_color, const float* __
                            const float4* __restrict__ hist_color, const float4* __restrict__ hist_xyz, int w, int h,
                            TaaUniforms U, float4* __restrict__ out_color, float4* __restrict__ out_xyz,
                            __nv_bfloat16* __restrict__ features) {
+    pdl_wait();   // launched as a programmatic dependent of the frame's previous kernel
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= w || y >= h) return;
@@ -152,12 +155,12 @@ static unsigned grid_for(size_t n, unsigned cap = 148 * 16) {
 }
 
 int launch_accum(const float4* sample, const float4* history, float n, float4* out, size_t npix, cudaStream_t s) {
-    accum_kernel<<<grid_for(npix), 256, 0, s>>>(sample, history, n, out, npix);
+    launch_pdl(accum_kernel, dim3(grid_for(npix)), dim3(256), 0, s, sample, history, n, out, npix);
     return 1;
 }
 
 int launch_to_half(const float4* src, uint16_t* dst, size_t npix, cudaStream_t s) {
-    to_half_kernel<<<grid_for(npix), 256, 0, s>>>(src, reinterpret_cast<uint2*>(dst), npix);
+    launch_pdl(to_half_kernel, dim3(grid_for(npix)), dim3(256), 0, s, src, reinterpret_cast<uint2*>(dst), npix);
     return 1;
 }
 
@@ -165,8 +168,8 @@ int launch_taa(const float4* cur_color, const float* cur_depth, const float4* hi
                int w, int h, const TaaUniforms& u, float4* out_color, float4* out_xyz, cudaStream_t s,
                void* features) {
     dim3 block(16, 16), grid((w + 15) / 16, (h + 15) / 16);
-    taa_kernel<<<grid, block, 0, s>>>(cur_color, cur_depth, hist_color, hist_xyz, w, h, u, out_color, out_xyz,
-                                      static_cast<__nv_bfloat16*>(features));
+    launch_pdl(taa_kernel, grid, block, 0, s, cur_color, cur_depth, hist_color, hist_xyz, w, h, u, out_color, out_xyz,
+               static_cast<__nv_bfloat16*>(features));
     return 1;
 }
 

@@ -34,11 +34,13 @@ __device__ __forceinline__ float hash01(uint32_t x) {
 }
 
 __global__ void gps_clear_kernel(unsigned long long* packed, size_t count) {
+    pdl_wait();   // launched as a programmatic dependent of the frame's previous kernel
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
         packed[i] = 0xFFFFFFFF00000000ull;
 }
 
 __global__ void gps_expand_kernel(GpsParams p, float4* __restrict__ prepared, uint2* __restrict__ work) {
+    pdl_wait();   // launched as a programmatic dependent of the frame's previous kernel
     const uint32_t n_vis = p.fc->visible_count;
     const float ss = (float)p.supersample;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n_vis; v += gridDim.x * blockDim.x) {
@@ -87,6 +89,7 @@ __global__ void gps_expand_kernel(GpsParams p, float4* __restrict__ prepared, ui
 
 __global__ void gps_splat_kernel(GpsParams p, const float4* __restrict__ prepared, const uint2* __restrict__ work,
                                  unsigned long long* __restrict__ packed) {
+    pdl_wait();   // launched as a programmatic dependent of the frame's previous kernel
     const uint32_t total = min(p.fc->gps_work[0], p.max_work_items);
     const int gw = p.width * (int)p.supersample, gh = p.height * (int)p.supersample;
     const float ss = (float)p.supersample;
@@ -134,6 +137,7 @@ __global__ void gps_splat_kernel(GpsParams p, const float4* __restrict__ prepare
 }
 
 __global__ void gps_resolve_kernel(GpsParams p, const unsigned long long* __restrict__ packed) {
+    pdl_wait();   // launched as a programmatic dependent of the frame's previous kernel
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= p.width || y >= p.height) return;
@@ -238,13 +242,13 @@ void release_gps_scene(GpsTargets& g) {
 int launch_gps(GpsTargets& g, const GpsParams& p, uint32_t n_cap, uint32_t num_sms, cudaStream_t s) {
     const size_t count = (size_t)g.width * g.ss * g.height * g.ss;
     unsigned cg = (unsigned)std::min<size_t>((count + 255) / 256, (size_t)num_sms * 16);
-    gps_clear_kernel<<<cg ? cg : 1, 256, 0, s>>>(g.packed, count);
+    launch_pdl(gps_clear_kernel, dim3(cg ? cg : 1), dim3(256), 0, s, g.packed, count);
     unsigned eg = (unsigned)std::min<size_t>((n_cap + 255) / 256, (size_t)num_sms * 8);
-    gps_expand_kernel<<<eg ? eg : 1, 256, 0, s>>>(p, g.prepared, g.work);
+    launch_pdl(gps_expand_kernel, dim3(eg ? eg : 1), dim3(256), 0, s, p, g.prepared, g.work);
     unsigned sg = (unsigned)std::min<size_t>(((size_t)g.work_cap + 255) / 256, (size_t)num_sms * 16);
-    gps_splat_kernel<<<sg ? sg : 1, 256, 0, s>>>(p, g.prepared, g.work, g.packed);
+    launch_pdl(gps_splat_kernel, dim3(sg ? sg : 1), dim3(256), 0, s, p, g.prepared, g.work, g.packed);
     dim3 block(16, 16), grid((p.width + 15) / 16, (p.height + 15) / 16);
-    gps_resolve_kernel<<<grid, block, 0, s>>>(p, g.packed);
+    launch_pdl(gps_resolve_kernel, grid, block, 0, s, p, g.packed);
     return 4;
 }
 

@@ -1948,7 +1948,10 @@ int stage_frame(gs_ctx* c, uint32_t k, const gs_camera* cam, void* out) {
         run_cull(c);
         run_depth_sort(c);
         run_binning(c, 0.0f, 0.0f, 0.0f, false, /*readback*/ false);
-        cudaMemcpyAsync(&c->h_slot_fc[k], c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->stream);
+        // on fc_stream: a copy between two kernels would idle the render stream
+        cudaEventRecord(c->binned, c->stream);
+        cudaStreamWaitEvent(c->fc_stream, c->binned, 0);
+        cudaMemcpyAsync(&c->h_slot_fc[k], c->fc, sizeof(FrameCounters), cudaMemcpyDeviceToHost, c->fc_stream);
         gs::RasterParams r = raster_params(c, background(c));
         r.out_rgba16f = static_cast<uint16_t*>(out);
         c->h_batch_params[k] = r;
@@ -1962,6 +1965,7 @@ int stage_frame(gs_ctx* c, uint32_t k, const gs_camera* cam, void* out) {
 int grow_overflowed(gs_ctx* c, uint32_t count, std::vector<uint32_t>& redo) {
     GS_CUDA(c, cudaEventRecord(c->batch_event, c->stream));
     GS_CUDA(c, cudaEventSynchronize(c->batch_event));
+    GS_CUDA(c, cudaStreamSynchronize(c->fc_stream));   // the slots' counters
     redo.clear();
     for (uint32_t k = 0; k < count; ++k) {
         const FrameCounters& fc = c->h_slot_fc[k];

@@ -630,14 +630,14 @@ int launch_raster_alpha(const RasterParams& p, cudaStream_t s) {
 int launch_raster_stochastic2(const RasterParams& p, cudaStream_t s) {
     const uint32_t tiles = (uint32_t)p.tiles_x * (uint32_t)p.tiles_y;
     if (tiles == 0) return 0;
-    raster_kernel<2><<<tiles, kRasterThreads, 0, s>>>(p);
+    launch_pdl(raster_kernel<2>, dim3(tiles), dim3(kRasterThreads), 0, s, p);
     return 1;
 }
 
 int launch_raster_stochastic(const RasterParams& p, cudaStream_t s) {
     const uint32_t tiles = (uint32_t)p.tiles_x * (uint32_t)p.tiles_y;
     if (tiles == 0) return 0;
-    raster_kernel<1><<<tiles, kRasterThreads, 0, s>>>(p);
+    launch_pdl(raster_kernel<1>, dim3(tiles), dim3(kRasterThreads), 0, s, p);
     return 1;
 }
 
