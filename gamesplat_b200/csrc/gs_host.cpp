@@ -2243,6 +2243,7 @@ int gs_read_stats(gs_ctx* c, gs_stats* s) {
 int gs_debug_read(gs_ctx* c, int which, void* dst, uint64_t bytes) {
     if (!c || !dst) return GS_ERR_BAD_ARG;
     GS_CUDA(c, cudaStreamSynchronize(c->stream));
+    GS_CUDA(c, cudaStreamSynchronize(c->fc_stream));   // h_fc of the last frame
     const uint64_t n = c->n;
     const uint32_t vis = c->h_fc->visible_count;
     const size_t npix = (size_t)c->width * c->height;
