@@ -35,6 +35,8 @@ _FLOAT_LIT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE]
 _LAYOUT = re.compile(r"\blayout\s*\([^)]*\)\s*")
 _BLOCK_HEAD = re.compile(r"^\s*(?:(?:readonly|writeonly|coherent|restrict|volatile)\s+)*(uniform|buffer)\s+\w+\s*\{\s*$")
 _BLOCK_END = re.compile(r"^\s*\}\s*\w*\s*;\s*$")
+_BLOCK_LINE = re.compile(r"^\s*(?:(?:readonly|writeonly|coherent|restrict|volatile)\s+)*(uniform|buffer)\s+\w+\s*"
+                         r"\{(.*)\}\s*;\s*$")
 _UNSIZED = re.compile(r"^(\s*)(\w+)\s+(\w+)\s*\[\s*\]\s*;\s*$")
 _OPAQUE = re.compile(r"^\s*uniform\s+(texture2D|sampler)\s+(\w+)\s*;\s*$")
 _IFACE = re.compile(r"^\s*(?:(?:flat|smooth|noperspective)\s+)?(?:in|out)\s+(\w+)\s+(\w+)\s*;\s*$")
@@ -78,6 +80,13 @@ def translate(lines: list[str]) -> str:
         if re.match(r"^\s*in\s*;\s*$", line):          # the local_size declaration
             continue
         if block is None:
+            m = _BLOCK_LINE.match(line)
+            if m:   # a block on one line: its members, one per declaration
+                for member in filter(None, (x.strip() for x in m.group(2).split(";"))):
+                    u = _UNSIZED.match(member + ";")
+                    out.append(f"{u.group(2)}* {u.group(3)} = nullptr;" if m.group(1) == "buffer" and u
+                               else member + ";")
+                continue
             m = _BLOCK_HEAD.match(line)
             if m:
                 block = m.group(1)

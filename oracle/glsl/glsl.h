@@ -149,6 +149,7 @@ template <typename T> struct tvec3 {
     explicit tvec3(T s) : d{s, s, s} {}
     tvec3(T a, T b, T c) : d{a, b, c} {}
     tvec3(const tvec2<T>& v, T c) : d{v.d[0], v.d[1], c} {}
+    tvec3(T a, const tvec2<T>& v) : d{a, v.d[0], v.d[1]} {}
     tvec3(const tvec3& o) : d{o.d[0], o.d[1], o.d[2]} {}
     template <typename U>
     explicit tvec3(const tvec3<U>& o) : d{cv<T>::of(o.d[0]), cv<T>::of(o.d[1]), cv<T>::of(o.d[2])} {}
@@ -348,6 +349,7 @@ inline float smoothstep(float e0, float e1, float x) {
 #define GLSL_VEC_FNS(V, N)                                                                     \
     GLSL_VEC_FN1(V, N, floor) GLSL_VEC_FN1(V, N, ceil) GLSL_VEC_FN1(V, N, fract)               \
     GLSL_VEC_FN1(V, N, round) GLSL_VEC_FN1(V, N, abs) GLSL_VEC_FN1(V, N, sqrt)                 \
+    GLSL_VEC_FN1(V, N, exp2) GLSL_VEC_FN1(V, N, log2)                                          \
     inline V min(const V& a, const V& b) { V r; for (int i = 0; i < N; ++i) r.d[i] = min(a.d[i], b.d[i]); return r; } \
     inline V max(const V& a, const V& b) { V r; for (int i = 0; i < N; ++i) r.d[i] = max(a.d[i], b.d[i]); return r; } \
     inline V min(const V& a, float s) { return min(a, V(s)); }                                \
@@ -375,6 +377,7 @@ GLSL_VEC_FNS(vec4, 4)
     inline V max(const V& a, const V& b) { V r; for (int i = 0; i < N; ++i) r.d[i] = max(a.d[i], b.d[i]); return r; } \
     inline V clamp(const V& x, const V& lo, const V& hi) { return min(max(x, lo), hi); }
 GLSL_IVEC_FNS(ivec2, int, 2)
+GLSL_IVEC_FNS(ivec3, int, 3)
 GLSL_IVEC_FNS(uvec2, uint, 2)
 #undef GLSL_IVEC_FNS
 

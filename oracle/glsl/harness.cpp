@@ -8,7 +8,7 @@
 //
 // Each entry point mirrors the oracle function of the same name (oc_cull,
 // oc_sort_pairs, oc_composite_alpha, oc_stochastic_sample, oc_gps_frame,
-// oc_accum, oc_taa):
+// oc_accum, oc_taa, oc_display):
 // same arguments, same output layout.  Only the fixed-function steps between
 // the stages are written here, as the oracle defines them: the quad's
 // rasterization (viewport transform, 1/256-pixel snap, pixel centres at
@@ -168,6 +168,20 @@ vec4 gl_FragCoord;
 bool gl_discarded;
 #include "accum_fs.inc"
 }  // namespace st_accum
+
+namespace st_blit {
+using namespace glsl;
+vec4 gl_FragCoord;
+bool gl_discarded;
+#include "blit_fs.inc"
+}  // namespace st_blit
+
+namespace st_display {
+using namespace glsl;
+vec4 gl_FragCoord;
+bool gl_discarded;
+#include "layers_display_fs.inc"
+}  // namespace st_display
 
 namespace st_taa {
 using namespace glsl;
@@ -610,6 +624,53 @@ void glsl_taa(const float* cur_color, const float* cur_depth, const float* hist_
     }
     flip_rows(oc.data(), out_color, width, height, 4);
     flip_rows(ox.data(), out_xyz, width, height, 4);
+}
+
+// blit_fs, or with a LUT layers_display_fs (shaders/accum.glsl:181-240),
+// over an RGBA16F frame, as oc_display: lut is n x n x n x 3 uint16 (z, y, x,
+// rgb), null for the blit; out is RGBA32F in the input's row order.
+void glsl_display(const uint16_t* in_half, int width, int height, const uint16_t* lut, int lut_size, float log2_min,
+                  float log2_max, float exposure_ev, float* out) {
+    const size_t npix = (size_t)width * (size_t)height;
+    std::vector<float> tex(npix * 4);
+    for (size_t i = 0; i < npix * 4; ++i) tex[i] = oc_half_to_float(in_half[i]);
+    glsl::texture2D t;
+    t.data = tex.data();
+    t.width = width;
+    t.height = height;
+    std::vector<uint32_t> words;
+    if (lut) {
+        const size_t entries = (size_t)lut_size * lut_size * lut_size * 3;
+        words.assign((entries + 1) / 2, 0u);
+        for (size_t i = 0; i < entries; ++i) words[i / 2] |= (uint32_t)lut[i] << ((i % 2) * 16);
+        st_display::linear_tex = t;
+        st_display::display_lut = reinterpret_cast<st_display::LutWord*>(words.data());
+        st_display::lut_size = lut_size;
+        st_display::log2_min = log2_min;
+        st_display::log2_max = log2_max;
+        st_display::exposure_ev = exposure_ev;
+    } else {
+        st_blit::display_tex = t;
+    }
+    for (int y = 0; y < height; ++y) {
+        for (int x = 0; x < width; ++x) {
+            const vec2 uv(((float)x + 0.5f) / (float)width, ((float)y + 0.5f) / (float)height);
+            const vec4 frag((float)x + 0.5f, (float)y + 0.5f, 0.0f, 1.0f);
+            vec4 c;
+            if (lut) {
+                st_display::uv = uv;
+                st_display::gl_FragCoord = frag;
+                st_display::stage_main();
+                c = st_display::out_color;
+            } else {
+                st_blit::uv = uv;
+                st_blit::gl_FragCoord = frag;
+                st_blit::stage_main();
+                c = st_blit::out_color;
+            }
+            for (int k = 0; k < 4; ++k) out[((size_t)y * width + x) * 4 + k] = c.d[k];
+        }
+    }
 }
 
 // radix_hist_cs, radix_prefix_cs and radix_scatter_cs for the four 8-bit

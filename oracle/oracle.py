@@ -211,6 +211,9 @@ def glsl():
                                 C.c_int, C.c_float, vp, C.c_int, vp, _u32p, _u32p, _f32p, _u32p, _u32p]
         G.ref_mat4_inverse.restype = C.c_int
         G.ref_mat4_inverse.argtypes = [_f32p, _f32p]
+        G.glsl_display.restype = None
+        G.glsl_display.argtypes = [_u16p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_float,
+                                   _f32p]
         G.glsl_sort_pairs.restype = None
         G.glsl_sort_pairs.argtypes = [_u32p, _u32p, C.c_uint32, _u32p, _u32p]
         G.glsl_composite_alpha.restype = C.c_uint64
@@ -653,3 +656,18 @@ def glsl_taa(cur_color, cur_depth, hist_color, hist_xyz, inv_view, prev_view, vi
                     f(viewport_ortho), f(focal_clip), f(prev_focal_clip), f(proj_z), float(history_valid),
                     float(view_changed), oc.reshape(-1), ox.reshape(-1))
     return oc, ox
+
+
+def glsl_display(img_half: np.ndarray, lut, log2_min: float, log2_max: float, exposure_ev: float) -> np.ndarray:
+    """blit_fs / layers_display_fs over an (H, W, 4) float16 frame, as display()."""
+    img = np.ascontiguousarray(img_half, np.float16)
+    h, w = img.shape[:2]
+    out = np.empty((h, w, 4), np.float32)
+    if lut is None:
+        lp, n = None, 0
+    else:
+        lut = np.ascontiguousarray(lut, np.uint16)
+        lp, n = lut.ctypes.data, lut.shape[0]
+    glsl().glsl_display(img.view(np.uint16).reshape(-1), w, h, lp, n, float(log2_min), float(log2_max),
+                        float(exposure_ev), out.reshape(-1))
+    return out

@@ -1,5 +1,5 @@
 """Generate tests/golden/shader_small.npz from the reference's own shader
-stages (shaders/cull.glsl, sort.glsl, splat.glsl, gps.glsl), compiled from their source
+stages (shaders/cull.glsl, sort.glsl, splat.glsl, gps.glsl, accum.glsl), compiled from their source
 for the CPU by oracle/Makefile into oracle/_ref/libglslref.so.
 
 Run in a checkout that has the reference sources:
@@ -27,6 +27,10 @@ inside the scene, which culls about half of it):
              pairs in and out (2 x n uint32) for t = cull (camera 3's keys and
              ids, invisible rows' sentinels included) and t = ties (5000 keys
              of 40 values with every byte varying, ids in index order)
+  disp_in, disp_lut, disp_params, disp_out, blit_out : layers_display_fs
+             (accum.glsl) on a seeded 40 x 64 RGBA16F frame (zero, huge,
+             subnormal and infinite channels included) with a 17^3 LUT and
+             (log2_min, log2_max, exposure_ev) = disp_params; blit_fs on it
   anim_ids, anim_proj_s : cull_cs with int8 deltas (`scene.anim_deltas(5, N,
              3)`, scales anim_scales) for camera 0 and the (state a, state b,
              weight) of anim_states[s]
@@ -90,6 +94,17 @@ def main() -> None:
         ko, io = O.glsl_sort_pairs(k, i)
         out[f"sort_in_{name}"] = np.stack([k, i])
         out[f"sort_out_{name}"] = np.stack([ko, io])
+    rng = np.random.default_rng(13)
+    img = (rng.random((40, 64, 4)) * 3.0).astype(np.float16)
+    img[0, :5, :3] = 0.0
+    img[1, :5, :3] = np.float16(60000.0)
+    img[2, :5, :3] = np.float16(6e-8)
+    img[3, :5, :3] = np.float16(np.inf)
+    lut = rng.integers(0, 65536, (17, 17, 17, 3), dtype=np.uint16)
+    params = np.array([-12.0, 4.0, 1.5], np.float32)
+    out["disp_in"], out["disp_lut"], out["disp_params"] = img, lut, params
+    out["disp_out"] = O.glsl_display(img, lut, *params)
+    out["blit_out"] = O.glsl_display(img, None, 0.0, 1.0, 0.0)
     deltas = scene.anim_deltas(5, N, 3)
     scales = np.linspace(0.002, 0.02, 48, dtype=np.float32)
     out["anim_scales"] = scales

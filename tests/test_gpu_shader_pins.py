@@ -1,6 +1,6 @@
 """GPU parity against the reference's own shader stages: the CUDA path,
 through the C ABI, compared with tests/golden/shader_small.npz, the outputs of
-shaders/cull.glsl, sort.glsl, splat.glsl and gps.glsl compiled from their source for the
+shaders/cull.glsl, sort.glsl, splat.glsl, gps.glsl and accum.glsl (the display transform) compiled from their source for the
 CPU (tests/golden/make_shader_golden.py).
 
 Projected records, the sort permutation (gs_sort_pairs), the stochastic sample (colour and D24 depth), GPS work
@@ -115,3 +115,21 @@ def test_sort_pairs_matches_shaders(fx, case):
     torch.cuda.synchronize()
     got = np.stack([ok.cpu().numpy().view(np.uint32), ov.cpu().numpy().view(np.uint32)])
     assert np.array_equal(got, fx[f"sort_out_{case}"])
+
+
+def test_display_matches_shaders(fx):
+    import torch
+
+    img, lut = fx["disp_in"], fx["disp_lut"]
+    lo, hi, ex = (float(v) for v in fx["disp_params"])
+    h, w = img.shape[:2]
+    with Renderer(0) as r:
+        src = torch.from_numpy(img.view(np.uint16).copy()).cuda()
+        dst = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
+        r.display(src.data_ptr(), dst.data_ptr(), w, h, 0.0)      # no LUT: the blit
+        torch.cuda.synchronize()
+        assert np.array_equal(dst.cpu().numpy().view(np.uint32), fx["blit_out"].view(np.uint32))
+        r.set_display_lut(lut, lo, hi)
+        r.display(src.data_ptr(), dst.data_ptr(), w, h, ex)
+        torch.cuda.synchronize()
+        assert np.array_equal(dst.cpu().numpy().view(np.uint32), fx["disp_out"].view(np.uint32))

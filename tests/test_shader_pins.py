@@ -1,5 +1,6 @@
 """CPU tests: pin the oracle against the reference's own shader stages
-(shaders/cull.glsl, sort.glsl, splat.glsl, gps.glsl, accum.glsl), compiled from their
+(shaders/cull.glsl, sort.glsl, splat.glsl, gps.glsl, accum.glsl with the
+display transform), compiled from their
 source for the CPU into oracle/_ref/libglslref.so (oracle/Makefile, with
 oracle/glsl/extract.py and oracle/glsl/harness.cpp), through the committed
 fixture tests/golden/shader_small.npz (tests/golden/make_shader_golden.py)
@@ -85,6 +86,13 @@ def test_oracle_sort_matches_shader_fixture(fx, case):
     k, i = fx[f"sort_in_{case}"]
     ko, io = O.sort_pairs(k, i)
     assert np.array_equal(np.stack([ko, io]), fx[f"sort_out_{case}"])
+
+
+def test_oracle_display_matches_shader_fixture(fx):
+    lo, hi, ex = (float(v) for v in fx["disp_params"])
+    got = O.display(fx["disp_in"], fx["disp_lut"], lo, hi, ex)
+    assert np.array_equal(_bits(got), _bits(fx["disp_out"]))
+    assert np.array_equal(_bits(O.display(fx["disp_in"], None, 0.0, 1.0, 0.0)), _bits(fx["blit_out"]))
 
 
 def test_oracle_anim_matches_shader_fixture(fx):
@@ -280,3 +288,22 @@ def test_accum_and_taa_match_shader():
         gc, gx = O.glsl_taa(avg, depth, gc, gx, inv, pv[:16], vo, fc, pfc, pz, float(has), changed)
         assert np.array_equal(_bits(hc), _bits(gc)) and np.array_equal(_bits(hx), _bits(gx)), k
         prev = cam
+
+
+@live
+def test_display_matches_shader():
+    """layers_display_fs (LUT sizes 2 to 65, exposures, log2 ranges) and blit_fs
+    on frames with zero, huge, subnormal and infinite channels: every output
+    bit for bit.  NaN radiance is left out: GLSL does not define it, and the
+    oracle defines it as the first lattice entry."""
+    rng = np.random.default_rng(31)
+    for n, lo, hi, ex in [(2, -10.0, 2.0, 0.0), (5, -3.0, 3.0, 0.5), (17, -12.0, 4.0, 1.5), (33, -6.0, 3.0, -2.25),
+                          (65, -16.0, 8.0, 3.0)]:
+        img = (rng.random((37, 53, 4)) * 4.0).astype(np.float16)
+        img[0, :7, :3] = 0.0
+        img[1, :7, :3] = np.float16(65504.0)
+        img[2, :7, :3] = np.float16(6e-8)
+        img[3, :7, :3] = np.float16(np.inf)
+        lut = rng.integers(0, 65536, (n, n, n, 3), dtype=np.uint16)
+        assert np.array_equal(_bits(O.display(img, lut, lo, hi, ex)), _bits(O.glsl_display(img, lut, lo, hi, ex))), n
+        assert np.array_equal(_bits(O.display(img, None, lo, hi, ex)), _bits(O.glsl_display(img, None, lo, hi, ex)))
