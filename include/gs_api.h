@@ -18,7 +18,8 @@
  *    reference renderer is used from one thread (src/main.cpp:1963).
  *  - Work is stream-ordered; only gs_render_host, gs_render_host_wait (and a
  *    gs_render_host_submit that retires an older frame), gs_read_stats and
- *    gs_debug_read synchronise.
+ *    gs_debug_read synchronise, and gs_render waits for its frame's tile
+ *    entry count (see there) while the rest of the frame stays queued.
  *  - Images are RGBA16F (IEEE half, 4 channels), row-major, top row first
  *    (the orientation of the reference harness's linear_capture,
  *    tests/gsanim_render.cpp:161-163).
@@ -246,9 +247,10 @@ uint64_t gs_scene_device_bytes(uint64_t count, uint32_t gps_work_items);
  * GS_ERR_BAD_ARG, since the WGPU backend's top-left fragment origin is not
  * what the kernels rasterise.
  * Alpha and stochastic frames count their (tile, splat) entries on the
- * device; the call waits for that count (read back right after the binning,
- * with the rest of the frame still queued, as the reference's draw_frame
- * reads back inside the frame) and, when the entries did not fit, grows the
+ * device; the call waits for that count (read back once the binning and the
+ * tile sort have run, on a stream of the context's own, with the rest of the
+ * frame still queued, as the reference's draw_frame reads back inside the
+ * frame) and, when the entries did not fit, grows the
  * buffers and renders the frame again before returning.  A GS_OK frame is
  * therefore complete; GS_ERR_TOO_LARGE if the entries exceed the largest
  * buffer (2^30 - 1 entries), GS_ERR_OOM if growing fails. */
